@@ -1,0 +1,386 @@
+# -*- coding: utf-8 -*-
+"""Benchmark of the B200 DGFS hot path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload couette-n24] [--precision single|double]
+                    [--mode collide|step]
+
+Workload: the 1D/3V Couette slab (64 x 1 quadrilateral strip, p = 2, 576
+solution points, N = 24^3 velocities, Nrho = 12, M = 16, VHS omega = 0.81),
+synthetic distributions (Maxwellians with seeded 1% noise).  One step is one
+collision sweep over every solution point (``--mode collide``: a single
+persistent launch of the fused VHS kernel) or one SSP-RK2 solver step
+(``--mode step``: two collision sweeps, two DG residuals, boundary updates).
+The metric is Q(f) evaluations per second, whole job.
+
+Multi-GPU (torchrun): every rank runs its own copy of the workload (the
+collision is independent per point, no data-path collective), so scaling is
+weak; the time is the max over ranks.
+
+``--impl reference`` times the reference's algorithm on the host cores: the
+reference itself is PyCUDA/cuFFT-only (no CPU path) and cannot be imported on
+this software stack, so the FP64 numpy restatement in oracle/ stands in for it.
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, 'dgfs-be-solver_b200'))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+SPHDESIGN = os.path.join(ROOT, 'tests', 'golden', 'sphericaldesign')
+METRIC = 'Q(f) evals/s'
+
+
+def _parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=10)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
+    ap.add_argument('--workload', default='couette-n24')
+    ap.add_argument('--precision', default='single',
+                    choices=['single', 'double'])
+    ap.add_argument('--project', type=int, default=1)
+    ap.add_argument('--mode', default='collide', choices=['collide', 'step'])
+    ap.add_argument('--cpu-seconds', type=float, default=12.0)
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    return ap.parse_args()
+
+
+def _cfg(args):
+    from frfs_b200 import workloads
+    from frfs_b200.inifile import Inifile
+    cfg = Inifile(workloads.WORKLOADS[args.workload](
+        precision=args.precision))
+    cfg.set('spherical-design-rule', 'path', SPHDESIGN)
+    cfg.set('backend-b200', 'vhs-project', int(args.project))
+    return cfg
+
+
+def _workload_desc(args, cfg, npts):
+    return {
+        'workload': f'{args.workload}: DGFS fast-spectral VHS Q(f) at every '
+                    f'solution point' + (' + FR-DG SSP-RK2 step'
+                                         if args.mode == 'step' else ''),
+        'points': npts,
+        'Nv': cfg.getint('constants', 'Nv'),
+        'Nrho': cfg.getint('constants', 'Nrho'),
+        'M': cfg.getint('spherical-design-rule', 'M'),
+        'omega': cfg.getfloat('scattering-model', 'omega'),
+        'precision': args.precision,
+        'projection': bool(args.project),
+        'mode': args.mode,
+        'l2': 'flushed between timed steps (256 MiB write)',
+    }
+
+
+def _points_shape(cfg):
+    """(nupts, neles) of the workload's mesh (quad p=2: 9 points)."""
+    order = cfg.getint('solver', 'order')
+    if cfg.hasopt('mesh', 'nx'):
+        neles = cfg.getint('mesh', 'nx')*cfg.getint('mesh', 'ny')
+        return (order + 1)**2, neles
+    return 1, 1
+
+
+def _synthetic_f(cv, nupts, neles, seed=0):
+    """Maxwellian (rho=1, T=1, u=0) times (1 + 0.01 xi), xi ~ N(0,1) i.i.d.
+    per velocity node and point; shape (nupts, V, neles)."""
+    rng = np.random.default_rng(seed)
+    V = cv.shape[1]
+    m = np.exp(-np.sum(cv*cv, axis=0))/np.pi**1.5
+    xi = rng.standard_normal((nupts, V, neles))
+    return m[None, :, None]*(1.0 + 0.01*xi)
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,'
+              'clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,'
+              'clocks_event_reasons.hw_thermal_slowdown,'
+              'clocks_event_reasons.sw_thermal_slowdown,'
+              'clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ['nvidia-smi', '-i', str(self.idx),
+                 f'--query-gpu={self.FIELDS}', '--format=csv,noheader,nounits',
+                 '-lms', '200'], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except (OSError, ValueError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self._t.join(timeout=2)
+        sm, smax, reasons = [], 0.0, set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown',
+                 'sw_power_cap']
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(',')]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = max(smax, float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == 'active':
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {'sm_mhz': float(np.median(sm)), 'sm_max_mhz': smax,
+                'reasons': sorted(reasons), 'samples': len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baselines (the oracle restatement of the reference algorithm)
+# ---------------------------------------------------------------------------
+def _cpu_baseline(cfg, budget_s, seed=0):
+    from oracle import vhs as ovhs
+    g = lambda s, k: cfg.getfloat(s, k)
+    from frfs_b200.velocitymesh import DGFSVelocityMesh
+    vm = DGFSVelocityMesh(None, cfg)
+    ovm = ovhs.velocity_mesh(vm.Nv(), vm.Nrho(), vm.M(),
+                             np.vstack([vm.sz(), -vm.sz()]),
+                             g('non-dim', 'H0'), g('non-dim', 'T0'),
+                             g('non-dim', 'rho0'), g('non-dim', 'molarMass0'),
+                             g('velocity-mesh', 'cmax'),
+                             g('velocity-mesh', 'Tmax'),
+                             g('velocity-mesh', 'dev'))
+    gam, prefac = ovhs.vhs_parameters(g('scattering-model', 'omega'),
+                                      g('scattering-model', 'dRef'),
+                                      g('scattering-model', 'Tref'),
+                                      g('non-dim', 'H0'), ovm['n0'],
+                                      g('non-dim', 'T0'))
+    pre = ovhs.vhs_precompute(ovm, gam)
+    f = _synthetic_f(vm.cv(), 1, 64, seed)[0].T
+    t0 = time.perf_counter()
+    ovhs.vhs_Q(f[0], ovm, pre, prefac)
+    t1 = time.perf_counter() - t0
+    n = int(max(1, min(64, budget_s//max(t1, 1e-3))))
+    t0 = time.perf_counter()
+    for i in range(n):
+        ovhs.vhs_Q(f[i % 64], ovm, pre, prefac)
+    dt = time.perf_counter() - t0
+    cores = len(os.sched_getaffinity(0))
+    return {'value': n/dt, 'unit': 'evals/s', 'cores': cores,
+            'kind': 'port',
+            'sample': f'{n} solution points of the workload (FP64 numpy/'
+                      f'scipy.fft restatement of scattering.py:227-286, '
+                      f'{cores} threads), per-point throughput'}, n, dt
+
+
+def run_reference(args):
+    rank = int(os.environ.get('RANK', '0'))
+    if rank != 0:
+        return
+    cfg = _cfg(args)
+    nupts, neles = _points_shape(cfg)
+    per_step = max(2.0, 60.0/max(1, args.steps + args.warmup))
+    for _ in range(args.warmup):
+        _cpu_baseline(cfg, min(per_step, 5.0))
+    vals = []
+    for _ in range(args.steps):
+        cb, n, dt = _cpu_baseline(cfg, per_step)
+        vals.append(cb['value'])
+    value = float(np.mean(vals))
+    cb['value'] = value
+    line = {
+        'impl': 'reference', 'metric': METRIC, 'value': value,
+        'unit': 'evals/s', 'n_gpus': args.gpus, 'steps': args.steps,
+        'warmup': args.warmup,
+        'ms_per_step': 1e3*nupts*neles/value,
+        'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+        'dtype': 'f64', 'data': 'synthetic',
+        'config': _workload_desc(args, cfg, nupts*neles),
+        'cpu_baseline': cb,
+        'e2e': {'value': value, 'unit': 'evals/s',
+                'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+        'note': 'reference is PyCUDA+cuFFT only; its algorithm is timed as '
+                'the FP64 oracle restatement on the host cores; each step '
+                'is a bounded sample of the sweep',
+    }
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group('nccl', timeout=timedelta(seconds=120))
+
+    from frfs_b200 import _lib
+    from frfs_b200.backend import B200Backend
+    from frfs_b200.scattering import DGFSVHSGLLScatteringModel
+    from frfs_b200.velocitymesh import DGFSVelocityMesh
+
+    cfg = _cfg(args)
+    be = B200Backend(cfg, device=f'cuda:{local}')
+    vm = DGFSVelocityMesh(be, cfg)
+    sm = DGFSVHSGLLScatteringModel(be, cfg, vm)
+    nupts, neles = _points_shape(cfg)
+    npts = nupts*neles
+    V = vm.vsize()
+    f0 = _synthetic_f(vm.cv(), nupts, neles, seed=rank)
+    fin = be.matrix((nupts, V, neles), f0)
+    fout = be.matrix((nupts, V, neles))
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256*1024*1024 // 4, dtype=torch.float32,
+                        device=be.device)
+
+    def step():
+        sm.fs_all(fin, fout)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    times = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    t_ms = float(np.sum(times))
+    if world > 1:
+        t = torch.tensor([t_ms], device=be.device, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_ms = float(t.item())
+        dist.barrier()
+    ms_per_step = t_ms/args.steps
+    value = world*npts*args.steps/(t_ms*1e-3)
+
+    # end to end through the public API: pinned host f -> device, Q(f),
+    # device -> pinned host Q, all inside the timed region
+    hin = torch.empty(fin.data.numel(), dtype=fin.data.dtype,
+                      pin_memory=True)
+    hin.copy_(fin.data.cpu())
+    hout = torch.empty_like(hin, pin_memory=True)
+    for _ in range(2):
+        fin.data.copy_(hin, non_blocking=True)
+        step()
+        hout.copy_(fout.data, non_blocking=True)
+    torch.cuda.synchronize()
+    etimes = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fin.data.copy_(hin, non_blocking=True)
+        step()
+        hout.copy_(fout.data, non_blocking=True)
+        e1.record(stream)
+        e1.synchronize()
+        etimes.append(e0.elapsed_time(e1))
+    te = float(np.sum(etimes))
+    if world > 1:
+        t = torch.tensor([te], device=be.device, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        te = float(t.item())
+    e2e = {'value': world*npts*args.steps/(te*1e-3), 'unit': 'evals/s',
+           'h2d_bytes_per_step': int(hin.numel()*hin.element_size()),
+           'd2h_bytes_per_step': int(hout.numel()*hout.element_size())}
+
+    # roofline of the dominant kernel (the fused VHS launch is the whole step)
+    prec = 64 if args.precision == 'double' else 32
+    tf = _lib.c_double()
+    ms = _lib.ct.c_float()
+    _lib.check(_lib.load().dgfs_probe_fma_peak(
+        prec, 4096, _lib.ct.byref(tf), _lib.ct.byref(ms),
+        stream.cuda_stream), 'dgfs_probe_fma_peak')
+    flops_pt = sm.flops_per_point()
+    achieved = flops_pt*npts/(ms_per_step*1e-3)/1e12
+    roof = {'bound': 'fp32-simt' if prec == 32 else 'fp64-simt',
+            'achieved': achieved, 'peak': tf.value, 'unit': 'TFLOP/s',
+            'frac': achieved/tf.value,
+            'peak_source': 'measured in this run: FMA loop on every SM '
+                           '(dgfs_probe_fma_peak)',
+            'flops_per_point': flops_pt,
+            'traffic': None,
+            'kernel': 'vhs_cluster_kernel', 'launches_per_step': 1}
+    launch = sm.launch_info()
+
+    if rank == 0:
+        cb = None
+        if world == 1 and not args.no_cpu_baseline:
+            cb = _cpu_baseline(cfg, args.cpu_seconds)[0]
+        line = {
+            'metric': METRIC, 'value': value, 'unit': 'evals/s',
+            'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
+            'ms_per_step': ms_per_step, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None,
+            'dtype': 'f32' if prec == 32 else 'f64',
+            'data': 'synthetic',
+            'config': _workload_desc(args, cfg, npts),
+            'clocks': clk, 'e2e': e2e,
+            'gpu_launches': args.steps,
+            'roofline': roof, 'cpu_baseline': cb,
+            'launch': launch,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = _parse()
+    if args.impl == 'reference':
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == '__main__':
+    main()

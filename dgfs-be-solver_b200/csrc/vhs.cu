@@ -1,0 +1,429 @@
+// Host side of the fast-spectral VHS operator: parameter validation, the
+// precomputed tables of frfs's perform_precomputation
+// (frfs/solvers/dgfs/scattering.py:67-224, vhs-gll.mako:45-101) and the
+// cluster-kernel dispatch behind the C ABI in include/dgfs_b200.h.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/dgfs_b200.h"
+#include "dgfs_internal.h"
+#include "vhs_kernel.cuh"
+
+namespace dgfs {
+
+// ---------------------------------------------------------------------------
+// Twiddle table: exp(2 pi i m / 96), m < 96, computed in long double
+// ---------------------------------------------------------------------------
+static std::mutex g_tw_mutex;
+static bool g_tw_ready[64];
+
+static int init_twiddles(int dev) {
+  std::lock_guard<std::mutex> lk(g_tw_mutex);
+  if (dev >= 0 && dev < 64 && g_tw_ready[dev]) return DGFS_OK;
+  double t64[2 * kTwBase];
+  float t32[2 * kTwBase];
+  const long double twopi = 6.283185307179586476925286766559005768L;
+  for (int m = 0; m < kTwBase; ++m) {
+    const long double ang = twopi * (long double)m / (long double)kTwBase;
+    t64[2 * m] = (double)cosl(ang);
+    t64[2 * m + 1] = (double)sinl(ang);
+    t32[2 * m] = (float)cosl(ang);
+    t32[2 * m + 1] = (float)sinl(ang);
+  }
+  if (cudaMemcpyToSymbol(c_tw64, t64, sizeof(t64)) != cudaSuccess ||
+      cudaMemcpyToSymbol(c_tw32, t32, sizeof(t32)) != cudaSuccess)
+    return set_error(DGFS_ERR_CUDA, "twiddle upload failed: %s", cudaGetErrorString(cudaGetLastError()));
+  if (dev >= 0 && dev < 64) g_tw_ready[dev] = true;
+  return DGFS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Kernel variants
+// ---------------------------------------------------------------------------
+struct VhsVariant {
+  int prec, N, C, threads;
+  size_t smem;
+  const void* fn;
+  cudaError_t (*launch32)(const VhsArgs<float>&, int, cudaStream_t);
+  cudaError_t (*launch64)(const VhsArgs<double>&, int, cudaStream_t);
+};
+
+template <typename T, int N, int C>
+static cudaError_t launch_vhs(const VhsArgs<T>& a, int nclusters, cudaStream_t s) {
+  using G = VhsGeom<N, C>;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nclusters * C, 1, 1);
+  cfg.blockDim = dim3(G::NT, 1, 1);
+  cfg.dynamicSmemBytes = G::SMEM_CX * sizeof(cx<T>);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, vhs_cluster_kernel<T, N, C>, a);
+}
+
+template <typename T, int N, int C> static VhsVariant make_variant() {
+  using G = VhsGeom<N, C>;
+  VhsVariant v{};
+  v.prec = sizeof(T) == 8 ? 64 : 32;
+  v.N = N;
+  v.C = C;
+  v.threads = G::NT;
+  v.smem = G::SMEM_CX * sizeof(cx<T>);
+  v.fn = (const void*)vhs_cluster_kernel<T, N, C>;
+  if constexpr (sizeof(T) == 8) v.launch64 = launch_vhs<double, N, C>;
+  else v.launch32 = launch_vhs<float, N, C>;
+  return v;
+}
+
+static const std::vector<VhsVariant>& variants() {
+  static const std::vector<VhsVariant> v = {
+      make_variant<double, 8, 1>(),  make_variant<double, 8, 2>(),
+      make_variant<double, 16, 2>(), make_variant<double, 16, 4>(),
+      make_variant<double, 24, 4>(), make_variant<double, 24, 8>(),
+      make_variant<double, 32, 8>(), make_variant<double, 32, 16>(),
+      make_variant<float, 8, 1>(),   make_variant<float, 8, 2>(),
+      make_variant<float, 16, 1>(),  make_variant<float, 16, 2>(),
+      make_variant<float, 16, 4>(),  make_variant<float, 24, 2>(),
+      make_variant<float, 24, 3>(),  make_variant<float, 24, 4>(),
+      make_variant<float, 24, 6>(),  make_variant<float, 24, 8>(),
+      make_variant<float, 32, 4>(),  make_variant<float, 32, 8>(),
+      make_variant<float, 32, 16>(),
+  };
+  return v;
+}
+
+static int default_cluster(int prec, int N) {
+  if (prec == 64) return N == 8 ? 1 : N == 16 ? 2 : N == 24 ? 8 : 16;
+  return N == 8 ? 1 : N == 16 ? 2 : N == 24 ? 4 : 8;
+}
+
+static const VhsVariant* find_variant(int prec, int N, int C) {
+  for (const auto& v : variants())
+    if (v.prec == prec && v.N == N && v.C == C) return &v;
+  return nullptr;
+}
+
+}  // namespace dgfs
+
+using namespace dgfs;
+
+struct dgfs_vhs {
+  int N, P, M, prec, V, device, project;
+  double prefac;
+  const VhsVariant* var;
+  int max_clusters;
+  void* phase;   // cx<T> [P][M][3][N]
+  void* w1;      // T [P][V]
+  void* b2;      // T [V]
+  double* ginv;  // [25]
+  double* cvec;  // [3][V]
+};
+
+static int select_variant(dgfs_vhs* h, int C) {
+  if (C <= 0) C = default_cluster(h->prec, h->N);
+  const VhsVariant* v = find_variant(h->prec, h->N, C);
+  if (!v)
+    return set_error(DGFS_ERR_UNSUPPORTED, "no VHS kernel for Nv=%d precision=%d cluster=%d", h->N, h->prec, C);
+  int maxsm = 0;
+  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
+  if ((int)v->smem > maxsm)
+    return set_error(DGFS_ERR_UNSUPPORTED, "VHS kernel Nv=%d cluster=%d needs %zu B shared memory (device max %d)",
+                     h->N, C, v->smem, maxsm);
+  if (cudaFuncSetAttribute(v->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v->smem) != cudaSuccess)
+    return set_error(DGFS_ERR_CUDA, "cudaFuncSetAttribute(smem): %s", cudaGetErrorString(cudaGetLastError()));
+  if (C > 8 && cudaFuncSetAttribute(v->fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+    return set_error(DGFS_ERR_CUDA, "non-portable cluster size %d refused: %s", C,
+                     cudaGetErrorString(cudaGetLastError()));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(C, 1, 1);
+  cfg.blockDim = dim3(v->threads, 1, 1);
+  cfg.dynamicSmemBytes = v->smem;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int ncl = 0;
+  if (cudaOccupancyMaxActiveClusters(&ncl, v->fn, &cfg) != cudaSuccess || ncl <= 0)
+    return set_error(DGFS_ERR_UNSUPPORTED, "cluster size %d cannot be scheduled: %s", C,
+                     cudaGetErrorString(cudaGetLastError()));
+  h->var = v;
+  h->max_clusters = ncl;
+  return DGFS_OK;
+}
+
+template <typename T> static int upload(void** dst, const std::vector<T>& src) {
+  if (cudaMalloc(dst, src.size() * sizeof(T)) != cudaSuccess) {
+    *dst = nullptr;
+    return set_error(DGFS_ERR_NOMEM, "cudaMalloc(%zu) failed", src.size() * sizeof(T));
+  }
+  if (cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
+    return set_error(DGFS_ERR_CUDA, "cudaMemcpy failed: %s", cudaGetErrorString(cudaGetLastError()));
+  return DGFS_OK;
+}
+
+// sinc as defined by the reference kernels (vhs-gll.mako:11-14)
+static double ref_sinc(double s) { return std::sin(s + 1e-15) / (s + 1e-15); }
+
+static bool invert5(const double* A, double* X) {
+  double a[5][10];
+  for (int i = 0; i < 5; ++i)
+    for (int j = 0; j < 10; ++j) a[i][j] = j < 5 ? A[i * 5 + j] : (j - 5 == i ? 1.0 : 0.0);
+  for (int c = 0; c < 5; ++c) {
+    int piv = c;
+    for (int r = c + 1; r < 5; ++r)
+      if (std::fabs(a[r][c]) > std::fabs(a[piv][c])) piv = r;
+    if (std::fabs(a[piv][c]) < 1e-300) return false;
+    if (piv != c)
+      for (int j = 0; j < 10; ++j) std::swap(a[c][j], a[piv][j]);
+    const double d = a[c][c];
+    for (int j = 0; j < 10; ++j) a[c][j] /= d;
+    for (int r = 0; r < 5; ++r)
+      if (r != c) {
+        const double f = a[r][c];
+        for (int j = 0; j < 10; ++j) a[r][j] -= f * a[c][j];
+      }
+  }
+  for (int i = 0; i < 5; ++i)
+    for (int j = 0; j < 5; ++j) X[i * 5 + j] = a[i][j + 5];
+  return true;
+}
+
+template <typename T> static int build_tables(dgfs_vhs* h, const dgfs_vhs_params* p) {
+  const int N = h->N, P = h->P, M = h->M, V = h->V;
+  const double L = p->L, pi = 3.14159265358979323846;
+  std::vector<double> l0(N);
+  for (int k = 0; k < N; ++k) l0[k] = k < N / 2 ? k : k - N;  // scattering.py:79
+
+  std::vector<cx<T>> phase((size_t)P * M * 3 * N);
+  for (int ip = 0; ip < P; ++ip) {
+    const double fac = pi / L * p->qz[ip] / 2.;  // vhs-gll.mako:58
+    for (int iq = 0; iq < M; ++iq)
+      for (int ax = 0; ax < 3; ++ax)
+        for (int k = 0; k < N; ++k) {
+          const double ang = fac * (p->sz[iq * 3 + ax] * l0[k]);
+          cx<T> e;
+          e.x = (T)std::cos(ang);
+          e.y = (T)std::sin(ang);
+          phase[((size_t)(ip * M + iq) * 3 + ax) * N + k] = e;
+        }
+  }
+  std::vector<T> w1((size_t)P * V), b2(V);
+  for (int v = 0; v < V; ++v) {
+    const double lx = l0[v / (N * N)], ly = l0[(v % (N * N)) / N], lz = l0[v % N];
+    const double cSqr = std::sqrt(lx * lx + ly * ly + lz * lz);  // vhs-gll.mako:84-86
+    double bsum = 0.;
+    for (int ip = 0; ip < P; ++ip) {
+      const double qz = p->qz[ip], qw = p->qw[ip];
+      const double b1 = std::pow(qz, p->gamma + 2.) * 4 * pi * ref_sinc(pi / L * qz / 2. * cSqr);
+      bsum += qw * std::pow(qz, p->gamma + 2.) * 16 * pi * pi * ref_sinc(pi / L * qz * cSqr);
+      w1[(size_t)ip * V + v] = (T)(2. * qw * p->sw / V * b1);  // computeQG, vhs-gll.mako:194
+    }
+    b2[v] = (T)bsum;
+  }
+  int rc;
+  if ((rc = upload(&h->phase, phase)) || (rc = upload(&h->w1, w1)) || (rc = upload(&h->b2, b2))) return rc;
+
+  if (h->project) {
+    // velocity grid (frfs/solvers/dgfs/velocitymesh.py:73-85) and the Gram
+    // matrix of phi = (1, cx, cy, cz, |c|^2) over it
+    std::vector<double> c0(N), cv((size_t)3 * V);
+    for (int i = 0; i < N; ++i) c0[i] = -L + L / N + i * (2.0 * L / N);
+    double G[25] = {0}, Gi[25];
+    for (int v = 0; v < V; ++v) {
+      const double c[3] = {c0[v / (N * N)], c0[(v % (N * N)) / N], c0[v % N]};
+      for (int a = 0; a < 3; ++a) cv[(size_t)a * V + v] = c[a];
+      const double phi[5] = {1.0, c[0], c[1], c[2], c[0] * c[0] + c[1] * c[1] + c[2] * c[2]};
+      for (int i = 0; i < 5; ++i)
+        for (int j = 0; j < 5; ++j) G[i * 5 + j] += phi[i] * phi[j];
+    }
+    if (!invert5(G, Gi)) return set_error(DGFS_ERR_INVALID, "singular moment Gram matrix");
+    std::vector<double> gi(Gi, Gi + 25);
+    if ((rc = upload((void**)&h->ginv, gi)) || (rc = upload((void**)&h->cvec, cv))) return rc;
+  }
+  return DGFS_OK;
+}
+
+static void free_handle(dgfs_vhs* h) {
+  if (!h) return;
+  cudaFree(h->phase);
+  cudaFree(h->w1);
+  cudaFree(h->b2);
+  cudaFree(h->ginv);
+  cudaFree(h->cvec);
+  delete h;
+}
+
+extern "C" int dgfs_vhs_create(const dgfs_vhs_params* p, dgfs_vhs** out) {
+  clear_error();
+  if (!p || !out) return set_error(DGFS_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (p->Nv != 8 && p->Nv != 16 && p->Nv != 24 && p->Nv != 32)
+    return set_error(DGFS_ERR_UNSUPPORTED, "Nv=%d not supported (8, 16, 24, 32)", p->Nv);
+  if (p->precision != 32 && p->precision != 64)
+    return set_error(DGFS_ERR_INVALID, "precision must be 32 or 64, got %d", p->precision);
+  if (p->Nrho < 1 || p->M < 1 || p->Nrho > 4096 || p->M > 4096)
+    return set_error(DGFS_ERR_INVALID, "bad quadrature sizes Nrho=%d M=%d", p->Nrho, p->M);
+  if (!p->qz || !p->qw || !p->sz) return set_error(DGFS_ERR_INVALID, "null quadrature array");
+  if (!(p->L > 0) || !std::isfinite(p->L)) return set_error(DGFS_ERR_INVALID, "bad L");
+  if (!std::isfinite(p->prefactor) || !std::isfinite(p->gamma) || !std::isfinite(p->sw))
+    return set_error(DGFS_ERR_INVALID, "non-finite scalar parameter");
+  for (int i = 0; i < p->Nrho; ++i)
+    if (!std::isfinite(p->qz[i]) || !std::isfinite(p->qw[i]))
+      return set_error(DGFS_ERR_INVALID, "non-finite radial quadrature");
+  for (int i = 0; i < 3 * p->M; ++i)
+    if (!std::isfinite(p->sz[i])) return set_error(DGFS_ERR_INVALID, "non-finite spherical design");
+
+  dgfs_vhs* h = new dgfs_vhs();
+  std::memset(h, 0, sizeof(*h));
+  h->N = p->Nv;
+  h->P = p->Nrho;
+  h->M = p->M;
+  h->prec = p->precision;
+  h->V = p->Nv * p->Nv * p->Nv;
+  h->prefac = p->prefactor;
+  h->project = p->project ? 1 : 0;
+  if (cudaGetDevice(&h->device) != cudaSuccess) {
+    delete h;
+    return set_error(DGFS_ERR_CUDA, "no CUDA device: %s", cudaGetErrorString(cudaGetLastError()));
+  }
+  int rc = init_twiddles(h->device);
+  if (!rc) rc = select_variant(h, p->cluster);
+  if (!rc) rc = h->prec == 64 ? build_tables<double>(h, p) : build_tables<float>(h, p);
+  if (rc) {
+    free_handle(h);
+    return rc;
+  }
+  *out = h;
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_vhs_destroy(dgfs_vhs* h) {
+  clear_error();
+  free_handle(h);
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_vhs_set_cluster(dgfs_vhs* h, int cluster) {
+  clear_error();
+  if (!h) return set_error(DGFS_ERR_INVALID, "null handle");
+  const VhsVariant* old = h->var;
+  const int oldmax = h->max_clusters;
+  int rc = select_variant(h, cluster);
+  if (rc) {
+    h->var = old;
+    h->max_clusters = oldmax;
+  }
+  return rc;
+}
+
+extern "C" int dgfs_vhs_info(const dgfs_vhs* h, int* cluster, int* threads, int* smem_bytes, int* max_clusters) {
+  clear_error();
+  if (!h) return set_error(DGFS_ERR_INVALID, "null handle");
+  if (cluster) *cluster = h->var->C;
+  if (threads) *threads = h->var->threads;
+  if (smem_bytes) *smem_bytes = (int)h->var->smem;
+  if (max_clusters) *max_clusters = h->max_clusters;
+  return DGFS_OK;
+}
+
+static int vhs_launch(dgfs_vhs* h, const void* f, void* Q, int nupts, int neles, long long ldim, int soasz,
+                      int pt0, int npts, void* stream) {
+  if (!h) return set_error(DGFS_ERR_INVALID, "null handle");
+  if (!f || !Q) return set_error(DGFS_ERR_INVALID, "null bank pointer");
+  if (nupts < 1 || neles < 1 || soasz < 1)
+    return set_error(DGFS_ERR_INVALID, "bad bank shape nupts=%d neles=%d soasz=%d", nupts, neles, soasz);
+  const long long nblk = (neles + soasz - 1) / soasz;
+  if (ldim < nblk * soasz * (long long)h->V)
+    return set_error(DGFS_ERR_INVALID, "ldim=%lld smaller than one AoSoA row (%lld)", ldim,
+                     nblk * soasz * (long long)h->V);
+  if (pt0 < 0 || npts < 0 || (long long)pt0 + npts > (long long)nupts * neles)
+    return set_error(DGFS_ERR_INVALID, "point range [%d, %d) outside 0..%lld", pt0, pt0 + npts,
+                     (long long)nupts * neles);
+  const size_t esz = h->prec == 64 ? 8 : 4;
+  const char* fb = (const char*)f;
+  const char* qb = (const char*)Q;
+  const size_t bytes = (size_t)nupts * (size_t)ldim * esz;
+  if (fb < qb + bytes && qb < fb + bytes) return set_error(DGFS_ERR_INVALID, "f and Q overlap");
+  if (((uintptr_t)f % esz) || ((uintptr_t)Q % esz)) return set_error(DGFS_ERR_INVALID, "misaligned bank");
+  int dev = -1;
+  cudaGetDevice(&dev);
+  if (dev != h->device)
+    return set_error(DGFS_ERR_INVALID, "handle built on device %d used on device %d", h->device, dev);
+  if (npts == 0) return DGFS_OK;
+
+  const int ncl = npts < h->max_clusters ? npts : h->max_clusters;
+  cudaError_t e;
+  if (h->prec == 64) {
+    VhsArgs<double> a{};
+    a.f = (const double*)f;
+    a.Q = (double*)Q;
+    a.ldim = ldim;
+    a.nupts = nupts;
+    a.neles = neles;
+    a.soasz = soasz;
+    a.pt0 = pt0;
+    a.npts = npts;
+    a.P = h->P;
+    a.M = h->M;
+    a.phase = (const double2*)h->phase;
+    a.w1 = (const double*)h->w1;
+    a.b2 = (const double*)h->b2;
+    a.prefac = h->prefac;
+    a.project = h->project;
+    a.ginv = h->ginv;
+    a.cvec = h->cvec;
+    e = h->var->launch64(a, ncl, (cudaStream_t)stream);
+  } else {
+    VhsArgs<float> a{};
+    a.f = (const float*)f;
+    a.Q = (float*)Q;
+    a.ldim = ldim;
+    a.nupts = nupts;
+    a.neles = neles;
+    a.soasz = soasz;
+    a.pt0 = pt0;
+    a.npts = npts;
+    a.P = h->P;
+    a.M = h->M;
+    a.phase = (const float2*)h->phase;
+    a.w1 = (const float*)h->w1;
+    a.b2 = (const float*)h->b2;
+    a.prefac = (float)h->prefac;
+    a.project = h->project;
+    a.ginv = h->ginv;
+    a.cvec = h->cvec;
+    e = h->var->launch32(a, ncl, (cudaStream_t)stream);
+  }
+  if (e != cudaSuccess) return set_error(DGFS_ERR_CUDA, "VHS launch failed: %s", cudaGetErrorString(e));
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_vhs_apply(dgfs_vhs* h, const void* f, void* Q, int nupts, int neles, long long ldim, int soasz,
+                              int elem, int upt, void* stream) {
+  clear_error();
+  if (elem >= 0) {
+    if (elem >= neles || upt < 0 || upt >= nupts)
+      return set_error(DGFS_ERR_INVALID, "point (elem=%d, upt=%d) outside bank (%d, %d)", elem, upt, neles, nupts);
+    return vhs_launch(h, f, Q, nupts, neles, ldim, soasz, upt * neles + elem, 1, stream);
+  }
+  return vhs_launch(h, f, Q, nupts, neles, ldim, soasz, 0, nupts * neles, stream);
+}
+
+extern "C" int dgfs_vhs_apply_range(dgfs_vhs* h, const void* f, void* Q, int nupts, int neles, long long ldim,
+                                    int soasz, int pt0, int npts, void* stream) {
+  clear_error();
+  return vhs_launch(h, f, Q, nupts, neles, ldim, soasz, pt0, npts, stream);
+}

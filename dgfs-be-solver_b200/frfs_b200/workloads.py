@@ -1,0 +1,205 @@
+# -*- coding: utf-8 -*-
+"""Named DGFS workloads as frfs-style ``.ini`` strings.
+
+Each workload is a complete configuration in the same sections and keys that
+frfs reads (``[constants]``, ``[non-dim]``, ``[velocity-mesh]``,
+``[spherical-design-rule]``, ``[scattering-model]``, ``[solver]``,
+``[soln-ics]``, ``[soln-bcs-*]``), plus the mesh description this package
+generates itself (``[mesh]``).  The key names follow
+frfs/solvers/dgfs/velocitymesh.py:25-135, frfs/solvers/dgfs/scattering.py:50-65,
+frfs/solvers/dgfs/initcond.py:39-116 and frfs/solvers/dgfs/inters.py:175-229.
+
+Workloads
+---------
+relax0d-n16   single point, N=16, Nrho=8, M=6, VHS omega=0.5, L=5 (hard
+              sphere 0D relaxation of two Maxwellians at u=(+-1.5,0,0)).
+couette-n24   64x1 quadrilateral strip, p=2, N=24, Nrho=12, M=16, omega=0.81,
+              diffuse walls at x=+-1/2 moving at uy=+-0.5 (nondimensional),
+              y-periodic.  M=16 replaces the requested M=12: the tabulated
+              symmetric designs hold 2M in {2,6,12,32,48,70,...} points only.
+channel-n32   48x24 quadrilaterals, p=2 (10368 points), N=32, Nrho=16, M=24,
+              x-periodic, diffuse walls at y=+-1/4, Maxwellian times
+              (1 + 0.01 xi) with xi ~ N(0,1) per velocity node and point.
+"""
+
+import numpy as np
+
+# Argon (frfs examples use the same reference gas)
+_MOLAR_MASS = 39.96e-3
+_R0 = 8.3144598
+
+
+def _u0(T0=273.0, molarMass0=_MOLAR_MASS):
+    return float(np.sqrt(2*_R0/molarMass0*T0))
+
+
+_BASE = """
+[backend]
+precision = {precision}
+
+[constants]
+Nv = {Nv}
+NvBatchSize = {NvBatchSize}
+Nrho = {Nrho}
+
+[non-dim]
+T0 = 273.0
+H0 = {H0}
+rho0 = {rho0}
+molarMass0 = {molarMass0}
+
+[velocity-mesh]
+cmax = {cmax}
+Tmax = 273.0
+dev = {dev}
+quad-rule = jacobi
+quad-rule-alpha = 0
+quad-rule-beta = 0
+
+[spherical-design-rule]
+ssrule = womersley
+M = {M}
+
+[scattering-model]
+type = vhs-gll
+omega = {omega}
+dRef = 4.17e-10
+Tref = 273.0
+
+[solver]
+system = dgfs
+order = {order}
+
+[solver-time-integrator]
+scheme = dgfs-tvd-rk2
+controller = none
+tstart = 0.0
+tend = {tend}
+dt = {dt}
+
+[solver-interfaces]
+riemann-solver = rusanov
+
+[solver-interfaces-line]
+flux-pts = gauss-legendre
+
+[solver-elements-quad]
+soln-pts = gauss-legendre
+"""
+
+
+def relax0d_n16(precision='double'):
+    """Space-homogeneous relaxation; BASELINE configuration 1."""
+    u0 = _u0()
+    ini = _BASE.format(precision=precision, Nv=16, NvBatchSize=4096, Nrho=8,
+                       H0=1e-3, rho0=1.5e-3, molarMass0=_MOLAR_MASS,
+                       cmax=0.0, dev=5.0, M=6, omega=0.5, order=2,
+                       tend=0.5, dt=0.01)
+    ini += f"""
+[soln-ics]
+type = bimaxwellian
+rho = 1.5e-3
+T = 273.0
+ux = {1.5*u0!r}
+uy = 0.0
+uz = 0.0
+"""
+    return ini
+
+
+def couette_n24(precision='double', M=16, nele=64):
+    """1D/3V Couette slab as a 64x1 quad strip; BASELINE configuration 2."""
+    u0 = _u0()
+    ini = _BASE.format(precision=precision, Nv=24, NvBatchSize=13824,
+                       Nrho=12, H0=1e-3, rho0=1.5e-3,
+                       molarMass0=_MOLAR_MASS, cmax=repr(0.5*u0), dev=5.0,
+                       M=M, omega=0.81, order=2, tend=2.0, dt=0.01)
+    ini += f"""
+[mesh]
+type = quad-strip
+nx = {nele}
+ny = 1
+xlo = -0.5
+xhi = 0.5
+ylo = 0.0
+yhi = {1.0/nele!r}
+periodic-y = 1
+
+[soln-ics]
+type = maxwellian
+rho = 1.5e-3
+T = 273.0
+ux = 0.0
+uy = 0.0
+uz = 0.0
+
+[soln-bcs-left]
+type = dgfs-wall-diffuse
+rho = 1.5e-3
+T = 273.0
+ux = 0.0
+uy = {-0.5*u0!r}
+uz = 0.0
+
+[soln-bcs-right]
+type = dgfs-wall-diffuse
+rho = 1.5e-3
+T = 273.0
+ux = 0.0
+uy = {0.5*u0!r}
+uz = 0.0
+"""
+    return ini
+
+
+def channel_n32(precision='double', nx=48, ny=24, Nv=32, Nrho=16, M=24):
+    """2D/3V channel on 48x24 quads; BASELINE configuration 3."""
+    ini = _BASE.format(precision=precision, Nv=Nv, NvBatchSize=Nv**3,
+                       Nrho=Nrho, H0=1e-3, rho0=1.5e-3,
+                       molarMass0=_MOLAR_MASS, cmax=0.0, dev=5.0, M=M,
+                       omega=0.81, order=2, tend=1.0, dt=0.002)
+    ini += f"""
+[mesh]
+type = quad-box
+nx = {nx}
+ny = {ny}
+xlo = -0.5
+xhi = 0.5
+ylo = -0.25
+yhi = 0.25
+periodic-x = 1
+
+[soln-ics]
+type = maxwellian
+rho = 1.5e-3
+T = 273.0
+ux = 0.0
+uy = 0.0
+uz = 0.0
+noise = 0.01
+seed = 0
+
+[soln-bcs-bottom]
+type = dgfs-wall-diffuse
+rho = 1.5e-3
+T = 273.0
+ux = 0.0
+uy = 0.0
+uz = 0.0
+
+[soln-bcs-top]
+type = dgfs-wall-diffuse
+rho = 1.5e-3
+T = 273.0
+ux = 0.0
+uy = 0.0
+uz = 0.0
+"""
+    return ini
+
+
+WORKLOADS = {
+    'relax0d-n16': relax0d_n16,
+    'couette-n24': couette_n24,
+    'channel-n32': channel_n32,
+}

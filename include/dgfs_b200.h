@@ -1,0 +1,126 @@
+/*
+ * dgfs_b200 -- C ABI of the B200-native DGFS hot path.
+ *
+ * Two operators of the DGFS solver (Ehsan-Roohi/DGFS-BE-Solver, package
+ * frfs) are provided as hand-written sm_100a CUDA behind plain C entry points:
+ *
+ *   - the fast-spectral VHS collision operator Q(f) at every solution point
+ *     (dgfs_vhs_*), replacing DGFSVHSGLLScatteringModel
+ *     (frfs/solvers/dgfs/scattering.py:44-286);
+ *   - the flux-reconstruction DG advection residual with its interface
+ *     and boundary kernels over all N^3 velocities (dgfs_dg_*), replacing
+ *     DGFSSystem.rhs / updatebc (frfs/solvers/dgfs/system.py:140-196) and
+ *     the integrator's axnpby glue (frfs/backends/cuda/blasext.py:14-43).
+ *
+ * Conventions
+ *   - All arrays passed to *_apply / *_rhs are DEVICE pointers owned by the
+ *     caller.  Distribution banks use frfs's AoSoA layout
+ *     (frfs/backends/base/types.py:26-47, frfs/backends/cuda/kernels/base.mako:4-6):
+ *     value (upt, v, ele) lives at  upt*ldim + ((ele/soasz)*nv + v)*soasz + ele%soasz.
+ *   - Host arrays passed to *_create are copied; the library owns its
+ *     device tables and frees them in *_destroy.
+ *   - precision: 64 = FP64 throughout; 32 = FP32 bulk arithmetic with FP64
+ *     moment sums in the optional conservation projection.
+ *   - stream: a cudaStream_t passed as void* (NULL = legacy default stream).
+ *     Work is stream-ordered; nothing synchronises the host.
+ *   - Every function returns 0 on success and a DGFS_ERR_* code otherwise;
+ *     dgfs_last_error() returns a message for the calling thread.  The
+ *     library never aborts the process.
+ *   - A handle is not thread-safe; distinct handles are independent.
+ */
+#ifndef DGFS_B200_H
+#define DGFS_B200_H
+
+#if defined(__GNUC__)
+#define DGFS_API __attribute__((visibility("default")))
+#else
+#define DGFS_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DGFS_OK 0
+#define DGFS_ERR_INVALID 1     /* bad argument (size, pointer, range)        */
+#define DGFS_ERR_CUDA 2        /* a CUDA runtime call failed                 */
+#define DGFS_ERR_UNSUPPORTED 3 /* size/precision/cluster not compiled in     */
+#define DGFS_ERR_NOMEM 4       /* device allocation failed                   */
+
+/* Message describing the last error on this thread ("" if none). */
+DGFS_API const char* dgfs_last_error(void);
+
+/* Library version string. */
+DGFS_API const char* dgfs_version(void);
+
+/* ------------------------------------------------------------------------
+ * Fast-spectral VHS collision operator
+ *
+ * Replaces: DGFSVHSGLLScatteringModel.__init__ / load_parameters /
+ * perform_precomputation (frfs/solvers/dgfs/scattering.py:44-224) and
+ * fs(d_arr_in, d_arr_out, elem, upt) (scattering.py:227-286).
+ * ---------------------------------------------------------------------- */
+typedef struct dgfs_vhs dgfs_vhs;
+
+typedef struct dgfs_vhs_params {
+  int Nv;             /* velocity points per direction (8, 16, 24, 32)       */
+  int Nrho;           /* Gauss radial nodes                                  */
+  int M;              /* half-sphere directions                              */
+  int precision;      /* 64 or 32                                            */
+  double L;           /* velocity domain half width (velocitymesh.py:62)     */
+  const double* qz;   /* [Nrho] radial nodes on [0, R]  (velocitymesh.py:124) */
+  const double* qw;   /* [Nrho] radial weights           (velocitymesh.py:125) */
+  const double* sz;   /* [M*3] half-sphere directions, row-major (:133)      */
+  double sw;          /* spherical weight 2 pi / M       (velocitymesh.py:134) */
+  double prefactor;   /* scattering.py:61-62                                 */
+  double gamma;       /* 2 (1 - omega)                   (scattering.py:53)  */
+  int project;        /* 1: FP64 mass/momentum/energy projection of Q        */
+  int cluster;        /* CTAs per point (0 = default for Nv/precision)       */
+} dgfs_vhs_params;
+
+/* Build the operator: validates sizes, precomputes the axis phases,
+ * radial weights b1 and loss kernel b2 (vhs-gll.mako:45-101) on the device
+ * current at call time.  Replaces scattering.py:67-224. */
+DGFS_API int dgfs_vhs_create(const dgfs_vhs_params* params, dgfs_vhs** out);
+
+DGFS_API int dgfs_vhs_destroy(dgfs_vhs* h);
+
+/* Q(f) for solution points of one element-type bank.
+ *   f, Q     : device banks (precision of the handle), AoSoA layout with
+ *              nv = Nv^3 variables, nupts rows of leading dimension ldim.
+ *   elem,upt : one point (elem >= 0), as fs(..., elem, upt)
+ *              (scattering.py:227); elem < 0 applies Q at all
+ *              nupts*neles points in one persistent launch, as
+ *              DGFSSystem.collide (frfs/solvers/dgfs/system.py:199-218).
+ * f and Q must not overlap. */
+DGFS_API int dgfs_vhs_apply(dgfs_vhs* h, const void* f, void* Q, int nupts, int neles,
+                   long long ldim, int soasz, int elem, int upt, void* stream);
+
+/* Same as dgfs_vhs_apply with elem < 0, restricted to the linear point
+ * range [pt0, pt0 + npts), point id = upt*neles + elem. */
+DGFS_API int dgfs_vhs_apply_range(dgfs_vhs* h, const void* f, void* Q, int nupts,
+                         int neles, long long ldim, int soasz, int pt0,
+                         int npts, void* stream);
+
+/* Launch geometry chosen by the handle (for reporting and tuning). */
+DGFS_API int dgfs_vhs_info(const dgfs_vhs* h, int* cluster, int* threads,
+                  int* smem_bytes, int* max_clusters);
+
+/* Change the cluster size (autotuning); 0 restores the default. */
+DGFS_API int dgfs_vhs_set_cluster(dgfs_vhs* h, int cluster);
+
+/* ------------------------------------------------------------------------
+ * Measurement helper (no counterpart in the reference)
+ * ---------------------------------------------------------------------- */
+
+/* Sustained SIMT FMA throughput of the current device (precision 32 or 64),
+ * measured with an FMA loop over every SM and CUDA events; the roofline
+ * denominator for the SIMT-bound collision kernel.  Blocks the host. */
+DGFS_API int dgfs_probe_fma_peak(int precision, int iters, double* tflops,
+                                 float* ms, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DGFS_B200_H */

@@ -1,0 +1,159 @@
+# -*- coding: utf-8 -*-
+"""Parity of the B200 VHS kernel with the FP64 oracle (GPU).
+
+Tolerances (normwise relative, max|Q_gpu - Q_oracle| / max|Q_oracle|):
+  FP64 mode: 1e-10 (the target the port must meet);
+  FP32 mode: 2e-4.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from helpers import config, oracle_for, random_states, rel_err
+from frfs_b200.backend import B200Backend
+from frfs_b200.scattering import DGFSVHSGLLScatteringModel
+from frfs_b200.velocitymesh import DGFSVelocityMesh
+from oracle import vhs as ovhs
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-10
+FP32_TOL = 2e-4
+
+
+def _cfg(name, precision):
+    if name == 'small-n8':
+        return config('channel-n32', precision, Nv=8, Nrho=4, M=6)
+    return config(name, precision)
+
+
+def _model(cfg):
+    be = B200Backend(cfg, device='cuda:0')
+    vm = DGFSVelocityMesh(be, cfg)
+    return be, vm, DGFSVHSGLLScatteringModel(be, cfg, vm)
+
+
+def _bank(be, vm, fpts):
+    """(nupts, neles) grid of distributions -> two banks (in, out)."""
+    nupts, neles, V = fpts.shape
+    arr = np.ascontiguousarray(fpts.transpose(0, 2, 1))  # (nupts, V, neles)
+    fin = be.matrix((nupts, V, neles), arr)
+    fout = be.matrix((nupts, V, neles))
+    return fin, fout
+
+
+@pytest.mark.parametrize('name', ['small-n8', 'relax0d-n16', 'couette-n24',
+                                  'channel-n32'])
+@pytest.mark.parametrize('precision', ['double', 'single'])
+def test_single_point_parity(name, precision):
+    cfg = _cfg(name, precision)
+    be, vm, sm = _model(cfg)
+    ovm, pre, prefac = oracle_for(cfg)
+    f = random_states(vm.cv(), 2, seed=11).reshape(1, 2, -1)
+    fin, fout = _bank(be, vm, f)
+    sm.fs(fin, fout, 1, 0)
+    torch.cuda.synchronize()
+    Qg = fout.get()[0, :, 1]
+    fin_used = fin.get()[0, :, 1].astype(np.float64)
+    Qo = ovhs.vhs_Q(fin_used, ovm, pre, prefac)
+    err = rel_err(Qg, Qo)
+    tol = FP64_TOL if precision == 'double' else FP32_TOL
+    assert err < tol, f'{name} {precision}: rel err {err:.3e}'
+    # the point that was not requested stays untouched (zero)
+    assert np.all(fout.get()[0, :, 0] == 0)
+
+
+@pytest.mark.parametrize('precision', ['double', 'single'])
+def test_all_points_bank_crossing_soa_blocks(precision):
+    cfg = _cfg('small-n8', precision)
+    be, vm, sm = _model(cfg)
+    ovm, pre, prefac = oracle_for(cfg)
+    nupts, neles = 3, 37
+    f = random_states(vm.cv(), nupts*neles, seed=5).reshape(nupts, neles, -1)
+    fin, fout = _bank(be, vm, f)
+    sm.fs_all(fin, fout)
+    torch.cuda.synchronize()
+    Qg = fout.get()
+    fused = fin.get().astype(np.float64)
+    tol = FP64_TOL if precision == 'double' else FP32_TOL
+    worst = 0.0
+    for u in range(nupts):
+        for e in range(neles):
+            Qo = ovhs.vhs_Q(fused[u, :, e], ovm, pre, prefac)
+            worst = max(worst, rel_err(Qg[u, :, e], Qo))
+    assert worst < tol, worst
+
+
+def test_range_and_single_agree_with_all():
+    cfg = _cfg('relax0d-n16', 'double')
+    be, vm, sm = _model(cfg)
+    f = random_states(vm.cv(), 6, seed=2).reshape(2, 3, -1)
+    fin, fa = _bank(be, vm, f)
+    _, fr = _bank(be, vm, f)
+    _, fs1 = _bank(be, vm, f)
+    sm.fs_all(fin, fa)
+    sm.fs_range(fin, fr, 0, 3)
+    sm.fs_range(fin, fr, 3, 3)
+    for u in range(2):
+        for e in range(3):
+            sm.fs(fin, fs1, e, u)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(fa.get(), fr.get())
+    np.testing.assert_array_equal(fa.get(), fs1.get())
+
+
+@pytest.mark.parametrize('name,clusters', [('small-n8', [1, 2]),
+                                           ('relax0d-n16', [2, 4]),
+                                           ('couette-n24', [4, 8])])
+def test_cluster_sizes_agree(name, clusters):
+    cfg = _cfg(name, 'double')
+    be, vm, sm = _model(cfg)
+    f = random_states(vm.cv(), 3, seed=9).reshape(1, 3, -1)
+    outs = []
+    for c in clusters:
+        sm.set_cluster(c)
+        fin, fout = _bank(be, vm, f)
+        sm.fs_all(fin, fout)
+        torch.cuda.synchronize()
+        outs.append(fout.get())
+    for o in outs[1:]:
+        assert rel_err(o, outs[0]) < 1e-13
+
+
+@pytest.mark.parametrize('precision', ['double', 'single'])
+def test_conservation_projection(precision):
+    cfg = _cfg('relax0d-n16', precision)
+    cfg.set('backend-b200', 'vhs-project', 1)
+    be, vm, sm = _model(cfg)
+    ovm, pre, prefac = oracle_for(cfg)
+    f = random_states(vm.cv(), 2, seed=4).reshape(1, 2, -1)
+    fin, fout = _bank(be, vm, f)
+    sm.fs_all(fin, fout)
+    torch.cuda.synchronize()
+    cv = vm.cv()
+    for e in range(2):
+        Qg = fout.get()[0, :, e].astype(np.float64)
+        fo = fin.get()[0, :, e].astype(np.float64)
+        Qo = ovhs.project_conservative(ovhs.vhs_Q(fo, ovm, pre, prefac), cv)
+        tol = FP64_TOL if precision == 'double' else FP32_TOL
+        assert rel_err(Qg, Qo) < tol
+        scale = np.abs(Qg).sum()
+        mom = np.array([Qg.sum(), *(Qg*cv).sum(axis=1),
+                        (Qg*(cv*cv).sum(axis=0)).sum()])
+        mtol = 1e-12 if precision == 'double' else 1e-6
+        assert np.all(np.abs(mom) < mtol*scale*np.array([1, 5, 5, 5, 25]))
+
+
+def test_invalid_arguments_raise():
+    from frfs_b200._lib import DgfsError
+    cfg = _cfg('small-n8', 'double')
+    be, vm, sm = _model(cfg)
+    f = random_states(vm.cv(), 2, seed=1).reshape(1, 2, -1)
+    fin, fout = _bank(be, vm, f)
+    with pytest.raises(DgfsError):
+        sm.fs(fin, fout, 5, 0)          # element out of range
+    with pytest.raises(DgfsError):
+        sm.fs(fin, fin, 0, 0)           # in-place is rejected
+    with pytest.raises(DgfsError):
+        sm.fs_range(fin, fout, 1, 5)    # range past the bank
