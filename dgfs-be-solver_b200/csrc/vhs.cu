@@ -90,13 +90,13 @@ static const std::vector<VhsVariant>& variants() {
       make_variant<double, 8, 1>(),  make_variant<double, 8, 2>(),
       make_variant<double, 16, 2>(), make_variant<double, 16, 4>(),
       make_variant<double, 24, 6>(), make_variant<double, 24, 8>(),
-      make_variant<double, 32, 8>(), make_variant<double, 32, 16>(),
+      make_variant<double, 32, 16>(),
       make_variant<float, 8, 1>(),   make_variant<float, 8, 2>(),
       make_variant<float, 16, 1>(),  make_variant<float, 16, 2>(),
       make_variant<float, 16, 4>(),
       make_variant<float, 24, 3>(),  make_variant<float, 24, 4>(),
       make_variant<float, 24, 6>(),  make_variant<float, 24, 8>(),
-      make_variant<float, 32, 4>(),  make_variant<float, 32, 8>(),
+      make_variant<float, 32, 8>(),
       make_variant<float, 32, 16>(),
   };
   return v;
