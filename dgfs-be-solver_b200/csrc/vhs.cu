@@ -46,16 +46,16 @@ static int init_twiddles(int dev) {
 // Kernel variants
 // ---------------------------------------------------------------------------
 struct VhsVariant {
-  int prec, N, C, threads;
+  int prec, N, C, db, minb, threads;
   size_t smem;
   const void* fn;
   cudaError_t (*launch32)(const VhsArgs<float>&, int, cudaStream_t);
   cudaError_t (*launch64)(const VhsArgs<double>&, int, cudaStream_t);
 };
 
-template <typename T, int N, int C>
+template <typename T, int N, int C, bool DB, int MINB>
 static cudaError_t launch_vhs(const VhsArgs<T>& a, int nclusters, cudaStream_t s) {
-  using G = VhsGeom<N, C>;
+  using G = VhsGeom<N, C, DB>;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(nclusters * C, 1, 1);
   cfg.blockDim = dim3(G::NT, 1, 1);
@@ -68,49 +68,53 @@ static cudaError_t launch_vhs(const VhsArgs<T>& a, int nclusters, cudaStream_t s
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, vhs_cluster_kernel<T, N, C>, a);
+  return cudaLaunchKernelEx(&cfg, vhs_cluster_kernel<T, N, C, DB, MINB>, a);
 }
 
-template <typename T, int N, int C> static VhsVariant make_variant() {
-  using G = VhsGeom<N, C>;
+template <typename T, int N, int C, bool DB, int MINB> static VhsVariant make_variant() {
+  using G = VhsGeom<N, C, DB>;
   VhsVariant v{};
   v.prec = sizeof(T) == 8 ? 64 : 32;
   v.N = N;
   v.C = C;
+  v.db = DB ? 1 : 0;
+  v.minb = MINB;
   v.threads = G::NT;
   v.smem = G::SMEM_CX * sizeof(cx<T>);
-  v.fn = (const void*)vhs_cluster_kernel<T, N, C>;
-  if constexpr (sizeof(T) == 8) v.launch64 = launch_vhs<double, N, C>;
-  else v.launch32 = launch_vhs<float, N, C>;
+  v.fn = (const void*)vhs_cluster_kernel<T, N, C, DB, MINB>;
+  if constexpr (sizeof(T) == 8) v.launch64 = launch_vhs<double, N, C, DB, MINB>;
+  else v.launch32 = launch_vhs<float, N, C, DB, MINB>;
   return v;
 }
 
+// Compiled launch shapes: (precision, N, cluster size, double-buffered
+// exchange, minimum CTAs per SM for the register budget).  The first entry
+// of each (precision, N) family is the default; the autotuner times the rest.
 static const std::vector<VhsVariant>& variants() {
   static const std::vector<VhsVariant> v = {
-      make_variant<double, 8, 1>(),  make_variant<double, 8, 2>(),
-      make_variant<double, 16, 2>(), make_variant<double, 16, 4>(),
-      make_variant<double, 24, 6>(), make_variant<double, 24, 8>(),
-      make_variant<double, 32, 16>(),
-      make_variant<float, 8, 1>(),   make_variant<float, 8, 2>(),
-      make_variant<float, 16, 1>(),  make_variant<float, 16, 2>(),
-      make_variant<float, 16, 4>(),
-      make_variant<float, 24, 3>(),  make_variant<float, 24, 4>(),
-      make_variant<float, 24, 6>(),  make_variant<float, 24, 8>(),
-      make_variant<float, 32, 8>(),
-      make_variant<float, 32, 16>(),
+      make_variant<double, 8, 1, true, 4>(),    make_variant<double, 8, 2, true, 8>(),
+      make_variant<double, 16, 4, true, 2>(),   make_variant<double, 16, 2, true, 1>(),
+      make_variant<double, 16, 4, false, 3>(),
+      make_variant<double, 24, 8, true, 1>(),   make_variant<double, 24, 8, false, 1>(),
+      make_variant<double, 24, 12, false, 2>(), make_variant<double, 24, 6, false, 1>(),
+      make_variant<double, 32, 16, true, 1>(),  make_variant<double, 32, 16, false, 1>(),
+      make_variant<float, 8, 1, true, 4>(),     make_variant<float, 8, 2, true, 8>(),
+      make_variant<float, 16, 2, true, 2>(),    make_variant<float, 16, 1, true, 1>(),
+      make_variant<float, 16, 4, true, 4>(),    make_variant<float, 16, 4, false, 6>(),
+      make_variant<float, 24, 8, true, 2>(),    make_variant<float, 24, 4, true, 1>(),
+      make_variant<float, 24, 4, false, 2>(),   make_variant<float, 24, 6, false, 2>(),
+      make_variant<float, 24, 8, false, 3>(),   make_variant<float, 24, 12, false, 4>(),
+      make_variant<float, 32, 16, true, 2>(),   make_variant<float, 32, 8, true, 1>(),
+      make_variant<float, 32, 8, false, 1>(),   make_variant<float, 32, 16, false, 3>(),
   };
   return v;
 }
 
-static int default_cluster(int prec, int N) {
-  if (prec == 64) return N == 8 ? 1 : N == 16 ? 2 : N == 24 ? 8 : 16;
-  return N == 8 ? 1 : N == 16 ? 2 : N == 24 ? 4 : 8;
-}
-
-static const VhsVariant* find_variant(int prec, int N, int C) {
+static std::vector<const VhsVariant*> family(int prec, int N) {
+  std::vector<const VhsVariant*> out;
   for (const auto& v : variants())
-    if (v.prec == prec && v.N == N && v.C == C) return &v;
-  return nullptr;
+    if (v.prec == prec && v.N == N) out.push_back(&v);
+  return out;
 }
 
 }  // namespace dgfs
@@ -120,6 +124,8 @@ using namespace dgfs;
 struct dgfs_vhs {
   int N, P, M, prec, V, device, project;
   double prefac;
+  std::vector<const VhsVariant*> fam;  // compiled shapes for (prec, N)
+  int vidx;                            // selected entry of fam
   const VhsVariant* var;
   int max_clusters;
   void* phase;   // cx<T> [P][M][3][N]
@@ -127,41 +133,75 @@ struct dgfs_vhs {
   void* b2;      // T [V]
   double* ginv;  // [25]
   double* cvec;  // [3][V]
+  void* fc;      // scratch: gain spectrum, one N^3 complex slice per cluster
+  size_t fc_bytes;
 };
 
-static int select_variant(dgfs_vhs* h, int C) {
-  if (C <= 0) C = default_cluster(h->prec, h->N);
-  const VhsVariant* v = find_variant(h->prec, h->N, C);
-  if (!v)
-    return set_error(DGFS_ERR_UNSUPPORTED, "no VHS kernel for Nv=%d precision=%d cluster=%d", h->N, h->prec, C);
+// Occupancy of variant v (clusters that can be resident at once), or an
+// error if it cannot run on this device.
+static int variant_clusters(const dgfs_vhs* h, const VhsVariant* v, int* ncl) {
   int maxsm = 0;
   cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
   if ((int)v->smem > maxsm)
     return set_error(DGFS_ERR_UNSUPPORTED, "VHS kernel Nv=%d cluster=%d needs %zu B shared memory (device max %d)",
-                     h->N, C, v->smem, maxsm);
+                     h->N, v->C, v->smem, maxsm);
   if (cudaFuncSetAttribute(v->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v->smem) != cudaSuccess)
     return set_error(DGFS_ERR_CUDA, "cudaFuncSetAttribute(smem): %s", cudaGetErrorString(cudaGetLastError()));
-  if (C > 8 && cudaFuncSetAttribute(v->fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
-    return set_error(DGFS_ERR_CUDA, "non-portable cluster size %d refused: %s", C,
+  if (v->C > 8 && cudaFuncSetAttribute(v->fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+    return set_error(DGFS_ERR_CUDA, "non-portable cluster size %d refused: %s", v->C,
                      cudaGetErrorString(cudaGetLastError()));
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(C, 1, 1);
+  cfg.gridDim = dim3(v->C, 1, 1);
   cfg.blockDim = dim3(v->threads, 1, 1);
   cfg.dynamicSmemBytes = v->smem;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = C;
+  attr[0].val.clusterDim.x = v->C;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  int ncl = 0;
-  if (cudaOccupancyMaxActiveClusters(&ncl, v->fn, &cfg) != cudaSuccess || ncl <= 0)
-    return set_error(DGFS_ERR_UNSUPPORTED, "cluster size %d cannot be scheduled: %s", C,
-                     cudaGetErrorString(cudaGetLastError()));
+  *ncl = 0;
+  if (cudaOccupancyMaxActiveClusters(ncl, v->fn, &cfg) != cudaSuccess || *ncl <= 0) {
+    cudaGetLastError();
+    return set_error(DGFS_ERR_UNSUPPORTED, "cluster size %d cannot be scheduled", v->C);
+  }
+  return DGFS_OK;
+}
+
+static int select_index(dgfs_vhs* h, int idx) {
+  if (idx < 0 || idx >= (int)h->fam.size())
+    return set_error(DGFS_ERR_INVALID, "variant %d outside 0..%d", idx, (int)h->fam.size() - 1);
+  const VhsVariant* v = h->fam[idx];
+  int ncl = 0, rc = variant_clusters(h, v, &ncl);
+  if (rc) return rc;
+  const size_t esz = h->prec == 64 ? 16 : 8;
+  const size_t need = (size_t)ncl * v->C * (size_t)h->N * h->N * h->N / v->C * esz;
+  if (need > h->fc_bytes) {
+    cudaFree(h->fc);
+    h->fc = nullptr;
+    h->fc_bytes = 0;
+    if (cudaMalloc(&h->fc, need) != cudaSuccess)
+      return set_error(DGFS_ERR_NOMEM, "cudaMalloc(%zu) for the gain-spectrum scratch failed", need);
+    h->fc_bytes = need;
+  }
+  h->vidx = idx;
   h->var = v;
   h->max_clusters = ncl;
   return DGFS_OK;
+}
+
+// First runnable variant, or the first with the requested cluster size.
+static int select_variant(dgfs_vhs* h, int C) {
+  int first_err = 0;
+  for (int i = 0; i < (int)h->fam.size(); ++i) {
+    if (C > 0 && h->fam[i]->C != C) continue;
+    int rc = select_index(h, i);
+    if (!rc) return DGFS_OK;
+    if (!first_err) first_err = rc;
+  }
+  if (first_err) return first_err;
+  return set_error(DGFS_ERR_UNSUPPORTED, "no VHS kernel for Nv=%d precision=%d cluster=%d", h->N, h->prec, C);
 }
 
 template <typename T> static int upload(void** dst, const std::vector<T>& src) {
@@ -263,6 +303,7 @@ static void free_handle(dgfs_vhs* h) {
   cudaFree(h->b2);
   cudaFree(h->ginv);
   cudaFree(h->cvec);
+  cudaFree(h->fc);
   delete h;
 }
 
@@ -287,7 +328,6 @@ extern "C" int dgfs_vhs_create(const dgfs_vhs_params* p, dgfs_vhs** out) {
     if (!std::isfinite(p->sz[i])) return set_error(DGFS_ERR_INVALID, "non-finite spherical design");
 
   dgfs_vhs* h = new dgfs_vhs();
-  std::memset(h, 0, sizeof(*h));
   h->N = p->Nv;
   h->P = p->Nrho;
   h->M = p->M;
@@ -299,6 +339,7 @@ extern "C" int dgfs_vhs_create(const dgfs_vhs_params* p, dgfs_vhs** out) {
     delete h;
     return set_error(DGFS_ERR_CUDA, "no CUDA device: %s", cudaGetErrorString(cudaGetLastError()));
   }
+  h->fam = family(h->prec, h->N);
   int rc = init_twiddles(h->device);
   if (!rc) rc = select_variant(h, p->cluster);
   if (!rc) rc = h->prec == 64 ? build_tables<double>(h, p) : build_tables<float>(h, p);
@@ -319,14 +360,50 @@ extern "C" int dgfs_vhs_destroy(dgfs_vhs* h) {
 extern "C" int dgfs_vhs_set_cluster(dgfs_vhs* h, int cluster) {
   clear_error();
   if (!h) return set_error(DGFS_ERR_INVALID, "null handle");
-  const VhsVariant* old = h->var;
-  const int oldmax = h->max_clusters;
+  const int old = h->vidx;
   int rc = select_variant(h, cluster);
   if (rc) {
-    h->var = old;
-    h->max_clusters = oldmax;
+    const int keep = rc;
+    std::string msg = dgfs_last_error();
+    select_index(h, old);
+    return set_error(keep, "%s", msg.c_str());
   }
-  return rc;
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_vhs_num_variants(const dgfs_vhs* h, int* count) {
+  clear_error();
+  if (!h || !count) return set_error(DGFS_ERR_INVALID, "null argument");
+  *count = (int)h->fam.size();
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_vhs_variant_info(const dgfs_vhs* h, int idx, int* cluster, int* double_buffered,
+                                     int* min_ctas_per_sm, int* threads, int* smem_bytes) {
+  clear_error();
+  if (!h) return set_error(DGFS_ERR_INVALID, "null handle");
+  if (idx < 0 || idx >= (int)h->fam.size()) return set_error(DGFS_ERR_INVALID, "variant %d out of range", idx);
+  const VhsVariant* v = h->fam[idx];
+  if (cluster) *cluster = v->C;
+  if (double_buffered) *double_buffered = v->db;
+  if (min_ctas_per_sm) *min_ctas_per_sm = v->minb;
+  if (threads) *threads = v->threads;
+  if (smem_bytes) *smem_bytes = (int)v->smem;
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_vhs_select(dgfs_vhs* h, int idx) {
+  clear_error();
+  if (!h) return set_error(DGFS_ERR_INVALID, "null handle");
+  const int old = h->vidx;
+  int rc = select_index(h, idx);
+  if (rc) {
+    const int keep = rc;
+    std::string msg = dgfs_last_error();
+    select_index(h, old);
+    return set_error(keep, "%s", msg.c_str());
+  }
+  return DGFS_OK;
 }
 
 extern "C" int dgfs_vhs_info(const dgfs_vhs* h, int* cluster, int* threads, int* smem_bytes, int* max_clusters) {
@@ -381,6 +458,7 @@ static int vhs_launch(dgfs_vhs* h, const void* f, void* Q, int nupts, int neles,
     a.phase = (const double2*)h->phase;
     a.w1 = (const double*)h->w1;
     a.b2 = (const double*)h->b2;
+    a.fc = (double2*)h->fc;
     a.prefac = h->prefac;
     a.project = h->project;
     a.ginv = h->ginv;
@@ -401,6 +479,7 @@ static int vhs_launch(dgfs_vhs* h, const void* f, void* Q, int nupts, int neles,
     a.phase = (const float2*)h->phase;
     a.w1 = (const float*)h->w1;
     a.b2 = (const float*)h->b2;
+    a.fc = (float2*)h->fc;
     a.prefac = (float)h->prefac;
     a.project = h->project;
     a.ginv = h->ginv;

@@ -23,12 +23,17 @@
 //
 // Data layout inside a cluster of C CTAs (N^3 grid, NS = N/C, NJ = N^2/C):
 //   slab    CTA r owns planes x1 in [r NS, (r+1) NS)       S  [NS][N][N+1]
-//   pencil  CTA r owns pencils (l2, l3), l2 in [r NS, ...)  F, fC [N][NJ]
+//   pencil  CTA r owns pencils (l2, l3), l2 in [r NS, ...)  F  [N][NJ]
 // A 3D transform is a local 1D pass over pencils (along x1/l1), an
 // exchange through distributed shared memory, then local 2D passes over the
-// slab planes (or the reverse for forward transforms).  All state of a point
-// stays in the cluster's shared memory; only f, Q and the small read-only
-// tables (axis phases, radial weights) touch global memory.
+// slab planes (or the reverse for forward transforms).  The gain spectrum
+// fC, touched once per radial node, lives in a per-CTA global scratch slice
+// (L2 resident); everything touched per (p, q) stays in shared memory.
+//
+// Exchange buffers: with DB (double buffering) two sets alternate between
+// "exchange" (read by peers) and "plane" (local 2D passes) roles, so one
+// cluster barrier per (p, q) suffices; without DB a second barrier protects
+// the single set before it is overwritten.
 #pragma once
 
 #include <cooperative_groups.h>
@@ -50,6 +55,7 @@ template <typename T> struct VhsArgs {
   const cx<T>* phase;   // [P][M][3][N] exp(i fac_p s_q[axis] l0[k])
   const T* w1;          // [P][V]  (2 qw_p sw / V) b1_p(l)
   const T* b2;          // [V]
+  cx<T>* fc;            // scratch [gridDim.x][N][NJ]: gain spectrum per CTA
   T prefac;
   // optional FP64 conservation projection (mass, momentum, energy)
   int project;
@@ -57,23 +63,43 @@ template <typename T> struct VhsArgs {
   const double* cvec;   // [3][V] velocity grid
 };
 
-template <int N, int C> struct VhsGeom {
+template <int N, int C, bool DB> struct VhsGeom {
   static constexpr int NS = N / C;        // slab planes per CTA
   static constexpr int NJ = N * N / C;    // pencils per CTA
   static constexpr int NTASK = 2 * NJ;    // pencil/row/column tasks per pass
   static constexpr int NT = (NTASK + 31) / 32 * 32;  // threads per CTA (whole warps)
   static constexpr int RP = N + 1;        // padded row length
   static constexpr int V = N * N * N;
-  static constexpr int BSZ = N * NS * RP; // exchange / plane buffer
-  static constexpr int SMEM_CX = 2 * N * NJ + 3 * BSZ;
+  static constexpr int BSZ = N * NS * RP; // one exchange / plane buffer
+  static constexpr int NSETS = DB ? 2 : 1;
+  // sF [N][NJ] + exchange sets [NSETS][2][BSZ] + S [BSZ] + phases [2][3N]
+  static constexpr int SMEM_CX = N * NJ + (2 * NSETS + 1) * BSZ + 6 * N;
   static_assert(N % C == 0, "cluster size must divide N");
 };
 
+// ---- distributed shared memory access (explicit shared::cluster space) ----
+__device__ __forceinline__ uint32_t cluster_addr(const void* p, uint32_t rank) {
+  uint32_t local = (uint32_t)__cvta_generic_to_shared(p), remote;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(local), "r"(rank));
+  return remote;
+}
+__device__ __forceinline__ float2 ld_cluster(const float2*, uint32_t a) {
+  float2 v;
+  asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(a) : "memory");
+  return v;
+}
+__device__ __forceinline__ double2 ld_cluster(const double2*, uint32_t a) {
+  double2 v;
+  asm volatile("ld.shared::cluster.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(a) : "memory");
+  return v;
+}
+
 // Forward 2D transform of this CTA's slab planes (rows along x3, then columns
-// along x2), in place.
-template <typename T, int N, int C>
+// along x2), in place; every thread takes part (tasks are split in two halves
+// so that all NT threads have work).
+template <typename T, int N, int C, bool DB>
 __device__ __forceinline__ void slab_forward_2d(cx<T>* __restrict__ sS, int tid) {
-  using G = VhsGeom<N, C>;
+  using G = VhsGeom<N, C, DB>;
   using CX = cx<T>;
   if (tid < G::NJ) {
     const int x1l = tid / N, x2 = tid % N;
@@ -101,55 +127,55 @@ __device__ __forceinline__ void slab_forward_2d(cx<T>* __restrict__ sS, int tid)
 
 // Gather pencil (l2, l3) along x1 from the slab planes of every CTA of the
 // cluster and transform it forward.
-template <typename T, int N, int C>
-__device__ __forceinline__ void gather_pencil_forward(cg::cluster_group& cluster, cx<T>* sS, int rank,
-                                                      int jl, cx<T> (&x)[N]) {
-  using G = VhsGeom<N, C>;
+template <typename T, int N, int C, bool DB>
+__device__ __forceinline__ void gather_pencil_forward(const cx<T>* sS, int rank, int jl, cx<T> (&x)[N]) {
+  using G = VhsGeom<N, C, DB>;
   const int l2 = rank * G::NS + jl / N, l3 = jl % N;
+  const cx<T>* base = sS + l2 * G::RP + l3;
 #pragma unroll
   for (int r = 0; r < C; ++r) {
-    const cx<T>* rs = cluster.map_shared_rank(sS, r);
+    const uint32_t a = cluster_addr(base, r);
 #pragma unroll
-    for (int k = 0; k < G::NS; ++k) x[r * G::NS + k] = rs[(k * N + l2) * G::RP + l3];
+    for (int k = 0; k < G::NS; ++k) x[r * G::NS + k] = ld_cluster(base, a + k * N * G::RP * sizeof(cx<T>));
   }
   fft<T, N, -1>(x);
 }
 
-// Second half of an inverse 3D transform: row pass along l3 reading the
-// pencil-layout exchange buffers of the owning CTAs, then (after the cluster
-// barrier) a column pass along l2 in the local plane buffer.  On return
-// sB0/sB1 hold this CTA's slab of both transformed fields,
-// [x1l][x2][x3] with row stride RP.
-template <typename T, int N, int C>
-__device__ __forceinline__ void inverse_rows_cols(cg::cluster_group& cluster, cx<T>* sB0, cx<T>* sB1,
-                                                  int rank, int tid) {
-  using G = VhsGeom<N, C>;
+// Inverse transform, second half: row pass along l3 reading the peers'
+// exchange buffers (pencil layout), written to the local plane buffers, then
+// the column pass along l2 in place.  On return the plane buffers hold this
+// CTA's slab of both fields, [x1l][x2][x3] with row stride RP.
+template <typename T, int N, int C, bool DB>
+__device__ __forceinline__ void inverse_rows_cols(cg::cluster_group& cluster, const cx<T>* xg,
+                                                  const cx<T>* xh, cx<T>* pg, cx<T>* ph, int rank,
+                                                  int tid) {
+  using G = VhsGeom<N, C, DB>;
   using CX = cx<T>;
   const bool active = tid < G::NTASK;
   const int which = active ? tid / G::NJ : 0, rem = tid % G::NJ;
-  CX* sB = which ? sB1 : sB0;
+  CX* pl = which ? ph : pg;
   CX x[N];
   if (active) {
     const int x1l = rem / N, l2 = rem % N;
     const int owner = l2 / G::NS, l2l = l2 % G::NS;
-    const CX* rB = cluster.map_shared_rank(sB, owner);
     const int x1 = rank * G::NS + x1l;
-    const CX* src = rB + (x1 * G::NS + l2l) * G::RP;
+    const CX* src = (which ? xh : xg) + (x1 * G::NS + l2l) * G::RP;
+    const uint32_t a = cluster_addr(src, owner);
 #pragma unroll
-    for (int k = 0; k < N; ++k) x[k] = src[k];
+    for (int k = 0; k < N; ++k) x[k] = ld_cluster(src, a + k * sizeof(CX));
     fft<T, N, +1>(x);
   }
-  cluster.sync();  // every remote read of the exchange buffers is complete
+  if constexpr (!DB) cluster.sync();  // peers have finished reading xg/xh == pg/ph
   if (active) {
     const int x1l = rem / N, l2 = rem % N;
-    CX* dst = sB + (x1l * N + l2) * G::RP;
+    CX* dst = pl + (x1l * N + l2) * G::RP;
 #pragma unroll
     for (int k = 0; k < N; ++k) dst[k] = x[k];
   }
   __syncthreads();
   if (active) {
     const int x1l = rem / N, x3 = rem % N;
-    CX* col = sB + x1l * N * G::RP + x3;
+    CX* col = pl + x1l * N * G::RP + x3;
 #pragma unroll
     for (int k = 0; k < N; ++k) x[k] = col[k * G::RP];
     fft<T, N, +1>(x);
@@ -159,18 +185,17 @@ __device__ __forceinline__ void inverse_rows_cols(cg::cluster_group& cluster, cx
   __syncthreads();
 }
 
-template <typename T, int N, int C>
-__global__ void __launch_bounds__(VhsGeom<N, C>::NT, 1) vhs_cluster_kernel(const VhsArgs<T> a) {
-  using G = VhsGeom<N, C>;
+template <typename T, int N, int C, bool DB, int MINB>
+__global__ void __launch_bounds__(VhsGeom<N, C, DB>::NT, MINB) vhs_cluster_kernel(const VhsArgs<T> a) {
+  using G = VhsGeom<N, C, DB>;
   using CX = cx<T>;
-  constexpr int NS = G::NS, NJ = G::NJ, NT = G::NT, RP = G::RP, V = G::V;
+  constexpr int NS = G::NS, NJ = G::NJ, NT = G::NT, RP = G::RP, V = G::V, BSZ = G::BSZ;
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  CX* sF = reinterpret_cast<CX*>(smem_raw);  // [N][NJ]  spectrum / V (pencils)
-  CX* sFC = sF + N * NJ;                     // [N][NJ]  gain spectrum accumulator
-  CX* sB0 = sFC + N * NJ;                    // exchange / plane buffer (g)
-  CX* sB1 = sB0 + G::BSZ;                    // exchange / plane buffer (h)
-  CX* sS = sB1 + G::BSZ;                     // [NS][N][RP] slab accumulator
+  CX* sF = reinterpret_cast<CX*>(smem_raw);      // [N][NJ]  spectrum / V (pencils)
+  CX* sX = sF + N * NJ;                          // exchange sets [NSETS][2][BSZ]
+  CX* sS = sX + 2 * G::NSETS * BSZ;              // [NS][N][RP] slab accumulator
+  CX* sPh = sS + BSZ;                            // [2][3N] axis phases of (p, q)
   __shared__ double sRed[5][NT / 32];
   __shared__ double sMom[5];
 
@@ -183,6 +208,15 @@ __global__ void __launch_bounds__(VhsGeom<N, C>::NT, 1) vhs_cluster_kernel(const
   const int l2g = rank * NS + jl / N, l3 = jl % N;  // pencil owned by task jl
   const int jglob = l2g * N + l3;
   const T invV = T(1) / T(V);
+  CX* fc = a.fc + (size_t)blockIdx.x * N * NJ;  // this CTA's gain spectrum [N][NJ]
+  const int npq = a.P * a.M;
+  int it = 0;  // running (p, q) counter: selects buffer sets and phase slots
+
+  auto xbuf = [&](int set, int w) -> CX* { return sX + (DB ? (set * 2 + w) : w) * BSZ; };
+  auto load_phases = [&](int pq, int slot) {
+    const CX* src = a.phase + (size_t)pq * 3 * N;
+    for (int i = tid; i < 3 * N; i += NT) sPh[slot * 3 * N + i] = src[i];
+  };
 
   for (int pt = a.pt0 + cid; pt < a.pt0 + a.npts; pt += ncl) {
     const int upt = pt / a.neles, elem = pt % a.neles;
@@ -194,25 +228,27 @@ __global__ void __launch_bounds__(VhsGeom<N, C>::NT, 1) vhs_cluster_kernel(const
       const T fv = a.f[soa_ix(upt, a.ldim, elem, v, V, a.soasz)];
       sS[(x1l * N + r2 / N) * RP + r2 % N] = mk<CX>(fv, T(0));
     }
+    load_phases(0, it & 1);
     __syncthreads();
-    slab_forward_2d<T, N, C>(sS, tid);
+    slab_forward_2d<T, N, C, DB>(sS, tid);
     cluster.sync();
     if (tid < NJ) {
       CX x[N];
-      gather_pencil_forward<T, N, C>(cluster, sS, rank, jl, x);
+      gather_pencil_forward<T, N, C, DB>(sS, rank, jl, x);
 #pragma unroll
       for (int k = 0; k < N; ++k) {
         sF[k * NJ + jl] = cscale(x[k], invV);
-        sFC[k * NJ + jl] = mk<CX>(T(0), T(0));
+        fc[k * NJ + jl] = mk<CX>(T(0), T(0));
       }
     }
     __syncthreads();
 
     for (int p = 0; p < a.P; ++p) {
-      for (int q = 0; q < a.M; ++q) {
+      for (int q = 0; q < a.M; ++q, ++it) {
+        const int cur = DB ? (it & 1) : 0, pl = DB ? (cur ^ 1) : 0;
+        const CX* ph = sPh + (it & 1) * 3 * N;
         // ---- pencil pass: g (which=0) and h (which=1) along l1 ----------
         if (active) {
-          const CX* ph = a.phase + (size_t)(p * a.M + q) * 3 * N;
           CX eyz = cmul(ph[N + l2g], ph[2 * N + l3]);
           if (which) eyz.y = -eyz.y;
           CX x[N];
@@ -223,40 +259,47 @@ __global__ void __launch_bounds__(VhsGeom<N, C>::NT, 1) vhs_cluster_kernel(const
             x[k] = cmul(cmul(sF[k * NJ + jl], e), eyz);
           }
           fft<T, N, +1>(x);
-          CX* sB = which ? sB1 : sB0;
+          CX* sB = xbuf(cur, which);
 #pragma unroll
           for (int k = 0; k < N; ++k) sB[(k * NS + jl / N) * RP + l3] = x[k];
         }
+        // prefetch the next (p, q)'s axis phases into the other slot
+        if (p * a.M + q + 1 < npq) load_phases(p * a.M + q + 1, (it + 1) & 1);
         cluster.sync();
-        inverse_rows_cols<T, N, C>(cluster, sB0, sB1, rank, tid);
+        inverse_rows_cols<T, N, C, DB>(cluster, xbuf(cur, 0), xbuf(cur, 1), xbuf(pl, 0), xbuf(pl, 1),
+                                       rank, tid);
         // ---- S_p (+)= g h ------------------------------------------------
-        for (int i = tid; i < NS * N * N; i += NT) {
-          const int idx = (i / N) * RP + i % N;
-          const CX gh = cmul(sB0[idx], sB1[idx]);
-          sS[idx] = q == 0 ? gh : cadd(sS[idx], gh);
+        {
+          const CX* g = xbuf(pl, 0);
+          const CX* h = xbuf(pl, 1);
+          for (int i = tid; i < NS * N * N; i += NT) {
+            const int idx = (i / N) * RP + i % N;
+            const CX gh = cmul(g[idx], h[idx]);
+            sS[idx] = q == 0 ? gh : cadd(sS[idx], gh);
+          }
         }
         __syncthreads();
       }
       // ---- fC += w1_p * FFT(S_p) ------------------------------------------
-      slab_forward_2d<T, N, C>(sS, tid);
+      slab_forward_2d<T, N, C, DB>(sS, tid);
       cluster.sync();
       if (tid < NJ) {
         CX x[N];
-        gather_pencil_forward<T, N, C>(cluster, sS, rank, jl, x);
+        gather_pencil_forward<T, N, C, DB>(sS, rank, jl, x);
         const T* w = a.w1 + (size_t)p * V + jglob;
 #pragma unroll
         for (int k = 0; k < N; ++k) {
           const T wk = w[k * N * N];
-          CX acc = sFC[k * NJ + jl];
+          CX acc = fc[k * NJ + jl];
           acc.x += wk * x[k].x;
           acc.y += wk * x[k].y;
-          sFC[k * NJ + jl] = acc;
+          fc[k * NJ + jl] = acc;
         }
       }
     }
 
     // ---- gain = IFFT(fC) (which=0), loss = IFFT(b2 F) (which=1) -----------
-    __syncthreads();
+    const int cur = DB ? (it & 1) : 0, pl = DB ? (cur ^ 1) : 0;
     if (active) {
       CX x[N];
       if (which) {
@@ -265,15 +308,19 @@ __global__ void __launch_bounds__(VhsGeom<N, C>::NT, 1) vhs_cluster_kernel(const
         for (int k = 0; k < N; ++k) x[k] = cscale(sF[k * NJ + jl], b[k * N * N]);
       } else {
 #pragma unroll
-        for (int k = 0; k < N; ++k) x[k] = sFC[k * NJ + jl];
+        for (int k = 0; k < N; ++k) x[k] = fc[k * NJ + jl];
       }
       fft<T, N, +1>(x);
-      CX* sB = which ? sB1 : sB0;
+      CX* sB = xbuf(cur, which);
 #pragma unroll
       for (int k = 0; k < N; ++k) sB[(k * NS + jl / N) * RP + l3] = x[k];
     }
+    ++it;
     cluster.sync();
-    inverse_rows_cols<T, N, C>(cluster, sB0, sB1, rank, tid);
+    inverse_rows_cols<T, N, C, DB>(cluster, xbuf(cur, 0), xbuf(cur, 1), xbuf(pl, 0), xbuf(pl, 1), rank,
+                                   tid);
+    CX* gain = xbuf(pl, 0);
+    const CX* loss = xbuf(pl, 1);
 
     // ---- Q = prefac (Re gain - f Re loss) [+ FP64 projection] --------------
     if (!a.project) {
@@ -282,10 +329,10 @@ __global__ void __launch_bounds__(VhsGeom<N, C>::NT, 1) vhs_cluster_kernel(const
         const int64_t v = (int64_t)(rank * NS + x1l) * (N * N) + r2;
         const int idx = (i / N) * RP + i % N;
         const int64_t ai = soa_ix(upt, a.ldim, elem, v, V, a.soasz);
-        a.Q[ai] = a.prefac * (sB0[idx].x - a.f[ai] * sB1[idx].x);
+        a.Q[ai] = a.prefac * (gain[idx].x - a.f[ai] * loss[idx].x);
       }
     } else {
-      // Moments m_k = cw sum_v phi_k(c_v) Q_v, phi = (1, cx, cy, cz, |c|^2),
+      // Moments m_k = sum_v phi_k(c_v) Q_v, phi = (1, cx, cy, cz, |c|^2),
       // reduced in FP64 over the cluster; Q -= sum_k lambda_k phi_k with
       // lambda = Ginv m (least-squares projection onto zero moments).
       double m[5] = {0, 0, 0, 0, 0};
@@ -294,8 +341,8 @@ __global__ void __launch_bounds__(VhsGeom<N, C>::NT, 1) vhs_cluster_kernel(const
         const int64_t v = (int64_t)(rank * NS + x1l) * (N * N) + r2;
         const int idx = (i / N) * RP + i % N;
         const int64_t ai = soa_ix(upt, a.ldim, elem, v, V, a.soasz);
-        const double qv = (double)(a.prefac * (sB0[idx].x - a.f[ai] * sB1[idx].x));
-        sB0[idx].y = (T)qv;  // keep Q in the spare imaginary slot
+        const double qv = (double)(a.prefac * (gain[idx].x - a.f[ai] * loss[idx].x));
+        gain[idx].y = (T)qv;  // keep Q in the spare imaginary slot
         const double c0 = a.cvec[v], c1 = a.cvec[V + v], c2 = a.cvec[2 * V + v];
         m[0] += qv;
         m[1] += qv * c0;
@@ -339,7 +386,7 @@ __global__ void __launch_bounds__(VhsGeom<N, C>::NT, 1) vhs_cluster_kernel(const
         const double c0 = a.cvec[v], c1 = a.cvec[V + v], c2 = a.cvec[2 * V + v];
         const double corr = lam[0] + lam[1] * c0 + lam[2] * c1 + lam[3] * c2 +
                             lam[4] * (c0 * c0 + c1 * c1 + c2 * c2);
-        a.Q[soa_ix(upt, a.ldim, elem, v, V, a.soasz)] = (T)((double)sB0[idx].y - corr);
+        a.Q[soa_ix(upt, a.ldim, elem, v, V, a.soasz)] = (T)((double)gain[idx].y - corr);
       }
       cluster.sync();  // sMom is read remotely above
     }

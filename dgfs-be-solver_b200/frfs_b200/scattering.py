@@ -156,6 +156,36 @@ class DGFSVHSGLLScatteringModel(DGFSScatteringModel):
         _lib.check(self._lib.dgfs_vhs_set_cluster(self._h, int(cluster)),
                    'dgfs_vhs_set_cluster')
 
+    def variants(self):
+        """Compiled launch shapes for this (Nv, precision)."""
+        n = ct.c_int()
+        _lib.check(self._lib.dgfs_vhs_num_variants(self._h, ct.byref(n)),
+                   'dgfs_vhs_num_variants')
+        out = []
+        for i in range(n.value):
+            vals = [ct.c_int() for _ in range(5)]
+            _lib.check(self._lib.dgfs_vhs_variant_info(
+                self._h, i, *[ct.byref(v) for v in vals]),
+                'dgfs_vhs_variant_info')
+            out.append(dict(zip(('cluster', 'double_buffered',
+                                 'min_ctas_per_sm', 'threads', 'smem_bytes'),
+                                (v.value for v in vals))))
+        return out
+
+    def select(self, idx):
+        _lib.check(self._lib.dgfs_vhs_select(self._h, int(idx)),
+                   'dgfs_vhs_select')
+        self._variant = int(idx)
+
+    def autotune(self, d_arr_in, d_arr_out, npts=None, reps=2,
+                 cache=True, verbose=False):
+        """Time every compiled launch shape on this bank and keep the
+        fastest.  Results are cached per (GPU, precision, Nv, Nrho, M,
+        points) in $DGFS_B200_CACHE or ~/.cache/dgfs_b200/vhs_tune.json."""
+        from frfs_b200 import autotune as at
+        return at.tune_vhs(self, d_arr_in, d_arr_out, npts=npts, reps=reps,
+                           cache=cache, verbose=verbose)
+
     def flops_per_point(self):
         """Algorithmic FLOPs of one Q(f) evaluation as implemented:
         5 V log2 V per complex 3D transform times (2 Nrho M + Nrho + 3)

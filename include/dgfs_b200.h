@@ -109,6 +109,17 @@ DGFS_API int dgfs_vhs_info(const dgfs_vhs* h, int* cluster, int* threads,
 /* Change the cluster size (autotuning); 0 restores the default. */
 DGFS_API int dgfs_vhs_set_cluster(dgfs_vhs* h, int cluster);
 
+/* Compiled launch shapes for the handle's (Nv, precision): count, and per
+ * index the cluster size, whether the exchange buffers are double-buffered
+ * (one cluster barrier per (p, q) instead of two), the CTAs per SM the
+ * register budget was compiled for, threads per CTA and shared memory. */
+DGFS_API int dgfs_vhs_num_variants(const dgfs_vhs* h, int* count);
+DGFS_API int dgfs_vhs_variant_info(const dgfs_vhs* h, int idx, int* cluster,
+                                   int* double_buffered, int* min_ctas_per_sm,
+                                   int* threads, int* smem_bytes);
+/* Use launch shape idx for subsequent applies (the autotuner's knob). */
+DGFS_API int dgfs_vhs_select(dgfs_vhs* h, int idx);
+
 /* ------------------------------------------------------------------------
  * Measurement helper (no counterpart in the reference)
  * ---------------------------------------------------------------------- */

@@ -103,22 +103,29 @@ def test_range_and_single_agree_with_all():
     np.testing.assert_array_equal(fa.get(), fs1.get())
 
 
-@pytest.mark.parametrize('name,precision,clusters', [
-    ('small-n8', 'double', [1, 2]), ('relax0d-n16', 'double', [2, 4]),
-    ('couette-n24', 'single', [3, 4, 6, 8]),
-    ('channel-n32', 'single', [8, 16])])
-def test_cluster_sizes_agree(name, precision, clusters):
-    """Every cluster size performs the same arithmetic per value."""
+@pytest.mark.parametrize('name,precision', [
+    ('small-n8', 'double'), ('relax0d-n16', 'double'),
+    ('relax0d-n16', 'single'), ('couette-n24', 'double'),
+    ('couette-n24', 'single'), ('channel-n32', 'double'),
+    ('channel-n32', 'single')])
+def test_launch_shapes_agree(name, precision):
+    """Every compiled launch shape (cluster size, buffering, occupancy)
+    performs the same arithmetic per value; each is also checked against
+    the oracle on one point."""
     cfg = _cfg(name, precision)
     be, vm, sm = _model(cfg)
+    ovm, pre, prefac = oracle_for(cfg)
     f = random_states(vm.cv(), 3, seed=9).reshape(1, 3, -1)
     outs = []
-    for c in clusters:
-        sm.set_cluster(c)
+    for i, v in enumerate(sm.variants()):
+        sm.select(i)
         fin, fout = _bank(be, vm, f)
         sm.fs_all(fin, fout)
         torch.cuda.synchronize()
         outs.append(fout.get())
+    Qo = ovhs.vhs_Q(fin.get()[0, :, 2].astype(np.float64), ovm, pre, prefac)
+    tol = FP64_TOL if precision == 'double' else FP32_TOL
+    assert rel_err(outs[0][0, :, 2], Qo) < tol
     for o in outs[1:]:
         assert rel_err(o, outs[0]) < (1e-13 if precision == 'double'
                                       else 1e-6)
@@ -146,6 +153,19 @@ def test_conservation_projection(precision):
                         (Qg*(cv*cv).sum(axis=0)).sum()])
         mtol = 1e-12 if precision == 'double' else 1e-6
         assert np.all(np.abs(mom) < mtol*scale*np.array([1, 5, 5, 5, 25]))
+
+
+def test_autotune_selects_a_runnable_shape(tmp_path, monkeypatch):
+    monkeypatch.setenv('DGFS_B200_CACHE', str(tmp_path))
+    cfg = _cfg('relax0d-n16', 'single')
+    be, vm, sm = _model(cfg)
+    f = random_states(vm.cv(), 8, seed=3).reshape(2, 4, -1)
+    fin, fout = _bank(be, vm, f)
+    entry = sm.autotune(fin, fout)
+    assert 0 <= entry['index'] < len(sm.variants())
+    assert (tmp_path / 'vhs_tune.json').exists()
+    again = sm.autotune(fin, fout)          # served from the cache
+    assert again['index'] == entry['index']
 
 
 def test_invalid_arguments_raise():
