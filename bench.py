@@ -53,6 +53,10 @@ def _parse():
     ap.add_argument('--mode', default='collide', choices=['collide', 'step'])
     ap.add_argument('--cpu-seconds', type=float, default=12.0)
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--variant', type=int, default=-1,
+                    help='VHS launch shape index (default: autotune)')
+    ap.add_argument('--graphs', type=int, default=1,
+                    help='CUDA graph per SSP-RK2 stage (--mode step)')
     return ap.parse_args()
 
 
@@ -237,6 +241,33 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # B200 arm
 # ---------------------------------------------------------------------------
+def _timed(fn, steps, stream, flush):
+    """Per-step CUDA-event times (ms) of fn on ``stream``; L2 is flushed
+    before every step, outside the events."""
+    import torch
+    times = []
+    for _ in range(steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    return times
+
+
+def _max_over_ranks(x, world, device):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
@@ -256,24 +287,47 @@ def run_b200(args):
 
     cfg = _cfg(args)
     be = B200Backend(cfg, device=f'cuda:{local}')
-    vm = DGFSVelocityMesh(be, cfg)
-    sm = DGFSVHSGLLScatteringModel(be, cfg, vm)
     nupts, neles = _points_shape(cfg)
     npts = nupts*neles
-    V = vm.vsize()
-    f0 = _synthetic_f(vm.cv(), nupts, neles, seed=rank)
-    fin = be.matrix((nupts, V, neles), f0)
-    fout = be.matrix((nupts, V, neles))
     stream = torch.cuda.current_stream()
     flush = torch.empty(256*1024*1024 // 4, dtype=torch.float32,
                         device=be.device)
 
-    def step():
-        sm.fs_all(fin, fout)
+    if args.mode == 'step':
+        from frfs_b200.steppers import StdTVDRK2DGFSStepper
+        from frfs_b200.system import DGFSSystem
+        cfg.set('backend-b200', 'cuda-graphs', int(args.graphs))
+        vm0 = DGFSVelocityMesh(None, cfg)
+        f0 = _synthetic_f(vm0.cv(), nupts, neles, seed=rank)
+        system = DGFSSystem(be, cfg, initsoln=f0)
+        vm, sm = system.vm, system.sm
+        stepper = StdTVDRK2DGFSStepper(system, cfg)
+        fin, fout = system.bank[0], system.bank[1]
+        evals_per_step = 2*npts
+        launches_per_step = 8   # per stage: VHS, interp, wall sums, residual
+
+        def step():
+            stepper.advance(1)
+    else:
+        vm = DGFSVelocityMesh(be, cfg)
+        sm = DGFSVHSGLLScatteringModel(be, cfg, vm)
+        V = vm.vsize()
+        f0 = _synthetic_f(vm.cv(), nupts, neles, seed=rank)
+        fin = be.matrix((nupts, V, neles), f0)
+        fout = be.matrix((nupts, V, neles))
+        evals_per_step = npts
+        launches_per_step = 1
+
+        def step():
+            sm.fs_all(fin, fout)
 
     # project-written autotuner: time every compiled launch shape on this
     # bank (setup, not timed) and keep the fastest
-    tune = sm.autotune(fin, fout, cache=False)
+    if args.variant >= 0:
+        sm.select(args.variant)
+        tune = {'variant': sm.variants()[args.variant], 'all_ms': {}}
+    else:
+        tune = sm.autotune(fin, fout, cache=False)
 
     for _ in range(args.warmup):
         step()
@@ -284,76 +338,85 @@ def run_b200(args):
         dist.barrier()
     torch.cuda.synchronize()
     clocks.start()
-    times = []
-    for _ in range(args.steps):
-        flush.zero_()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        step()
-        e1.record(stream)
-        e1.synchronize()
-        times.append(e0.elapsed_time(e1))
+    times = _timed(step, args.steps, stream, flush)
     torch.cuda.synchronize()
     clk = clocks.stop()
-    t_ms = float(np.sum(times))
+    t_ms = _max_over_ranks(float(np.sum(times)), world, be.device)
     if world > 1:
-        t = torch.tensor([t_ms], device=be.device, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_ms = float(t.item())
         dist.barrier()
     ms_per_step = t_ms/args.steps
-    value = world*npts*args.steps/(t_ms*1e-3)
+    value = world*evals_per_step*args.steps/(t_ms*1e-3)
 
-    # end to end through the public API: pinned host f -> device, Q(f),
-    # device -> pinned host Q, all inside the timed region
-    hin = torch.empty(fin.data.numel(), dtype=fin.data.dtype,
+    # end to end through the public API: pinned host distribution ->
+    # device, the step, device -> pinned host result, all timed
+    src_bank = fin
+    dst_bank = fin if args.mode == 'step' else fout
+    hin = torch.empty(src_bank.data.numel(), dtype=src_bank.data.dtype,
                       pin_memory=True)
-    hin.copy_(fin.data.cpu())
+    hin.copy_(src_bank.data.cpu())
     hout = torch.empty_like(hin, pin_memory=True)
+
+    def e2e_step():
+        src_bank.data.copy_(hin, non_blocking=True)
+        step()
+        hout.copy_(dst_bank.data, non_blocking=True)
     for _ in range(2):
-        fin.data.copy_(hin, non_blocking=True)
-        step()
-        hout.copy_(fout.data, non_blocking=True)
+        e2e_step()
     torch.cuda.synchronize()
-    etimes = []
-    for _ in range(args.steps):
-        flush.zero_()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        fin.data.copy_(hin, non_blocking=True)
-        step()
-        hout.copy_(fout.data, non_blocking=True)
-        e1.record(stream)
-        e1.synchronize()
-        etimes.append(e0.elapsed_time(e1))
-    te = float(np.sum(etimes))
-    if world > 1:
-        t = torch.tensor([te], device=be.device, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        te = float(t.item())
-    e2e = {'value': world*npts*args.steps/(te*1e-3), 'unit': 'evals/s',
+    te = _max_over_ranks(float(np.sum(_timed(e2e_step, args.steps, stream,
+                                               flush))), world, be.device)
+    e2e = {'value': world*evals_per_step*args.steps/(te*1e-3),
+           'unit': 'evals/s',
            'h2d_bytes_per_step': int(hin.numel()*hin.element_size()),
            'd2h_bytes_per_step': int(hout.numel()*hout.element_size())}
 
-    # roofline of the dominant kernel (the fused VHS launch is the whole step)
+    # dominant kernel: the fused VHS launch, timed alone on the same bank
     prec = 64 if args.precision == 'double' else 32
+    vhs_ms = float(np.mean(_timed(lambda: sm.fs_all(fin, fout),
+                                  max(2, min(args.steps, 5)), stream,
+                                  flush)))
     tf = _lib.c_double()
-    ms = _lib.ct.c_float()
+    pms = _lib.ct.c_float()
     _lib.check(_lib.load().dgfs_probe_fma_peak(
-        prec, 4096, _lib.ct.byref(tf), _lib.ct.byref(ms),
+        prec, 4096, _lib.ct.byref(tf), _lib.ct.byref(pms),
         stream.cuda_stream), 'dgfs_probe_fma_peak')
     flops_pt = sm.flops_per_point()
-    achieved = flops_pt*npts/(ms_per_step*1e-3)/1e12
+    achieved = flops_pt*npts/(vhs_ms*1e-3)/1e12
     roof = {'bound': 'fp32-simt' if prec == 32 else 'fp64-simt',
             'achieved': achieved, 'peak': tf.value, 'unit': 'TFLOP/s',
             'frac': achieved/tf.value,
             'peak_source': 'measured in this run: FMA loop on every SM '
                            '(dgfs_probe_fma_peak)',
-            'flops_per_point': flops_pt,
-            'traffic': None,
-            'kernel': 'vhs_cluster_kernel', 'launches_per_step': 1}
+            'flops_per_point': flops_pt, 'launch_ms': vhs_ms,
+            'traffic': None, 'kernel': 'vhs_cluster_kernel'}
+    extra = {}
+    if args.mode == 'step':
+        extra['dg_step_ms'] = ms_per_step
+        # DG residual + RK combination, HBM bound: time it alone
+        dg_ms = float(np.mean(_timed(
+            lambda: system.rk_stage(1, 0, 0.5, 0, 0.5, 1, 1e-3, 2,
+                                    interp=True),
+            max(2, min(args.steps, 5)), stream, flush)))
+        esz = 8 if prec == 64 else 4
+        U, F, V = system.nupts, system.nfpts, vm.vsize()
+        # interp: read u, write uf; residual: read u, A, B, C, uf of the
+        # partners, write out
+        dg_bytes = (U + F + 4*U + F + U)*V*neles*esz
+        peaks = {}
+        try:
+            with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as fh:
+                peaks = json.load(fh)
+        except (OSError, ValueError):
+            pass
+        hbm = peaks.get('hbm_gbs', 6650.0)
+        extra['dg_roofline'] = {
+            'bound': 'hbm', 'achieved': dg_bytes/(dg_ms*1e-3)/1e9,
+            'peak': hbm, 'unit': 'GB/s',
+            'frac': dg_bytes/(dg_ms*1e-3)/1e9/hbm,
+            'peak_source': 'MEASURED_PEAKS.json hbm_gbs' if peaks
+            else 'fallback 6650 GB/s',
+            'bytes_per_launch': dg_bytes, 'launch_ms': dg_ms,
+            'kernels': 'dg_interp_kernel + dg_residual_kernel'}
     launch = sm.launch_info()
 
     if rank == 0:
@@ -369,12 +432,13 @@ def run_b200(args):
             'data': 'synthetic',
             'config': _workload_desc(args, cfg, npts),
             'clocks': clk, 'e2e': e2e,
-            'gpu_launches': args.steps,
+            'gpu_launches': args.steps*launches_per_step,
             'roofline': roof, 'cpu_baseline': cb,
             'launch': launch,
             'autotune': {'selected': tune['variant'],
                          'ms_by_variant': tune['all_ms']},
         }
+        line.update(extra)
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()

@@ -1,0 +1,357 @@
+// Host side of the FR-DG residual: validation, device copies of geometry and
+// boundary data, the flux-point scratch and the launches behind the C ABI.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "../../include/dgfs_b200.h"
+#include "dg_kernel.cuh"
+#include "dgfs_internal.h"
+
+using namespace dgfs;
+
+struct dgfs_dg {
+  int prec, D, U, F, V, E, nb, ngroups, device;
+  long long ldim_u, ldim_f;
+  double cw;
+  std::vector<double> m0, m132, m3;  // host copies (operators travel as params)
+  void *smats, *rcpdjac, *nrm, *mag, *cvx, *cvy, *cvz, *guw, *gfw;
+  int *part, *bkind, *bgroup, *bfpt, *bele, *grefl;
+  double* bcvals;
+  void* uf;  // flux-point scratch [F][ldim_f]
+};
+
+namespace {
+
+template <typename T> int upload_as(void** dst, const double* src, size_t n) {
+  std::vector<T> h(n);
+  for (size_t i = 0; i < n; ++i) h[i] = (T)src[i];
+  if (cudaMalloc(dst, n * sizeof(T) + 16) != cudaSuccess) {
+    *dst = nullptr;
+    return set_error(DGFS_ERR_NOMEM, "cudaMalloc(%zu) failed", n * sizeof(T));
+  }
+  if (n && cudaMemcpy(*dst, h.data(), n * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
+    return set_error(DGFS_ERR_CUDA, "cudaMemcpy: %s", cudaGetErrorString(cudaGetLastError()));
+  return DGFS_OK;
+}
+
+int upload_int(int** dst, const int* src, size_t n) {
+  if (cudaMalloc((void**)dst, n * sizeof(int) + 16) != cudaSuccess) {
+    *dst = nullptr;
+    return set_error(DGFS_ERR_NOMEM, "cudaMalloc(%zu) failed", n * sizeof(int));
+  }
+  if (n && cudaMemcpy(*dst, src, n * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+    return set_error(DGFS_ERR_CUDA, "cudaMemcpy: %s", cudaGetErrorString(cudaGetLastError()));
+  return DGFS_OK;
+}
+
+template <typename T> int upload_geom(dgfs_dg* h, const dgfs_dg_params* p) {
+  const size_t D = h->D, U = h->U, F = h->F, E = h->E, V = h->V;
+  int rc;
+  if ((rc = upload_as<T>(&h->smats, p->smats, D * U * D * E))) return rc;
+  if ((rc = upload_as<T>(&h->rcpdjac, p->rcpdjac, U * E))) return rc;
+  if ((rc = upload_as<T>(&h->nrm, p->nrm, F * D * E))) return rc;
+  if ((rc = upload_as<T>(&h->mag, p->mag, F * E))) return rc;
+  if ((rc = upload_as<T>(&h->cvx, p->cv, V))) return rc;
+  if ((rc = upload_as<T>(&h->cvy, p->cv + V, V))) return rc;
+  if ((rc = upload_as<T>(&h->cvz, p->cv + 2 * V, V))) return rc;
+  const size_t G = h->ngroups;
+  std::vector<double> uw(3 * (G ? G : 1), 0.0), fw(V * (G ? G : 1), 0.0);
+  if (G) {
+    std::memcpy(uw.data(), p->guw, 3 * G * sizeof(double));
+    std::memcpy(fw.data(), p->gfw, V * G * sizeof(double));
+  }
+  if ((rc = upload_as<T>(&h->guw, uw.data(), uw.size()))) return rc;
+  if ((rc = upload_as<T>(&h->gfw, fw.data(), fw.size()))) return rc;
+  return DGFS_OK;
+}
+
+template <typename T> DgArgs<T> make_args(const dgfs_dg* h) {
+  DgArgs<T> a{};
+  a.V = h->V;
+  a.neles = h->E;
+  a.ldim_u = h->ldim_u;
+  a.ldim_f = h->ldim_f;
+  a.uf = (T*)h->uf;
+  a.smats = (const T*)h->smats;
+  a.rcpdjac = (const T*)h->rcpdjac;
+  a.nrm = (const T*)h->nrm;
+  a.mag = (const T*)h->mag;
+  a.part = h->part;
+  a.cvx = (const T*)h->cvx;
+  a.cvy = (const T*)h->cvy;
+  a.cvz = (const T*)h->cvz;
+  a.bkind = h->bkind;
+  a.bgroup = h->bgroup;
+  a.guw = (const T*)h->guw;
+  a.gfw = (const T*)h->gfw;
+  a.grefl = h->grefl;
+  a.bcvals = h->bcvals;
+  return a;
+}
+
+template <typename T, int U, int F, int D> DgOps<T, U, F, D> make_ops(const dgfs_dg* h) {
+  DgOps<T, U, F, D> o;
+  for (int f = 0; f < F; ++f)
+    for (int i = 0; i < U; ++i) o.m0[f][i] = (T)h->m0[f * U + i];
+  for (int r = 0; r < U; ++r)
+    for (int j = 0; j < D * U; ++j) o.m132[r][j] = (T)h->m132[r * D * U + j];
+  for (int r = 0; r < U; ++r)
+    for (int f = 0; f < F; ++f) o.m3[r][f] = (T)h->m3[r * F + f];
+  return o;
+}
+
+inline unsigned grid_for(const dgfs_dg* h, int nv) {
+  const long long nblk = (h->E + 31) / 32;
+  return (unsigned)((nblk * nv * 32 + 255) / 256);
+}
+
+template <typename T, int U, int F, int D>
+cudaError_t run_interp(const dgfs_dg* h, const void* u, int v0, int nv, cudaStream_t s) {
+  DgArgs<T> a = make_args<T>(h);
+  a.u = (const T*)u;
+  a.v0 = v0;
+  a.nv = nv;
+  dg_interp_kernel<T, U, F, D><<<grid_for(h, nv), 256, 0, s>>>(a, make_ops<T, U, F, D>(h));
+  return cudaGetLastError();
+}
+
+template <typename T, int U, int F, int D>
+cudaError_t run_rhs(const dgfs_dg* h, const void* u, void* out, int v0, int nv, double alpha, const void* A,
+                    double beta, const void* B, double gamma, const void* C, cudaStream_t s) {
+  DgArgs<T> a = make_args<T>(h);
+  a.u = (const T*)u;
+  a.out = (T*)out;
+  a.A = (const T*)A;
+  a.B = (const T*)B;
+  a.Cq = (const T*)C;
+  a.alpha = (T)alpha;
+  a.beta = (T)beta;
+  a.gamma = (T)gamma;
+  a.v0 = v0;
+  a.nv = nv;
+  dg_residual_kernel<T, U, F, D><<<grid_for(h, nv), 256, 0, s>>>(a, make_ops<T, U, F, D>(h));
+  return cudaGetLastError();
+}
+
+// (U, F, D) shapes compiled in: quadrilaterals of order 1, 2, 3
+#define DG_DISPATCH(PREC, CALL)                                         \
+  do {                                                                  \
+    if (h->D == 2 && h->U == 4 && h->F == 8) {                          \
+      CALL(PREC, 4, 8, 2);                                              \
+    } else if (h->D == 2 && h->U == 9 && h->F == 12) {                  \
+      CALL(PREC, 9, 12, 2);                                             \
+    } else if (h->D == 2 && h->U == 16 && h->F == 16) {                 \
+      CALL(PREC, 16, 16, 2);                                            \
+    } else {                                                            \
+      return set_error(DGFS_ERR_UNSUPPORTED, "no DG kernel for D=%d U=%d F=%d", h->D, h->U, h->F); \
+    }                                                                   \
+  } while (0)
+
+bool supported_shape(int D, int U, int F) {
+  return D == 2 && ((U == 4 && F == 8) || (U == 9 && F == 12) || (U == 16 && F == 16));
+}
+
+int check_bank(const dgfs_dg* h, const void* p, const char* what) {
+  if (!p) return set_error(DGFS_ERR_INVALID, "null %s bank", what);
+  const size_t esz = h->prec == 64 ? 8 : 4;
+  if ((uintptr_t)p % esz) return set_error(DGFS_ERR_INVALID, "misaligned %s bank", what);
+  return DGFS_OK;
+}
+
+int check_range(const dgfs_dg* h, int v0, int nv) {
+  if (v0 < 0 || nv < 1 || (long long)v0 + nv > h->V)
+    return set_error(DGFS_ERR_INVALID, "velocity range [%d, %d) outside 0..%d", v0, v0 + nv, h->V);
+  int dev = -1;
+  cudaGetDevice(&dev);
+  if (dev != h->device)
+    return set_error(DGFS_ERR_INVALID, "handle built on device %d used on device %d", h->device, dev);
+  return DGFS_OK;
+}
+
+void free_dg(dgfs_dg* h) {
+  if (!h) return;
+  void* ptrs[] = {h->smats, h->rcpdjac, h->nrm, h->mag, h->cvx, h->cvy, h->cvz, h->guw, h->gfw,
+                  h->part, h->bkind, h->bgroup, h->bfpt, h->bele, h->grefl, h->bcvals, h->uf};
+  for (void* q : ptrs) cudaFree(q);
+  delete h;
+}
+
+}  // namespace
+
+extern "C" int dgfs_dg_create(const dgfs_dg_params* p, dgfs_dg** out) {
+  clear_error();
+  if (!p || !out) return set_error(DGFS_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (p->precision != 32 && p->precision != 64) return set_error(DGFS_ERR_INVALID, "precision must be 32 or 64");
+  if (!supported_shape(p->ndims, p->nupts, p->nfpts))
+    return set_error(DGFS_ERR_UNSUPPORTED, "no DG kernel for ndims=%d nupts=%d nfpts=%d", p->ndims, p->nupts,
+                     p->nfpts);
+  if (p->nvars < 1 || p->neles < 1) return set_error(DGFS_ERR_INVALID, "bad sizes nvars=%d neles=%d", p->nvars, p->neles);
+  if (p->soasz != 32) return set_error(DGFS_ERR_UNSUPPORTED, "DG kernels need soasz = 32, got %d", p->soasz);
+  const long long nblk = (p->neles + 31) / 32;
+  if (p->ldim < nblk * 32 * (long long)p->nvars)
+    return set_error(DGFS_ERR_INVALID, "ldim %lld smaller than one AoSoA row", p->ldim);
+  if (!p->m0 || !p->m132 || !p->m3 || !p->smats || !p->rcpdjac || !p->nrm || !p->mag || !p->partner || !p->cv)
+    return set_error(DGFS_ERR_INVALID, "null operator or geometry array");
+  if (p->nbfpts < 0 || p->ngroups < 0 || (p->nbfpts && (!p->bkind || !p->bgroup || !p->bfpt || !p->bele)))
+    return set_error(DGFS_ERR_INVALID, "bad boundary description");
+  if (p->ngroups && (!p->guw || !p->gfw)) return set_error(DGFS_ERR_INVALID, "null boundary group data");
+  const int U = p->nupts, F = p->nfpts, D = p->ndims, E = p->neles;
+  for (int i = 0; i < F * E; ++i) {
+    const int q = p->partner[i];
+    if (q >= 0 ? (long long)q >= (long long)F * E : (-q - 1) >= p->nbfpts)
+      return set_error(DGFS_ERR_INVALID, "partner entry %d = %d out of range", i, q);
+  }
+  for (int b = 0; b < p->nbfpts; ++b) {
+    if (p->bkind[b] < 0 || p->bkind[b] > BC_WALL_SPECULAR) return set_error(DGFS_ERR_INVALID, "bad boundary kind");
+    if (p->bgroup[b] < 0 || p->bgroup[b] >= p->ngroups) return set_error(DGFS_ERR_INVALID, "bad boundary group");
+    if (p->bfpt[b] < 0 || p->bfpt[b] >= F || p->bele[b] < 0 || p->bele[b] >= E)
+      return set_error(DGFS_ERR_INVALID, "bad boundary flux point");
+    if (p->bkind[b] == BC_WALL_SPECULAR && !p->grefl)
+      return set_error(DGFS_ERR_INVALID, "specular wall without a reflection map");
+  }
+  if (p->grefl)
+    for (long long i = 0; i < (long long)p->ngroups * p->nvars; ++i)
+      if (p->grefl[i] < 0 || p->grefl[i] >= p->nvars) return set_error(DGFS_ERR_INVALID, "bad reflection map");
+
+  dgfs_dg* h = new dgfs_dg();
+  h->prec = p->precision;
+  h->D = D;
+  h->U = U;
+  h->F = F;
+  h->V = p->nvars;
+  h->E = E;
+  h->nb = p->nbfpts;
+  h->ngroups = p->ngroups;
+  h->ldim_u = p->ldim;
+  h->cw = p->cw;
+  h->m0.assign(p->m0, p->m0 + F * U);
+  h->m132.assign(p->m132, p->m132 + U * D * U);
+  h->m3.assign(p->m3, p->m3 + U * F);
+  const size_t esz = h->prec == 64 ? 8 : 4;
+  const long long row = nblk * 32 * (long long)h->V;
+  const long long ldmod = 128 / (long long)esz;
+  h->ldim_f = (row + ldmod - 1) / ldmod * ldmod;
+  int rc = cudaGetDevice(&h->device) == cudaSuccess ? DGFS_OK : set_error(DGFS_ERR_CUDA, "no CUDA device");
+  if (!rc) rc = h->prec == 64 ? upload_geom<double>(h, p) : upload_geom<float>(h, p);
+  if (!rc) rc = upload_int(&h->part, p->partner, (size_t)F * E);
+  const int nb = h->nb ? h->nb : 1;
+  std::vector<int> zeros(nb, 0);
+  if (!rc) rc = upload_int(&h->bkind, h->nb ? p->bkind : zeros.data(), nb);
+  if (!rc) rc = upload_int(&h->bgroup, h->nb ? p->bgroup : zeros.data(), nb);
+  if (!rc) rc = upload_int(&h->bfpt, h->nb ? p->bfpt : zeros.data(), nb);
+  if (!rc) rc = upload_int(&h->bele, h->nb ? p->bele : zeros.data(), nb);
+  if (!rc) {
+    const size_t n = (size_t)(p->ngroups ? p->ngroups : 1) * h->V;
+    std::vector<int> refl(n, 0);
+    if (p->grefl) std::memcpy(refl.data(), p->grefl, (size_t)p->ngroups * h->V * sizeof(int));
+    rc = upload_int(&h->grefl, refl.data(), n);
+  }
+  if (!rc) {
+    std::vector<double> ones(2 * nb, 1.0);  // frfs initialises bc_vals to 1 (inters.py:203)
+    if (cudaMalloc((void**)&h->bcvals, 2 * nb * sizeof(double)) != cudaSuccess ||
+        cudaMemcpy(h->bcvals, ones.data(), 2 * nb * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+      rc = set_error(DGFS_ERR_NOMEM, "boundary value allocation failed");
+  }
+  if (!rc) {
+    const size_t bytes = (size_t)F * h->ldim_f * esz;
+    if (cudaMalloc(&h->uf, bytes) != cudaSuccess)
+      rc = set_error(DGFS_ERR_NOMEM, "cudaMalloc(%zu) for the flux-point scratch failed", bytes);
+    else
+      cudaMemset(h->uf, 0, bytes);
+  }
+  if (rc) {
+    free_dg(h);
+    return rc;
+  }
+  *out = h;
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_dg_destroy(dgfs_dg* h) {
+  clear_error();
+  free_dg(h);
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_dg_interp(dgfs_dg* h, const void* u, int v0, int nv, void* stream) {
+  clear_error();
+  if (!h) return set_error(DGFS_ERR_INVALID, "null handle");
+  int rc = check_bank(h, u, "solution");
+  if (!rc) rc = check_range(h, v0, nv);
+  if (rc) return rc;
+  cudaError_t e = cudaSuccess;
+#define CALL(P, U, F, D) e = run_interp<P, U, F, D>(h, u, v0, nv, (cudaStream_t)stream)
+  if (h->prec == 64)
+    DG_DISPATCH(double, CALL);
+  else
+    DG_DISPATCH(float, CALL);
+#undef CALL
+  if (e != cudaSuccess) return set_error(DGFS_ERR_CUDA, "DG interp launch: %s", cudaGetErrorString(e));
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_dg_updatebc(dgfs_dg* h, int v0, int nv, int reset, void* stream) {
+  clear_error();
+  if (!h) return set_error(DGFS_ERR_INVALID, "null handle");
+  int rc = check_range(h, v0, nv);
+  if (rc) return rc;
+  if (h->nb == 0) return DGFS_OK;
+  const unsigned grid = (unsigned)((h->nb + 31) / 32);
+  if (h->prec == 64) {
+    DgArgs<double> a = make_args<double>(h);
+    a.v0 = v0;
+    a.nv = nv;
+    dg_bcsum_kernel<double, 2><<<grid, 256, 0, (cudaStream_t)stream>>>(a, h->bfpt, h->bele, h->nb, h->cw,
+                                                                        h->bcvals, reset);
+  } else {
+    DgArgs<float> a = make_args<float>(h);
+    a.v0 = v0;
+    a.nv = nv;
+    dg_bcsum_kernel<float, 2><<<grid, 256, 0, (cudaStream_t)stream>>>(a, h->bfpt, h->bele, h->nb, h->cw,
+                                                                       h->bcvals, reset);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(DGFS_ERR_CUDA, "DG boundary update launch: %s", cudaGetErrorString(e));
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_dg_rhs(dgfs_dg* h, const void* u, void* out, int v0, int nv, double alpha, const void* A,
+                           double beta, const void* B, double gamma, const void* C, void* stream) {
+  clear_error();
+  if (!h) return set_error(DGFS_ERR_INVALID, "null handle");
+  int rc = check_bank(h, u, "solution");
+  if (!rc) rc = check_bank(h, out, "output");
+  if (!rc) rc = check_range(h, v0, nv);
+  if (rc) return rc;
+  if (out == u) return set_error(DGFS_ERR_INVALID, "output bank must differ from the solution bank");
+  if (!std::isfinite(alpha) || !std::isfinite(beta) || !std::isfinite(gamma))
+    return set_error(DGFS_ERR_INVALID, "non-finite combination coefficient");
+  cudaError_t e = cudaSuccess;
+#define CALL(P, U, F, D) e = run_rhs<P, U, F, D>(h, u, out, v0, nv, alpha, A, beta, B, gamma, C, (cudaStream_t)stream)
+  if (h->prec == 64)
+    DG_DISPATCH(double, CALL);
+  else
+    DG_DISPATCH(float, CALL);
+#undef CALL
+  if (e != cudaSuccess) return set_error(DGFS_ERR_CUDA, "DG residual launch: %s", cudaGetErrorString(e));
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_dg_bcvals(const dgfs_dg* h, double* host, int n) {
+  clear_error();
+  if (!h || !host) return set_error(DGFS_ERR_INVALID, "null argument");
+  if (n < 2 * h->nb) return set_error(DGFS_ERR_INVALID, "buffer holds %d values, need %d", n, 2 * h->nb);
+  if (h->nb && cudaMemcpy(host, h->bcvals, 2 * h->nb * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return set_error(DGFS_ERR_CUDA, "cudaMemcpy: %s", cudaGetErrorString(cudaGetLastError()));
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_dg_fpts(const dgfs_dg* h, void** ptr, long long* ldim) {
+  clear_error();
+  if (!h || !ptr || !ldim) return set_error(DGFS_ERR_INVALID, "null argument");
+  *ptr = h->uf;
+  *ldim = h->ldim_f;
+  return DGFS_OK;
+}

@@ -1,0 +1,221 @@
+// FR-DG advection residual over all discrete velocities.
+//
+// One thread per (velocity v, element e); a warp covers the 32 elements of
+// one AoSoA block at one velocity, so every bank access is a coalesced
+// 32-element row.  The element operators travel in the kernel parameters
+// (constant bank) and every loop over them is unrolled, so matrix entries are
+// FMA operands, not loads.
+//
+//   dg_interp_kernel    uf = M0 u at the flux points (frfs/solvers/dgfs/
+//                        elements.py:55-59, 'disu')
+//   dg_bcsum_kernel     diffuse-wall sums over velocities in FP64
+//                        (kernels/bcs/dgfs-wall-diffuse-update.mako:14-36)
+//   dg_residual_kernel  R = -(1/|J|)[(M1 - M3 M2) F~ + M3 F^] with the upwind
+//                        common flux at every flux point (interfaces and
+//                        boundaries), fused with the Runge-Kutta combination
+//                        out = a A + b B + g (R + C)
+//                        (elements.py:49-118, intcflux.mako, bccflux.mako,
+//                        rusanov.mako:46-50, negdivconf.mako, axnpby.mako)
+#pragma once
+
+#include "dgfs_common.cuh"
+
+namespace dgfs {
+
+enum DgBcKind { BC_WALL_DIFFUSE = 0, BC_INLET = 1, BC_OUTLET = 2, BC_VANISH = 3, BC_WALL_SPECULAR = 4 };
+
+template <typename T, int U, int F, int D> struct DgOps {
+  T m0[F][U];
+  T m132[U][D * U];
+  T m3[U][F];
+};
+
+template <typename T> struct DgArgs {
+  int V, neles, v0, nv;
+  int64_t ldim_u;          // leading dimension of solution banks
+  int64_t ldim_f;          // leading dimension of the flux-point scratch
+  const T* u;              // solution bank [U][V][E] (AoSoA 32)
+  T* uf;                   // flux-point values [F][V][E] (AoSoA 32)
+  T* out;                  // residual / RK output bank
+  const T* A;              // optional terms of out = a A + b B + g (R + C)
+  const T* B;
+  const T* Cq;
+  T alpha, beta, gamma;
+  // geometry (SoA over elements)
+  const T* smats;          // [D][U][D][E]
+  const T* rcpdjac;        // [U][E]
+  const T* nrm;            // [F][D][E] unit outward normals
+  const T* mag;            // [F][E]    |S^T n|
+  const int* part;         // [F][E]    fpt_r*E + e_r, or -(b+1) for boundary b
+  const T* cvx;            // [V] velocity grid
+  const T* cvy;
+  const T* cvz;
+  // boundaries
+  const int* bkind;        // [nb]
+  const int* bgroup;       // [nb]
+  const T* guw;            // [ngroups][3]
+  const T* gfw;            // [ngroups][V]
+  const int* grefl;        // [ngroups][V]
+  const double* bcvals;    // [nb][2]
+};
+
+__device__ __forceinline__ int64_t aos32(int64_t row, int64_t ldim, int64_t e, int64_t v, int64_t V) {
+  return row * ldim + ((e >> 5) * V + v) * 32 + (e & 31);
+}
+
+template <typename T, int U, int F, int D>
+__global__ void __launch_bounds__(256) dg_interp_kernel(const DgArgs<T> a, const DgOps<T, U, F, D> op) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = (int)(t & 31);
+  const int64_t w = t >> 5;
+  const int v = a.v0 + (int)(w % a.nv);
+  const int64_t e = (w / a.nv) * 32 + lane;
+  if (e >= a.neles) return;
+  T u[U];
+#pragma unroll
+  for (int i = 0; i < U; ++i) u[i] = a.u[aos32(i, a.ldim_u, e, v, a.V)];
+#pragma unroll
+  for (int f = 0; f < F; ++f) {
+    T s = T(0);
+#pragma unroll
+    for (int i = 0; i < U; ++i) s = fma(op.m0[f][i], u[i], s);
+    a.uf[aos32(f, a.ldim_f, e, v, a.V)] = s;
+  }
+}
+
+// One block per 32 boundary flux points; 8 velocity lanes per point reduce in
+// FP64 and write bcvals[b] = (sum_{c.n>=0} (c-Uw).n f cw, sum_{c.n<0} (c-Uw).n fw cw).
+template <typename T, int D>
+__global__ void __launch_bounds__(256) dg_bcsum_kernel(const DgArgs<T> a, const int* __restrict__ bfpt,
+                                                      const int* __restrict__ bele, int nb, double cw,
+                                                      double* __restrict__ bcvals, int reset) {
+  __shared__ double s0[8][32], s1[8][32];
+  const int bl = threadIdx.x & 31, vg = threadIdx.x >> 5;
+  const int b = blockIdx.x * 32 + bl;
+  double acc0 = 0.0, acc1 = 0.0;
+  if (b < nb && a.bkind[b] == BC_WALL_DIFFUSE) {
+    const int j = bfpt[b], e = bele[b], g = a.bgroup[b];
+    double n[D], uw[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      n[d] = (double)a.nrm[((int64_t)j * D + d) * a.neles + e];
+      uw[d] = (double)a.guw[g * 3 + d];
+    }
+    for (int v = a.v0 + vg; v < a.v0 + a.nv; v += 8) {
+      double fac = ((double)a.cvx[v] - uw[0]) * n[0];
+      if (D > 1) fac += ((double)a.cvy[v] - uw[1]) * n[1];
+      if (D > 2) fac += ((double)a.cvz[v] - uw[2]) * n[2];
+      if (fac >= 0.0)
+        acc0 += fac * (double)a.uf[aos32(j, a.ldim_f, e, v, a.V)] * cw;
+      else
+        acc1 += fac * (double)a.gfw[(int64_t)g * a.V + v] * cw;
+    }
+  }
+  s0[vg][bl] = acc0;
+  s1[vg][bl] = acc1;
+  __syncthreads();
+  if (vg == 0 && b < nb && a.bkind[b] == BC_WALL_DIFFUSE) {
+    double r0 = 0.0, r1 = 0.0;
+    for (int k = 0; k < 8; ++k) {
+      r0 += s0[k][bl];
+      r1 += s1[k][bl];
+    }
+    if (reset) {
+      bcvals[2 * b] = r0;
+      bcvals[2 * b + 1] = r1;
+    } else {
+      bcvals[2 * b] += r0;
+      bcvals[2 * b + 1] += r1;
+    }
+  }
+}
+
+template <typename T, int U, int F, int D>
+__global__ void __launch_bounds__(256) dg_residual_kernel(const DgArgs<T> a, const DgOps<T, U, F, D> op) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = (int)(t & 31);
+  const int64_t w = t >> 5;
+  const int v = a.v0 + (int)(w % a.nv);
+  const int64_t e = (w / a.nv) * 32 + lane;
+  if (e >= a.neles) return;
+  const int64_t E = a.neles;
+
+  T u[U];
+#pragma unroll
+  for (int i = 0; i < U; ++i) u[i] = a.u[aos32(i, a.ldim_u, e, v, a.V)];
+  const T c[3] = {a.cvx[v], a.cvy[v], a.cvz[v]};
+
+  // common normal fluxes at this element's flux points
+  T fh[F];
+#pragma unroll
+  for (int f = 0; f < F; ++f) {
+    T ul = T(0);
+#pragma unroll
+    for (int i = 0; i < U; ++i) ul = fma(op.m0[f][i], u[i], ul);
+    T n[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) n[d] = a.nrm[((int64_t)f * D + d) * E + e];
+    T nc = n[0] * c[0];
+#pragma unroll
+    for (int d = 1; d < D; ++d) nc = fma(n[d], c[d], nc);
+    const int p = a.part[(int64_t)f * E + e];
+    T ur;
+    if (p >= 0) {
+      const int64_t fr = p / E, er = p % E;
+      ur = a.uf[aos32(fr, a.ldim_f, er, v, a.V)];
+    } else {
+      const int b = -p - 1;
+      const int kind = a.bkind[b], g = a.bgroup[b];
+      if (kind == BC_WALL_DIFFUSE || kind == BC_INLET) {
+        T fac = (c[0] - a.guw[g * 3]) * n[0];
+#pragma unroll
+        for (int d = 1; d < D; ++d) fac = fma(c[d] - a.guw[g * 3 + d], n[d], fac);
+        if (fac < T(0)) {
+          const T fw = a.gfw[(int64_t)g * a.V + v];
+          ur = kind == BC_INLET ? fw : fw * (T)(-a.bcvals[2 * b] / a.bcvals[2 * b + 1]);
+        } else {
+          ur = ul;
+        }
+      } else if (kind == BC_VANISH) {
+        ur = nc < T(0) ? T(0) : ul;
+      } else if (kind == BC_WALL_SPECULAR) {
+        const int vr = a.grefl[(int64_t)g * a.V + v];
+        ur = a.uf[aos32(f, a.ldim_f, e, vr, a.V)];
+      } else {
+        ur = ul;  // outlet
+      }
+    }
+    // upwind flux 0.5 (n.c)(ul + ur) + 0.5 |n.c| (ul - ur)  (rusanov.mako:46-50)
+    const T fn = T(0.5) * nc * (ul + ur) + T(0.5) * fabs(nc) * (ul - ur);
+    fh[f] = a.mag[(int64_t)f * E + e] * fn;
+  }
+
+  // transformed flux at the solution points F~_i = sum_k S_ik c_k u
+  T ft[D * U];
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+      T s = T(0);
+#pragma unroll
+      for (int kk = 0; kk < D; ++kk) s = fma(a.smats[(((int64_t)i * U + k) * D + kk) * E + e], c[kk], s);
+      ft[i * U + k] = s * u[k];
+    }
+
+#pragma unroll
+  for (int r = 0; r < U; ++r) {
+    T s = T(0);
+#pragma unroll
+    for (int j = 0; j < D * U; ++j) s = fma(op.m132[r][j], ft[j], s);
+#pragma unroll
+    for (int f = 0; f < F; ++f) s = fma(op.m3[r][f], fh[f], s);
+    const T R = -a.rcpdjac[(int64_t)r * E + e] * s;
+    const int64_t o = aos32(r, a.ldim_u, e, v, a.V);
+    T res = a.gamma * (a.Cq ? R + a.Cq[o] : R);
+    if (a.A) res = fma(a.alpha, a.A[o], res);
+    if (a.B) res = fma(a.beta, a.B[o], res);
+    a.out[o] = res;
+  }
+}
+
+}  // namespace dgfs

@@ -1,0 +1,297 @@
+# -*- coding: utf-8 -*-
+"""DGFS system: the solver-side operator API of frfs on the B200 library.
+
+Keeps the interface of DGFSSystem (frfs/solvers/dgfs/system.py:17-231) that
+the DGFS steppers and the ARS explicit stage call:
+
+  collide(t, uinbank, foutbank)                       system.py:199-218
+  updatebc(t, uinbank, foutbank, batch, varidx)       system.py:180-196
+  rhs(t, uinbank, foutbank, batch, varidx)            system.py:140-177
+
+with the distribution banks addressed by register index
+(``eles_scal_upts_inb_full``, system.py:127-136).  ``collide`` evaluates
+Q(f) at every solution point in one persistent launch instead of a Python
+loop of per-point launches; ``rhs`` and ``updatebc`` act on the velocity
+slice [varidx, varidx + NvBatchSize) of the full banks in place (frfs copies
+that slice through register banks first, system.py:140-196 with
+integrators/base.py:166-214; the values are the same).  ``rk_stage`` fuses a
+residual with the Runge-Kutta combination for the steppers.
+"""
+
+import ctypes as ct
+
+import numpy as np
+
+from frfs_b200 import _lib
+from frfs_b200 import mesh as meshmod
+from frfs_b200.elements import ElementGeometry
+from frfs_b200.initcond import MaxwellianSection, initial_distribution
+from frfs_b200.scattering import DGFSScatteringModel, subclass_where
+from frfs_b200.shapes import QuadShape
+from frfs_b200.velocitymesh import DGFSVelocityMesh
+
+c_int, c_ll, c_double, c_void_p = ct.c_int, ct.c_longlong, ct.c_double, \
+    ct.c_void_p
+c_dp, c_ip = ct.POINTER(ct.c_double), ct.POINTER(ct.c_int)
+
+
+class DgParams(ct.Structure):
+    """dgfs_dg_params (include/dgfs_b200.h)."""
+    _fields_ = [('precision', c_int), ('ndims', c_int), ('nupts', c_int),
+                ('nfpts', c_int), ('nvars', c_int), ('neles', c_int),
+                ('soasz', c_int), ('ldim', c_ll), ('m0', c_dp),
+                ('m132', c_dp), ('m3', c_dp), ('smats', c_dp),
+                ('rcpdjac', c_dp), ('nrm', c_dp), ('mag', c_dp),
+                ('partner', c_ip), ('cv', c_dp), ('cw', c_double),
+                ('nbfpts', c_int), ('bkind', c_ip), ('bgroup', c_ip),
+                ('bfpt', c_ip), ('bele', c_ip), ('ngroups', c_int),
+                ('guw', c_dp), ('gfw', c_dp), ('grefl', c_ip)]
+
+
+_lib.declare('dgfs_dg_create', c_int, [ct.POINTER(DgParams),
+                                       ct.POINTER(c_void_p)])
+_lib.declare('dgfs_dg_destroy', c_int, [c_void_p])
+_lib.declare('dgfs_dg_interp', c_int, [c_void_p, c_void_p, c_int, c_int,
+                                       c_void_p])
+_lib.declare('dgfs_dg_updatebc', c_int, [c_void_p, c_int, c_int, c_int,
+                                         c_void_p])
+_lib.declare('dgfs_dg_rhs', c_int, [c_void_p, c_void_p, c_void_p, c_int,
+                                    c_int, c_double, c_void_p, c_double,
+                                    c_void_p, c_double, c_void_p, c_void_p])
+_lib.declare('dgfs_dg_bcvals', c_int, [c_void_p, c_dp, c_int])
+_lib.declare('dgfs_dg_fpts', c_int, [c_void_p, ct.POINTER(c_void_p),
+                                     ct.POINTER(c_ll)])
+
+BC_KINDS = {'dgfs-wall-diffuse': 0, 'dgfs-inlet': 1, 'dgfs-outlet': 2,
+            'dgfs-vanish': 3, 'dgfs-wall-specular': 4}
+
+
+def _ptr(a, kind=c_dp):
+    return a.ctypes.data_as(kind)
+
+
+def specular_map(cv, n):
+    """Reflected-velocity indices for a flat wall of unit normal n
+    (frfs/solvers/dgfs/inters.py:258-275)."""
+    n3 = np.zeros(3)
+    n3[:len(n)] = n
+    dot = n3 @ cv
+    cr = cv - 2*dot[None, :]*n3[:, None]
+    idx = np.empty(cv.shape[1], dtype=np.int32)
+    for j in range(cv.shape[1]):
+        idx[j] = np.argmin(np.sum((cr[:, j:j + 1] - cv)**2, axis=0))
+    if not np.all(np.sort(idx) == np.arange(cv.shape[1])):
+        raise ValueError('Non-unique specular map')
+    return idx
+
+
+class DGFSSystem:
+    name = 'dgfs'
+
+    def __init__(self, backend, cfg, mesh=None, nreg=3, initsoln=None,
+                 sphdesign_paths=None):
+        self.backend = backend
+        self.cfg = cfg
+        self.vm = vm = DGFSVelocityMesh(backend, cfg, sphdesign_paths)
+        self.mesh = mesh if mesh is not None else meshmod.from_config(cfg)
+        order = cfg.getint('solver', 'order')
+        self.shape = sh = QuadShape(order)
+        spt = self.mesh['spt_quad_p0']
+        self.geo = geo = ElementGeometry(sh, spt)
+        self.ndims = 2
+        self.neles, self.nupts, self.nfpts = geo.neles, sh.nupts, sh.nfpts
+        self.ele_types = ['quad']
+
+        smn = cfg.get('scattering-model', 'type')
+        self.sm = subclass_where(DGFSScatteringModel,
+                                 scattering_model=smn)(backend, cfg, vm)
+
+        V = vm.vsize()
+        shape = (self.nupts, V, self.neles)
+        if initsoln is None:
+            f0 = initial_distribution(cfg, vm, self.nupts, self.neles)
+        else:
+            f0 = np.asarray(initsoln).reshape(shape)
+        mats = [backend.matrix(shape, f0 if i == 0 else None)
+                for i in range(nreg)]
+        self.bank = backend.matrix_bank(mats)
+        self.eles_scal_upts_inb_full = [self.bank]
+
+        # time step for unit CFL (system.py:50-56)
+        djac = geo.djac_at(sh.upts)
+        self.unit_cfl_dt = float(np.sqrt(djac.min())/vm.L()/self.ndims)
+
+        self._build_dg()
+
+    # -- DG handle ----------------------------------------------------------
+    def _build_dg(self):
+        sh, geo, vm, cfg = self.shape, self.geo, self.vm, self.cfg
+        E, F, V = self.neles, self.nfpts, vm.vsize()
+        part = np.full((F, E), np.iinfo(np.int32).min, dtype=np.int64)
+        lhs, rhs = self.mesh['con_p0']
+        srtd = geo.srtd_face_fpts
+        for l, r in zip(lhs, rhs):
+            el, fl, er, fr = int(l['eidx']), int(l['fidx']), int(r['eidx']), \
+                int(r['fidx'])
+            for jl, jr in zip(srtd[fl][el], srtd[fr][er]):
+                part[jl, el] = jr*E + er
+                part[jr, er] = jl*E + el
+
+        bnames = sorted(k[5:-3] for k in self.mesh
+                        if k.startswith('bcon_') and k.endswith('_p0'))
+        bpts, guw, gfw, grefl, kinds = [], [], [], [], []
+        self.bc_sections = {}
+        for g, name in enumerate(bnames):
+            sect = f'soln-bcs-{name}'
+            btype = cfg.get(sect, 'type')
+            if btype not in BC_KINDS:
+                raise ValueError(f'unsupported boundary type {btype!r}')
+            kinds.append(BC_KINDS[btype])
+            if btype in ('dgfs-wall-diffuse', 'dgfs-inlet'):
+                ms = MaxwellianSection(cfg, vm, sect)
+                guw.append(ms.u)
+                gfw.append(ms.values)
+            else:
+                guw.append(np.zeros(3))
+                gfw.append(np.zeros(V))
+            recs = self.mesh[f'bcon_{name}_p0']
+            for rec in recs:
+                e, f = int(rec['eidx']), int(rec['fidx'])
+                for j in srtd[f][e]:
+                    bpts.append((g, int(j), e))
+            if btype == 'dgfs-wall-specular':
+                e0, f0 = int(recs[0]['eidx']), int(recs[0]['fidx'])
+                n = geo.norm_pnorm_fpts[srtd[f0][e0][0], e0]
+                for rec in recs:
+                    e, f = int(rec['eidx']), int(rec['fidx'])
+                    if not np.allclose(geo.norm_pnorm_fpts[srtd[f][e], e], n):
+                        raise ValueError('specular walls must be flat')
+                grefl.append(specular_map(vm.cv(), n))
+            else:
+                grefl.append(np.arange(V, dtype=np.int32))
+            self.bc_sections[name] = (g, btype)
+        bpts.sort(key=lambda x: (x[0], x[1], x[2]))
+        nb = len(bpts)
+        bkind = np.array([kinds[g] for g, _, _ in bpts], dtype=np.int32)
+        bgroup = np.array([g for g, _, _ in bpts], dtype=np.int32)
+        bfpt = np.array([j for _, j, _ in bpts], dtype=np.int32)
+        bele = np.array([e for _, _, e in bpts], dtype=np.int32)
+        for b, (g, j, e) in enumerate(bpts):
+            part[j, e] = -(b + 1)
+        if np.any(part == np.iinfo(np.int32).min):
+            raise ValueError('mesh has flux points on no interface or '
+                             'boundary')
+        self.bpts = bpts
+
+        d = lambda x: np.ascontiguousarray(x, dtype=np.float64)
+        self._keep = keep = dict(
+            m0=d(sh.opmat('M0')), m132=d(sh.opmat('M1 - M3*M2')),
+            m3=d(sh.opmat('M3')), smats=d(geo.smat_at(sh.upts)),
+            rcpdjac=d(geo.rcpdjac_at(sh.upts)),
+            nrm=d(geo.norm_pnorm_fpts.transpose(0, 2, 1)),
+            mag=d(geo.mag_pnorm_fpts),
+            part=np.ascontiguousarray(part, dtype=np.int32),
+            cv=d(vm.cv()), bkind=bkind, bgroup=bgroup, bfpt=bfpt, bele=bele,
+            guw=d(np.array(guw).reshape(-1, 3)),
+            gfw=d(np.array(gfw).reshape(-1, V)),
+            grefl=np.ascontiguousarray(np.array(grefl).reshape(-1, V),
+                                       dtype=np.int32))
+        nrow, ldim, _ = self.bank[0].traits
+        p = DgParams(
+            precision=self.backend.precision, ndims=2, nupts=self.nupts,
+            nfpts=F, nvars=V, neles=E, soasz=self.backend.soasz, ldim=ldim,
+            m0=_ptr(keep['m0']), m132=_ptr(keep['m132']), m3=_ptr(keep['m3']),
+            smats=_ptr(keep['smats']), rcpdjac=_ptr(keep['rcpdjac']),
+            nrm=_ptr(keep['nrm']), mag=_ptr(keep['mag']),
+            partner=_ptr(keep['part'], c_ip), cv=_ptr(keep['cv']),
+            cw=vm.cw(), nbfpts=nb, bkind=_ptr(bkind, c_ip),
+            bgroup=_ptr(bgroup, c_ip), bfpt=_ptr(bfpt, c_ip),
+            bele=_ptr(bele, c_ip), ngroups=len(bnames),
+            guw=_ptr(keep['guw']), gfw=_ptr(keep['gfw']),
+            grefl=_ptr(keep['grefl'], c_ip))
+        h = c_void_p()
+        lib = _lib.load()
+        _lib.check(lib.dgfs_dg_create(ct.byref(p), ct.byref(h)),
+                   'dgfs_dg_create')
+        self._dg, self._lib = h, lib
+
+    def __del__(self):
+        h = getattr(self, '_dg', None)
+        if h:
+            self._lib.dgfs_dg_destroy(h)
+            self._dg = None
+
+    # -- frfs operator API ---------------------------------------------------
+    def _range(self, batch, varidx):
+        nvbs = self.vm.NvBatchSize()
+        return int(varidx), nvbs
+
+    def collide(self, t, uinbank, foutbank):
+        """Q(f) at every solution point (system.py:199-218)."""
+        self.sm.fs_all(self.bank[uinbank], self.bank[foutbank])
+
+    def updatebc(self, t, uinbank, foutbank, batch, varidx):
+        """Face values of the slice and the diffuse-wall sums; the sums are
+        reset on the slice that starts at velocity 0 (system.py:180-196)."""
+        v0, nv = self._range(batch, varidx)
+        u = self.bank[uinbank]
+        s = self.backend.stream
+        _lib.check(self._lib.dgfs_dg_interp(self._dg, u._as_parameter_, v0,
+                                            nv, s), 'dgfs_dg_interp')
+        _lib.check(self._lib.dgfs_dg_updatebc(self._dg, v0, nv,
+                                              1 if v0 == 0 else 0, s),
+                   'dgfs_dg_updatebc')
+
+    def rhs(self, t, uinbank, foutbank, batch, varidx):
+        """foutbank[slice] = -div F(uinbank[slice]) (system.py:140-177)."""
+        v0, nv = self._range(batch, varidx)
+        self.rk_stage(uinbank, foutbank, 0.0, None, 0.0, None, 1.0, None,
+                      v0=v0, nv=nv)
+
+    def rk_stage(self, uin, out, alpha, A, beta, B, gamma, C, v0=0, nv=None,
+                 interp=True):
+        """bank[out] = alpha bank[A] + beta bank[B] + gamma (L(bank[uin]) +
+        bank[C]) on velocities [v0, v0 + nv) (bank indices or None)."""
+        nv = self.vm.vsize() - v0 if nv is None else nv
+        u = self.bank[uin]
+        s = self.backend.stream
+        if interp:
+            _lib.check(self._lib.dgfs_dg_interp(self._dg, u._as_parameter_,
+                                                v0, nv, s), 'dgfs_dg_interp')
+        ptr = lambda i: None if i is None else self.bank[i]._as_parameter_
+        _lib.check(self._lib.dgfs_dg_rhs(
+            self._dg, u._as_parameter_, self.bank[out]._as_parameter_, v0,
+            nv, alpha, ptr(A), beta, ptr(B), gamma, ptr(C), s),
+            'dgfs_dg_rhs')
+
+    def bc_values(self):
+        nb = len(self.bpts)
+        buf = np.zeros(max(2*nb, 2))
+        _lib.check(self._lib.dgfs_dg_bcvals(self._dg, _ptr(buf), buf.size),
+                   'dgfs_dg_bcvals')
+        return buf[:2*nb].reshape(nb, 2)
+
+    def face_values(self):
+        """Host copy of the face-value scratch (nfpts, V, neles)."""
+        import torch
+        p, ld = c_void_p(), c_ll()
+        _lib.check(self._lib.dgfs_dg_fpts(self._dg, ct.byref(p),
+                                          ct.byref(ld)), 'dgfs_dg_fpts')
+        n = self.nfpts*ld.value
+        view = _DeviceArray(p.value, n, '<f8' if self.backend.precision == 64
+                            else '<f4')
+        torch.cuda.synchronize(self.backend.device)
+        buf = torch.as_tensor(view, device=self.backend.device)
+        V, E = self.vm.vsize(), self.neles
+        nblk = (E + 31)//32
+        a = buf.view(self.nfpts, ld.value)[:, :nblk*32*V].cpu().numpy()
+        a = a.reshape(self.nfpts, nblk, V, 32).transpose(0, 2, 1, 3)
+        return a.reshape(self.nfpts, V, nblk*32)[:, :, :E]
+
+
+class _DeviceArray:
+    """A device allocation described through __cuda_array_interface__."""
+
+    def __init__(self, ptr, n, typestr):
+        self.__cuda_array_interface__ = {'shape': (n,), 'typestr': typestr,
+                                         'data': (ptr, False), 'version': 3}

@@ -121,6 +121,84 @@ DGFS_API int dgfs_vhs_variant_info(const dgfs_vhs* h, int idx, int* cluster,
 DGFS_API int dgfs_vhs_select(dgfs_vhs* h, int idx);
 
 /* ------------------------------------------------------------------------
+ * FR-DG advection residual over all velocities
+ *
+ * Replaces: the element/interface kernels behind DGFSSystem.rhs and
+ * DGFSSystem.updatebc (frfs/solvers/dgfs/system.py:140-196; elements.py:49-118;
+ * inters.py:17-229; kernels/{tflux,flux,intcflux,bccflux,bccupdate,
+ * negdivconf}.mako, rsolvers/rusanov.mako, bcs/dgfs-*.mako) and the
+ * integrator's axnpby combination (frfs/backends/cuda/blasext.py:14-43).
+ * The flux-point values live in a library-owned scratch bank.
+ * ---------------------------------------------------------------------- */
+typedef struct dgfs_dg dgfs_dg;
+
+#define DGFS_BC_WALL_DIFFUSE 0  /* dgfs-wall-diffuse  (inters.py:175-229)  */
+#define DGFS_BC_INLET 1         /* dgfs-inlet         (inters.py:312-350)  */
+#define DGFS_BC_OUTLET 2        /* dgfs-outlet        (inters.py:386-413)  */
+#define DGFS_BC_VANISH 3        /* dgfs-vanish        (inters.py:416-443)  */
+#define DGFS_BC_WALL_SPECULAR 4 /* dgfs-wall-specular (inters.py:232-309)  */
+
+typedef struct dgfs_dg_params {
+  int precision;          /* 64 or 32                                       */
+  int ndims;              /* 2 (quadrilaterals)                             */
+  int nupts, nfpts;       /* solution / flux points per element             */
+  int nvars;              /* discrete velocities V = Nv^3                   */
+  int neles;              /* elements                                       */
+  int soasz;              /* AoSoA width of the banks (32)                  */
+  long long ldim;         /* leading dimension of the solution banks        */
+  const double* m0;       /* [nfpts][nupts]            operator M0          */
+  const double* m132;     /* [nupts][ndims*nupts]      operator M1 - M3*M2  */
+  const double* m3;       /* [nupts][nfpts]            operator M3          */
+  const double* smats;    /* [ndims][nupts][ndims][neles] metric terms      */
+  const double* rcpdjac;  /* [nupts][neles]            1/|J|                */
+  const double* nrm;      /* [nfpts][ndims][neles]     unit outward normals */
+  const double* mag;      /* [nfpts][neles]            |S^T n|              */
+  const int* partner;     /* [nfpts][neles]: fpt'*neles + ele' of the other
+                             side, or -(b+1) for boundary flux point b      */
+  const double* cv;       /* [3][nvars] velocity grid                       */
+  double cw;              /* velocity cell weight                           */
+  int nbfpts;             /* boundary flux points                           */
+  const int* bkind;       /* [nbfpts] DGFS_BC_*                             */
+  const int* bgroup;      /* [nbfpts] boundary region index                 */
+  const int* bfpt;        /* [nbfpts] flux point within its element         */
+  const int* bele;        /* [nbfpts] element                               */
+  int ngroups;            /* boundary regions                               */
+  const double* guw;      /* [ngroups][3] wall / inlet velocity             */
+  const double* gfw;      /* [ngroups][nvars] wall / inlet Maxwellian       */
+  const int* grefl;       /* [ngroups][nvars] specular reflection map, or NULL */
+} dgfs_dg_params;
+
+DGFS_API int dgfs_dg_create(const dgfs_dg_params* params, dgfs_dg** out);
+DGFS_API int dgfs_dg_destroy(dgfs_dg* h);
+
+/* Face values uf = M0 u for velocities [v0, v0+nv) into the scratch bank
+ * ('disu', frfs/solvers/dgfs/elements.py:55-59). */
+DGFS_API int dgfs_dg_interp(dgfs_dg* h, const void* u, int v0, int nv,
+                            void* stream);
+
+/* Diffuse-wall sums over velocities [v0, v0+nv) of the current face values,
+ * accumulated in FP64; reset != 0 starts from zero (the vidx == 0 reset of
+ * bcs/dgfs-wall-diffuse-update.mako:21-24). */
+DGFS_API int dgfs_dg_updatebc(dgfs_dg* h, int v0, int nv, int reset,
+                              void* stream);
+
+/* out = alpha*A + beta*B + gamma*(L(u) + C) on velocities [v0, v0+nv),
+ * L(u) = -div of the upwind FR-DG flux (DGFSSystem.rhs,
+ * frfs/solvers/dgfs/system.py:140-177).  A, B, C may be NULL (term absent)
+ * and may alias out; out must differ from u.  Needs dgfs_dg_interp of the
+ * same u first (and dgfs_dg_updatebc when diffuse walls are present). */
+DGFS_API int dgfs_dg_rhs(dgfs_dg* h, const void* u, void* out, int v0, int nv,
+                         double alpha, const void* A, double beta,
+                         const void* B, double gamma, const void* C,
+                         void* stream);
+
+/* Copy the 2*nbfpts diffuse-wall sums to host memory (synchronous). */
+DGFS_API int dgfs_dg_bcvals(const dgfs_dg* h, double* host, int n);
+
+/* Device pointer and leading dimension of the face-value scratch bank. */
+DGFS_API int dgfs_dg_fpts(const dgfs_dg* h, void** ptr, long long* ldim);
+
+/* ------------------------------------------------------------------------
  * Measurement helper (no counterpart in the reference)
  * ---------------------------------------------------------------------- */
 

@@ -181,6 +181,61 @@ flux-pts = gauss-legendre
                             **arrs)
 
 
+def dg_fixture(Inifile, out):
+    """Element geometry and interface pairing from frfs's own element code
+    (frfs/solvers/base/elements.py:137-354, dgfs/elements.py:198-212) on a
+    distorted 4x3 quadrilateral mesh, x-periodic, p = 2."""
+    elmod = _load('frfs.solvers.base.elements')
+    import frfs.shapes as shapes
+    from frfs_b200 import mesh as mgen
+
+    class _VM:
+        def NvBatchSize(self):
+            return 8
+
+    for order, jitter in ((2, 0.2), (1, 0.15), (3, 0.1)):
+        m = mgen.quad_box(4, 3, 0.0, 1.0, 0.0, 0.75, periodic_x=True,
+                          jitter=jitter, seed=order)
+        cfg = Inifile(f"""
+[solver]
+order = {order}
+[solver-elements-quad]
+soln-pts = gauss-legendre
+[solver-interfaces-line]
+flux-pts = gauss-legendre
+""")
+
+        class Eles(elmod.BaseElements):
+            privarmap = {2: ['f_%d' % i for i in range(8)]}
+            convarmap = privarmap
+            _scratch_bufs = set()
+
+            def set_backend(self, *a):
+                pass
+
+            @staticmethod
+            def pri_to_con(p, c):
+                return p
+
+        ele = Eles(shapes.QuadShape, m['spt_quad_p0'], cfg)
+        srtd = np.array([[list(x) for x in face]
+                         for face in ele._srtd_face_fpts])
+        arrs = dict(
+            spt=m['spt_quad_p0'], con=m['con_p0'],
+            bcon_bottom=m['bcon_bottom_p0'], bcon_top=m['bcon_top_p0'],
+            smats_upts=ele.smat_at_np('upts'),
+            rcpdjac_upts=ele.rcpdjac_at_np('upts'),
+            djac_upts=ele.djac_at_np('upts'),
+            ploc_upts=ele.ploc_at_np('upts'),
+            plocfpts=ele.plocfpts,
+            norm_pnorm_fpts=ele._norm_pnorm_fpts,
+            mag_pnorm_fpts=ele._mag_pnorm_fpts,
+            srtd_face_fpts=srtd,
+        )
+        np.savez_compressed(os.path.join(out, f'ref_dg_quad_p{order}.npz'),
+                            **arrs)
+
+
 def main():
     _install_shims()
     vmmod = _load('frfs.solvers.dgfs.velocitymesh')
@@ -202,6 +257,10 @@ def main():
         velocity_fixture(name, ini, icmod, vmmod, scmod, Inifile, HERE,
                          with_ics=(name != 'small-n8'))
     shapes_fixture(Inifile, HERE)
+    import contextlib
+    import io
+    with contextlib.redirect_stdout(io.StringIO()):
+        dg_fixture(Inifile, HERE)
     print('golden fixtures written to', HERE)
 
 

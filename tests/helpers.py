@@ -72,3 +72,38 @@ def rel_err(a, b):
     """max |a - b| / max |b| (normwise relative error)."""
     return float(np.max(np.abs(np.asarray(a) - np.asarray(b))) /
                  np.max(np.abs(np.asarray(b))))
+
+
+def dg_setup(cfg, mesh):
+    """Product-side operators/geometry (pinned to reference fixtures by
+    test_geometry.py) and an oracle DG instance on the same mesh."""
+    from frfs_b200.elements import ElementGeometry
+    from frfs_b200.initcond import MaxwellianSection
+    from frfs_b200.shapes import QuadShape
+    from frfs_b200.velocitymesh import DGFSVelocityMesh
+    from oracle.dg import DGOracle
+
+    sh = QuadShape(cfg.getint('solver', 'order'))
+    geo = ElementGeometry(sh, mesh['spt_quad_p0'])
+    vm = DGFSVelocityMesh(None, cfg)
+    ops = {'M0': sh.opmat('M0'), 'M132': sh.opmat('M1 - M3*M2'),
+           'M3': sh.opmat('M3')}
+    g = {'smats': geo.smat_at(sh.upts), 'rcpdjac': geo.rcpdjac_at(sh.upts),
+         'nrm': geo.norm_pnorm_fpts, 'mag': geo.mag_pnorm_fpts,
+         'srtd': geo.srtd_face_fpts}
+    lhs, rhs = mesh['con_p0']
+    con = ([(int(r['eidx']), int(r['fidx'])) for r in lhs],
+           [(int(r['eidx']), int(r['fidx'])) for r in rhs])
+    bcons, bcs = {}, {}
+    for k in mesh:
+        if k.startswith('bcon_'):
+            name = k[5:-3]
+            bcons[name] = [(int(r['eidx']), int(r['fidx'])) for r in mesh[k]]
+            sect = f'soln-bcs-{name}'
+            btype = cfg.get(sect, 'type')
+            if btype in ('dgfs-wall-diffuse', 'dgfs-inlet'):
+                ms = MaxwellianSection(cfg, vm, sect)
+                bcs[name] = {'type': btype, 'fw': ms.values, 'uw': ms.u}
+            else:
+                bcs[name] = {'type': btype, 'fw': None, 'uw': np.zeros(3)}
+    return DGOracle(ops, g, con, bcons, vm.cv(), vm.cw(), bcs), sh, geo, vm

@@ -1,0 +1,147 @@
+# -*- coding: utf-8 -*-
+"""Parity of the B200 FR-DG kernels with the FP64 oracle (GPU).
+
+Tolerances (normwise relative): FP64 1e-10, FP32 2e-5.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from helpers import config, dg_setup, oracle_for, random_states, rel_err
+from frfs_b200 import mesh as mgen
+from frfs_b200.backend import B200Backend
+from frfs_b200.system import DGFSSystem
+from oracle import dg as odg
+from oracle import vhs as ovhs
+
+pytestmark = pytest.mark.gpu
+
+TOL = {'double': 1e-10, 'single': 2e-5}
+
+
+def _cfg(precision, bottom='dgfs-wall-diffuse', top='dgfs-wall-diffuse',
+         order=2, batch=None):
+    cfg = config('relax0d-n16', precision)
+    cfg.set('solver', 'order', order)
+    if batch:
+        cfg.set('constants', 'NvBatchSize', batch)
+    u0 = np.sqrt(2*8.3144598/39.96e-3*273.0)
+    for name, kind, uy in (('bottom', bottom, -0.3), ('top', top, 0.4)):
+        sect = f'soln-bcs-{name}'
+        cfg.set(sect, 'type', kind)
+        cfg.set(sect, 'rho', 1.5e-3)
+        cfg.set(sect, 'T', 273.0*(1.1 if name == 'top' else 0.9))
+        cfg.set(sect, 'ux', 0.1*u0)
+        cfg.set(sect, 'uy', 0.0 if kind == 'dgfs-inlet' else uy*u0)
+        cfg.set(sect, 'uz', 0.0)
+    return cfg
+
+
+def _mesh(order=2):
+    return mgen.quad_box(4, 3, 0.0, 1.0, 0.0, 0.75, periodic_x=True,
+                         jitter=0.2, seed=order)
+
+
+def _system(cfg, mesh, u):
+    be = B200Backend(cfg, device='cuda:0')
+    sys_ = DGFSSystem(be, cfg, mesh=mesh, initsoln=u)
+    return be, sys_
+
+
+def _states(vm, nupts, neles, seed=0):
+    f = random_states(vm.cv(), nupts*neles, seed=seed, noise=0.02)
+    return f.reshape(nupts, neles, -1).transpose(0, 2, 1).copy()
+
+
+@pytest.mark.parametrize('precision', ['double', 'single'])
+@pytest.mark.parametrize('order', [1, 2, 3])
+def test_residual_and_wall_sums(precision, order):
+    cfg, m = _cfg(precision, order=order), _mesh(order)
+    dg, sh, geo, vm = dg_setup(cfg, m)
+    u = _states(vm, sh.nupts, geo.neles, seed=order)
+    be, s = _system(cfg, m, u)
+    u_used = s.bank[0].get().astype(np.float64)
+    s.updatebc(0.0, 0, 1, 0, 0)
+    s.rhs(0.0, 0, 1, 0, 0)
+    torch.cuda.synchronize()
+    # face values and diffuse-wall sums
+    uf = dg.disu(u_used)
+    assert rel_err(s.face_values(), uf) < TOL[precision]
+    dg.update_bc(uf)
+    bcg = s.bc_values()
+    for b, (g, j, e) in enumerate(s.bpts):
+        name = sorted(dg.bpts)[g]
+        k = dg.bpts[name].index((j, e))
+        ref = dg.bcvals[name][:, k]
+        assert abs(bcg[b, 0] - ref[0]) <= TOL[precision]*abs(ref[0]) + 1e-14
+        assert abs(bcg[b, 1] - ref[1]) <= TOL[precision]*abs(ref[1]) + 1e-14
+    R = dg.rhs(u_used, uf)
+    err = rel_err(s.bank[1].get(), R)
+    assert err < TOL[precision], err
+
+
+@pytest.mark.parametrize('kinds', [('dgfs-inlet', 'dgfs-outlet'),
+                                   ('dgfs-vanish', 'dgfs-wall-specular'),
+                                   ('dgfs-wall-specular', 'dgfs-wall-diffuse')])
+def test_boundary_kinds(kinds):
+    cfg, m = _cfg('double', *kinds), _mesh()
+    dg, sh, geo, vm = dg_setup(cfg, m)
+    u = _states(vm, sh.nupts, geo.neles, seed=7)
+    be, s = _system(cfg, m, u)
+    s.updatebc(0.0, 0, 1, 0, 0)
+    s.rhs(0.0, 0, 1, 0, 0)
+    torch.cuda.synchronize()
+    uf = dg.disu(u)
+    dg.update_bc(uf)
+    assert rel_err(s.bank[1].get(), dg.rhs(u, uf)) < TOL['double']
+
+
+def test_velocity_batches_match_full_range():
+    cfg, m = _cfg('double', batch=1024), _mesh()
+    dg, sh, geo, vm = dg_setup(cfg, m)
+    u = _states(vm, sh.nupts, geo.neles, seed=3)
+    be, s = _system(cfg, m, u)
+    for b in range(vm.NvBatches()):
+        s.updatebc(0.0, 0, 1, b, b*vm.NvBatchSize())
+    for b in range(vm.NvBatches()):
+        s.rhs(0.0, 0, 1, b, b*vm.NvBatchSize())
+    torch.cuda.synchronize()
+    uf = dg.disu(u)
+    dg.update_bc(uf)
+    assert rel_err(s.bank[1].get(), dg.rhs(u, uf)) < TOL['double']
+
+
+@pytest.mark.parametrize('precision', ['double', 'single'])
+@pytest.mark.parametrize('graphs', [0, 1])
+def test_ssp_rk2_steps_match_oracle(precision, graphs):
+    """Two SSP-RK2 steps (collision + advection) against the oracle."""
+    from frfs_b200.steppers import StdTVDRK2DGFSStepper
+    cfg, m = _cfg(precision), mgen.quad_box(2, 2, 0.0, 0.5, 0.0, 0.5,
+                                            periodic_x=True, jitter=0.1)
+    cfg.set('backend-b200', 'cuda-graphs', graphs)
+    dg, sh, geo, vm = dg_setup(cfg, m)
+    ovm, pre, prefac = oracle_for(cfg)
+    u = _states(vm, sh.nupts, geo.neles, seed=5)
+    be, s = _system(cfg, m, u)
+    st = StdTVDRK2DGFSStepper(s, cfg)
+    dt = 1e-3
+    st.dt = dt
+    st.advance(2)
+    torch.cuda.synchronize()
+
+    def Q(x):
+        out = np.empty_like(x)
+        for i in range(x.shape[0]):
+            for e in range(x.shape[2]):
+                out[i, :, e] = ovhs.vhs_Q(x[i, :, e], ovm, pre, prefac)
+        return out
+
+    uo = s.bank[1].get()*0 + u  # FP32 banks start from the rounded input
+    uo = s.bank[0].get().astype(np.float64) if False else uo
+    u0 = u.astype(np.float32).astype(np.float64) if precision == 'single' \
+        else u
+    for _ in range(2):
+        u0 = odg.ssp_rk2_step(dg, Q, u0, dt)
+    err = rel_err(s.bank[st._idxcurr].get(), u0)
+    assert err < (1e-10 if precision == 'double' else 1e-5), err
