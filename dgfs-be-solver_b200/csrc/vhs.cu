@@ -12,7 +12,7 @@
 
 #include "../../include/dgfs_b200.h"
 #include "dgfs_internal.h"
-#include "vhs_kernel.cuh"
+#include "vhs_push.cuh"
 
 namespace dgfs {
 
@@ -46,7 +46,7 @@ static int init_twiddles(int dev) {
 // Kernel variants
 // ---------------------------------------------------------------------------
 struct VhsVariant {
-  int prec, N, C, db, minb, threads;
+  int prec, N, C, db, minb, threads, push;
   size_t smem;
   const void* fn;
   cudaError_t (*launch32)(const VhsArgs<float>&, int, cudaStream_t);
@@ -87,11 +87,53 @@ template <typename T, int N, int C, bool DB, int MINB> static VhsVariant make_va
   return v;
 }
 
+template <typename T, int N, int C, int MINB>
+static cudaError_t launch_push(const VhsArgs<T>& a, int nclusters, cudaStream_t s) {
+  using P = PushGeom<N, C>;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nclusters * C, 1, 1);
+  cfg.blockDim = dim3(P::NT, 1, 1);
+  cfg.dynamicSmemBytes = P::SMEM_CX * sizeof(cx<T>);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, vhs_push_kernel<T, N, C, MINB>, a);
+}
+
+template <typename T, int N, int C, int MINB> static VhsVariant make_push() {
+  using P = PushGeom<N, C>;
+  VhsVariant v{};
+  v.prec = sizeof(T) == 8 ? 64 : 32;
+  v.N = N;
+  v.C = C;
+  v.db = 1;
+  v.push = 1;
+  v.minb = MINB;
+  v.threads = P::NT;
+  v.smem = P::SMEM_CX * sizeof(cx<T>);
+  v.fn = (const void*)vhs_push_kernel<T, N, C, MINB>;
+  if constexpr (sizeof(T) == 8) v.launch64 = launch_push<double, N, C, MINB>;
+  else v.launch32 = launch_push<float, N, C, MINB>;
+  return v;
+}
+
 // Compiled launch shapes: (precision, N, cluster size, double-buffered
 // exchange, minimum CTAs per SM for the register budget).  The first entry
 // of each (precision, N) family is the default; the autotuner times the rest.
 static const std::vector<VhsVariant>& variants() {
   static const std::vector<VhsVariant> v = {
+      make_push<double, 8, 1, 4>(),             make_push<double, 16, 4, 2>(),
+      make_push<double, 16, 2, 1>(),            make_push<double, 24, 8, 1>(),
+      make_push<double, 24, 12, 1>(),           make_push<double, 32, 16, 1>(),
+      make_push<float, 8, 1, 4>(),              make_push<float, 16, 2, 2>(),
+      make_push<float, 16, 4, 4>(),             make_push<float, 24, 8, 2>(),
+      make_push<float, 24, 4, 1>(),             make_push<float, 24, 12, 3>(),
+      make_push<float, 32, 16, 2>(),            make_push<float, 32, 8, 1>(),
       make_variant<double, 8, 1, true, 4>(),    make_variant<double, 8, 2, true, 8>(),
       make_variant<double, 16, 4, true, 2>(),   make_variant<double, 16, 2, true, 1>(),
       make_variant<double, 16, 4, false, 3>(),
@@ -135,6 +177,7 @@ struct dgfs_vhs {
   double* cvec;  // [3][V]
   void* fc;      // scratch: gain spectrum, one N^3 complex slice per cluster
   size_t fc_bytes;
+  int* err;      // device flag: a bounded wait in the kernel gave up
 };
 
 // Occupancy of variant v (clusters that can be resident at once), or an
@@ -304,6 +347,7 @@ static void free_handle(dgfs_vhs* h) {
   cudaFree(h->ginv);
   cudaFree(h->cvec);
   cudaFree(h->fc);
+  cudaFree(h->err);
   delete h;
 }
 
@@ -341,6 +385,9 @@ extern "C" int dgfs_vhs_create(const dgfs_vhs_params* p, dgfs_vhs** out) {
   }
   h->fam = family(h->prec, h->N);
   int rc = init_twiddles(h->device);
+  if (!rc && (cudaMalloc((void**)&h->err, sizeof(int)) != cudaSuccess ||
+              cudaMemset(h->err, 0, sizeof(int)) != cudaSuccess))
+    rc = set_error(DGFS_ERR_NOMEM, "error flag allocation failed");
   if (!rc) rc = select_variant(h, p->cluster);
   if (!rc) rc = h->prec == 64 ? build_tables<double>(h, p) : build_tables<float>(h, p);
   if (rc) {
@@ -371,10 +418,32 @@ extern "C" int dgfs_vhs_set_cluster(dgfs_vhs* h, int cluster) {
   return DGFS_OK;
 }
 
+extern "C" int dgfs_vhs_status(dgfs_vhs* h, void* stream, int* flag) {
+  clear_error();
+  if (!h || !flag) return set_error(DGFS_ERR_INVALID, "null argument");
+  cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+  if (e != cudaSuccess) return set_error(DGFS_ERR_CUDA, "stream: %s", cudaGetErrorString(e));
+  int v = 0;
+  if (cudaMemcpy(&v, h->err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemset(h->err, 0, sizeof(int)) != cudaSuccess)
+    return set_error(DGFS_ERR_CUDA, "error flag: %s", cudaGetErrorString(cudaGetLastError()));
+  *flag = v;
+  if (v) return set_error(DGFS_ERR_CUDA, "a VHS launch gave up waiting for cluster data (flag %d)", v);
+  return DGFS_OK;
+}
+
 extern "C" int dgfs_vhs_num_variants(const dgfs_vhs* h, int* count) {
   clear_error();
   if (!h || !count) return set_error(DGFS_ERR_INVALID, "null argument");
   *count = (int)h->fam.size();
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_vhs_variant_kind(const dgfs_vhs* h, int idx, int* push) {
+  clear_error();
+  if (!h || !push) return set_error(DGFS_ERR_INVALID, "null argument");
+  if (idx < 0 || idx >= (int)h->fam.size()) return set_error(DGFS_ERR_INVALID, "variant %d out of range", idx);
+  *push = h->fam[idx]->push;
   return DGFS_OK;
 }
 
@@ -459,6 +528,7 @@ static int vhs_launch(dgfs_vhs* h, const void* f, void* Q, int nupts, int neles,
     a.w1 = (const double*)h->w1;
     a.b2 = (const double*)h->b2;
     a.fc = (double2*)h->fc;
+    a.err = h->err;
     a.prefac = h->prefac;
     a.project = h->project;
     a.ginv = h->ginv;
@@ -480,6 +550,7 @@ static int vhs_launch(dgfs_vhs* h, const void* f, void* Q, int nupts, int neles,
     a.w1 = (const float*)h->w1;
     a.b2 = (const float*)h->b2;
     a.fc = (float2*)h->fc;
+    a.err = h->err;
     a.prefac = (float)h->prefac;
     a.project = h->project;
     a.ginv = h->ginv;

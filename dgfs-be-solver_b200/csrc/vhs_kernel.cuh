@@ -56,6 +56,7 @@ template <typename T> struct VhsArgs {
   const T* w1;          // [P][V]  (2 qw_p sw / V) b1_p(l)
   const T* b2;          // [V]
   cx<T>* fc;            // scratch [gridDim.x][N][NJ]: gain spectrum per CTA
+  int* err;             // set to 1 when a bounded wait gives up
   T prefac;
   // optional FP64 conservation projection (mass, momentum, energy)
   int project;

@@ -167,10 +167,23 @@ class DGFSVHSGLLScatteringModel(DGFSScatteringModel):
             _lib.check(self._lib.dgfs_vhs_variant_info(
                 self._h, i, *[ct.byref(v) for v in vals]),
                 'dgfs_vhs_variant_info')
-            out.append(dict(zip(('cluster', 'double_buffered',
-                                 'min_ctas_per_sm', 'threads', 'smem_bytes'),
-                                (v.value for v in vals))))
+            d = dict(zip(('cluster', 'double_buffered', 'min_ctas_per_sm',
+                          'threads', 'smem_bytes'), (v.value for v in vals)))
+            k = ct.c_int()
+            _lib.check(self._lib.dgfs_vhs_variant_kind(self._h, i,
+                                                       ct.byref(k)),
+                       'dgfs_vhs_variant_kind')
+            d['exchange'] = 'push' if k.value else 'pull'
+            out.append(d)
         return out
+
+    def status(self):
+        """Synchronise and raise if a launch gave up waiting for cluster
+        data (the push kernels bound every wait)."""
+        flag = ct.c_int()
+        _lib.check(self._lib.dgfs_vhs_status(self._h, self.backend.stream,
+                                             ct.byref(flag)),
+                   'dgfs_vhs_status')
 
     def select(self, idx):
         _lib.check(self._lib.dgfs_vhs_select(self._h, int(idx)),

@@ -120,6 +120,15 @@ DGFS_API int dgfs_vhs_variant_info(const dgfs_vhs* h, int idx, int* cluster,
 /* Use launch shape idx for subsequent applies (the autotuner's knob). */
 DGFS_API int dgfs_vhs_select(dgfs_vhs* h, int idx);
 
+/* 1 if launch shape idx exchanges by remote pushes (st.async into the
+ * owner's shared memory, mbarrier completion), 0 if by remote loads. */
+DGFS_API int dgfs_vhs_variant_kind(const dgfs_vhs* h, int idx, int* push);
+
+/* Synchronise `stream`, then report and clear the kernel error flag: the
+ * push kernels bound every wait on cluster data (a few seconds) and set the
+ * flag instead of hanging.  Returns DGFS_ERR_CUDA when it was set. */
+DGFS_API int dgfs_vhs_status(dgfs_vhs* h, void* stream, int* flag);
+
 /* ------------------------------------------------------------------------
  * FR-DG advection residual over all velocities
  *
