@@ -49,15 +49,20 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-// Wait for phase `parity` of `bar`, giving up after ~4 s (error flag set).
+// Wait for phase `parity` of `bar`, giving up after ~1 s (error flag set).
+// Once the flag is set every later wait of the launch returns at once, so a
+// failed exchange costs one timeout, not one per (p, q).
 __device__ __forceinline__ void mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err) {
   if (mbar_try_wait(bar, parity)) return;
   const uint64_t t0 = globaltimer_ns();
   for (uint32_t i = 1;; ++i) {
     if (mbar_try_wait(bar, parity)) return;
-    if ((i & 255u) == 0 && globaltimer_ns() - t0 > 4000000000ull) {
-      atomicExch(err, 1);
-      return;
+    if ((i & 255u) == 0) {
+      if (*(volatile int*)err) return;
+      if (globaltimer_ns() - t0 > 1000000000ull) {
+        atomicExch(err, 1);
+        return;
+      }
     }
   }
 }
