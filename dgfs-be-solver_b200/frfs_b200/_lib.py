@@ -52,6 +52,9 @@ _SIGS = {
     'dgfs_vhs_select': (c_int, [c_void_p, c_int]),
     'dgfs_vhs_variant_kind': (c_int, [c_void_p, c_int, ct.POINTER(c_int)]),
     'dgfs_vhs_status': (c_int, [c_void_p, c_void_p, ct.POINTER(c_int)]),
+    'dgfs_vhs_apply_noalloc': (c_int, [ct.POINTER(VhsParams), c_void_p,
+                                       c_void_p, c_int, c_int, c_ll, c_int,
+                                       c_int, c_int, c_void_p]),
     'dgfs_probe_fma_peak': (c_int, [c_int, c_int, ct.POINTER(c_double),
                                     ct.POINTER(ct.c_float), c_void_p]),
 }

@@ -129,6 +129,24 @@ DGFS_API int dgfs_vhs_variant_kind(const dgfs_vhs* h, int idx, int* push);
  * flag instead of hanging.  Returns DGFS_ERR_CUDA when it was set. */
 DGFS_API int dgfs_vhs_status(dgfs_vhs* h, void* stream, int* flag);
 
+/* Allocation-free variant of dgfs_vhs_apply (no counterpart in the
+ * reference).  For callers that cannot allocate device memory while they
+ * run -- a host whose memory manager owns the device heap, a plugin that may
+ * only touch the buffers it is handed, a loop where cudaMalloc's implicit
+ * synchronisation is not acceptable.  It takes the same parameters as
+ * dgfs_vhs_create and the same bank arguments as dgfs_vhs_apply, builds the
+ * tables itself and keeps them and its scratch in one file-scope device array
+ * of 24 MiB (held on every GPU that uses this entry point until the process
+ * exits); it never calls cudaMalloc or cudaFree.  Limits: Nrho <= 32 and
+ * M <= 128 (every such size, up to Nv = 32 in FP64 with the projection,
+ * fits in the array); larger sizes are rejected with DGFS_ERR_INVALID.  The first call on a device sets it up (symbol address,
+ * twiddles, kernel attributes) and should come before any stream capture.
+ * All calls share the array: calls that can overlap on the GPU race. */
+DGFS_API int dgfs_vhs_apply_noalloc(const dgfs_vhs_params* params,
+                                    const void* f, void* Q, int nupts,
+                                    int neles, long long ldim, int soasz,
+                                    int elem, int upt, void* stream);
+
 /* ------------------------------------------------------------------------
  * FR-DG advection residual over all velocities
  *
