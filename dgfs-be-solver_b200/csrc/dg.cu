@@ -18,8 +18,11 @@ struct dgfs_dg {
   void *smats, *rcpdjac, *nrm, *mag, *cvx, *cvy, *cvz, *guw, *gfw;
   int *part, *bkind, *bgroup, *bfpt, *bele, *grefl;
   double* bcvals;
-  void* uf;  // flux-point scratch [F][ldim_f]
+  double* bcpart;  // [kBcChunks][nb][2] partial wall sums
+  void* uf;        // flux-point scratch [F][ldim_f]
 };
+
+constexpr int kBcChunks = 64;  // velocity chunks of the wall-sum reduction
 
 namespace {
 
@@ -172,7 +175,7 @@ int check_range(const dgfs_dg* h, int v0, int nv) {
 void free_dg(dgfs_dg* h) {
   if (!h) return;
   void* ptrs[] = {h->smats, h->rcpdjac, h->nrm, h->mag, h->cvx, h->cvy, h->cvz, h->guw, h->gfw,
-                  h->part, h->bkind, h->bgroup, h->bfpt, h->bele, h->grefl, h->bcvals, h->uf};
+                  h->part, h->bkind, h->bgroup, h->bfpt, h->bele, h->grefl, h->bcvals, h->bcpart, h->uf};
   for (void* q : ptrs) cudaFree(q);
   delete h;
 }
@@ -251,7 +254,8 @@ extern "C" int dgfs_dg_create(const dgfs_dg_params* p, dgfs_dg** out) {
   if (!rc) {
     std::vector<double> ones(2 * nb, 1.0);  // frfs initialises bc_vals to 1 (inters.py:203)
     if (cudaMalloc((void**)&h->bcvals, 2 * nb * sizeof(double)) != cudaSuccess ||
-        cudaMemcpy(h->bcvals, ones.data(), 2 * nb * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+        cudaMemcpy(h->bcvals, ones.data(), 2 * nb * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMalloc((void**)&h->bcpart, (size_t)kBcChunks * 2 * nb * sizeof(double)) != cudaSuccess)
       rc = set_error(DGFS_ERR_NOMEM, "boundary value allocation failed");
   }
   if (!rc) {
@@ -298,20 +302,23 @@ extern "C" int dgfs_dg_updatebc(dgfs_dg* h, int v0, int nv, int reset, void* str
   int rc = check_range(h, v0, nv);
   if (rc) return rc;
   if (h->nb == 0) return DGFS_OK;
-  const unsigned grid = (unsigned)((h->nb + 31) / 32);
+  const int chunk = (nv + kBcChunks - 1) / kBcChunks;
+  const int nchunks = (nv + chunk - 1) / chunk;
+  const dim3 grid((unsigned)nchunks, (unsigned)((h->nb + 31) / 32));
+  cudaStream_t s = (cudaStream_t)stream;
   if (h->prec == 64) {
     DgArgs<double> a = make_args<double>(h);
     a.v0 = v0;
     a.nv = nv;
-    dg_bcsum_kernel<double, 2><<<grid, 256, 0, (cudaStream_t)stream>>>(a, h->bfpt, h->bele, h->nb, h->cw,
-                                                                        h->bcvals, reset);
+    dg_bcsum_kernel<double, 2><<<grid, 256, 0, s>>>(a, h->bfpt, h->bele, h->nb, h->cw, chunk, h->bcpart);
   } else {
     DgArgs<float> a = make_args<float>(h);
     a.v0 = v0;
     a.nv = nv;
-    dg_bcsum_kernel<float, 2><<<grid, 256, 0, (cudaStream_t)stream>>>(a, h->bfpt, h->bele, h->nb, h->cw,
-                                                                       h->bcvals, reset);
+    dg_bcsum_kernel<float, 2><<<grid, 256, 0, s>>>(a, h->bfpt, h->bele, h->nb, h->cw, chunk, h->bcpart);
   }
+  dg_bcsum_finish_kernel<<<(h->nb + 255) / 256, 256, 0, s>>>(h->bkind, h->nb, nchunks, h->bcpart, h->bcvals,
+                                                              reset);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_error(DGFS_ERR_CUDA, "DG boundary update launch: %s", cudaGetErrorString(e));
   return DGFS_OK;

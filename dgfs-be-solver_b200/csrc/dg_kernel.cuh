@@ -83,15 +83,19 @@ __global__ void __launch_bounds__(256) dg_interp_kernel(const DgArgs<T> a, const
   }
 }
 
-// One block per 32 boundary flux points; 8 velocity lanes per point reduce in
-// FP64 and write bcvals[b] = (sum_{c.n>=0} (c-Uw).n f cw, sum_{c.n<0} (c-Uw).n fw cw).
+// Diffuse-wall sums, pass 1: block (chunk, group) reduces 32 boundary flux
+// points over one chunk of the velocity range in FP64 (8 velocity lanes per
+// point) and writes partials[chunk][b] = (sum_{c.n>=0} (c-Uw).n f cw,
+// sum_{c.n<0} (c-Uw).n fw cw).
 template <typename T, int D>
 __global__ void __launch_bounds__(256) dg_bcsum_kernel(const DgArgs<T> a, const int* __restrict__ bfpt,
                                                       const int* __restrict__ bele, int nb, double cw,
-                                                      double* __restrict__ bcvals, int reset) {
+                                                      int chunk, double* __restrict__ partials) {
   __shared__ double s0[8][32], s1[8][32];
   const int bl = threadIdx.x & 31, vg = threadIdx.x >> 5;
-  const int b = blockIdx.x * 32 + bl;
+  const int b = blockIdx.y * 32 + bl;
+  const int vbeg = a.v0 + blockIdx.x * chunk;
+  const int vend = min(a.v0 + a.nv, vbeg + chunk);
   double acc0 = 0.0, acc1 = 0.0;
   if (b < nb && a.bkind[b] == BC_WALL_DIFFUSE) {
     const int j = bfpt[b], e = bele[b], g = a.bgroup[b];
@@ -101,7 +105,7 @@ __global__ void __launch_bounds__(256) dg_bcsum_kernel(const DgArgs<T> a, const 
       n[d] = (double)a.nrm[((int64_t)j * D + d) * a.neles + e];
       uw[d] = (double)a.guw[g * 3 + d];
     }
-    for (int v = a.v0 + vg; v < a.v0 + a.nv; v += 8) {
+    for (int v = vbeg + vg; v < vend; v += 8) {
       double fac = ((double)a.cvx[v] - uw[0]) * n[0];
       if (D > 1) fac += ((double)a.cvy[v] - uw[1]) * n[1];
       if (D > 2) fac += ((double)a.cvz[v] - uw[2]) * n[2];
@@ -114,19 +118,34 @@ __global__ void __launch_bounds__(256) dg_bcsum_kernel(const DgArgs<T> a, const 
   s0[vg][bl] = acc0;
   s1[vg][bl] = acc1;
   __syncthreads();
-  if (vg == 0 && b < nb && a.bkind[b] == BC_WALL_DIFFUSE) {
+  if (vg == 0 && b < nb) {
     double r0 = 0.0, r1 = 0.0;
     for (int k = 0; k < 8; ++k) {
       r0 += s0[k][bl];
       r1 += s1[k][bl];
     }
-    if (reset) {
-      bcvals[2 * b] = r0;
-      bcvals[2 * b + 1] = r1;
-    } else {
-      bcvals[2 * b] += r0;
-      bcvals[2 * b + 1] += r1;
-    }
+    partials[((int64_t)blockIdx.x * nb + b) * 2] = r0;
+    partials[((int64_t)blockIdx.x * nb + b) * 2 + 1] = r1;
+  }
+}
+
+// Pass 2: sum the chunks in a fixed order (deterministic) into bcvals.
+__global__ void __launch_bounds__(256) dg_bcsum_finish_kernel(const int* __restrict__ bkind, int nb, int nchunks,
+                                                             const double* __restrict__ partials,
+                                                             double* __restrict__ bcvals, int reset) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb || bkind[b] != BC_WALL_DIFFUSE) return;
+  double r0 = 0.0, r1 = 0.0;
+  for (int c = 0; c < nchunks; ++c) {
+    r0 += partials[((int64_t)c * nb + b) * 2];
+    r1 += partials[((int64_t)c * nb + b) * 2 + 1];
+  }
+  if (reset) {
+    bcvals[2 * b] = r0;
+    bcvals[2 * b + 1] = r1;
+  } else {
+    bcvals[2 * b] += r0;
+    bcvals[2 * b + 1] += r1;
   }
 }
 

@@ -55,6 +55,8 @@ _SIGS = {
     'dgfs_vhs_apply_noalloc': (c_int, [ct.POINTER(VhsParams), c_void_p,
                                        c_void_p, c_int, c_int, c_ll, c_int,
                                        c_int, c_int, c_void_p]),
+    'dgfs_moments': (c_int, [c_int, c_void_p, c_int, c_int, c_ll, c_int,
+                             c_double, c_double, c_void_p, c_void_p]),
     'dgfs_probe_fma_peak': (c_int, [c_int, c_int, ct.POINTER(c_double),
                                     ct.POINTER(ct.c_float), c_void_p]),
 }

@@ -264,6 +264,16 @@ class DGFSSystem:
             nv, alpha, ptr(A), beta, ptr(B), gamma, ptr(C), s),
             'dgfs_dg_rhs')
 
+    def moments(self, bankidx=None):
+        """FP64 moments at every solution point of a bank, shape
+        (nupts, neles, 14): rho, u(3), T, q(3), P(xx, xy, xz, yy, yz, zz)
+        (frfs/plugins/dgfsmomwriterstd.py:154-214, nondimensional)."""
+        return bank_moments(self.bank[self._active(bankidx)], self.vm,
+                            self.backend)
+
+    def _active(self, idx):
+        return self.bank.active if idx is None else idx
+
     def bc_values(self):
         nb = len(self.bpts)
         buf = np.zeros(max(2*nb, 2))
@@ -287,6 +297,19 @@ class DGFSSystem:
         a = buf.view(self.nfpts, ld.value)[:, :nblk*32*V].cpu().numpy()
         a = a.reshape(self.nfpts, nblk, V, 32).transpose(0, 2, 1, 3)
         return a.reshape(self.nfpts, V, nblk*32)[:, :, :E]
+
+
+def bank_moments(bank, vm, backend):
+    """FP64 moments of a distribution bank on the device (dgfs_moments)."""
+    import torch
+    nupts, _, neles = bank.ioshape
+    _, ldim, _ = bank.traits
+    out = torch.empty(nupts*neles*14, dtype=torch.float64,
+                      device=backend.device)
+    _lib.check(_lib.load().dgfs_moments(
+        backend.precision, bank._as_parameter_, nupts, neles, ldim, vm.Nv(),
+        vm.L(), vm.cw(), out.data_ptr(), backend.stream), 'dgfs_moments')
+    return out.view(nupts, neles, 14).cpu().numpy()
 
 
 class _DeviceArray:

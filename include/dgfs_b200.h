@@ -226,6 +226,20 @@ DGFS_API int dgfs_dg_bcvals(const dgfs_dg* h, double* host, int n);
 DGFS_API int dgfs_dg_fpts(const dgfs_dg* h, void** ptr, long long* ldim);
 
 /* ------------------------------------------------------------------------
+ * Macroscopic moments
+ *
+ * Replaces: the 3D moment formulas of DGFSMomWriterStdPlugin
+ * (frfs/plugins/dgfsmomwriterstd.py:154-214), which copy the whole bank to
+ * the host.  For every solution point of a bank (AoSoA, soasz 32, Nv^3
+ * variables on the cell-centred grid of half width L, weight cw) writes 14
+ * FP64 values out[(upt*neles + ele)*14 + k]: rho, ux, uy, uz, T, qx, qy, qz,
+ * Pxx, Pxy, Pxz, Pyy, Pyz, Pzz (nondimensional).  `out` is a device array.
+ * ---------------------------------------------------------------------- */
+DGFS_API int dgfs_moments(int precision, const void* f, int nupts, int neles,
+                          long long ldim, int Nv, double L, double cw,
+                          double* out, void* stream);
+
+/* ------------------------------------------------------------------------
  * Measurement helper (no counterpart in the reference)
  * ---------------------------------------------------------------------- */
 
