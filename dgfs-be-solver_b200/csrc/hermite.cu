@@ -1,0 +1,395 @@
+// Hermite embedding and reconstruction of distributions for the learned
+// collision surrogate (no counterpart in the reference).
+//
+// Local frame of a point: rho, u, T from the FP64 moments of f (the formulas
+// of frfs/plugins/dgfsmomwriterstd.py:154-190), c^ = (c - u)/sqrt(T).
+// Basis: phi_n(x) = He_n(sqrt(2) x)/sqrt(n!) (probabilists' Hermite),
+// orthonormal for the weight e^{-x^2}/sqrt(pi); in 3D
+// phi_ijk(c^) = phi_i phi_j phi_k, weight W(c^) = pi^{-3/2} e^{-|c^|^2}, and a
+// Maxwellian is rho T^{-3/2} W(c^).  Modes: total degree i+j+k <= 9
+// (220 modes, ordered by degree, then i, then j, both descending).
+//
+//   embedding   a_k = (1/rho) cw sum_v f(c_v) phi_k(c^_v)
+//               (a_000 = 1 and the first-order modes vanish by construction)
+//   target      b_k = cw sum_v Q(c_v) phi_k(c^_v) / (prefac rho^2 T^{gamma/2})
+//   reconstruct Q(c) = prefac rho^2 T^{gamma/2} T^{-3/2} W(c^) sum_k b_k phi_k(c^)
+//               followed by the FP64 least-squares projection onto zero
+//               mass, momentum and energy moments.
+// The velocity grid is a tensor product, so every sum factorises into three
+// 1D contractions.  One CTA per solution point.
+#include <cmath>
+#include <cuda_runtime.h>
+
+#include "../../include/dgfs_b200.h"
+#include "dgfs_common.cuh"
+#include "dgfs_internal.h"
+
+namespace {
+
+constexpr int kDeg = 9;
+constexpr int kP = kDeg + 1;       // 1D polynomials per axis
+constexpr int kModes = 220;        // (i, j, k) with i + j + k <= 9
+constexpr int kFeat = 256;         // feature vector width
+constexpr int kThreads = 256;
+constexpr int kMaxN = 32;
+
+__constant__ unsigned char c_mi[kModes], c_mj[kModes], c_mk[kModes];
+// index of mode (i, j, k) in the 220-vector, -1 if degree > 9
+__constant__ short c_midx[kP][kP][kP];
+
+struct FrameArgs {
+  int N, nupts, neles;
+  long long ldim;
+  double L, cw, prefac, gamma;
+};
+
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double s = 0;
+  for (int w = 0; w < kThreads / 32; ++w) s += red[w];
+  return s;
+}
+
+// rho, u, T of the point's distribution (two passes, FP64)
+template <typename T>
+__device__ void point_frame(const T* f, int upt, int e, const FrameArgs& a, double* red, double* mom) {
+  const int N = a.N;
+  const long long V = (long long)N * N * N;
+  const double h = 2.0 * a.L / N, c00 = -a.L + a.L / N;
+  double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+  for (long long v = threadIdx.x; v < V; v += kThreads) {
+    const double fv = (double)f[dgfs::soa_ix(upt, a.ldim, e, v, V, 32)];
+    s0 += fv;
+    s1 += fv * (c00 + (v / (N * N)) * h);
+    s2 += fv * (c00 + ((v / N) % N) * h);
+    s3 += fv * (c00 + (v % N) * h);
+  }
+  const double m0 = block_sum(s0, red), m1 = block_sum(s1, red), m2 = block_sum(s2, red),
+               m3 = block_sum(s3, red);
+  const double rho = m0 * a.cw, ux = m1 / m0, uy = m2 / m0, uz = m3 / m0;
+  double t = 0;
+  for (long long v = threadIdx.x; v < V; v += kThreads) {
+    const double fv = (double)f[dgfs::soa_ix(upt, a.ldim, e, v, V, 32)];
+    const double cx = c00 + (v / (N * N)) * h - ux, cy = c00 + ((v / N) % N) * h - uy, cz = c00 + (v % N) * h - uz;
+    t += fv * (cx * cx + cy * cy + cz * cz);
+  }
+  const double m4 = block_sum(t, red);
+  mom[0] = rho;
+  mom[1] = ux;
+  mom[2] = uy;
+  mom[3] = uz;
+  mom[4] = m4 * (2.0 / 3.0) / m0;
+}
+
+// H[ax][I][n] = phi_n((c0_I - u_ax)/sqrt(T)) for the three axes
+__device__ void basis_tables(const FrameArgs& a, const double* mom, double (*H)[kMaxN][kP]) {
+  const int N = a.N;
+  const double h = 2.0 * a.L / N, c00 = -a.L + a.L / N, rt = rsqrt(mom[4]);
+  for (int t = threadIdx.x; t < 3 * N; t += kThreads) {
+    const int ax = t / N, I = t % N;
+    const double y = 1.4142135623730950488 * (c00 + I * h - mom[1 + ax]) * rt;
+    double p0 = 1.0, p1 = y;
+    H[ax][I][0] = p0;
+    H[ax][I][1] = p1;
+    for (int n = 1; n < kDeg; ++n) {
+      // phi_{n+1} = (y phi_n - sqrt(n) phi_{n-1}) / sqrt(n+1)
+      const double p2 = (y * p1 - sqrt((double)n) * p0) * rsqrt((double)(n + 1));
+      H[ax][I][n + 1] = p2;
+      p0 = p1;
+      p1 = p2;
+    }
+  }
+}
+
+// out[m] = cw sum_v g(c_v) phi_m(c^_v) for the 220 modes, g read from a bank
+template <typename T>
+__device__ void project_modes(const T* g, int upt, int e, const FrameArgs& a, double (*H)[kMaxN][kP],
+                              double* t1, double* t2, double* out) {
+  const int N = a.N;
+  const long long V = (long long)N * N * N;
+  // t1[I][J][k] = sum_K g[I][J][K] Hz[K][k]
+  for (int r = threadIdx.x; r < N * N; r += kThreads) {
+    double acc[kP];
+#pragma unroll
+    for (int k = 0; k < kP; ++k) acc[k] = 0;
+    for (int K = 0; K < N; ++K) {
+      const double gv = (double)g[dgfs::soa_ix(upt, a.ldim, e, (long long)r * N + K, V, 32)];
+#pragma unroll
+      for (int k = 0; k < kP; ++k) acc[k] += gv * H[2][K][k];
+    }
+#pragma unroll
+    for (int k = 0; k < kP; ++k) t1[r * kP + k] = acc[k];
+  }
+  __syncthreads();
+  // t2[I][j][k] = sum_J t1[I][J][k] Hy[J][j]   (j + k <= 9)
+  for (int t = threadIdx.x; t < N * kP * kP; t += kThreads) {
+    const int I = t / (kP * kP), j = (t / kP) % kP, k = t % kP;
+    if (j + k > kDeg) continue;
+    double s = 0;
+    for (int J = 0; J < N; ++J) s += t1[(I * N + J) * kP + k] * H[1][J][j];
+    t2[(I * kP + j) * kP + k] = s;
+  }
+  __syncthreads();
+  // out[i][j][k] = cw sum_I t2[I][j][k] Hx[I][i]
+  for (int m = threadIdx.x; m < kModes; m += kThreads) {
+    const int i = c_mi[m], j = c_mj[m], k = c_mk[m];
+    double s = 0;
+    for (int I = 0; I < N; ++I) s += t2[(I * kP + j) * kP + k] * H[0][I][i];
+    out[m] = s * a.cw;
+  }
+  __syncthreads();
+}
+
+// Features X[pt][256] (a_k, then sqrt(T)/L and u/L), frame mom[pt][5],
+// non-equilibrium measure eps[pt] = |a_k, degree >= 2|, and optionally the
+// targets B[pt][256] of a collision bank Q.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) embed_kernel(const T* __restrict__ f, const T* __restrict__ Q,
+                                                         FrameArgs a, float* __restrict__ X,
+                                                         float* __restrict__ B, double* __restrict__ mom_out,
+                                                         float* __restrict__ eps) {
+  extern __shared__ double sm[];
+  __shared__ double red[kThreads / 32];
+  __shared__ double mom[5];
+  __shared__ double H[3][kMaxN][kP];
+  __shared__ double coef[kModes];
+  const int N = a.N;
+  double* t1 = sm;                    // [N*N][kP]
+  double* t2 = sm + N * N * kP;       // [N][kP][kP]
+  const int pt = blockIdx.x, upt = pt / a.neles, e = pt % a.neles;
+
+  double m[5];
+  point_frame<T>(f, upt, e, a, red, m);
+  if (threadIdx.x < 5) mom[threadIdx.x] = m[threadIdx.x];
+  __syncthreads();
+  basis_tables(a, mom, H);
+  __syncthreads();
+
+  project_modes<T>(f, upt, e, a, H, t1, t2, coef);
+  const double rho = mom[0];
+  double ne = 0;
+  for (int k = threadIdx.x; k < kFeat; k += kThreads) {
+    float x = 0.f;
+    if (k < kModes) {
+      x = (float)(coef[k] / rho);
+      if (c_mi[k] + c_mj[k] + c_mk[k] >= 2) ne += (coef[k] / rho) * (coef[k] / rho);
+    } else if (k == kModes) {
+      x = (float)(sqrt(mom[4]) / a.L);
+    } else if (k < kModes + 4) {
+      x = (float)(mom[k - kModes] / a.L);
+    }
+    X[(long long)pt * kFeat + k] = x;
+  }
+  ne = block_sum(ne, red);
+  if (threadIdx.x == 0) {
+    eps[pt] = (float)sqrt(ne);
+    for (int k = 0; k < 5; ++k) mom_out[(long long)pt * 5 + k] = mom[k];
+  }
+  if (Q) {
+    project_modes<T>(Q, upt, e, a, H, t1, t2, coef);
+    const double s = 1.0 / (a.prefac * rho * rho * pow(mom[4], 0.5 * a.gamma));
+    for (int k = threadIdx.x; k < kFeat; k += kThreads)
+      B[(long long)pt * kFeat + k] = k < kModes ? (float)(coef[k] * s) : 0.f;
+  }
+}
+
+// Q at the gated points from predicted coefficients Bp[pt][256]:
+// reconstruction, FP64 projection onto zero mass/momentum/energy, store.
+// gate[pt] != 0 selects the points written; others are left untouched.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) reconstruct_kernel(const float* __restrict__ Bp,
+                                                               const double* __restrict__ mom_in,
+                                                               const int* __restrict__ gate, FrameArgs a,
+                                                               const double* __restrict__ ginv,
+                                                               T* __restrict__ Q) {
+  extern __shared__ double sm[];
+  __shared__ double red[kThreads / 32];
+  __shared__ double H[3][kMaxN][kP];
+  __shared__ double b[kModes];
+  __shared__ double mom[5];
+  const int pt = blockIdx.x;
+  if (gate && !gate[pt]) return;  // uniform over the CTA
+  const int N = a.N, upt = pt / a.neles, e = pt % a.neles;
+  const long long V = (long long)N * N * N;
+  double* r1 = sm;                    // [kP][kP][N]   (i, j, K)
+  double* r2 = sm + kP * kP * N;      // [kP][N][N]    (i, J, K)
+  if (threadIdx.x < 5) mom[threadIdx.x] = mom_in[(long long)pt * 5 + threadIdx.x];
+  for (int k = threadIdx.x; k < kModes; k += kThreads) b[k] = (double)Bp[(long long)pt * kFeat + k];
+  __syncthreads();
+  basis_tables(a, mom, H);
+  __syncthreads();
+  // r1[i][j][K] = sum_k b[i][j][k] Hz[K][k]
+  for (int t = threadIdx.x; t < kP * kP * N; t += kThreads) {
+    const int i = t / (kP * N), j = (t / N) % kP, K = t % N;
+    double s = 0;
+    if (i + j <= kDeg)
+      for (int k = 0; k + i + j <= kDeg; ++k) s += b[c_midx[i][j][k]] * H[2][K][k];
+    r1[t] = s;
+  }
+  __syncthreads();
+  // r2[i][J][K] = sum_j r1[i][j][K] Hy[J][j]
+  for (int t = threadIdx.x; t < kP * N * N; t += kThreads) {
+    const int i = t / (N * N), J = (t / N) % N, K = t % N;
+    double s = 0;
+    for (int j = 0; j + i <= kDeg; ++j) s += r1[(i * kP + j) * N + K] * H[1][J][j];
+    r2[t] = s;
+  }
+  __syncthreads();
+  const double rho = mom[0], Tt = mom[4];
+  // pi^{-3/2}
+  const double scale = a.prefac * rho * rho * pow(Tt, 0.5 * a.gamma) * pow(Tt, -1.5) * 0.17958712212516656;
+  const double h = 2.0 * a.L / N, c00 = -a.L + a.L / N, rt = rsqrt(Tt);
+  // Q(c) = scale e^{-|c^|^2} sum_i r2[i][J][K] Hx[I][i]; moments for the projection
+  double mm[5] = {0, 0, 0, 0, 0};
+  for (long long v = threadIdx.x; v < V; v += kThreads) {
+    const int I = (int)(v / (N * N)), J = (int)((v / N) % N), K = (int)(v % N);
+    double s = 0;
+    for (int i = 0; i < kP; ++i) s += r2[((long long)i * N + J) * N + K] * H[0][I][i];
+    const double cx = c00 + I * h, cy = c00 + J * h, cz = c00 + K * h;
+    const double dx = (cx - mom[1]) * rt, dy = (cy - mom[2]) * rt, dz = (cz - mom[3]) * rt;
+    const double q = scale * exp(-(dx * dx + dy * dy + dz * dz)) * s;
+    Q[dgfs::soa_ix(upt, a.ldim, e, v, V, 32)] = (T)q;
+    mm[0] += q;
+    mm[1] += q * cx;
+    mm[2] += q * cy;
+    mm[3] += q * cz;
+    mm[4] += q * (cx * cx + cy * cy + cz * cz);
+  }
+  double lam[5];
+  {
+    double mt[5];
+    for (int k = 0; k < 5; ++k) mt[k] = block_sum(mm[k], red);
+    for (int k = 0; k < 5; ++k) {
+      double s = 0;
+      for (int j = 0; j < 5; ++j) s += ginv[k * 5 + j] * mt[j];
+      lam[k] = s;
+    }
+  }
+  // each thread corrects the values it stored itself
+  for (long long v = threadIdx.x; v < V; v += kThreads) {
+    const int I = (int)(v / (N * N)), J = (int)((v / N) % N), K = (int)(v % N);
+    const double cx = c00 + I * h, cy = c00 + J * h, cz = c00 + K * h;
+    const long long ix = dgfs::soa_ix(upt, a.ldim, e, v, V, 32);
+    Q[ix] = (T)((double)Q[ix] -
+                (lam[0] + lam[1] * cx + lam[2] * cy + lam[3] * cz + lam[4] * (cx * cx + cy * cy + cz * cz)));
+  }
+}
+
+// gate[pt] = eps[pt] < threshold; points that fail go to the plain list
+// (order of the list is irrelevant: every point is independent)
+__global__ void gate_kernel(int npts, const float* __restrict__ eps, float threshold, int* __restrict__ gate,
+                            int* __restrict__ plain, int* __restrict__ nplain) {
+  const int pt = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pt >= npts) return;
+  const int g = (eps[pt] < threshold) ? 1 : 0;
+  gate[pt] = g;
+  if (!g) plain[atomicAdd(nplain, 1)] = pt;
+}
+
+bool g_modes_ready[64];
+
+int init_modes() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < 64 && g_modes_ready[dev]) return DGFS_OK;
+  unsigned char mi[kModes], mj[kModes], mk[kModes];
+  short idx[kP][kP][kP];
+  for (int i = 0; i < kP; ++i)
+    for (int j = 0; j < kP; ++j)
+      for (int k = 0; k < kP; ++k) idx[i][j][k] = -1;
+  int m = 0;
+  for (int d = 0; d <= kDeg; ++d)
+    for (int i = d; i >= 0; --i)
+      for (int j = d - i; j >= 0; --j) {
+        const int k = d - i - j;
+        mi[m] = (unsigned char)i;
+        mj[m] = (unsigned char)j;
+        mk[m] = (unsigned char)k;
+        idx[i][j][k] = (short)m;
+        ++m;
+      }
+  if (cudaMemcpyToSymbol(c_mi, mi, sizeof(mi)) != cudaSuccess ||
+      cudaMemcpyToSymbol(c_mj, mj, sizeof(mj)) != cudaSuccess ||
+      cudaMemcpyToSymbol(c_mk, mk, sizeof(mk)) != cudaSuccess ||
+      cudaMemcpyToSymbol(c_midx, idx, sizeof(idx)) != cudaSuccess)
+    return dgfs::set_error(DGFS_ERR_CUDA, "mode table upload failed");
+  if (dev >= 0 && dev < 64) g_modes_ready[dev] = true;
+  return DGFS_OK;
+}
+
+int check_frame(int precision, int N, int nupts, int neles, long long ldim, double L, double cw) {
+  using dgfs::set_error;
+  if (precision != 32 && precision != 64) return set_error(DGFS_ERR_INVALID, "precision must be 32 or 64");
+  if (N < 4 || N > kMaxN) return set_error(DGFS_ERR_UNSUPPORTED, "Nv=%d outside 4..%d", N, kMaxN);
+  if (nupts < 1 || neles < 1 || !(L > 0) || !(cw > 0)) return set_error(DGFS_ERR_INVALID, "bad sizes");
+  const long long V = (long long)N * N * N;
+  if (ldim < (neles + 31) / 32 * 32 * V) return set_error(DGFS_ERR_INVALID, "ldim too small");
+  if ((long long)nupts * neles > 0x7fffffffLL) return set_error(DGFS_ERR_UNSUPPORTED, "too many points");
+  return DGFS_OK;
+}
+
+}  // namespace
+
+extern "C" int dgfs_hermite_embed(int precision, const void* f, const void* Q, int nupts, int neles,
+                                  long long ldim, int Nv, double L, double cw, double prefactor, double gamma,
+                                  float* X, float* B, double* mom, float* eps, void* stream) {
+  dgfs::clear_error();
+  if (!f || !X || !mom || !eps || (Q && !B)) return dgfs::set_error(DGFS_ERR_INVALID, "null pointer");
+  int rc = check_frame(precision, Nv, nupts, neles, ldim, L, cw);
+  if (!rc) rc = init_modes();
+  if (rc) return rc;
+  FrameArgs a{Nv, nupts, neles, ldim, L, cw, prefactor, gamma};
+  const size_t smem = ((size_t)Nv * Nv * kP + (size_t)Nv * kP * kP) * sizeof(double);
+  const void* fn = precision == 64 ? (const void*)embed_kernel<double> : (const void*)embed_kernel<float>;
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return dgfs::set_error(DGFS_ERR_CUDA, "smem attribute");
+  const unsigned grid = (unsigned)(nupts * neles);
+  if (precision == 64)
+    embed_kernel<double><<<grid, kThreads, smem, (cudaStream_t)stream>>>((const double*)f, (const double*)Q, a, X, B,
+                                                                          mom, eps);
+  else
+    embed_kernel<float><<<grid, kThreads, smem, (cudaStream_t)stream>>>((const float*)f, (const float*)Q, a, X, B,
+                                                                         mom, eps);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return dgfs::set_error(DGFS_ERR_CUDA, "embed launch: %s", cudaGetErrorString(e));
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_hermite_reconstruct(int precision, const float* B, const double* mom, const int* gate,
+                                        int nupts, int neles, long long ldim, int Nv, double L, double cw,
+                                        double prefactor, double gamma, const double* ginv, void* Q,
+                                        void* stream) {
+  dgfs::clear_error();
+  if (!B || !mom || !ginv || !Q) return dgfs::set_error(DGFS_ERR_INVALID, "null pointer");
+  int rc = check_frame(precision, Nv, nupts, neles, ldim, L, cw);
+  if (!rc) rc = init_modes();
+  if (rc) return rc;
+  FrameArgs a{Nv, nupts, neles, ldim, L, cw, prefactor, gamma};
+  const size_t smem = ((size_t)kP * kP * Nv + (size_t)kP * Nv * Nv) * sizeof(double);
+  const void* fn =
+      precision == 64 ? (const void*)reconstruct_kernel<double> : (const void*)reconstruct_kernel<float>;
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return dgfs::set_error(DGFS_ERR_CUDA, "smem attribute");
+  const unsigned grid = (unsigned)(nupts * neles);
+  if (precision == 64)
+    reconstruct_kernel<double><<<grid, kThreads, smem, (cudaStream_t)stream>>>(B, mom, gate, a, ginv, (double*)Q);
+  else
+    reconstruct_kernel<float><<<grid, kThreads, smem, (cudaStream_t)stream>>>(B, mom, gate, a, ginv, (float*)Q);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return dgfs::set_error(DGFS_ERR_CUDA, "reconstruct launch: %s", cudaGetErrorString(e));
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_surrogate_gate(int npts, const float* eps, float threshold, int* gate, int* plain, int* nplain,
+                                   void* stream) {
+  dgfs::clear_error();
+  if (npts < 1 || !eps || !gate || !plain || !nplain) return dgfs::set_error(DGFS_ERR_INVALID, "bad arguments");
+  cudaError_t e = cudaMemsetAsync(nplain, 0, sizeof(int), (cudaStream_t)stream);
+  if (e != cudaSuccess) return dgfs::set_error(DGFS_ERR_CUDA, "gate counter reset: %s", cudaGetErrorString(e));
+  gate_kernel<<<(npts + 255) / 256, 256, 0, (cudaStream_t)stream>>>(npts, eps, threshold, gate, plain, nplain);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? DGFS_OK : dgfs::set_error(DGFS_ERR_CUDA, "gate launch: %s", cudaGetErrorString(e));
+}

@@ -486,7 +486,7 @@ extern "C" int dgfs_vhs_info(const dgfs_vhs* h, int* cluster, int* threads, int*
 }
 
 static int vhs_launch(dgfs_vhs* h, const void* f, void* Q, int nupts, int neles, long long ldim, int soasz,
-                      int pt0, int npts, void* stream) {
+                      int pt0, int npts, void* stream, const int* plist = nullptr, const int* pcount = nullptr) {
   if (!h) return set_error(DGFS_ERR_INVALID, "null handle");
   if (!f || !Q) return set_error(DGFS_ERR_INVALID, "null bank pointer");
   if (nupts < 1 || neles < 1 || soasz < 1)
@@ -495,9 +495,11 @@ static int vhs_launch(dgfs_vhs* h, const void* f, void* Q, int nupts, int neles,
   if (ldim < nblk * soasz * (long long)h->V)
     return set_error(DGFS_ERR_INVALID, "ldim=%lld smaller than one AoSoA row (%lld)", ldim,
                      nblk * soasz * (long long)h->V);
-  if (pt0 < 0 || npts < 0 || (long long)pt0 + npts > (long long)nupts * neles)
+  if (!plist && (pt0 < 0 || npts < 0 || (long long)pt0 + npts > (long long)nupts * neles))
     return set_error(DGFS_ERR_INVALID, "point range [%d, %d) outside 0..%lld", pt0, pt0 + npts,
                      (long long)nupts * neles);
+  if (plist && (npts < 0 || npts > nupts * neles))
+    return set_error(DGFS_ERR_INVALID, "point list of %d entries for a bank of %d points", npts, nupts * neles);
   const size_t esz = h->prec == 64 ? 8 : 4;
   const char* fb = (const char*)f;
   const char* qb = (const char*)Q;
@@ -529,6 +531,8 @@ static int vhs_launch(dgfs_vhs* h, const void* f, void* Q, int nupts, int neles,
     a.b2 = (const double*)h->b2;
     a.fc = (double2*)h->fc;
     a.err = h->err;
+    a.plist = plist;
+    a.pcount = pcount;
     a.prefac = h->prefac;
     a.project = h->project;
     a.ginv = h->ginv;
@@ -551,6 +555,8 @@ static int vhs_launch(dgfs_vhs* h, const void* f, void* Q, int nupts, int neles,
     a.b2 = (const float*)h->b2;
     a.fc = (float2*)h->fc;
     a.err = h->err;
+    a.plist = plist;
+    a.pcount = pcount;
     a.prefac = (float)h->prefac;
     a.project = h->project;
     a.ginv = h->ginv;
@@ -576,4 +582,11 @@ extern "C" int dgfs_vhs_apply_range(dgfs_vhs* h, const void* f, void* Q, int nup
                                     int soasz, int pt0, int npts, void* stream) {
   clear_error();
   return vhs_launch(h, f, Q, nupts, neles, ldim, soasz, pt0, npts, stream);
+}
+
+extern "C" int dgfs_vhs_apply_list(dgfs_vhs* h, const void* f, void* Q, int nupts, int neles, long long ldim,
+                                   int soasz, const int* pts, const int* count, int max_points, void* stream) {
+  clear_error();
+  if (!pts) return set_error(DGFS_ERR_INVALID, "null point list");
+  return vhs_launch(h, f, Q, nupts, neles, ldim, soasz, 0, max_points, stream, pts, count);
 }

@@ -57,6 +57,8 @@ template <typename T> struct VhsArgs {
   const T* b2;          // [V]
   cx<T>* fc;            // scratch [gridDim.x][N][NJ]: gain spectrum per CTA
   int* err;             // set to 1 when a bounded wait gives up
+  const int* plist;     // optional device list of linear points (NULL: pt0 + i)
+  const int* pcount;    // optional device count capping npts (NULL: npts)
   T prefac;
   // optional FP64 conservation projection (mass, momentum, energy)
   int project;
@@ -219,7 +221,13 @@ __global__ void __launch_bounds__(VhsGeom<N, C, DB>::NT, MINB) vhs_cluster_kerne
     for (int i = tid; i < 3 * N; i += NT) sPh[slot * 3 * N + i] = src[i];
   };
 
-  for (int pt = a.pt0 + cid; pt < a.pt0 + a.npts; pt += ncl) {
+  const int npts = a.pcount ? min(a.npts, *a.pcount) : a.npts;
+  for (int ip = cid; ip < npts; ip += ncl) {
+    const int pt = a.plist ? a.plist[a.pt0 + ip] : a.pt0 + ip;
+    // listed ids come from device memory: skip one outside the bank (every
+    // CTA of the cluster reads the same entry, so all skip together and the
+    // cluster barriers stay paired)
+    if ((unsigned)pt >= (unsigned)(a.nupts * a.neles)) continue;
     const int upt = pt / a.neles, elem = pt % a.neles;
 
     // ---- F = FFT(f) / V -------------------------------------------------

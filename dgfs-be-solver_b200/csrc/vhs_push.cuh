@@ -186,7 +186,13 @@ __global__ void __launch_bounds__(PushGeom<N, C>::NT, MINB) vhs_push_kernel(cons
   cl_wait();
   cl_arrive();  // pending: nothing to protect yet
 
-  for (int pt = a.pt0 + cid; pt < a.pt0 + a.npts; pt += ncl) {
+  const int npts = a.pcount ? min(a.npts, *a.pcount) : a.npts;
+  for (int ip = cid; ip < npts; ip += ncl) {
+    const int pt = a.plist ? a.plist[a.pt0 + ip] : a.pt0 + ip;
+    // listed ids come from device memory: skip one outside the bank (every
+    // CTA of the cluster reads the same entry, so all skip together and the
+    // cluster barriers stay paired)
+    if ((unsigned)pt >= (unsigned)(a.nupts * a.neles)) continue;
     const int upt = pt / a.neles, elem = pt % a.neles;
 
     // ---- F = FFT(f) / V -------------------------------------------------

@@ -42,6 +42,9 @@ _SIGS = {
     'dgfs_vhs_apply_range': (c_int, [c_void_p, c_void_p, c_void_p, c_int,
                                      c_int, c_ll, c_int, c_int, c_int,
                                      c_void_p]),
+    'dgfs_vhs_apply_list': (c_int, [c_void_p, c_void_p, c_void_p, c_int,
+                                    c_int, c_ll, c_int, c_void_p, c_void_p,
+                                    c_int, c_void_p]),
     'dgfs_vhs_info': (c_int, [c_void_p, ct.POINTER(c_int),
                               ct.POINTER(c_int), ct.POINTER(c_int),
                               ct.POINTER(c_int)]),

@@ -50,6 +50,7 @@ class BaseDGFSStepper:
         if not self.use_graphs:
             fn()
             return
+        key = key + (self.system.graph_key,)
         g = self._graphs.get(key)
         if g is None:
             # First use: run the stage for real on a side stream (this is

@@ -1,0 +1,557 @@
+# -*- coding: utf-8 -*-
+"""Learned collision surrogate with the plain fast-spectral operator as
+fallback and judge (no counterpart in the reference).
+
+Per solution point:
+
+1. FP64 moments rho, u, T define a local frame c^ = (c - u)/sqrt(T);
+2. the distribution is embedded as 220 Hermite coefficients (total degree
+   <= 9) in that frame plus sqrt(T)/L and u/L (256 features);
+3. an MLP (256 -> 512 -> 512 -> 512 -> 256, tanh, with a linear skip from the
+   input; BF16 weights, FP32 accumulation) predicts the Hermite coefficients
+   of Q(f) scaled by prefac rho^2 T^{gamma/2};
+4. Q is rebuilt on the velocity grid and projected in FP64 onto zero mass,
+   momentum and energy moments.
+
+A point uses the surrogate when its non-equilibrium measure eps (the norm of
+its Hermite coefficients of degree >= 2, a local Knudsen indicator: Grad's
+expansion deviates from the Maxwellian at O(Kn)) is below the threshold;
+every other point runs the plain operator through a device point list, with
+no host round trip.  ``residual_check`` re-evaluates a sample of surrogate
+points with the plain operator and reports their relative error, which the
+caller compares with its tolerance to fall back to the plain operator.
+
+All arithmetic runs in libdgfs_b200.so (embedding, gate, MLP forward and
+backward, Adam, reconstruction); PyTorch allocates the buffers.
+"""
+
+import ctypes as ct
+
+import numpy as np
+import torch
+
+from frfs_b200 import _lib
+
+c_int, c_ll, c_double, c_float, c_void_p = (ct.c_int, ct.c_longlong,
+                                            ct.c_double, ct.c_float,
+                                            ct.c_void_p)
+_lib.declare('dgfs_hermite_embed', c_int,
+             [c_int, c_void_p, c_void_p, c_int, c_int, c_ll, c_int, c_double,
+              c_double, c_double, c_double, c_void_p, c_void_p, c_void_p,
+              c_void_p, c_void_p])
+_lib.declare('dgfs_hermite_reconstruct', c_int,
+             [c_int, c_void_p, c_void_p, c_void_p, c_int, c_int, c_ll, c_int,
+              c_double, c_double, c_double, c_double, c_void_p, c_void_p,
+              c_void_p])
+_lib.declare('dgfs_surrogate_gate', c_int,
+             [c_int, c_void_p, c_float, c_void_p, c_void_p, c_void_p,
+              c_void_p])
+_lib.declare('dgfs_mlp_gemm', c_int,
+             [c_int, c_int, c_int, c_void_p, c_ll, c_ll, c_void_p, c_int,
+              c_ll, c_ll, c_void_p, c_void_p, c_void_p, c_ll, c_int, c_int,
+              c_void_p])
+_lib.declare('dgfs_mlp_tanh_bwd', c_int, [c_ll, c_void_p, c_void_p,
+                                          c_void_p, c_void_p])
+_lib.declare('dgfs_mlp_colsum', c_int, [c_int, c_int, c_void_p, c_ll,
+                                        c_void_p, c_int, c_void_p])
+_lib.declare('dgfs_mlp_mse', c_int, [c_int, c_int, c_int, c_void_p, c_void_p,
+                                     c_void_p, c_void_p, c_void_p, c_void_p])
+_lib.declare('dgfs_mlp_adam', c_int, [c_ll, c_void_p, c_void_p, c_void_p,
+                                      c_void_p, c_void_p, c_float, c_float,
+                                      c_float, c_float, c_int, c_float,
+                                      c_void_p])
+_lib.declare('dgfs_mlp_affine', c_int, [c_int, c_int, c_void_p, c_void_p,
+                                        c_void_p, c_void_p, c_int, c_void_p])
+_lib.declare('dgfs_f32_to_bf16', c_int, [c_ll, c_void_p, c_void_p, c_void_p])
+
+NFEAT = 256
+NMODES = 220
+WIDTH = 512
+
+
+def _p(t):
+    return None if t is None else t.data_ptr()
+
+
+class _Workspace:
+    """Buffers reused across calls, keyed by name, shape and dtype, so that a
+    CUDA graph captured around a call keeps pointing at live memory."""
+
+    def __init__(self, device):
+        self.device = device
+        self._bufs = {}
+
+    def get(self, name, shape, dtype=torch.float32):
+        key = (name, tuple(shape), dtype)
+        t = self._bufs.get(key)
+        if t is None:
+            t = self._bufs[key] = torch.empty(shape, dtype=dtype,
+                                              device=self.device)
+        return t
+
+
+class MLP:
+    """4 layers of width 512 with a linear input->output skip; FP32 master
+    weights, BF16 copies for the products, Adam optimiser; every kernel is
+    libdgfs_b200's.  Weights are stored W[in][out], activations row-major
+    [batch][features]."""
+
+    names = ('W1', 'b1', 'W2', 'b2', 'W3', 'b3', 'W4', 'b4', 'Ws')
+
+    def __init__(self, device, nin=NFEAT, width=WIDTH, nout=NFEAT, seed=0):
+        self.device = device
+        self.nin, self.width, self.nout = nin, width, nout
+        rng = np.random.default_rng(seed)
+        shapes = {'W1': (nin, width), 'b1': (width,), 'W2': (width, width),
+                  'b2': (width,), 'W3': (width, width), 'b3': (width,),
+                  'W4': (width, nout), 'b4': (nout,), 'Ws': (nin, nout)}
+        self.w, self.g, self.m1, self.m2, self.wb = {}, {}, {}, {}, {}
+        for k, shp in shapes.items():
+            if k in ('W1', 'W2', 'W3'):
+                a = rng.standard_normal(shp)/np.sqrt(shp[0])
+            elif k == 'W4':
+                a = 0.1*rng.standard_normal(shp)/np.sqrt(shp[0])
+            else:
+                a = np.zeros(shp)
+            self.w[k] = torch.tensor(a, dtype=torch.float32, device=device)
+            self.g[k] = torch.zeros_like(self.w[k])
+            self.m1[k] = torch.zeros_like(self.w[k])
+            self.m2[k] = torch.zeros_like(self.w[k])
+            if k.startswith('W'):
+                self.wb[k] = torch.empty(self.w[k].shape, dtype=torch.bfloat16,
+                                         device=device)
+        self.step = 0
+        self.ws = _Workspace(device)
+        self.sync_bf16()
+        self._cache = None
+
+    @property
+    def _s(self):
+        return torch.cuda.current_stream(self.device).cuda_stream
+
+    def nparams(self):
+        return sum(t.numel() for t in self.w.values())
+
+    def sync_bf16(self):
+        lib = _lib.load()
+        for k, t in self.wb.items():
+            _lib.check(lib.dgfs_f32_to_bf16(t.numel(), _p(self.w[k]), _p(t),
+                                            self._s), 'dgfs_f32_to_bf16')
+
+    def _gemm(self, A, B, C, M, N, K, sam, sak, sbk, sbn, bf16, bias=None,
+              act=0, acc=0):
+        _lib.check(_lib.load().dgfs_mlp_gemm(
+            M, N, K, _p(A), sam, sak, _p(B), 1 if bf16 else 0, sbk, sbn,
+            _p(bias), None, _p(C), N, act, acc, self._s), 'dgfs_mlp_gemm')
+
+    def forward(self, X, keep=False):
+        """Y = W4 tanh(W3 tanh(W2 tanh(W1 X + b1) + b2) + b3) + b4 + Ws X."""
+        B = X.shape[0]
+        nin, wd, nout = self.nin, self.width, self.nout
+        tag = 'train' if keep else 'infer'
+        H1 = self.ws.get(tag + 'H1', (B, wd))
+        H2 = self.ws.get(tag + 'H2', (B, wd))
+        H3 = self.ws.get(tag + 'H3', (B, wd))
+        Y = self.ws.get(tag + 'Y', (B, nout))
+        wb, w = self.wb, self.w
+        self._gemm(X, wb['W1'], H1, B, wd, nin, nin, 1, wd, 1, True,
+                   w['b1'], act=1)
+        self._gemm(H1, wb['W2'], H2, B, wd, wd, wd, 1, wd, 1, True,
+                   w['b2'], act=1)
+        self._gemm(H2, wb['W3'], H3, B, wd, wd, wd, 1, wd, 1, True,
+                   w['b3'], act=1)
+        self._gemm(H3, wb['W4'], Y, B, nout, wd, wd, 1, nout, 1, True,
+                   w['b4'])
+        self._gemm(X, wb['Ws'], Y, B, nout, nin, nin, 1, nout, 1, True,
+                   acc=1)
+        if keep:
+            self._cache = (X, H1, H2, H3)
+        return Y
+
+    def backward(self, dY):
+        """Gradients of every parameter into self.g: weight gradients from
+        the FP32 activations, input gradients through the BF16 weights that
+        the forward pass used."""
+        lib = _lib.load()
+        X, H1, H2, H3 = self._cache
+        B = X.shape[0]
+        nin, wd, nout = self.nin, self.width, self.nout
+        g, wb = self.g, self.wb
+        dH = self.ws.get('dH', (B, wd))
+        dZ = self.ws.get('dZ', (B, wd))
+
+        def wgrad(A, D, name, k, n):          # g = A^T D, (k x n), K = B
+            self._gemm(A, D, g[name], k, n, B, 1, k, n, 1, False)
+
+        def bgrad(D, name, n):
+            _lib.check(lib.dgfs_mlp_colsum(B, n, _p(D), n, _p(g[name]), 0,
+                                           self._s), 'dgfs_mlp_colsum')
+
+        def through(D, nd, W, H):
+            # dZ = (D W^T) o (1 - H^2); D may be dZ itself: the product is
+            # complete (same stream) before dZ is overwritten
+            self._gemm(D, W, dH, B, wd, nd, nd, 1, 1, nd, True)
+            _lib.check(lib.dgfs_mlp_tanh_bwd(dH.numel(), _p(H), _p(dH),
+                                             _p(dZ), self._s),
+                       'dgfs_mlp_tanh_bwd')
+
+        wgrad(H3, dY, 'W4', wd, nout)
+        bgrad(dY, 'b4', nout)
+        wgrad(X, dY, 'Ws', nin, nout)
+        through(dY, nout, wb['W4'], H3)
+        wgrad(H2, dZ, 'W3', wd, wd)
+        bgrad(dZ, 'b3', wd)
+        through(dZ, wd, wb['W3'], H2)
+        wgrad(H1, dZ, 'W2', wd, wd)
+        bgrad(dZ, 'b2', wd)
+        through(dZ, wd, wb['W2'], H1)
+        wgrad(X, dZ, 'W1', nin, wd)
+        bgrad(dZ, 'b1', wd)
+        return g
+
+    def adam(self, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8, wd=0.0):
+        lib = _lib.load()
+        self.step += 1
+        for k in self.names:
+            _lib.check(lib.dgfs_mlp_adam(
+                self.w[k].numel(), _p(self.w[k]), _p(self.wb.get(k)),
+                _p(self.g[k]), _p(self.m1[k]), _p(self.m2[k]), lr, beta1,
+                beta2, eps, self.step, wd if k.startswith('W') else 0.0,
+                self._s), 'dgfs_mlp_adam')
+
+    def state(self):
+        return {k: v.detach().cpu().numpy() for k, v in self.w.items()}
+
+    def load(self, state):
+        for k, v in state.items():
+            self.w[k].copy_(torch.as_tensor(v, dtype=torch.float32))
+        self.sync_bf16()
+
+
+class VHSSurrogate:
+    """Surrogate for a DGFSVHSGLLScatteringModel ``sm``.
+
+    ``collide(fbank, qbank)`` is stream-ordered and allocation-free after
+    the first call for a bank shape, so a stage that contains it can be
+    captured in a CUDA graph."""
+
+    def __init__(self, sm, threshold=0.05, seed=0):
+        self.sm = sm
+        self.backend = sm.backend
+        self.vm = sm.vm
+        self.device = sm.backend.device
+        self.threshold = float(threshold)
+        self.mlp = MLP(self.device, seed=seed)
+        self.ws = _Workspace(self.device)
+        z = lambda: torch.zeros(NFEAT, device=self.device)
+        o = lambda: torch.ones(NFEAT, device=self.device)
+        self.mu_x, self.is_x, self.mu_y, self.is_y = z(), o(), z(), o()
+        cv = self.vm.cv()
+        phi = np.vstack([np.ones(cv.shape[1]), cv, np.sum(cv*cv, axis=0)])
+        self.ginv = torch.tensor(np.linalg.inv(phi @ phi.T).ravel(),
+                                 dtype=torch.float64, device=self.device)
+        self.loss_history = []
+        self._last = None
+
+    @property
+    def _s(self):
+        return self.backend.stream
+
+    # -- features ------------------------------------------------------------
+    def embed(self, fbank, qbank=None, out=None):
+        """Features X, targets B (when qbank), frame mom, measure eps."""
+        nupts, _, neles = fbank.ioshape
+        npts = nupts*neles
+        _, ldim, _ = fbank.traits
+        if out is None:
+            X = torch.empty(npts, NFEAT, device=self.device)
+            B = torch.empty(npts, NFEAT, device=self.device) if qbank \
+                else None
+            mom = torch.empty(npts, 5, dtype=torch.float64,
+                              device=self.device)
+            eps = torch.empty(npts, device=self.device)
+        else:
+            X, B, mom, eps = out
+        _lib.check(_lib.load().dgfs_hermite_embed(
+            self.backend.precision, fbank._as_parameter_,
+            qbank._as_parameter_ if qbank else None, nupts, neles, ldim,
+            self.vm.Nv(), self.vm.L(), self.vm.cw(), self.sm.prefactor,
+            self.sm._gamma, _p(X), _p(B), _p(mom), _p(eps), self._s),
+            'dgfs_hermite_embed')
+        return X, B, mom, eps
+
+    def _affine(self, X, mu, isg, inverse=False, out=None):
+        Y = torch.empty_like(X) if out is None else out
+        _lib.check(_lib.load().dgfs_mlp_affine(
+            X.shape[0], X.shape[1], _p(X), _p(mu), _p(isg), _p(Y),
+            1 if inverse else 0, self._s), 'dgfs_mlp_affine')
+        return Y
+
+    def set_normalisation(self, X, B):
+        """Per-feature standardisation from training data.  Features that
+        are constant by construction (a_000 = 1, first-order modes) get a
+        zero scale; targets are centred and divided by one global scale, so
+        that the loss is the physical L2 error of Q in the orthonormal
+        Hermite basis."""
+        mu, sd = X.mean(dim=0), X.std(dim=0)
+        self.mu_x = mu.contiguous()
+        self.is_x = torch.where(sd > 1e-5, 1.0/sd.clamp(min=1e-30),
+                                torch.zeros_like(sd)).contiguous()
+        mu, sd = B.mean(dim=0), B.std(dim=0)
+        ref = float(torch.sqrt(torch.mean(sd[:NMODES]**2)))
+        ref = ref if ref > 0 else 1.0
+        self.mu_y = mu.contiguous()
+        self.is_y = torch.full_like(sd, 1.0/ref)
+
+    # -- training ------------------------------------------------------------
+    def train(self, X, B, epochs=20, batch=1024, lr=1e-3, seed=0,
+              lr_min=0.05, weight_decay=0.0):
+        """Mini-batch Adam on normalised features/targets with the
+        project's kernels (cosine learning-rate decay to lr*lr_min);
+        returns the per-epoch mean loss."""
+        Xn = self._affine(X, self.mu_x, self.is_x)
+        Bn = self._affine(B, self.mu_y, self.is_y)
+        n = X.shape[0]
+        batch = min(batch, n)
+        g = torch.Generator(device='cpu').manual_seed(seed)
+        lib = _lib.load()
+        nb = n//batch
+        total = max(epochs*nb, 1)
+        dY = torch.empty(batch, NFEAT, device=self.device)
+        rl = torch.empty(nb, batch, dtype=torch.float64, device=self.device)
+        hist = []
+        it = 0
+        for ep in range(epochs):
+            perm = torch.randperm(n, generator=g).to(self.device)
+            for b in range(nb):
+                idx = perm[b*batch:(b + 1)*batch]
+                xb = Xn.index_select(0, idx)
+                yb = Bn.index_select(0, idx)
+                Y = self.mlp.forward(xb, keep=True)
+                _lib.check(lib.dgfs_mlp_mse(
+                    batch, NFEAT, NMODES, _p(Y), _p(yb), None, _p(dY),
+                    _p(rl[b]), self._s), 'dgfs_mlp_mse')
+                self.mlp.backward(dY)
+                frac = it/total
+                lr_t = lr*(lr_min + (1 - lr_min)*0.5*(1 + np.cos(np.pi*frac)))
+                self.mlp.adam(lr=lr_t, wd=weight_decay)
+                it += 1
+            hist.append(float(rl.sum())/(nb*batch*NMODES))
+        self.loss_history += hist
+        return hist
+
+    def predict(self, X):
+        npts = X.shape[0]
+        Xn = self._affine(X, self.mu_x, self.is_x,
+                          out=self.ws.get('Xn', (npts, NFEAT)))
+        Yn = self.mlp.forward(Xn)
+        return self._affine(Yn, self.mu_y, self.is_y, inverse=True,
+                            out=self.ws.get('Bp', (npts, NFEAT)))
+
+    # -- use -----------------------------------------------------------------
+    def collide(self, fbank, qbank, threshold=None):
+        """Q into qbank: surrogate where eps < threshold, plain operator
+        elsewhere (device gate and point list).  Returns the gate tensor."""
+        thr = self.threshold if threshold is None else threshold
+        nupts, _, neles = fbank.ioshape
+        npts = nupts*neles
+        _, ldim, _ = fbank.traits
+        lib = _lib.load()
+        ws = self.ws
+        out = (ws.get('X', (npts, NFEAT)), None,
+               ws.get('mom', (npts, 5), torch.float64),
+               ws.get('eps', (npts,)))
+        X, _, mom, eps = self.embed(fbank, out=out)
+        gate = ws.get('gate', (npts,), torch.int32)
+        plain = ws.get('plain', (npts,), torch.int32)
+        nplain = ws.get('nplain', (1,), torch.int32)
+        _lib.check(lib.dgfs_surrogate_gate(npts, _p(eps), thr, _p(gate),
+                                           _p(plain), _p(nplain), self._s),
+                   'dgfs_surrogate_gate')
+        Bp = self.predict(X)
+        _lib.check(lib.dgfs_hermite_reconstruct(
+            self.backend.precision, _p(Bp), _p(mom), _p(gate), nupts, neles,
+            ldim, self.vm.Nv(), self.vm.L(), self.vm.cw(),
+            self.sm.prefactor, self.sm._gamma, _p(self.ginv),
+            qbank._as_parameter_, self._s), 'dgfs_hermite_reconstruct')
+        _lib.check(lib.dgfs_vhs_apply_list(
+            self.sm._h, fbank._as_parameter_, qbank._as_parameter_, nupts,
+            neles, ldim, self.backend.soasz, _p(plain), _p(nplain), npts,
+            self._s), 'dgfs_vhs_apply_list')
+        self._last = (gate, eps)
+        return gate
+
+    # kernels one collide() launches: embed, gate (+ counter reset),
+    # 2 affine, 5 GEMMs, reconstruct, plain list
+    launches_per_collide = 11
+
+    def residual_check(self, fbank, qbank, scratch, sample=16, seed=0):
+        """Plain Q at a random sample of the last call's surrogate points
+        (into ``scratch``) against the surrogate's values in ``qbank``;
+        returns sqrt(sum |dQ|^2 / sum |Q_plain|^2) over the sample (0 when no
+        point used the surrogate).  The caller compares it with its
+        tolerance and drops the surrogate when it is exceeded."""
+        gate, _ = self._last
+        sur = torch.nonzero(gate).flatten()
+        if sur.numel() == 0:
+            return 0.0
+        g = torch.Generator(device='cpu').manual_seed(seed)
+        pick = sur[torch.randperm(sur.numel(), generator=g)[:sample]
+                   .to(sur.device)].to(torch.int32).contiguous()
+        nupts, _, neles = fbank.ioshape
+        _, ldim, _ = fbank.traits
+        _lib.check(_lib.load().dgfs_vhs_apply_list(
+            self.sm._h, fbank._as_parameter_, scratch._as_parameter_, nupts,
+            neles, ldim, self.backend.soasz, _p(pick), None, pick.numel(),
+            self._s), 'dgfs_vhs_apply_list')
+        qa, qb = qbank.get(), scratch.get()
+        num = den = 0.0
+        for pt in pick.cpu().numpy():
+            u, e = divmod(int(pt), neles)
+            num += float(np.sum((qa[u, :, e].astype(np.float64) -
+                                 qb[u, :, e])**2))
+            den += float(np.sum(qb[u, :, e].astype(np.float64)**2))
+        return float(np.sqrt(num/max(den, 1e-300)))
+
+    def save(self, path):
+        st = self.mlp.state()
+        st.update(mu_x=self.mu_x.cpu().numpy(), is_x=self.is_x.cpu().numpy(),
+                  mu_y=self.mu_y.cpu().numpy(), is_y=self.is_y.cpu().numpy(),
+                  threshold=self.threshold)
+        np.savez(path, **st)
+
+    def load(self, path):
+        d = np.load(path)
+        self.mlp.load({k: d[k] for k in MLP.names})
+        for k in ('mu_x', 'is_x', 'mu_y', 'is_y'):
+            setattr(self, k, torch.tensor(d[k], device=self.device))
+        self.threshold = float(d['threshold'])
+
+
+# --------------------------------------------------------------------------
+# Training data from the solver's own trajectories
+# --------------------------------------------------------------------------
+def _ball(rng):
+    d = rng.standard_normal(3)
+    return d/np.linalg.norm(d)*rng.uniform()**(1/3)
+
+
+def random_uniform_state(vm, rng, bimodal):
+    """A spatially uniform initial distribution: a Maxwellian with
+    rho ~ U[0.5, 2], T ~ U[0.5, 3], u uniform in the unit ball, or (bimodal)
+    the equal mixture of two such Maxwellians at +-u, renormalised to
+    rho."""
+    from frfs_b200.initcond import maxwellian_values
+    rho, T = rng.uniform(0.5, 2.0), rng.uniform(0.5, 3.0)
+    u = _ball(rng)
+    if not bimodal:
+        return maxwellian_values(vm, rho, T, u)
+    f = 0.5*(maxwellian_values(vm, 1.0, T, u) +
+             maxwellian_values(vm, 1.0, T, -u))
+    return f*rho/(np.sum(f)*vm.cw())
+
+
+def random_point_states(vm, n, rng):
+    """n positive distributions spanning far from and near equilibrium:
+    two-Maxwellian mixtures (random weights, velocities in the unit ball,
+    temperatures in [0.5, 3]) and anisotropic Gaussians (one temperature per
+    axis), with densities in [0.5, 2]; shape (n, V)."""
+    cv = vm.cv()
+    out = np.empty((n, cv.shape[1]))
+    for i in range(n):
+        if rng.uniform() < 0.6:
+            w = rng.uniform(0.2, 0.8)
+            f = 0.0
+            for wk in (w, 1 - w):
+                T = rng.uniform(0.5, 3.0)
+                u = _ball(rng)
+                f = f + wk*np.exp(-np.sum((cv - u[:, None])**2, axis=0)/T) \
+                    / (np.pi*T)**1.5
+        else:
+            Tk = rng.uniform(0.5, 3.0)*rng.uniform(0.6, 1.4, 3)
+            u = _ball(rng)
+            f = np.exp(-np.sum((cv - u[:, None])**2/Tk[:, None], axis=0)) \
+                / np.sqrt(np.pi**3*np.prod(Tk))
+        out[i] = f*rng.uniform(0.5, 2.0)/(np.sum(f)*vm.cw())
+    return out
+
+
+class Harvester:
+    """Collects (features, targets) of every (f, Q) pair it is called with
+    (installed as ``system.collide_hook``), keeping points with
+    eps < eps_max."""
+
+    def __init__(self, sur, eps_max):
+        self.sur = sur
+        self.eps_max = eps_max
+        self.X, self.B = [], []
+        self.seen = 0
+
+    def __call__(self, fbank, qbank):
+        X, B, _, eps = self.sur.embed(fbank, qbank)
+        keep = eps < self.eps_max
+        self.X.append(X[keep])
+        self.B.append(B[keep])
+        self.seen += eps.numel()
+
+    def data(self):
+        return torch.cat(self.X), torch.cat(self.B)
+
+
+def _subsample(X, B, max_pairs, seed):
+    if max_pairs is not None and X.shape[0] > max_pairs:
+        g = torch.Generator(device='cpu').manual_seed(seed)
+        idx = torch.randperm(X.shape[0], generator=g)[:max_pairs].to(X.device)
+        X, B = X.index_select(0, idx), B.index_select(0, idx)
+    return X, B
+
+
+def harvest(system, stepper_cls, sur, runs, steps, seed=1, eps_max=0.2,
+            bimodal_every=3, max_pairs=None):
+    """Run ``runs`` trajectories of ``steps`` steps of the plain solver from
+    random uniform initial states (seeds seed .. seed+runs-1; every
+    ``bimodal_every``-th is a bimodal mixture) and collect the (f, Q(f))
+    pairs of every collide (a seeded random subset of ``max_pairs`` when
+    given).  Returns X, B on the device."""
+    h = Harvester(sur, eps_max)
+    vm = system.vm
+    shape = system.bank[0].ioshape
+    old_hook, old_sur = system.collide_hook, system.surrogate
+    system.collide_hook, system.surrogate = h, None
+    try:
+        for r in range(runs):
+            rng = np.random.default_rng(seed + r)
+            f = random_uniform_state(vm, rng, (r % bimodal_every) ==
+                                     bimodal_every - 1)
+            system.bank[0].set(np.broadcast_to(f[None, :, None], shape))
+            st = stepper_cls(system, system.cfg)
+            st.use_graphs = False
+            st.advance(steps)
+    finally:
+        system.collide_hook, system.surrogate = old_hook, old_sur
+    return _subsample(*h.data(), max_pairs, seed)
+
+
+def harvest_relaxation(sm, sur, npts, steps, dt, seed=0, eps_max=0.2,
+                       nupts=1, max_pairs=None):
+    """(f, Q(f)) pairs along space-homogeneous relaxations (SSP-RK2 of
+    df/dt = Q(f), plain operator) of ``npts`` random states
+    (random_point_states), so that the data cover the whole path from far
+    from equilibrium to equilibrium.  Training-data utility: its RK
+    combinations are PyTorch element-wise operations on the banks."""
+    be, vm = sm.backend, sm.vm
+    rng = np.random.default_rng(seed)
+    neles = -(-npts//nupts)
+    f0 = random_point_states(vm, nupts*neles, rng)
+    shape = (nupts, vm.vsize(), neles)
+    f = be.matrix(shape, f0.reshape(nupts, neles, -1).transpose(0, 2, 1))
+    f1, q = be.matrix(shape), be.matrix(shape)
+    h = Harvester(sur, eps_max)
+    for _ in range(steps):
+        sm.fs_all(f, q)
+        h(f, q)
+        f1.data.copy_(f.data).add_(q.data, alpha=dt)
+        sm.fs_all(f1, q)
+        h(f1, q)
+        f.data.mul_(0.5).add_(f1.data, alpha=0.5).add_(q.data, alpha=0.5*dt)
+    return _subsample(*h.data(), max_pairs, seed)

@@ -121,6 +121,8 @@ class DGFSSystem:
         djac = geo.djac_at(sh.upts)
         self.unit_cfl_dt = float(np.sqrt(djac.min())/vm.L()/self.ndims)
 
+        self.surrogate = None
+        self.collide_hook = None
         self._build_dg()
 
     # -- DG handle ----------------------------------------------------------
@@ -227,8 +229,24 @@ class DGFSSystem:
         return int(varidx), nvbs
 
     def collide(self, t, uinbank, foutbank):
-        """Q(f) at every solution point (system.py:199-218)."""
-        self.sm.fs_all(self.bank[uinbank], self.bank[foutbank])
+        """Q(f) at every solution point (system.py:199-218); through the
+        attached learned surrogate (with its plain fallback) when
+        ``self.surrogate`` is set.  ``collide_hook(fin, fout)``, when set,
+        sees every (f, Q) pair (training-data collection)."""
+        fin, fout = self.bank[uinbank], self.bank[foutbank]
+        if self.surrogate is not None:
+            self.surrogate.collide(fin, fout)
+        else:
+            self.sm.fs_all(fin, fout)
+        if self.collide_hook is not None:
+            self.collide_hook(fin, fout)
+
+    @property
+    def graph_key(self):
+        """Part of a captured stage's key that changes with the collision
+        path (plain, or a surrogate and its threshold)."""
+        s = self.surrogate
+        return None if s is None else (id(s), s.threshold)
 
     def updatebc(self, t, uinbank, foutbank, batch, varidx):
         """Face values of the slice and the diffuse-wall sums; the sums are

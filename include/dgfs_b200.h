@@ -102,6 +102,17 @@ DGFS_API int dgfs_vhs_apply_range(dgfs_vhs* h, const void* f, void* Q, int nupts
                          int neles, long long ldim, int soasz, int pt0,
                          int npts, void* stream);
 
+/* Q(f) at the points of a device list pts[0 .. n), point id =
+ * upt*neles + elem, n = min(max_points, *count) when `count` (a device int
+ * written by an earlier kernel) is given, else max_points.  Listed ids
+ * outside the bank are skipped.  The count is read on the device, so a gate
+ * kernel can choose the points without a host round trip.  Used by the
+ * learned surrogate's plain fallback; no counterpart in the reference. */
+DGFS_API int dgfs_vhs_apply_list(dgfs_vhs* h, const void* f, void* Q, int nupts,
+                                 int neles, long long ldim, int soasz,
+                                 const int* pts, const int* count,
+                                 int max_points, void* stream);
+
 /* Launch geometry chosen by the handle (for reporting and tuning). */
 DGFS_API int dgfs_vhs_info(const dgfs_vhs* h, int* cluster, int* threads,
                   int* smem_bytes, int* max_clusters);
@@ -238,6 +249,76 @@ DGFS_API int dgfs_dg_fpts(const dgfs_dg* h, void** ptr, long long* ldim);
 DGFS_API int dgfs_moments(int precision, const void* f, int nupts, int neles,
                           long long ldim, int Nv, double L, double cw,
                           double* out, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Learned collision surrogate (no counterpart in the reference)
+ *
+ * Per point: FP64 frame rho, u, T (the formulas of dgfs_moments);
+ * c^ = (c - u)/sqrt(T); phi_n(x) = He_n(sqrt(2) x)/sqrt(n!); 220 modes
+ * (i, j, k), i + j + k <= 9, ordered by degree, then i, then j (both
+ * descending).  Feature row X[pt][256]: a_k = cw/rho sum_v f phi_k(c^_v)
+ * (k < 220), sqrt(T)/L, ux/L, uy/L, uz/L, zeros.  Target row B[pt][256]:
+ * b_k = cw sum_v Q phi_k(c^_v) / (prefactor rho^2 T^{gamma/2}).  mom[pt][5]
+ * = rho, ux, uy, uz, T; eps[pt] = |a_k, degree >= 2| (non-equilibrium
+ * measure).  Nv <= 32, soasz 32.  All pointers are device pointers; point
+ * id pt = upt*neles + elem.
+ * ---------------------------------------------------------------------- */
+DGFS_API int dgfs_hermite_embed(int precision, const void* f, const void* Q,
+                                int nupts, int neles, long long ldim, int Nv,
+                                double L, double cw, double prefactor,
+                                double gamma, float* X, float* B, double* mom,
+                                float* eps, void* stream);
+
+/* Q(c) = prefactor rho^2 T^{gamma/2} T^{-3/2} pi^{-3/2} e^{-|c^|^2}
+ * sum_k B[pt][k] phi_k(c^), then the FP64 projection onto zero mass,
+ * momentum and energy with the 5x5 inverse Gram matrix ginv of
+ * (1, c, |c|^2) on the grid; written only where gate[pt] != 0 (all points
+ * when gate is NULL). */
+DGFS_API int dgfs_hermite_reconstruct(int precision, const float* B,
+                                      const double* mom, const int* gate,
+                                      int nupts, int neles, long long ldim,
+                                      int Nv, double L, double cw,
+                                      double prefactor, double gamma,
+                                      const double* ginv, void* Q,
+                                      void* stream);
+
+/* gate[pt] = eps[pt] < threshold; the other points are appended to
+ * plain[0 .. *nplain) (unordered) for dgfs_vhs_apply_list. */
+DGFS_API int dgfs_surrogate_gate(int npts, const float* eps, float threshold,
+                                 int* gate, int* plain, int* nplain,
+                                 void* stream);
+
+/* Surrogate MLP kernels (FP32 accumulation; B operand FP32 or BF16):
+ * C[m*ldc+n] = act(sum_k A[m*sam+k*sak] B[k*sbk+n*sbn] + bias[n]) (+ C),
+ * act 0 identity, 1 tanh; Z (optional) receives the pre-activation. */
+DGFS_API int dgfs_mlp_gemm(int M, int N, int K, const float* A, long long sam,
+                           long long sak, const void* B, int b_bf16,
+                           long long sbk, long long sbn, const float* bias,
+                           float* Z, float* C, long long ldc, int act,
+                           int accumulate, void* stream);
+/* dZ = dH (1 - H^2) */
+DGFS_API int dgfs_mlp_tanh_bwd(long long n, const float* H, const float* dH,
+                               float* dZ, void* stream);
+/* out[n] (+)= sum_m X[m*ldx+n], fixed order */
+DGFS_API int dgfs_mlp_colsum(int M, int N, const float* X, long long ldx,
+                             float* out, int accumulate, void* stream);
+/* rowloss[m] = sum_{n<nused} w_n (Y-T)^2, dY = 2 w (Y-T)/(M nused) (0 for
+ * n >= nused); w may be NULL. */
+DGFS_API int dgfs_mlp_mse(int M, int N, int nused, const float* Y,
+                          const float* T, const float* w, float* dY,
+                          double* rowloss, void* stream);
+/* Adam with bias correction; L2 weight decay is added to the gradient
+ * (g + wd w); refreshes the BF16 copy wbf16 when not NULL. */
+DGFS_API int dgfs_mlp_adam(long long n, float* w, void* wbf16, const float* g,
+                           float* m1, float* m2, float lr, float beta1,
+                           float beta2, float eps, int step,
+                           float weight_decay, void* stream);
+/* Y = (X - mu) inv_sigma per column, or X / inv_sigma + mu (inverse). */
+DGFS_API int dgfs_mlp_affine(int M, int N, const float* X, const float* mu,
+                             const float* inv_sigma, float* Y, int inverse,
+                             void* stream);
+DGFS_API int dgfs_f32_to_bf16(long long n, const float* x, void* y,
+                              void* stream);
 
 /* ------------------------------------------------------------------------
  * Measurement helper (no counterpart in the reference)

@@ -1,0 +1,124 @@
+# -*- coding: utf-8 -*-
+"""FP64 restatement of the collision surrogate's pieces -- TEST
+INFRASTRUCTURE ONLY (see ``oracle/__init__.py``).
+
+The surrogate has no counterpart in the reference; these functions define
+what the B200 kernels must compute so that their results and gradients can
+be checked: the Hermite embedding of a distribution in its local frame, the
+reconstruction of Q from Hermite coefficients with the conservation
+projection, and the MLP forward/backward pass.  The frame moments follow
+frfs/plugins/dgfsmomwriterstd.py:154-190 (nondimensional).
+"""
+
+from math import factorial
+
+import numpy as np
+
+from oracle.vhs import project_conservative
+
+DEG = 9
+
+
+def modes(deg=DEG):
+    """(i, j, k) with i+j+k <= deg, ordered by degree, then i, then j
+    (descending), as the device tables."""
+    out = []
+    for d in range(deg + 1):
+        for i in range(d, -1, -1):
+            for j in range(d - i, -1, -1):
+                out.append((i, j, d - i - j))
+    return out
+
+
+def phi(n, x):
+    """phi_n(x) = He_n(sqrt(2) x)/sqrt(n!) (probabilists' Hermite)."""
+    y = np.sqrt(2.0)*x
+    p = [np.ones_like(y), y]
+    for k in range(1, n):
+        p.append(y*p[k] - k*p[k - 1])
+    return p[n]/np.sqrt(factorial(n))
+
+
+def frame(f, cv, cw):
+    f = np.asarray(f, np.float64)
+    m0 = f.sum()
+    u = (cv*f).sum(axis=1)/m0
+    c = cv - u[:, None]
+    T = (f*np.sum(c*c, axis=0)).sum()*(2.0/3.0)/m0
+    return m0*cw, u, T
+
+
+def basis(cv, u, T, deg=DEG):
+    ch = (cv - u[:, None])/np.sqrt(T)
+    return np.stack([np.prod([phi(m[a], ch[a]) for a in range(3)], axis=0)
+                     for m in modes(deg)])                      # (nmodes, V)
+
+
+def embed(f, cv, cw, L, Q=None, prefac=1.0, gamma=0.0):
+    """Features x (256), frame (rho, u, T), eps and (if Q) targets b (256)."""
+    rho, u, T = frame(f, cv, cw)
+    Phi = basis(cv, u, T)
+    a = Phi @ np.asarray(f, np.float64)*cw/rho
+    x = np.zeros(256)
+    x[:len(a)] = a
+    x[len(a)] = np.sqrt(T)/L
+    x[len(a) + 1:len(a) + 4] = u/L
+    deg = np.array([sum(m) for m in modes()])
+    eps = np.sqrt(np.sum(a[deg >= 2]**2))
+    b = None
+    if Q is not None:
+        b = np.zeros(256)
+        b[:len(a)] = Phi @ np.asarray(Q, np.float64)*cw/(
+            prefac*rho*rho*T**(0.5*gamma))
+    return x, (rho, u, T), eps, b
+
+
+def reconstruct(b, mom, cv, prefac=1.0, gamma=0.0):
+    rho, u, T = mom
+    Phi = basis(cv, u, T)
+    ch2 = np.sum(((cv - u[:, None])/np.sqrt(T))**2, axis=0)
+    W = np.pi**-1.5*np.exp(-ch2)
+    Q = prefac*rho*rho*T**(0.5*gamma)*T**-1.5*W*(
+        np.asarray(b[:Phi.shape[0]], np.float64) @ Phi)
+    return project_conservative(Q, cv)
+
+
+# --------------------------------------------------------------------------
+# MLP: x -> tanh(W1) -> tanh(W2) -> tanh(W3) -> W4 (+ Ws x); W[in][out]
+# --------------------------------------------------------------------------
+def mlp_forward(params, X):
+    W1, b1, W2, b2, W3, b3, W4, b4, Ws = params
+    H1 = np.tanh(X @ W1 + b1)
+    H2 = np.tanh(H1 @ W2 + b2)
+    H3 = np.tanh(H2 @ W3 + b3)
+    Y = H3 @ W4 + b4 + X @ Ws
+    return Y, (X, H1, H2, H3)
+
+
+def mlp_backward(params, cache, dY):
+    W1, b1, W2, b2, W3, b3, W4, b4, Ws = params
+    X, H1, H2, H3 = cache
+    g = {}
+    g['W4'] = H3.T @ dY
+    g['b4'] = dY.sum(axis=0)
+    g['Ws'] = X.T @ dY
+    dZ3 = (dY @ W4.T)*(1 - H3**2)
+    g['W3'] = H2.T @ dZ3
+    g['b3'] = dZ3.sum(axis=0)
+    dZ2 = (dZ3 @ W3.T)*(1 - H2**2)
+    g['W2'] = H1.T @ dZ2
+    g['b2'] = dZ2.sum(axis=0)
+    dZ1 = (dZ2 @ W2.T)*(1 - H1**2)
+    g['W1'] = X.T @ dZ1
+    g['b1'] = dZ1.sum(axis=0)
+    return g
+
+
+def mse(Y, T, nused, w=None):
+    d = (Y - T)[:, :nused]
+    wt = np.ones(nused) if w is None else np.asarray(w)[:nused]
+    M = Y.shape[0]
+    loss = np.sum(wt*d*d)/(M*nused)
+    dY = np.zeros_like(Y)
+    dY[:, :nused] = 2*wt*d/(M*nused)
+    return loss, dY

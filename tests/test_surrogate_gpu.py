@@ -1,0 +1,321 @@
+# -*- coding: utf-8 -*-
+"""Kernels of the learned collision surrogate against the FP64 oracle
+(GPU): Hermite embedding and reconstruction, gate and device point list,
+the MLP's forward/backward/Adam kernels, and the assembled collide path.
+
+Tolerances:
+  embedding features/targets (FP32 outputs): 1e-5 normwise relative;
+  frame moments (FP64): 1e-12;
+  reconstruction: 1e-10 (FP64 banks), 2e-6 (FP32 banks);
+  MLP gradients (BF16 weights, FP32 accumulation) against FP64 with the
+  same BF16-rounded weights: 1e-4 normwise relative per tensor.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from helpers import config, random_states, rel_err
+from frfs_b200 import _lib
+from frfs_b200.backend import B200Backend
+from frfs_b200.scattering import DGFSVHSGLLScatteringModel
+from frfs_b200.surrogate import MLP, VHSSurrogate, NFEAT, NMODES
+from frfs_b200.velocitymesh import DGFSVelocityMesh
+from oracle import surrogate as osur
+from oracle import vhs as ovhs
+
+pytestmark = pytest.mark.gpu
+
+
+def _model(precision, name='couette-n24'):
+    cfg = config(name, precision)
+    be = B200Backend(cfg, device='cuda:0')
+    vm = DGFSVelocityMesh(be, cfg)
+    return be, vm, DGFSVHSGLLScatteringModel(be, cfg, vm)
+
+
+def _bank(be, f):
+    nupts, neles, V = f.shape
+    return be.matrix((nupts, V, neles),
+                     np.ascontiguousarray(f.transpose(0, 2, 1)))
+
+
+def _near_eq(cv, n, seed, amp=0.02):
+    """Maxwellians with random moments times a smooth small deviation."""
+    rng = np.random.default_rng(seed)
+    out = np.empty((n, cv.shape[1]))
+    for i in range(n):
+        rho, T = rng.uniform(0.6, 1.8), rng.uniform(0.7, 1.5)
+        u = rng.uniform(-0.3, 0.3, 3)
+        c = (cv - u[:, None])/np.sqrt(T)
+        h = amp*(rng.standard_normal()*c[0]*c[1] +
+                 rng.standard_normal()*c[2]*(np.sum(c*c, axis=0) - 2.5))
+        out[i] = ovhs.maxwellian(cv, rho, u, T)*(1 + h)
+    return out
+
+
+@pytest.mark.parametrize('precision', ['double', 'single'])
+def test_embed_matches_oracle(precision):
+    be, vm, sm = _model(precision)
+    cv, cw = vm.cv(), vm.cw()
+    nupts, neles = 2, 5
+    f = random_states(cv, nupts*neles, seed=3).reshape(nupts, neles, -1)
+    q = random_states(cv, nupts*neles, seed=4).reshape(nupts, neles, -1)
+    fb, qb = _bank(be, f), _bank(be, q)
+    sur = VHSSurrogate(sm)
+    X, B, mom, eps = sur.embed(fb, qb)
+    torch.cuda.synchronize()
+    X, B, mom, eps = (t.cpu().numpy() for t in (X, B, mom, eps))
+    fu, qu = fb.get().astype(np.float64), qb.get().astype(np.float64)
+    for u in range(nupts):
+        for e in range(neles):
+            pt = u*neles + e
+            x, (rho, uu, T), ep, b = osur.embed(
+                fu[u, :, e], cv, cw, vm.L(), Q=qu[u, :, e],
+                prefac=sm.prefactor, gamma=sm._gamma)
+            assert rel_err(mom[pt], np.r_[rho, uu, T]) < 1e-12
+            assert rel_err(X[pt], x) < 1e-5
+            assert rel_err(B[pt], b) < 1e-5
+            assert abs(eps[pt] - ep) < 1e-5*ep
+
+
+@pytest.mark.parametrize('precision', ['double', 'single'])
+def test_reconstruct_matches_oracle_and_gate(precision):
+    be, vm, sm = _model(precision)
+    cv = vm.cv()
+    nupts, neles = 2, 3
+    npts = nupts*neles
+    rng = np.random.default_rng(8)
+    deg = np.array([sum(t) for t in osur.modes()])
+    Bp = np.zeros((npts, NFEAT), np.float32)
+    Bp[:, :NMODES] = rng.standard_normal((npts, NMODES))*0.5**deg
+    mom = np.c_[rng.uniform(0.5, 2, npts), rng.uniform(-0.3, 0.3, (npts, 3)),
+                rng.uniform(0.7, 1.5, npts)]
+    gate = np.array([1, 0, 1, 1, 0, 1], np.int32)
+    dev = be.device
+    out = be.matrix((nupts, vm.vsize(), neles))
+    sur = VHSSurrogate(sm)
+    d_b = torch.tensor(Bp, device=dev)
+    d_mom = torch.tensor(mom, device=dev)
+    d_gate = torch.tensor(gate, device=dev)
+    _lib.check(_lib.load().dgfs_hermite_reconstruct(
+        be.precision, d_b.data_ptr(), d_mom.data_ptr(), d_gate.data_ptr(),
+        nupts, neles, out.traits[1], vm.Nv(), vm.L(), vm.cw(), sm.prefactor,
+        sm._gamma, sur.ginv.data_ptr(), out._as_parameter_, be.stream),
+        'dgfs_hermite_reconstruct')
+    torch.cuda.synchronize()
+    Q = out.get()
+    tol = 1e-10 if precision == 'double' else 2e-6
+    for pt in range(npts):
+        u, e = divmod(pt, neles)
+        if not gate[pt]:
+            assert np.all(Q[u, :, e] == 0)
+            continue
+        Qo = osur.reconstruct(Bp[pt].astype(np.float64),
+                              (mom[pt, 0], mom[pt, 1:4], mom[pt, 4]), cv,
+                              sm.prefactor, sm._gamma)
+        assert rel_err(Q[u, :, e], Qo) < tol
+
+
+def test_gate_builds_the_plain_list():
+    dev = torch.device('cuda:0')
+    rng = np.random.default_rng(2)
+    eps = rng.uniform(0, 0.1, 1000).astype(np.float32)
+    e = torch.tensor(eps, device=dev)
+    gate = torch.empty(1000, dtype=torch.int32, device=dev)
+    plain = torch.full((1000,), -1, dtype=torch.int32, device=dev)
+    n = torch.empty(1, dtype=torch.int32, device=dev)
+    s = torch.cuda.current_stream().cuda_stream
+    _lib.check(_lib.load().dgfs_surrogate_gate(
+        1000, e.data_ptr(), 0.05, gate.data_ptr(), plain.data_ptr(),
+        n.data_ptr(), s), 'dgfs_surrogate_gate')
+    torch.cuda.synchronize()
+    g = gate.cpu().numpy()
+    assert np.array_equal(g, (eps < np.float32(0.05)).astype(np.int32))
+    k = int(n.item())
+    assert k == int(np.sum(g == 0))
+    assert sorted(plain.cpu().numpy()[:k]) == list(np.nonzero(g == 0)[0])
+
+
+@pytest.mark.parametrize('precision', ['double', 'single'])
+def test_apply_list_matches_apply(precision):
+    be, vm, sm = _model(precision, 'couette-n24' if precision == 'single'
+                        else 'relax0d-n16')
+    nupts, neles = 3, 37
+    npts = nupts*neles
+    f = random_states(vm.cv(), npts, seed=5).reshape(nupts, neles, -1)
+    fin = _bank(be, f)
+    full = be.matrix(fin.ioshape)
+    sm.fs_all(fin, full)
+    rng = np.random.default_rng(1)
+    pts = rng.permutation(npts)[:17].astype(np.int32)
+    pts_bad = np.r_[pts, npts + 5, -1].astype(np.int32)  # skipped entries
+    dev = be.device
+    d_pts = torch.tensor(pts_bad, device=dev)
+    lib = _lib.load()
+    ldim = fin.traits[1]
+    out = be.matrix(fin.ioshape)
+    _lib.check(lib.dgfs_vhs_apply_list(
+        sm._h, fin._as_parameter_, out._as_parameter_, nupts, neles, ldim,
+        be.soasz, d_pts.data_ptr(), None, len(pts_bad), be.stream),
+        'dgfs_vhs_apply_list')
+    # a device count caps the list at its first 5 entries
+    cnt = torch.tensor([5], dtype=torch.int32, device=dev)
+    out2 = be.matrix(fin.ioshape)
+    _lib.check(lib.dgfs_vhs_apply_list(
+        sm._h, fin._as_parameter_, out2._as_parameter_, nupts, neles, ldim,
+        be.soasz, d_pts.data_ptr(), cnt.data_ptr(), len(pts), be.stream),
+        'dgfs_vhs_apply_list')
+    sm.status()
+    Qf, Ql, Q5 = full.get(), out.get(), out2.get()
+    for pt in range(npts):
+        u, e = divmod(pt, neles)
+        if pt in pts:
+            assert np.array_equal(Ql[u, :, e], Qf[u, :, e])
+        else:
+            assert np.all(Ql[u, :, e] == 0)
+        if pt in pts[:5]:
+            assert np.array_equal(Q5[u, :, e], Qf[u, :, e])
+        else:
+            assert np.all(Q5[u, :, e] == 0)
+    with pytest.raises(_lib.DgfsError):
+        _lib.check(lib.dgfs_vhs_apply_list(
+            sm._h, fin._as_parameter_, out._as_parameter_, nupts, neles,
+            ldim, be.soasz, None, None, 3, be.stream), 'dgfs_vhs_apply_list')
+
+
+def _bf16(t):
+    return t.to(torch.bfloat16).to(torch.float64).cpu().numpy()
+
+
+def test_mlp_gradients_match_oracle():
+    dev = torch.device('cuda:0')
+    mlp = MLP(dev, seed=4)
+    rng = np.random.default_rng(6)
+    for k in ('b1', 'b2', 'b3', 'b4'):
+        mlp.w[k].copy_(torch.tensor(0.1*rng.standard_normal(mlp.w[k].shape)))
+    mlp.w['Ws'].copy_(torch.tensor(
+        0.05*rng.standard_normal(mlp.w['Ws'].shape)))
+    mlp.sync_bf16()
+    Bt = 70                                   # not a multiple of the tile
+    X = torch.tensor(rng.standard_normal((Bt, NFEAT)), dtype=torch.float32,
+                     device=dev)
+    T = torch.tensor(rng.standard_normal((Bt, NFEAT)), dtype=torch.float32,
+                     device=dev)
+    w = torch.tensor(rng.uniform(0.5, 2, NFEAT), dtype=torch.float32,
+                     device=dev)
+    Y = mlp.forward(X, keep=True)
+    dY = torch.empty_like(Y)
+    rl = torch.empty(Bt, dtype=torch.float64, device=dev)
+    _lib.check(_lib.load().dgfs_mlp_mse(
+        Bt, NFEAT, NMODES, Y.data_ptr(), T.data_ptr(), w.data_ptr(),
+        dY.data_ptr(), rl.data_ptr(), torch.cuda.current_stream().cuda_stream),
+        'dgfs_mlp_mse')
+    g = mlp.backward(dY)
+    torch.cuda.synchronize()
+    P = [(_bf16(mlp.w[k]) if k.startswith('W') else
+          mlp.w[k].double().cpu().numpy()) for k in MLP.names]
+    Xn = X.double().cpu().numpy()
+    Yo, cache = osur.mlp_forward(P, Xn)
+    loss, dYo = osur.mse(Yo, T.double().cpu().numpy(), NMODES,
+                         w.double().cpu().numpy())
+    assert rel_err(Y.cpu().numpy(), Yo) < 1e-4
+    assert abs(float(rl.sum())/(Bt*NMODES) - loss) < 1e-4*loss
+    go = osur.mlp_backward(P, cache, dYo)
+    for k in MLP.names:
+        assert rel_err(g[k].cpu().numpy(), go[k]) < 1e-4, k
+
+
+def test_adam_step_matches_formula():
+    dev = torch.device('cuda:0')
+    rng = np.random.default_rng(9)
+    n = 1000
+    w0, g0 = rng.standard_normal(n), rng.standard_normal(n)
+    w = torch.tensor(w0, dtype=torch.float32, device=dev)
+    wb = torch.empty(n, dtype=torch.bfloat16, device=dev)
+    g = torch.tensor(g0, dtype=torch.float32, device=dev)
+    m1, m2 = torch.zeros_like(w), torch.zeros_like(w)
+    s = torch.cuda.current_stream().cuda_stream
+    lib = _lib.load()
+    mo1, mo2 = np.zeros(n), np.zeros(n)
+    wo = w0.astype(np.float32).astype(np.float64)
+    for step in (1, 2, 3):
+        _lib.check(lib.dgfs_mlp_adam(n, w.data_ptr(), wb.data_ptr(),
+                                     g.data_ptr(), m1.data_ptr(),
+                                     m2.data_ptr(), 1e-2, 0.9, 0.999, 1e-8,
+                                     step, 1e-3, s), 'dgfs_mlp_adam')
+        gi = g0.astype(np.float32) + 1e-3*wo
+        mo1 = 0.9*mo1 + 0.1*gi
+        mo2 = 0.999*mo2 + 0.001*gi*gi
+        wo = wo - 1e-2*(mo1/(1 - 0.9**step))/(np.sqrt(mo2/(1 - 0.999**step))
+                                              + 1e-8)
+    torch.cuda.synchronize()
+    assert np.max(np.abs(w.cpu().numpy() - wo)) < 1e-5
+    assert torch.equal(wb, w.to(torch.bfloat16))
+
+
+def test_training_reduces_loss():
+    """A learnable synthetic map (linear part plus a tanh part) is fitted
+    by the project's kernels: the loss falls by more than 10x."""
+    dev = torch.device('cuda:0')
+    be, vm, sm = _model('single')
+    sur = VHSSurrogate(sm, seed=1)
+    rng = np.random.default_rng(0)
+    n = 8192
+    Xh = rng.standard_normal((n, NFEAT))
+    A = rng.standard_normal((NFEAT, NFEAT))/np.sqrt(NFEAT)
+    C = rng.standard_normal((NFEAT, NFEAT))/np.sqrt(NFEAT)
+    Yh = Xh @ A + 0.3*np.tanh(Xh @ C)
+    X = torch.tensor(Xh, dtype=torch.float32, device=dev)
+    Y = torch.tensor(Yh, dtype=torch.float32, device=dev)
+    sur.set_normalisation(X, Y)
+    hist = sur.train(X, Y, epochs=20, batch=512, lr=2e-3)
+    assert hist[-1] < 0.1*hist[0], hist
+
+
+def test_collide_routes_points_and_conserves():
+    """threshold 0: every point takes the plain operator (bit-identical to
+    fs_all); threshold huge: every point takes the network and its Q has
+    zero mass, momentum and energy; in between the routing follows eps."""
+    be, vm, sm = _model('single')
+    cv = vm.cv()
+    nupts, neles = 3, 12
+    npts = nupts*neles
+    f = np.concatenate([_near_eq(cv, npts - 8, seed=2),
+                        random_states(cv, 8, seed=3)]).reshape(
+                            nupts, neles, -1)
+    fb = _bank(be, f)
+    ref = be.matrix(fb.ioshape)
+    sm.fs_all(fb, ref)
+    sur = VHSSurrogate(sm, seed=0)
+    out = be.matrix(fb.ioshape)
+    g = sur.collide(fb, out, threshold=0.0)
+    torch.cuda.synchronize()
+    assert int(g.sum()) == 0
+    assert np.array_equal(out.get(), ref.get())
+
+    out2 = be.matrix(fb.ioshape)
+    g = sur.collide(fb, out2, threshold=1e30)
+    torch.cuda.synchronize()
+    assert int(g.sum()) == npts
+    Q = out2.get().astype(np.float64)
+    phi = np.vstack([np.ones(cv.shape[1]), cv, np.sum(cv*cv, axis=0)])
+    for u in range(nupts):
+        for e in range(neles):
+            m = phi @ Q[u, :, e]
+            scale = np.abs(phi) @ np.abs(Q[u, :, e])
+            assert np.all(np.abs(m) < 1e-5*scale)
+
+    _, _, _, eps = sur.embed(fb)
+    e = eps.cpu().numpy()
+    thr = float(np.median(e))
+    out3 = be.matrix(fb.ioshape)
+    g = sur.collide(fb, out3, threshold=thr).cpu().numpy()
+    torch.cuda.synchronize()
+    assert np.array_equal(g, (e < np.float32(thr)).astype(np.int32))
+    Q3, Qr, Q2 = out3.get(), ref.get(), out2.get()
+    for pt in range(npts):
+        u, el = divmod(pt, neles)
+        want = Q2 if g[pt] else Qr
+        assert np.array_equal(Q3[u, :, el], want[u, :, el])
+    assert sur.residual_check(fb, out3, be.matrix(fb.ioshape)) > 0

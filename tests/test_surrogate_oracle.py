@@ -1,0 +1,111 @@
+# -*- coding: utf-8 -*-
+"""Self-consistency of the surrogate's FP64 oracle (CPU): the Hermite basis,
+the embedding/reconstruction pair and the MLP gradients that the GPU
+kernels are checked against."""
+
+import numpy as np
+
+from helpers import config
+from frfs_b200.velocitymesh import DGFSVelocityMesh
+from oracle import surrogate as osur
+from oracle import vhs as ovhs
+
+
+def _vm():
+    return DGFSVelocityMesh(None, config('couette-n24'))
+
+
+def test_modes_count_and_order():
+    m = osur.modes()
+    assert len(m) == 220 and len(set(m)) == 220
+    deg = [sum(t) for t in m]
+    assert deg == sorted(deg)
+    assert m[:4] == [(0, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1)]
+
+
+def test_phi_orthonormal():
+    x, w = np.polynomial.hermite.hermgauss(30)
+    w = w/np.sqrt(np.pi)
+    G = np.array([[np.sum(w*osur.phi(m, x)*osur.phi(n, x))
+                   for n in range(10)] for m in range(10)])
+    assert np.max(np.abs(G - np.eye(10))) < 1e-12
+
+
+def test_embedding_of_a_maxwellian():
+    vm = _vm()
+    cv, cw = vm.cv(), vm.cw()
+    f = ovhs.maxwellian(cv, 1.3, [0.2, -0.1, 0.05], 1.2)
+    x, (rho, u, T), eps, _ = osur.embed(f, cv, cw, vm.L())
+    assert abs(rho - 1.3) < 1e-6 and abs(T - 1.2) < 1e-6
+    assert np.max(np.abs(u - [0.2, -0.1, 0.05])) < 1e-6
+    assert abs(x[0] - 1.0) < 1e-12
+    assert np.max(np.abs(x[1:4])) < 1e-12      # first moments vanish exactly
+    assert eps < 1e-6
+    assert abs(x[220] - np.sqrt(T)/vm.L()) < 1e-15
+
+
+def test_reconstruct_then_embed_round_trip():
+    """Coefficients with zero mass, momentum and energy survive
+    reconstruction (incl. the projection) and re-embedding."""
+    vm = _vm()
+    cv, cw = vm.cv(), vm.cw()
+    rng = np.random.default_rng(3)
+    deg = np.array([sum(t) for t in osur.modes()])
+    b = np.zeros(256)
+    b[:220] = rng.standard_normal(220)*0.5**deg
+    b[:4] = 0.0
+    tr = [osur.modes().index(t) for t in ((2, 0, 0), (0, 2, 0), (0, 0, 2))]
+    b[tr] -= b[tr].mean()
+    mom = (1.1, np.array([0.1, 0.0, -0.2]), 0.9)
+    prefac, gamma = 0.7, 0.38
+    Q = osur.reconstruct(b, mom, cv, prefac, gamma)
+    f = ovhs.maxwellian(cv, mom[0], mom[1], mom[2])
+    _, _, _, b2 = osur.embed(f, cv, cw, vm.L(), Q=Q, prefac=prefac,
+                             gamma=gamma)
+    # grid quadrature of degree-18 polynomials times the Gaussian weight
+    assert np.max(np.abs(b2[:220] - b[:220])) < 1e-6*np.max(np.abs(b))
+    phi = np.vstack([np.ones(cv.shape[1]), cv, np.sum(cv*cv, axis=0)])
+    assert np.max(np.abs(phi @ Q)) < 1e-12*np.max(np.abs(Q))*cv.shape[1]
+
+
+def _params(rng, nin, wd, nout):
+    return [rng.standard_normal((nin, wd))/np.sqrt(nin),
+            0.1*rng.standard_normal(wd),
+            rng.standard_normal((wd, wd))/np.sqrt(wd),
+            0.1*rng.standard_normal(wd),
+            rng.standard_normal((wd, wd))/np.sqrt(wd),
+            0.1*rng.standard_normal(wd),
+            rng.standard_normal((wd, nout))/np.sqrt(wd),
+            0.1*rng.standard_normal(nout),
+            0.1*rng.standard_normal((nin, nout))]
+
+
+def test_mlp_backward_matches_finite_differences():
+    rng = np.random.default_rng(0)
+    nin, wd, nout, B = 7, 6, 5, 4
+    P = _params(rng, nin, wd, nout)
+    X = rng.standard_normal((B, nin))
+    T = rng.standard_normal((B, nout))
+    w = rng.uniform(0.5, 2.0, nout)
+
+    def loss(P):
+        Y, _ = osur.mlp_forward(P, X)
+        return osur.mse(Y, T, nout - 1, w)[0]
+
+    Y, cache = osur.mlp_forward(P, X)
+    _, dY = osur.mse(Y, T, nout - 1, w)
+    g = osur.mlp_backward(P, cache, dY)
+    names = ['W1', 'b1', 'W2', 'b2', 'W3', 'b3', 'W4', 'b4', 'Ws']
+    h = 1e-6
+    for k, name in enumerate(names):
+        flat = P[k].reshape(-1)
+        for i in rng.choice(flat.size, size=min(5, flat.size), replace=False):
+            old = flat[i]
+            flat[i] = old + h
+            lp = loss(P)
+            flat[i] = old - h
+            lm = loss(P)
+            flat[i] = old
+            fd = (lp - lm)/(2*h)
+            assert abs(fd - g[name].reshape(-1)[i]) < 1e-7 + 1e-5*abs(fd), \
+                (name, i, fd, g[name].reshape(-1)[i])
