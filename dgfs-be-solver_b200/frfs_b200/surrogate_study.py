@@ -1,0 +1,189 @@
+# -*- coding: utf-8 -*-
+"""Train the collision surrogate on the solver's own trajectories and judge
+it with the plain operator (no counterpart in the reference).
+
+``run_study`` does, on one GPU:
+
+1. harvest (f, Q(f)) pairs from the plain FP32 solver started from random
+   uniform states (Maxwellians with rho in [0.5, 2], T in [0.5, 3],
+   |u| <= 1, and bimodal mixtures), and from space-homogeneous relaxations
+   of random per-point states (which cross every distance from
+   equilibrium);
+2. train the MLP with the project's kernels;
+3. run the workload from its own initial state: plain FP64 (the reference
+   solution), plain FP32, surrogate-assisted FP32 (with a sampled residual
+   check every ``check_every`` steps that drops the surrogate when it
+   fails), and an ablation in which the gated points get Q = 0 (the gate
+   without the network);
+4. report the relative L2 errors of rho, u and T against the FP64 solution
+   and the Q(f) evaluations per second of a plain and of a
+   surrogate-assisted collision sweep on the final state.
+"""
+
+import time
+
+import numpy as np
+import torch
+
+from frfs_b200.backend import B200Backend
+from frfs_b200.initcond import initial_distribution
+from frfs_b200.inifile import Inifile
+from frfs_b200.steppers import StdTVDRK2DGFSStepper
+from frfs_b200.surrogate import VHSSurrogate, harvest, harvest_relaxation
+from frfs_b200.system import DGFSSystem
+
+
+class ZeroSurrogate(VHSSurrogate):
+    """The gate without the network: gated points get Q = 0."""
+
+    def predict(self, X):
+        Bp = self.ws.get('Bp0', (X.shape[0], X.shape[1]))
+        Bp.zero_()
+        return Bp
+
+
+def make_system(ini, precision, device, sphdesign=None, graphs=True):
+    cfg = Inifile(ini(precision=precision))
+    if sphdesign:
+        cfg.set('spherical-design-rule', 'path', sphdesign)
+    cfg.set('backend-b200', 'cuda-graphs', '1' if graphs else '0')
+    be = B200Backend(cfg, device=device)
+    return DGFSSystem(be, cfg)
+
+
+def _reset(system):
+    nupts, V, neles = system.bank[0].ioshape
+    system.bank[0].set(initial_distribution(system.cfg, system.vm, nupts,
+                                            neles))
+
+
+def rel_l2(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b)/np.linalg.norm(b))
+
+
+def run_workload(system, nsteps, sur=None, check_every=0, tol=0.05,
+                 scratch=None):
+    """nsteps SSP-RK2 steps from the workload's initial state; returns the
+    final (rho, u, T), the bank index and the residual-check record."""
+    system.surrogate = sur
+    _reset(system)
+    st = StdTVDRK2DGFSStepper(system, system.cfg)
+    fallbacks, checks, worst = [], 0, 0.0
+    done = 0
+    while done < nsteps:
+        n = min(check_every or nsteps, nsteps - done)
+        st.advance(n)
+        done += n
+        if sur is not None and check_every and system.surrogate is not None \
+                and done < nsteps:
+            cur = system.bank[st._idxcurr]
+            sur.collide(cur, scratch[0])
+            r = sur.residual_check(cur, scratch[0], scratch[1], seed=done)
+            checks += 1
+            worst = max(worst, r)
+            if r > tol:
+                fallbacks.append(done)
+                system.surrogate = None
+    torch.cuda.synchronize(system.backend.device)
+    m = system.moments(st._idxcurr)
+    system.surrogate = None
+    return ((m[..., 0], m[..., 1:4], m[..., 4]), st._idxcurr,
+            {'checks': checks, 'worst_residual': worst,
+             'fallback_at_step': fallbacks})
+
+
+def time_sweep(fn, reps, device):
+    """Mean device time (ms) of fn() over reps calls (CUDA events)."""
+    s = torch.cuda.current_stream(device)
+    fn()
+    torch.cuda.synchronize(device)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(reps):
+        fn()
+    e1.record(s)
+    torch.cuda.synchronize(device)
+    return e0.elapsed_time(e1)/reps
+
+
+def run_study(ini, device='cuda:0', runs=5, steps=100, nsteps=200,
+              epochs=20, batch=1024, lr=1e-3, threshold=0.05, eps_max=0.2,
+              check_every=50, tol=0.05, reps=10, sphdesign=None, seed=1,
+              max_pairs=200000, relax_points=576, relax_steps=100,
+              relax_dt=0.005, log=None):
+    t0 = time.time()
+    say = log or (lambda *a: None)
+    s32 = make_system(ini, 'single', device, sphdesign)
+    npts = s32.nupts*s32.neles
+    sur = VHSSurrogate(s32.sm, threshold=threshold, seed=0)
+
+    # 1. data from the plain solver's trajectories
+    th = time.time()
+    X, B = harvest(s32, StdTVDRK2DGFSStepper, sur, runs, steps, seed=seed,
+                   eps_max=eps_max, max_pairs=max_pairs)
+    npairs_solver = int(X.shape[0])
+    if relax_steps:
+        Xr, Br = harvest_relaxation(s32.sm, sur, relax_points, relax_steps,
+                                    relax_dt, seed=seed, eps_max=eps_max,
+                                    max_pairs=max_pairs)
+        X, B = torch.cat([X, Xr]), torch.cat([B, Br])
+        del Xr, Br
+    torch.cuda.synchronize(device)
+    t_harvest = time.time() - th
+    npairs = int(X.shape[0])
+    say(f'harvest: {npairs_solver} solver pairs, {npairs} in total, '
+        f'in {t_harvest:.1f} s')
+
+    # 2. training
+    tt = time.time()
+    sur.set_normalisation(X, B)
+    hist = sur.train(X, B, epochs=epochs, batch=batch, lr=lr)
+    torch.cuda.synchronize(device)
+    t_train = time.time() - tt
+    say(f'train: loss {hist[0]:.3e} -> {hist[-1]:.3e} in {t_train:.1f} s')
+    del X, B
+
+    # 3. the workload from its own initial state
+    s64 = make_system(ini, 'double', device, sphdesign)
+    (r64, u64, T64), _, _ = run_workload(s64, nsteps)
+    del s64
+    torch.cuda.empty_cache()
+    (r32, u32, T32), _, _ = run_workload(s32, nsteps)
+    zero = ZeroSurrogate(s32.sm, threshold=threshold)
+    (rz, uz, Tz), _, _ = run_workload(s32, nsteps, zero)
+    scratch = [s32.backend.matrix(s32.bank[0].ioshape) for _ in range(2)]
+    (rs, us, Ts), idx, chk = run_workload(s32, nsteps, sur, check_every,
+                                          tol, scratch)
+
+    def errs(r, u, T):
+        return {'rho': rel_l2(r, r64), 'u': rel_l2(u, u64),
+                'T': rel_l2(T, T64)}
+
+    # 4. throughput of one collision sweep on the surrogate run's final state
+    fin = s32.bank[idx]
+    out = scratch[0]
+    t_plain = time_sweep(lambda: s32.sm.fs_all(fin, out), reps, device)
+    t_sur = time_sweep(lambda: sur.collide(fin, out), reps, device)
+    gfrac = float(sur._last[0].float().mean())
+    eps = sur._last[1].cpu().numpy()
+    return {
+        'points': npts, 'pairs': npairs, 'pairs_solver': npairs_solver,
+        'train_loss_first': hist[0], 'train_loss_last': hist[-1],
+        'harvest_s': t_harvest, 'train_s': t_train,
+        'epochs': epochs, 'runs': runs, 'steps_per_run': steps,
+        'nsteps': nsteps, 'threshold': threshold,
+        'err_surrogate': errs(rs, us, Ts),
+        'err_plain_fp32': errs(r32, u32, T32),
+        'err_gate_without_network': errs(rz, uz, Tz),
+        'residual_checks': chk,
+        'gate_fraction': gfrac,
+        'eps_quantiles': [float(q) for q in
+                          np.quantile(eps, [0.1, 0.5, 0.9, 0.99])],
+        'plain_ms_per_sweep': t_plain, 'surrogate_ms_per_sweep': t_sur,
+        'plain_evals_per_s': npts/(t_plain*1e-3),
+        'surrogate_evals_per_s': npts/(t_sur*1e-3),
+        'speedup': t_plain/t_sur,
+        'wall_s': time.time() - t0,
+    }

@@ -15,13 +15,17 @@ relax0d-n16   single point, N=16, Nrho=8, M=6, VHS omega=0.5, L=5 (hard
               sphere 0D relaxation of two Maxwellians at u=(+-1.5,0,0)).
 couette-n24   64x1 quadrilateral strip, p=2, N=24, Nrho=12, M=16, omega=0.81,
               diffuse walls at x=+-1/2 moving at uy=+-0.5 (nondimensional),
-              y-periodic; dt = 2.5e-4 (advective CFL number
-              max|c| dt / h = 0.085 for the p=2 DG with SSP-RK2).  M=16 replaces the requested M=12: the tabulated
+              y-periodic; dt = 1e-4: the p=2 FR-DG operator with SSP-RK2 is
+              stable for |c| dt / h <= 0.056 at the corner velocity
+              |cx| = |cy| = 5.27 on this strip (eigenvalues of the operator);
+              1e-4 gives 0.034.  M=16 replaces the requested M=12: the tabulated
               symmetric designs hold 2M in {2,6,12,32,48,70,...} points only.
 channel-n32   48x24 quadrilaterals, p=2 (10368 points), N=32, Nrho=16, M=24,
               x-periodic, diffuse walls at y=+-1/4, Maxwellian times
               (1 + 0.01 xi) with xi ~ N(0,1) per velocity node and point;
-              dt = 2e-4 ((|cx| + |cy|) dt / h = 0.10).
+              dt = 1e-4 (|c| dt / h = 0.023 at the corner velocity; the
+              p=2 FR-DG operator with SSP-RK2 on a 2D periodic box is
+              stable up to 0.036).
 """
 
 import numpy as np
@@ -115,7 +119,7 @@ def couette_n24(precision='double', M=16, nele=64):
     ini = _BASE.format(precision=precision, Nv=24, NvBatchSize=13824,
                        Nrho=12, H0=1e-3, rho0=1.5e-3,
                        molarMass0=_MOLAR_MASS, cmax=repr(0.5*u0), dev=5.0,
-                       M=M, omega=0.81, order=2, tend=0.05, dt=2.5e-4)
+                       M=M, omega=0.81, order=2, tend=0.02, dt=1e-4)
     ini += f"""
 [mesh]
 type = quad-strip
@@ -159,7 +163,7 @@ def channel_n32(precision='double', nx=48, ny=24, Nv=32, Nrho=16, M=24):
     ini = _BASE.format(precision=precision, Nv=Nv, NvBatchSize=Nv**3,
                        Nrho=Nrho, H0=1e-3, rho0=1.5e-3,
                        molarMass0=_MOLAR_MASS, cmax=0.0, dev=5.0, M=M,
-                       omega=0.81, order=2, tend=0.04, dt=2e-4)
+                       omega=0.81, order=2, tend=0.02, dt=1e-4)
     ini += f"""
 [mesh]
 type = quad-box
