@@ -9,10 +9,15 @@
 // Maxwellian is rho T^{-3/2} W(c^).  Modes: total degree i+j+k <= 9
 // (220 modes, ordered by degree, then i, then j, both descending).
 //
-//   embedding   a_k = (1/rho) cw sum_v f(c_v) phi_k(c^_v)
-//               (a_000 = 1 and the first-order modes vanish by construction)
-//   target      b_k = cw sum_v Q(c_v) phi_k(c^_v) / (prefac rho^2 T^{gamma/2})
-//   reconstruct Q(c) = prefac rho^2 T^{gamma/2} T^{-3/2} W(c^) sum_k b_k phi_k(c^)
+//   window      chi(c^) = erfc((|c^| - 4) / 0.4) / 2: the degree-9
+//               polynomials reach 1e4..1e6 at the corners of the velocity
+//               box, where f and Q hold only round-off; the window keeps that
+//               noise out of the coefficients
+//   embedding   a_k = (1/rho) cw sum_v chi f(c_v) phi_k(c^_v)
+//   target      b_k = cw sum_v chi Q(c_v) phi_k(c^_v) / (prefac rho^2 T^{gamma/2})
+//   reconstruct Q(c) = prefac rho^2 T^{gamma/2} T^{-3/2} W(c^) sum_k d_k phi_k(c^),
+//               d = Gw^{-1} b with Gw_kl = int chi W phi_k phi_l dc^ (the
+//               windowed Gram matrix, condition number 1.75, passed in),
 //               followed by the FP64 least-squares projection onto zero
 //               mass, momentum and energy moments.
 // The velocity grid is a tensor product, so every sum factorises into three
@@ -32,6 +37,8 @@ constexpr int kModes = 220;        // (i, j, k) with i + j + k <= 9
 constexpr int kFeat = 256;         // feature vector width
 constexpr int kThreads = 256;
 constexpr int kMaxN = 32;
+constexpr double kWinR = 4.0;      // window centre |c^|
+constexpr double kWinW = 0.4;      // window width
 
 __constant__ unsigned char c_mi[kModes], c_mj[kModes], c_mk[kModes];
 // index of mode (i, j, k) in the 220-vector, -1 if degree > 9
@@ -106,17 +113,22 @@ __device__ void basis_tables(const FrameArgs& a, const double* mom, double (*H)[
 
 // out[m] = cw sum_v g(c_v) phi_m(c^_v) for the 220 modes, g read from a bank
 template <typename T>
-__device__ void project_modes(const T* g, int upt, int e, const FrameArgs& a, double (*H)[kMaxN][kP],
-                              double* t1, double* t2, double* out) {
+__device__ void project_modes(const T* g, int upt, int e, const FrameArgs& a, const double* mom,
+                              double (*H)[kMaxN][kP], double* t1, double* t2, double* out) {
   const int N = a.N;
   const long long V = (long long)N * N * N;
-  // t1[I][J][k] = sum_K g[I][J][K] Hz[K][k]
+  const double h = 2.0 * a.L / N, c00 = -a.L + a.L / N, rt = rsqrt(mom[4]);
+  // t1[I][J][k] = sum_K chi g[I][J][K] Hz[K][k]
   for (int r = threadIdx.x; r < N * N; r += kThreads) {
     double acc[kP];
 #pragma unroll
     for (int k = 0; k < kP; ++k) acc[k] = 0;
+    const double dx = (c00 + (r / N) * h - mom[1]) * rt, dy = (c00 + (r % N) * h - mom[2]) * rt;
+    const double r2xy = dx * dx + dy * dy;
     for (int K = 0; K < N; ++K) {
-      const double gv = (double)g[dgfs::soa_ix(upt, a.ldim, e, (long long)r * N + K, V, 32)];
+      const double dz = (c00 + K * h - mom[3]) * rt;
+      const double chi = 0.5 * erfc((sqrt(r2xy + dz * dz) - kWinR) * (1.0 / kWinW));
+      const double gv = chi * (double)g[dgfs::soa_ix(upt, a.ldim, e, (long long)r * N + K, V, 32)];
 #pragma unroll
       for (int k = 0; k < kP; ++k) acc[k] += gv * H[2][K][k];
     }
@@ -168,7 +180,7 @@ __global__ void __launch_bounds__(kThreads) embed_kernel(const T* __restrict__ f
   basis_tables(a, mom, H);
   __syncthreads();
 
-  project_modes<T>(f, upt, e, a, H, t1, t2, coef);
+  project_modes<T>(f, upt, e, a, mom, H, t1, t2, coef);
   const double rho = mom[0];
   double ne = 0;
   for (int k = threadIdx.x; k < kFeat; k += kThreads) {
@@ -189,7 +201,7 @@ __global__ void __launch_bounds__(kThreads) embed_kernel(const T* __restrict__ f
     for (int k = 0; k < 5; ++k) mom_out[(long long)pt * 5 + k] = mom[k];
   }
   if (Q) {
-    project_modes<T>(Q, upt, e, a, H, t1, t2, coef);
+    project_modes<T>(Q, upt, e, a, mom, H, t1, t2, coef);
     const double s = 1.0 / (a.prefac * rho * rho * pow(mom[4], 0.5 * a.gamma));
     for (int k = threadIdx.x; k < kFeat; k += kThreads)
       B[(long long)pt * kFeat + k] = k < kModes ? (float)(coef[k] * s) : 0.f;
@@ -204,10 +216,12 @@ __global__ void __launch_bounds__(kThreads) reconstruct_kernel(const float* __re
                                                                const double* __restrict__ mom_in,
                                                                const int* __restrict__ gate, FrameArgs a,
                                                                const double* __restrict__ ginv,
+                                                               const double* __restrict__ gwinv,
                                                                T* __restrict__ Q) {
   extern __shared__ double sm[];
   __shared__ double red[kThreads / 32];
   __shared__ double H[3][kMaxN][kP];
+  __shared__ double bw[kModes];
   __shared__ double b[kModes];
   __shared__ double mom[5];
   const int pt = blockIdx.x;
@@ -217,8 +231,17 @@ __global__ void __launch_bounds__(kThreads) reconstruct_kernel(const float* __re
   double* r1 = sm;                    // [kP][kP][N]   (i, j, K)
   double* r2 = sm + kP * kP * N;      // [kP][N][N]    (i, J, K)
   if (threadIdx.x < 5) mom[threadIdx.x] = mom_in[(long long)pt * 5 + threadIdx.x];
-  for (int k = threadIdx.x; k < kModes; k += kThreads) b[k] = (double)Bp[(long long)pt * kFeat + k];
+  for (int k = threadIdx.x; k < kModes; k += kThreads) bw[k] = (double)Bp[(long long)pt * kFeat + k];
   __syncthreads();
+  // d = Gw^{-1} b (windowed coefficients to expansion coefficients)
+  for (int k = threadIdx.x; k < kModes; k += kThreads) {
+    double s = 0;
+    if (gwinv)
+      for (int l = 0; l < kModes; ++l) s += gwinv[k * kModes + l] * bw[l];
+    else
+      s = bw[k];
+    b[k] = s;
+  }
   basis_tables(a, mom, H);
   __syncthreads();
   // r1[i][j][K] = sum_k b[i][j][k] Hz[K][k]
@@ -360,8 +383,8 @@ extern "C" int dgfs_hermite_embed(int precision, const void* f, const void* Q, i
 
 extern "C" int dgfs_hermite_reconstruct(int precision, const float* B, const double* mom, const int* gate,
                                         int nupts, int neles, long long ldim, int Nv, double L, double cw,
-                                        double prefactor, double gamma, const double* ginv, void* Q,
-                                        void* stream) {
+                                        double prefactor, double gamma, const double* ginv,
+                                        const double* gwinv, void* Q, void* stream) {
   dgfs::clear_error();
   if (!B || !mom || !ginv || !Q) return dgfs::set_error(DGFS_ERR_INVALID, "null pointer");
   int rc = check_frame(precision, Nv, nupts, neles, ldim, L, cw);
@@ -375,9 +398,11 @@ extern "C" int dgfs_hermite_reconstruct(int precision, const float* B, const dou
     return dgfs::set_error(DGFS_ERR_CUDA, "smem attribute");
   const unsigned grid = (unsigned)(nupts * neles);
   if (precision == 64)
-    reconstruct_kernel<double><<<grid, kThreads, smem, (cudaStream_t)stream>>>(B, mom, gate, a, ginv, (double*)Q);
+    reconstruct_kernel<double><<<grid, kThreads, smem, (cudaStream_t)stream>>>(B, mom, gate, a, ginv, gwinv,
+                                                                               (double*)Q);
   else
-    reconstruct_kernel<float><<<grid, kThreads, smem, (cudaStream_t)stream>>>(B, mom, gate, a, ginv, (float*)Q);
+    reconstruct_kernel<float><<<grid, kThreads, smem, (cudaStream_t)stream>>>(B, mom, gate, a, ginv, gwinv,
+                                                                              (float*)Q);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return dgfs::set_error(DGFS_ERR_CUDA, "reconstruct launch: %s", cudaGetErrorString(e));
   return DGFS_OK;

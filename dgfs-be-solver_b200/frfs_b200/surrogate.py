@@ -6,11 +6,15 @@ Per solution point:
 
 1. FP64 moments rho, u, T define a local frame c^ = (c - u)/sqrt(T);
 2. the distribution is embedded as 220 Hermite coefficients (total degree
-   <= 9) in that frame plus sqrt(T)/L and u/L (256 features);
+   <= 9) in that frame, taken under the radial window erfc((|c^| - 4)/0.4)/2
+   (the polynomials would otherwise amplify the round-off that f and Q hold
+   at the corners of the velocity box), plus sqrt(T)/L and u/L (256
+   features);
 3. an MLP (256 -> 512 -> 512 -> 512 -> 256, tanh, with a linear skip from the
    input; BF16 weights, FP32 accumulation) predicts the Hermite coefficients
    of Q(f) scaled by prefac rho^2 T^{gamma/2};
-4. Q is rebuilt on the velocity grid and projected in FP64 onto zero mass,
+4. Q is rebuilt on the velocity grid (windowed coefficients mapped back by
+   the inverse windowed Gram matrix) and projected in FP64 onto zero mass,
    momentum and energy moments.
 
 A point uses the surrogate when its non-equilibrium measure eps (the norm of
@@ -42,7 +46,7 @@ _lib.declare('dgfs_hermite_embed', c_int,
 _lib.declare('dgfs_hermite_reconstruct', c_int,
              [c_int, c_void_p, c_void_p, c_void_p, c_int, c_int, c_ll, c_int,
               c_double, c_double, c_double, c_double, c_void_p, c_void_p,
-              c_void_p])
+              c_void_p, c_void_p])
 _lib.declare('dgfs_surrogate_gate', c_int,
              [c_int, c_void_p, c_float, c_void_p, c_void_p, c_void_p,
               c_void_p])
@@ -67,6 +71,44 @@ _lib.declare('dgfs_f32_to_bf16', c_int, [c_ll, c_void_p, c_void_p, c_void_p])
 NFEAT = 256
 NMODES = 220
 WIDTH = 512
+DEG = 9
+WIN_R, WIN_W = 4.0, 0.4       # the kernels' window erfc((|c^| - 4)/0.4)/2
+
+
+def hermite_modes():
+    """(i, j, k), i + j + k <= 9, in the kernels' order (degree, then i,
+    then j, both descending)."""
+    return [(i, j, d - i - j) for d in range(DEG + 1)
+            for i in range(d, -1, -1) for j in range(d - i, -1, -1)]
+
+
+def window_gram_inverse(nq=100):
+    """Inverse of Gw_kl = int chi(c^) W(c^) phi_k(c^) phi_l(c^) dc^, the
+    Gram matrix of the windowed Hermite projection (condition number 1.75),
+    by an nq-point Gauss-Hermite product rule: pair products of the 1D
+    polynomials are contracted against the window one axis at a time.
+    Row-major (220, 220) float64."""
+    from scipy.special import erfc
+    x, w = np.polynomial.hermite.hermgauss(nq)
+    w = w/np.sqrt(np.pi)
+    P = np.empty((DEG + 1, nq))
+    P[0], P[1] = 1.0, np.sqrt(2.0)*x
+    for n in range(1, DEG):
+        P[n + 1] = (np.sqrt(2.0)*x*P[n] - np.sqrt(n)*P[n - 1])/np.sqrt(n + 1)
+    P2 = (P[:, None, :]*P[None, :, :]*w).reshape(-1, nq)    # (100, nq)
+    r = np.sqrt(x[:, None, None]**2 + x[None, :, None]**2 +
+                x[None, None, :]**2)
+    chi = 0.5*erfc((r - WIN_R)/WIN_W)
+    T = np.einsum('abc,rc->abr', chi, P2)
+    T = np.einsum('abr,qb->aqr', T, P2)
+    T = np.einsum('aqr,pa->pqr', T, P2)                       # (100,)*3
+    T = T.reshape((DEG + 1,)*6)                                # i i' j j' k k'
+    m = hermite_modes()
+    G = np.empty((len(m), len(m)))
+    for p, (i, j, k) in enumerate(m):
+        for q, (a, b, c) in enumerate(m):
+            G[p, q] = T[i, a, j, b, k, c]
+    return np.linalg.inv(G)
 
 
 def _p(t):
@@ -250,6 +292,8 @@ class VHSSurrogate:
         phi = np.vstack([np.ones(cv.shape[1]), cv, np.sum(cv*cv, axis=0)])
         self.ginv = torch.tensor(np.linalg.inv(phi @ phi.T).ravel(),
                                  dtype=torch.float64, device=self.device)
+        self.gwinv = torch.tensor(window_gram_inverse().ravel(),
+                                  dtype=torch.float64, device=self.device)
         self.loss_history = []
         self._last = None
 
@@ -373,7 +417,8 @@ class VHSSurrogate:
             self.backend.precision, _p(Bp), _p(mom), _p(gate), nupts, neles,
             ldim, self.vm.Nv(), self.vm.L(), self.vm.cw(),
             self.sm.prefactor, self.sm._gamma, _p(self.ginv),
-            qbank._as_parameter_, self._s), 'dgfs_hermite_reconstruct')
+            _p(self.gwinv), qbank._as_parameter_, self._s),
+            'dgfs_hermite_reconstruct')
         _lib.check(lib.dgfs_vhs_apply_list(
             self.sm._h, fbank._as_parameter_, qbank._as_parameter_, nupts,
             neles, ldim, self.backend.soasz, _p(plain), _p(nplain), npts,

@@ -256,9 +256,10 @@ DGFS_API int dgfs_moments(int precision, const void* f, int nupts, int neles,
  * Per point: FP64 frame rho, u, T (the formulas of dgfs_moments);
  * c^ = (c - u)/sqrt(T); phi_n(x) = He_n(sqrt(2) x)/sqrt(n!); 220 modes
  * (i, j, k), i + j + k <= 9, ordered by degree, then i, then j (both
- * descending).  Feature row X[pt][256]: a_k = cw/rho sum_v f phi_k(c^_v)
- * (k < 220), sqrt(T)/L, ux/L, uy/L, uz/L, zeros.  Target row B[pt][256]:
- * b_k = cw sum_v Q phi_k(c^_v) / (prefactor rho^2 T^{gamma/2}).  mom[pt][5]
+ * descending); window chi(c^) = erfc((|c^| - 4)/0.4)/2.  Feature row
+ * X[pt][256]: a_k = cw/rho sum_v chi f phi_k(c^_v) (k < 220), sqrt(T)/L,
+ * ux/L, uy/L, uz/L, zeros.  Target row B[pt][256]:
+ * b_k = cw sum_v chi Q phi_k(c^_v) / (prefactor rho^2 T^{gamma/2}).  mom[pt][5]
  * = rho, ux, uy, uz, T; eps[pt] = |a_k, degree >= 2| (non-equilibrium
  * measure).  Nv <= 32, soasz 32.  All pointers are device pointers; point
  * id pt = upt*neles + elem.
@@ -270,17 +271,18 @@ DGFS_API int dgfs_hermite_embed(int precision, const void* f, const void* Q,
                                 float* eps, void* stream);
 
 /* Q(c) = prefactor rho^2 T^{gamma/2} T^{-3/2} pi^{-3/2} e^{-|c^|^2}
- * sum_k B[pt][k] phi_k(c^), then the FP64 projection onto zero mass,
- * momentum and energy with the 5x5 inverse Gram matrix ginv of
- * (1, c, |c|^2) on the grid; written only where gate[pt] != 0 (all points
- * when gate is NULL). */
+ * sum_k d_k phi_k(c^) with d = gwinv B[pt] (gwinv: 220x220 row-major
+ * inverse of the windowed Gram matrix int chi W phi_k phi_l dc^; NULL uses
+ * d = B[pt]), then the FP64 projection onto zero mass, momentum and energy
+ * with the 5x5 inverse Gram matrix ginv of (1, c, |c|^2) on the grid;
+ * written only where gate[pt] != 0 (all points when gate is NULL). */
 DGFS_API int dgfs_hermite_reconstruct(int precision, const float* B,
                                       const double* mom, const int* gate,
                                       int nupts, int neles, long long ldim,
                                       int Nv, double L, double cw,
                                       double prefactor, double gamma,
-                                      const double* ginv, void* Q,
-                                      void* stream);
+                                      const double* ginv, const double* gwinv,
+                                      void* Q, void* stream);
 
 /* gate[pt] = eps[pt] < threshold; the other points are appended to
  * plain[0 .. *nplain) (unordered) for dgfs_vhs_apply_list. */

@@ -4,19 +4,21 @@ INFRASTRUCTURE ONLY (see ``oracle/__init__.py``).
 
 The surrogate has no counterpart in the reference; these functions define
 what the B200 kernels must compute so that their results and gradients can
-be checked: the Hermite embedding of a distribution in its local frame, the
-reconstruction of Q from Hermite coefficients with the conservation
-projection, and the MLP forward/backward pass.  The frame moments follow
+be checked: the windowed Hermite embedding of a distribution in its local
+frame, the reconstruction of Q from windowed Hermite coefficients with the
+conservation projection, and the MLP forward/backward pass.  The frame moments follow
 frfs/plugins/dgfsmomwriterstd.py:154-190 (nondimensional).
 """
 
 from math import factorial
 
 import numpy as np
+from scipy.special import erfc
 
 from oracle.vhs import project_conservative
 
 DEG = 9
+WIN_R, WIN_W = 4.0, 0.4     # window chi(c^) = erfc((|c^| - WIN_R)/WIN_W)/2
 
 
 def modes(deg=DEG):
@@ -48,6 +50,32 @@ def frame(f, cv, cw):
     return m0*cw, u, T
 
 
+def window(cv, u, T):
+    ch = (cv - u[:, None])/np.sqrt(T)
+    return 0.5*erfc((np.sqrt(np.sum(ch*ch, axis=0)) - WIN_R)/WIN_W)
+
+
+def window_gram(nq=80):
+    """Gw_kl = int chi(c^) W(c^) phi_k phi_l dc^ by a 3D Gauss-Hermite
+    product rule of nq points per axis (mode by mode)."""
+    x, w = np.polynomial.hermite.hermgauss(nq)
+    w = w/np.sqrt(np.pi)
+    P = np.stack([phi(n, x) for n in range(DEG + 1)])
+    X, Y, Z = np.meshgrid(x, x, x, indexing='ij')
+    cw3 = (0.5*erfc((np.sqrt(X*X + Y*Y + Z*Z) - WIN_R)/WIN_W) *
+           w[:, None, None]*w[None, :, None]*w[None, None, :])
+    m = modes()
+    G = np.empty((len(m), len(m)))
+    for p, (i, j, k) in enumerate(m):
+        A = cw3*P[i][:, None, None]*P[j][None, :, None]*P[k][None, None, :]
+        Ax = np.einsum('abc,la->lbc', A, P)
+        Axy = np.einsum('lbc,mb->lmc', Ax, P)
+        Axyz = np.einsum('lmc,nc->lmn', Axy, P)
+        for q, (a, b, c) in enumerate(m):
+            G[p, q] = Axyz[a, b, c]
+    return G
+
+
 def basis(cv, u, T, deg=DEG):
     ch = (cv - u[:, None])/np.sqrt(T)
     return np.stack([np.prod([phi(m[a], ch[a]) for a in range(3)], axis=0)
@@ -58,7 +86,8 @@ def embed(f, cv, cw, L, Q=None, prefac=1.0, gamma=0.0):
     """Features x (256), frame (rho, u, T), eps and (if Q) targets b (256)."""
     rho, u, T = frame(f, cv, cw)
     Phi = basis(cv, u, T)
-    a = Phi @ np.asarray(f, np.float64)*cw/rho
+    chi = window(cv, u, T)
+    a = Phi @ (chi*np.asarray(f, np.float64))*cw/rho
     x = np.zeros(256)
     x[:len(a)] = a
     x[len(a)] = np.sqrt(T)/L
@@ -68,18 +97,23 @@ def embed(f, cv, cw, L, Q=None, prefac=1.0, gamma=0.0):
     b = None
     if Q is not None:
         b = np.zeros(256)
-        b[:len(a)] = Phi @ np.asarray(Q, np.float64)*cw/(
+        b[:len(a)] = Phi @ (chi*np.asarray(Q, np.float64))*cw/(
             prefac*rho*rho*T**(0.5*gamma))
     return x, (rho, u, T), eps, b
 
 
-def reconstruct(b, mom, cv, prefac=1.0, gamma=0.0):
+def reconstruct(b, mom, cv, prefac=1.0, gamma=0.0, Gw=None):
+    """Q from windowed coefficients b: d = Gw^{-1} b (Gw = window_gram();
+    None: d = b), Q = prefac rho^2 T^{gamma/2} T^{-3/2} W(c^) sum d_k phi_k,
+    then the conservation projection."""
     rho, u, T = mom
     Phi = basis(cv, u, T)
     ch2 = np.sum(((cv - u[:, None])/np.sqrt(T))**2, axis=0)
     W = np.pi**-1.5*np.exp(-ch2)
-    Q = prefac*rho*rho*T**(0.5*gamma)*T**-1.5*W*(
-        np.asarray(b[:Phi.shape[0]], np.float64) @ Phi)
+    d = np.asarray(b[:Phi.shape[0]], np.float64)
+    if Gw is not None:
+        d = np.linalg.solve(Gw, d)
+    Q = prefac*rho*rho*T**(0.5*gamma)*T**-1.5*W*(d @ Phi)
     return project_conservative(Q, cv)
 
 

@@ -1,6 +1,7 @@
 # -*- coding: utf-8 -*-
 """Kernels of the learned collision surrogate against the FP64 oracle
-(GPU): Hermite embedding and reconstruction, gate and device point list,
+(GPU): windowed Hermite embedding and reconstruction, gate and device point
+list,
 the MLP's forward/backward/Adam kernels, and the assembled collide path.
 
 Tolerances:
@@ -98,11 +99,13 @@ def test_reconstruct_matches_oracle_and_gate(precision):
     d_b = torch.tensor(Bp, device=dev)
     d_mom = torch.tensor(mom, device=dev)
     d_gate = torch.tensor(gate, device=dev)
+    Gw = osur.window_gram()
+    d_gwinv = torch.tensor(np.linalg.inv(Gw).ravel(), device=dev)
     _lib.check(_lib.load().dgfs_hermite_reconstruct(
         be.precision, d_b.data_ptr(), d_mom.data_ptr(), d_gate.data_ptr(),
         nupts, neles, out.traits[1], vm.Nv(), vm.L(), vm.cw(), sm.prefactor,
-        sm._gamma, sur.ginv.data_ptr(), out._as_parameter_, be.stream),
-        'dgfs_hermite_reconstruct')
+        sm._gamma, sur.ginv.data_ptr(), d_gwinv.data_ptr(),
+        out._as_parameter_, be.stream), 'dgfs_hermite_reconstruct')
     torch.cuda.synchronize()
     Q = out.get()
     tol = 1e-10 if precision == 'double' else 2e-6
@@ -113,7 +116,7 @@ def test_reconstruct_matches_oracle_and_gate(precision):
             continue
         Qo = osur.reconstruct(Bp[pt].astype(np.float64),
                               (mom[pt, 0], mom[pt, 1:4], mom[pt, 4]), cv,
-                              sm.prefactor, sm._gamma)
+                              sm.prefactor, sm._gamma, Gw=Gw)
         assert rel_err(Q[u, :, e], Qo) < tol
 
 

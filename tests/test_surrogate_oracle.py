@@ -38,34 +38,51 @@ def test_embedding_of_a_maxwellian():
     x, (rho, u, T), eps, _ = osur.embed(f, cv, cw, vm.L())
     assert abs(rho - 1.3) < 1e-6 and abs(T - 1.2) < 1e-6
     assert np.max(np.abs(u - [0.2, -0.1, 0.05])) < 1e-6
-    assert abs(x[0] - 1.0) < 1e-12
-    assert np.max(np.abs(x[1:4])) < 1e-12      # first moments vanish exactly
-    assert eps < 1e-6
+    assert abs(x[0] - 1.0) < 1e-5      # the window drops the far tail
+    assert np.max(np.abs(x[1:4])) < 1e-6
+    # the windowed Maxwellian keeps degree-2+ coefficients Gw[k, 0]: eps has
+    # a floor of 7e-4, far below the gate threshold 0.05
+    assert eps < 1e-3
     assert abs(x[220] - np.sqrt(T)/vm.L()) < 1e-15
 
 
 def test_reconstruct_then_embed_round_trip():
-    """Coefficients with zero mass, momentum and energy survive
-    reconstruction (incl. the projection) and re-embedding."""
+    """Windowed coefficients with zero mass, momentum and energy survive
+    reconstruction (inverse windowed Gram, projection) and re-embedding, up
+    to the grid quadrature of the window integrals."""
     vm = _vm()
     cv, cw = vm.cv(), vm.cw()
     rng = np.random.default_rng(3)
     deg = np.array([sum(t) for t in osur.modes()])
-    b = np.zeros(256)
-    b[:220] = rng.standard_normal(220)*0.5**deg
-    b[:4] = 0.0
+    Gw = osur.window_gram()
+    d = np.zeros(220)
+    d[:] = rng.standard_normal(220)*0.5**deg
+    d[:4] = 0.0
     tr = [osur.modes().index(t) for t in ((2, 0, 0), (0, 2, 0), (0, 0, 2))]
-    b[tr] -= b[tr].mean()
+    d[tr] -= d[tr].mean()
+    b = np.zeros(256)
+    b[:220] = Gw @ d
     mom = (1.1, np.array([0.1, 0.0, -0.2]), 0.9)
     prefac, gamma = 0.7, 0.38
-    Q = osur.reconstruct(b, mom, cv, prefac, gamma)
+    Q = osur.reconstruct(b, mom, cv, prefac, gamma, Gw=Gw)
     f = ovhs.maxwellian(cv, mom[0], mom[1], mom[2])
     _, _, _, b2 = osur.embed(f, cv, cw, vm.L(), Q=Q, prefac=prefac,
                              gamma=gamma)
-    # grid quadrature of degree-18 polynomials times the Gaussian weight
-    assert np.max(np.abs(b2[:220] - b[:220])) < 1e-6*np.max(np.abs(b))
+    # grid (spacing 0.48 in c^) against continuum window integrals
+    assert np.max(np.abs(b2[:220] - b[:220])) < 3e-5*np.max(np.abs(b))
     phi = np.vstack([np.ones(cv.shape[1]), cv, np.sum(cv*cv, axis=0)])
     assert np.max(np.abs(phi @ Q)) < 1e-12*np.max(np.abs(Q))*cv.shape[1]
+
+
+def test_window_gram_of_the_product_matches():
+    """The host table the surrogate passes to the reconstruction kernel
+    (frfs_b200.surrogate.window_gram_inverse) inverts the oracle's Gram."""
+    from frfs_b200.surrogate import hermite_modes, window_gram_inverse
+    assert hermite_modes() == osur.modes()
+    G = osur.window_gram()
+    assert np.max(np.abs(window_gram_inverse() @ G - np.eye(220))) < 1e-7
+    ev = np.linalg.eigvalsh(0.5*(G + G.T))
+    assert 1.7 < ev.max()/ev.min() < 1.8
 
 
 def _params(rng, nin, wd, nout):
