@@ -432,11 +432,18 @@ class VHSSurrogate:
 
     def residual_check(self, fbank, qbank, scratch, sample=16, seed=0):
         """Plain Q at a random sample of the last call's surrogate points
-        (into ``scratch``) against the surrogate's values in ``qbank``;
-        returns sqrt(sum |dQ|^2 / sum |Q_plain|^2) over the sample (0 when no
-        point used the surrogate).  The caller compares it with its
-        tolerance and drops the surrogate when it is exceeded."""
+        (into ``scratch``) against the surrogate's values in ``qbank``.
+
+        Returns r = sqrt(sum |dQ|^2 / sum (prefac rho T^{gamma/2} |f|)^2)
+        over the sample (0 when no point used the surrogate): the error in
+        units of a collision rate times f, so that r nu K dt bounds the
+        relative change of f that K steps of size dt accumulate (nu, the
+        dimensionless collision rate, is O(10) for VHS).  Near equilibrium
+        |Q| itself tends to zero, which makes |dQ|/|Q| meaningless there.
+        The caller compares r with its tolerance and drops the surrogate
+        when it is exceeded."""
         gate, _ = self._last
+        mom = self.ws.get('mom', (gate.numel(), 5), torch.float64)
         sur = torch.nonzero(gate).flatten()
         if sur.numel() == 0:
             return 0.0
@@ -449,13 +456,15 @@ class VHSSurrogate:
             self.sm._h, fbank._as_parameter_, scratch._as_parameter_, nupts,
             neles, ldim, self.backend.soasz, _p(pick), None, pick.numel(),
             self._s), 'dgfs_vhs_apply_list')
-        qa, qb = qbank.get(), scratch.get()
+        qa, qb, fa = qbank.get(), scratch.get(), fbank.get()
+        m = mom.cpu().numpy()
         num = den = 0.0
         for pt in pick.cpu().numpy():
             u, e = divmod(int(pt), neles)
             num += float(np.sum((qa[u, :, e].astype(np.float64) -
                                  qb[u, :, e])**2))
-            den += float(np.sum(qb[u, :, e].astype(np.float64)**2))
+            rate = self.sm.prefactor*m[pt, 0]*m[pt, 4]**(0.5*self.sm._gamma)
+            den += rate**2*float(np.sum(fa[u, :, e].astype(np.float64)**2))
         return float(np.sqrt(num/max(den, 1e-300)))
 
     def save(self, path):
