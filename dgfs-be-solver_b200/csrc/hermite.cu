@@ -418,3 +418,30 @@ extern "C" int dgfs_surrogate_gate(int npts, const float* eps, float threshold, 
   e = cudaGetLastError();
   return e == cudaSuccess ? DGFS_OK : dgfs::set_error(DGFS_ERR_CUDA, "gate launch: %s", cudaGetErrorString(e));
 }
+
+namespace {
+
+// In place on rows of X[M][ld]: columns [c0, c1) divided (inverse: multiplied)
+// by s = max(eps[m], eps0); column logcol (when >= 0, forward only) := log(s).
+__global__ void scale_rows_kernel(int M, int ld, const float* __restrict__ eps, float eps0, int c0, int c1,
+                                  int logcol, int inverse, float* __restrict__ X) {
+  const int m = blockIdx.x;
+  if (m >= M) return;
+  const float s = fmaxf(eps[m], eps0);
+  const float k = inverse ? s : 1.f / s;
+  for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) X[(long long)m * ld + c] *= k;
+  if (!inverse && logcol >= 0 && threadIdx.x == 0) X[(long long)m * ld + logcol] = logf(s);
+}
+
+}  // namespace
+
+extern "C" int dgfs_surrogate_scale(int M, int ld, const float* eps, float eps0, int c0, int c1, int logcol,
+                                    int inverse, float* X, void* stream) {
+  dgfs::clear_error();
+  if (M < 1 || ld < 1 || !eps || !X || !(eps0 > 0.f) || c0 < 0 || c1 > ld || c0 > c1 || logcol >= ld ||
+      (logcol >= c0 && logcol < c1))
+    return dgfs::set_error(DGFS_ERR_INVALID, "bad arguments");
+  scale_rows_kernel<<<M, 128, 0, (cudaStream_t)stream>>>(M, ld, eps, eps0, c0, c1, logcol, inverse, X);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? DGFS_OK : dgfs::set_error(DGFS_ERR_CUDA, "scale launch: %s", cudaGetErrorString(e));
+}

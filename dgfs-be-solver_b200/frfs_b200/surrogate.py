@@ -10,9 +10,12 @@ Per solution point:
    (the polynomials would otherwise amplify the round-off that f and Q hold
    at the corners of the velocity box), plus sqrt(T)/L and u/L (256
    features);
-3. an MLP (256 -> 512 -> 512 -> 512 -> 256, tanh, with a linear skip from the
-   input; BF16 weights, FP32 accumulation) predicts the Hermite coefficients
-   of Q(f) scaled by prefac rho^2 T^{gamma/2};
+3. the degree >= 2 coefficients are divided by the deviation size
+   s = max(eps, 1e-3) and log(s) is appended; an MLP (256 -> 512 -> 512 ->
+   512 -> 256, tanh, with a linear skip from the input; BF16 weights, FP32
+   accumulation) predicts the windowed Hermite coefficients of Q(f) divided
+   by prefac rho^2 T^{gamma/2} s (near equilibrium Q is linear in f - M, so
+   both sides are O(1) whatever the distance from equilibrium);
 4. Q is rebuilt on the velocity grid (windowed coefficients mapped back by
    the inverse windowed Gram matrix) and projected in FP64 onto zero mass,
    momentum and energy moments.
@@ -67,11 +70,16 @@ _lib.declare('dgfs_mlp_adam', c_int, [c_ll, c_void_p, c_void_p, c_void_p,
 _lib.declare('dgfs_mlp_affine', c_int, [c_int, c_int, c_void_p, c_void_p,
                                         c_void_p, c_void_p, c_int, c_void_p])
 _lib.declare('dgfs_f32_to_bf16', c_int, [c_ll, c_void_p, c_void_p, c_void_p])
+_lib.declare('dgfs_surrogate_scale', c_int,
+             [c_int, c_int, c_void_p, c_float, c_int, c_int, c_int, c_int,
+              c_void_p, c_void_p])
 
 NFEAT = 256
 NMODES = 220
 WIDTH = 512
 DEG = 9
+EPS0 = 1e-3     # floor of the deviation scale (the window alone gives 7e-4)
+LOGCOL = 224    # feature column that carries log(max(eps, EPS0))
 WIN_R, WIN_W = 4.0, 0.4       # the kernels' window erfc((|c^| - 4)/0.4)/2
 
 
@@ -331,6 +339,26 @@ class VHSSurrogate:
             1 if inverse else 0, self._s), 'dgfs_mlp_affine')
         return Y
 
+    def _scale(self, X, eps, c0, c1, logcol=-1, inverse=False):
+        _lib.check(_lib.load().dgfs_surrogate_scale(
+            X.shape[0], X.shape[1], _p(eps), EPS0, c0, c1, logcol,
+            1 if inverse else 0, _p(X), self._s), 'dgfs_surrogate_scale')
+        return X
+
+    def scale_features(self, X, eps):
+        """In place: degree >= 2 coefficients divided by the deviation
+        size s = max(eps, EPS0), log(s) into column LOGCOL."""
+        return self._scale(X, eps, 4, NMODES, LOGCOL)
+
+    def scale_targets(self, B, eps, inverse=False):
+        """In place: targets divided (inverse: multiplied) by s."""
+        return self._scale(B, eps, 0, NMODES, inverse=inverse)
+
+    def embed_scaled(self, fbank, qbank):
+        """Training pair rows (scaled features, scaled targets) and eps."""
+        X, B, _, eps = self.embed(fbank, qbank)
+        return self.scale_features(X, eps), self.scale_targets(B, eps), eps
+
     def set_normalisation(self, X, B):
         """Per-feature standardisation from training data.  Features that
         are constant by construction (a_000 = 1, first-order modes) get a
@@ -406,13 +434,14 @@ class VHSSurrogate:
                ws.get('mom', (npts, 5), torch.float64),
                ws.get('eps', (npts,)))
         X, _, mom, eps = self.embed(fbank, out=out)
+        self.scale_features(X, eps)
         gate = ws.get('gate', (npts,), torch.int32)
         plain = ws.get('plain', (npts,), torch.int32)
         nplain = ws.get('nplain', (1,), torch.int32)
         _lib.check(lib.dgfs_surrogate_gate(npts, _p(eps), thr, _p(gate),
                                            _p(plain), _p(nplain), self._s),
                    'dgfs_surrogate_gate')
-        Bp = self.predict(X)
+        Bp = self.scale_targets(self.predict(X), eps, inverse=True)
         _lib.check(lib.dgfs_hermite_reconstruct(
             self.backend.precision, _p(Bp), _p(mom), _p(gate), nupts, neles,
             ldim, self.vm.Nv(), self.vm.L(), self.vm.cw(),
@@ -426,9 +455,9 @@ class VHSSurrogate:
         self._last = (gate, eps)
         return gate
 
-    # kernels one collide() launches: embed, gate (+ counter reset),
-    # 2 affine, 5 GEMMs, reconstruct, plain list
-    launches_per_collide = 11
+    # kernels one collide() launches: embed, 2 scale, gate (+ counter
+    # reset), 2 affine, 5 GEMMs, reconstruct, plain list
+    launches_per_collide = 13
 
     def residual_check(self, fbank, qbank, scratch, sample=16, seed=0):
         """Plain Q at a random sample of the last call's surrogate points
@@ -531,8 +560,8 @@ def random_point_states(vm, n, rng):
 
 
 class Harvester:
-    """Collects (features, targets) of every (f, Q) pair it is called with
-    (installed as ``system.collide_hook``), keeping points with
+    """Collects the scaled (features, targets) of every (f, Q) pair it is
+    called with (installed as ``system.collide_hook``), keeping points with
     eps < eps_max."""
 
     def __init__(self, sur, eps_max):
@@ -542,7 +571,7 @@ class Harvester:
         self.seen = 0
 
     def __call__(self, fbank, qbank):
-        X, B, _, eps = self.sur.embed(fbank, qbank)
+        X, B, eps = self.sur.embed_scaled(fbank, qbank)
         keep = eps < self.eps_max
         self.X.append(X[keep])
         self.B.append(B[keep])

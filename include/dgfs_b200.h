@@ -290,6 +290,15 @@ DGFS_API int dgfs_surrogate_gate(int npts, const float* eps, float threshold,
                                  int* gate, int* plain, int* nplain,
                                  void* stream);
 
+/* Scale-free surrogate rows, in place on X[M][ld]: columns [c0, c1) are
+ * divided (inverse != 0: multiplied) by s = max(eps[m], eps0); forward
+ * only, column logcol (>= 0, outside [c0, c1)) receives log(s).  Near
+ * equilibrium Q is linear in the deviation f - M, so features and targets
+ * divided by the deviation size eps are O(1) across the whole range. */
+DGFS_API int dgfs_surrogate_scale(int M, int ld, const float* eps, float eps0,
+                                  int c0, int c1, int logcol, int inverse,
+                                  float* X, void* stream);
+
 /* Surrogate MLP kernels (FP32 accumulation; B operand FP32 or BF16):
  * C[m*ldc+n] = act(sum_k A[m*sam+k*sak] B[k*sbk+n*sbn] + bias[n]) (+ C),
  * act 0 identity, 1 tanh; Z (optional) receives the pre-activation. */

@@ -322,3 +322,36 @@ def test_collide_routes_points_and_conserves():
         want = Q2 if g[pt] else Qr
         assert np.array_equal(Q3[u, :, el], want[u, :, el])
     assert sur.residual_check(fb, out3, be.matrix(fb.ioshape)) > 0
+
+
+def test_scale_rows_matches_numpy():
+    """Scale-free rows: degree >= 2 columns divided by max(eps, 1e-3), log
+    of that scale in the spare column; the inverse multiplies back."""
+    dev = torch.device('cuda:0')
+    rng = np.random.default_rng(4)
+    M = 300
+    X = rng.standard_normal((M, NFEAT)).astype(np.float32)
+    eps = np.abs(rng.standard_normal(M)).astype(np.float32)*0.05
+    eps[:10] = 1e-5                                   # below the floor
+    d_x = torch.tensor(X, device=dev)
+    d_e = torch.tensor(eps, device=dev)
+    s = torch.cuda.current_stream().cuda_stream
+    lib = _lib.load()
+    _lib.check(lib.dgfs_surrogate_scale(M, NFEAT, d_e.data_ptr(), 1e-3, 4,
+                                        NMODES, 224, 0, d_x.data_ptr(), s),
+               'dgfs_surrogate_scale')
+    sc = np.maximum(eps, np.float32(1e-3))
+    want = X.copy()
+    want[:, 4:NMODES] /= sc[:, None]
+    want[:, 224] = np.log(sc)
+    got = d_x.cpu().numpy()
+    assert np.allclose(got, want, rtol=1e-6, atol=1e-7)
+    _lib.check(lib.dgfs_surrogate_scale(M, NFEAT, d_e.data_ptr(), 1e-3, 0,
+                                        NMODES, -1, 1, d_x.data_ptr(), s),
+               'dgfs_surrogate_scale')
+    want[:, :NMODES] *= sc[:, None]
+    assert np.allclose(d_x.cpu().numpy(), want, rtol=1e-6, atol=1e-7)
+    with pytest.raises(_lib.DgfsError):   # log column inside the range
+        _lib.check(lib.dgfs_surrogate_scale(M, NFEAT, d_e.data_ptr(), 1e-3,
+                                            0, NMODES, 10, 0, d_x.data_ptr(),
+                                            s), 'dgfs_surrogate_scale')
