@@ -14,12 +14,17 @@
 //               box, where f and Q hold only round-off; the window keeps that
 //               noise out of the coefficients
 //   embedding   a_k = (1/rho) cw sum_v chi f(c_v) phi_k(c^_v)
-//   target      b_k = cw sum_v chi Q(c_v) phi_k(c^_v) / (prefac rho^2 T^{gamma/2})
-//   reconstruct Q(c) = prefac rho^2 T^{gamma/2} T^{-3/2} W(c^) sum_k d_k phi_k(c^),
+//   target      b_k = cw sum_v chi g(c_v) phi_k(c^_v) / (prefac rho^2 T^{gamma/2})
+//               with g = Q, or, given the collision frequency nu (Q = G -
+//               nu f), the gain deviation g = G - nu M = Q + nu (f - M), M
+//               the local Maxwellian: smooth even where f jumps (diffuse
+//               walls), and O(f - M) near equilibrium
+//   reconstruct g(c) = prefac rho^2 T^{gamma/2} T^{-3/2} W(c^) sum_k d_k phi_k(c^),
 //               d = Gw^{-1} b with Gw_kl = int chi W phi_k phi_l dc^ (the
-//               windowed Gram matrix, condition number 1.75, passed in),
-//               followed by the FP64 least-squares projection onto zero
-//               mass, momentum and energy moments.
+//               windowed Gram matrix, condition number 1.75, passed in);
+//               Q = g, or Q = g - nu (f - M) given nu; then the FP64
+//               least-squares projection onto zero mass, momentum and
+//               energy moments.
 // The velocity grid is a tensor product, so every sum factorises into three
 // 1D contractions.  One CTA per solution point.
 #include <cmath>
@@ -111,13 +116,29 @@ __device__ void basis_tables(const FrameArgs& a, const double* mom, double (*H)[
   }
 }
 
-// out[m] = cw sum_v g(c_v) phi_m(c^_v) for the 220 modes, g read from a bank
-template <typename T>
-__device__ void project_modes(const T* g, int upt, int e, const FrameArgs& a, const double* mom,
+// Fields projected by project_modes: a bank value, or the gain deviation
+// G - nu M = Q + nu (f - M) of a collision bank Q given the collision
+// frequency nu and the local Maxwellian M (value Mv at the node).
+template <typename T> struct BankField {
+  const T* g;
+  __device__ double operator()(long long ix, double) const { return (double)g[ix]; }
+};
+template <typename T> struct GainDevField {
+  const T *q, *nu, *f;
+  __device__ double operator()(long long ix, double Mv) const {
+    return (double)q[ix] + (double)nu[ix] * ((double)f[ix] - Mv);
+  }
+};
+
+// out[m] = cw sum_v chi g(c_v) phi_m(c^_v) for the 220 modes
+template <typename Field>
+__device__ void project_modes(const Field& g, int upt, int e, const FrameArgs& a, const double* mom,
                               double (*H)[kMaxN][kP], double* t1, double* t2, double* out) {
   const int N = a.N;
   const long long V = (long long)N * N * N;
   const double h = 2.0 * a.L / N, c00 = -a.L + a.L / N, rt = rsqrt(mom[4]);
+  // local Maxwellian rho T^{-3/2} pi^{-3/2} e^{-|c^|^2}
+  const double m0 = mom[0] * rt * rt * rt * 0.17958712212516656;
   // t1[I][J][k] = sum_K chi g[I][J][K] Hz[K][k]
   for (int r = threadIdx.x; r < N * N; r += kThreads) {
     double acc[kP];
@@ -127,8 +148,9 @@ __device__ void project_modes(const T* g, int upt, int e, const FrameArgs& a, co
     const double r2xy = dx * dx + dy * dy;
     for (int K = 0; K < N; ++K) {
       const double dz = (c00 + K * h - mom[3]) * rt;
-      const double chi = 0.5 * erfc((sqrt(r2xy + dz * dz) - kWinR) * (1.0 / kWinW));
-      const double gv = chi * (double)g[dgfs::soa_ix(upt, a.ldim, e, (long long)r * N + K, V, 32)];
+      const double r2 = r2xy + dz * dz;
+      const double chi = 0.5 * erfc((sqrt(r2) - kWinR) * (1.0 / kWinW));
+      const double gv = chi * g(dgfs::soa_ix(upt, a.ldim, e, (long long)r * N + K, V, 32), m0 * exp(-r2));
 #pragma unroll
       for (int k = 0; k < kP; ++k) acc[k] += gv * H[2][K][k];
     }
@@ -160,6 +182,7 @@ __device__ void project_modes(const T* g, int upt, int e, const FrameArgs& a, co
 // targets B[pt][256] of a collision bank Q.
 template <typename T>
 __global__ void __launch_bounds__(kThreads) embed_kernel(const T* __restrict__ f, const T* __restrict__ Q,
+                                                         const T* __restrict__ nu,
                                                          FrameArgs a, float* __restrict__ X,
                                                          float* __restrict__ B, double* __restrict__ mom_out,
                                                          float* __restrict__ eps) {
@@ -180,7 +203,7 @@ __global__ void __launch_bounds__(kThreads) embed_kernel(const T* __restrict__ f
   basis_tables(a, mom, H);
   __syncthreads();
 
-  project_modes<T>(f, upt, e, a, mom, H, t1, t2, coef);
+  project_modes(BankField<T>{f}, upt, e, a, mom, H, t1, t2, coef);
   const double rho = mom[0];
   double ne = 0;
   for (int k = threadIdx.x; k < kFeat; k += kThreads) {
@@ -201,7 +224,10 @@ __global__ void __launch_bounds__(kThreads) embed_kernel(const T* __restrict__ f
     for (int k = 0; k < 5; ++k) mom_out[(long long)pt * 5 + k] = mom[k];
   }
   if (Q) {
-    project_modes<T>(Q, upt, e, a, mom, H, t1, t2, coef);
+    if (nu)
+      project_modes(GainDevField<T>{Q, nu, f}, upt, e, a, mom, H, t1, t2, coef);
+    else
+      project_modes(BankField<T>{Q}, upt, e, a, mom, H, t1, t2, coef);
     const double s = 1.0 / (a.prefac * rho * rho * pow(mom[4], 0.5 * a.gamma));
     for (int k = threadIdx.x; k < kFeat; k += kThreads)
       B[(long long)pt * kFeat + k] = k < kModes ? (float)(coef[k] * s) : 0.f;
@@ -217,6 +243,8 @@ __global__ void __launch_bounds__(kThreads) reconstruct_kernel(const float* __re
                                                                const int* __restrict__ gate, FrameArgs a,
                                                                const double* __restrict__ ginv,
                                                                const double* __restrict__ gwinv,
+                                                               const T* __restrict__ f,
+                                                               const T* __restrict__ nu,
                                                                T* __restrict__ Q) {
   extern __shared__ double sm[];
   __shared__ double red[kThreads / 32];
@@ -265,6 +293,7 @@ __global__ void __launch_bounds__(kThreads) reconstruct_kernel(const float* __re
   // pi^{-3/2}
   const double scale = a.prefac * rho * rho * pow(Tt, 0.5 * a.gamma) * pow(Tt, -1.5) * 0.17958712212516656;
   const double h = 2.0 * a.L / N, c00 = -a.L + a.L / N, rt = rsqrt(Tt);
+  const double mscale = rho * rt * rt * rt * 0.17958712212516656;  // local Maxwellian
   // Q(c) = scale e^{-|c^|^2} sum_i r2[i][J][K] Hx[I][i]; moments for the projection
   double mm[5] = {0, 0, 0, 0, 0};
   for (long long v = threadIdx.x; v < V; v += kThreads) {
@@ -273,8 +302,11 @@ __global__ void __launch_bounds__(kThreads) reconstruct_kernel(const float* __re
     for (int i = 0; i < kP; ++i) s += r2[((long long)i * N + J) * N + K] * H[0][I][i];
     const double cx = c00 + I * h, cy = c00 + J * h, cz = c00 + K * h;
     const double dx = (cx - mom[1]) * rt, dy = (cy - mom[2]) * rt, dz = (cz - mom[3]) * rt;
-    const double q = scale * exp(-(dx * dx + dy * dy + dz * dz)) * s;
-    Q[dgfs::soa_ix(upt, a.ldim, e, v, V, 32)] = (T)q;
+    const double ex = exp(-(dx * dx + dy * dy + dz * dz));
+    const long long ix = dgfs::soa_ix(upt, a.ldim, e, v, V, 32);
+    double q = scale * ex * s;
+    if (nu) q -= (double)nu[ix] * ((double)f[ix] - mscale * ex);  // Q = dG - nu (f - M)
+    Q[ix] = (T)q;
     mm[0] += q;
     mm[1] += q * cx;
     mm[2] += q * cy;
@@ -356,11 +388,11 @@ int check_frame(int precision, int N, int nupts, int neles, long long ldim, doub
 
 }  // namespace
 
-extern "C" int dgfs_hermite_embed(int precision, const void* f, const void* Q, int nupts, int neles,
-                                  long long ldim, int Nv, double L, double cw, double prefactor, double gamma,
-                                  float* X, float* B, double* mom, float* eps, void* stream) {
+extern "C" int dgfs_hermite_embed(int precision, const void* f, const void* Q, const void* nu, int nupts,
+                                  int neles, long long ldim, int Nv, double L, double cw, double prefactor,
+                                  double gamma, float* X, float* B, double* mom, float* eps, void* stream) {
   dgfs::clear_error();
-  if (!f || !X || !mom || !eps || (Q && !B)) return dgfs::set_error(DGFS_ERR_INVALID, "null pointer");
+  if (!f || !X || !mom || !eps || (Q && !B) || (nu && !Q)) return dgfs::set_error(DGFS_ERR_INVALID, "null pointer");
   int rc = check_frame(precision, Nv, nupts, neles, ldim, L, cw);
   if (!rc) rc = init_modes();
   if (rc) return rc;
@@ -371,11 +403,11 @@ extern "C" int dgfs_hermite_embed(int precision, const void* f, const void* Q, i
     return dgfs::set_error(DGFS_ERR_CUDA, "smem attribute");
   const unsigned grid = (unsigned)(nupts * neles);
   if (precision == 64)
-    embed_kernel<double><<<grid, kThreads, smem, (cudaStream_t)stream>>>((const double*)f, (const double*)Q, a, X, B,
-                                                                          mom, eps);
+    embed_kernel<double><<<grid, kThreads, smem, (cudaStream_t)stream>>>((const double*)f, (const double*)Q,
+                                                                          (const double*)nu, a, X, B, mom, eps);
   else
-    embed_kernel<float><<<grid, kThreads, smem, (cudaStream_t)stream>>>((const float*)f, (const float*)Q, a, X, B,
-                                                                         mom, eps);
+    embed_kernel<float><<<grid, kThreads, smem, (cudaStream_t)stream>>>((const float*)f, (const float*)Q,
+                                                                         (const float*)nu, a, X, B, mom, eps);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return dgfs::set_error(DGFS_ERR_CUDA, "embed launch: %s", cudaGetErrorString(e));
   return DGFS_OK;
@@ -384,9 +416,10 @@ extern "C" int dgfs_hermite_embed(int precision, const void* f, const void* Q, i
 extern "C" int dgfs_hermite_reconstruct(int precision, const float* B, const double* mom, const int* gate,
                                         int nupts, int neles, long long ldim, int Nv, double L, double cw,
                                         double prefactor, double gamma, const double* ginv,
-                                        const double* gwinv, void* Q, void* stream) {
+                                        const double* gwinv, const void* f, const void* nu, void* Q,
+                                        void* stream) {
   dgfs::clear_error();
-  if (!B || !mom || !ginv || !Q) return dgfs::set_error(DGFS_ERR_INVALID, "null pointer");
+  if (!B || !mom || !ginv || !Q || (nu && !f)) return dgfs::set_error(DGFS_ERR_INVALID, "null pointer");
   int rc = check_frame(precision, Nv, nupts, neles, ldim, L, cw);
   if (!rc) rc = init_modes();
   if (rc) return rc;
@@ -398,11 +431,11 @@ extern "C" int dgfs_hermite_reconstruct(int precision, const float* B, const dou
     return dgfs::set_error(DGFS_ERR_CUDA, "smem attribute");
   const unsigned grid = (unsigned)(nupts * neles);
   if (precision == 64)
-    reconstruct_kernel<double><<<grid, kThreads, smem, (cudaStream_t)stream>>>(B, mom, gate, a, ginv, gwinv,
-                                                                               (double*)Q);
+    reconstruct_kernel<double><<<grid, kThreads, smem, (cudaStream_t)stream>>>(
+        B, mom, gate, a, ginv, gwinv, (const double*)f, (const double*)nu, (double*)Q);
   else
-    reconstruct_kernel<float><<<grid, kThreads, smem, (cudaStream_t)stream>>>(B, mom, gate, a, ginv, gwinv,
-                                                                              (float*)Q);
+    reconstruct_kernel<float><<<grid, kThreads, smem, (cudaStream_t)stream>>>(
+        B, mom, gate, a, ginv, gwinv, (const float*)f, (const float*)nu, (float*)Q);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return dgfs::set_error(DGFS_ERR_CUDA, "reconstruct launch: %s", cudaGetErrorString(e));
   return DGFS_OK;

@@ -590,3 +590,151 @@ extern "C" int dgfs_vhs_apply_list(dgfs_vhs* h, const void* f, void* Q, int nupt
   if (!pts) return set_error(DGFS_ERR_INVALID, "null point list");
   return vhs_launch(h, f, Q, nupts, neles, ldim, soasz, 0, max_points, stream, pts, count);
 }
+
+// ---------------------------------------------------------------------------
+// Collision frequency nu(c) = prefac Re IFFT(b2 FFT(f) / V)(c), the loss rate
+// of Q = prefac (gain - f Re IFFT(b2 F)) (vhs-gll.mako:209-220, 246-266).
+// One CTA per point; FP32 arithmetic whatever the bank precision (the
+// surrogate needs nu to ~1e-6 relative).  f is real, so the transform along
+// the last axis keeps the N/2+1 non-negative frequencies; b2 is even on the
+// index grid (its Nyquist index maps onto itself), so b2 F stays Hermitian
+// and the complex-to-real inverse along that axis returns the real part the
+// reference takes.  Shared memory: N^2 (N/2+1) complex floats.
+// ---------------------------------------------------------------------------
+namespace {
+
+template <typename TB, int N>
+__global__ void __launch_bounds__(256) loss_rate_kernel(const TB* __restrict__ f, TB* __restrict__ nu, int64_t ldim,
+                                                        int nupts, int neles, int soasz, const TB* __restrict__ b2,
+                                                        float prefac, const int* __restrict__ gate) {
+  using C = cx<float>;
+  constexpr int H = N / 2 + 1, V = N * N * N;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* s = reinterpret_cast<C*>(smem_raw);  // [N][N][H]
+  const int pt = blockIdx.x;
+  if (gate && !gate[pt]) return;  // uniform over the CTA
+  const int upt = pt / neles, elem = pt % neles;
+  const int tid = threadIdx.x, NT = blockDim.x;
+
+  // forward along k (real to half spectrum)
+  for (int line = tid; line < N * N; line += NT) {
+    C x[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k)
+      x[k] = mk<C>((float)f[soa_ix(upt, ldim, elem, (int64_t)line * N + k, V, soasz)], 0.f);
+    fft<float, N, -1>(x);
+#pragma unroll
+    for (int k = 0; k < H; ++k) s[line * H + k] = x[k];
+  }
+  __syncthreads();
+  // forward along j, then along i
+  for (int line = tid; line < N * H; line += NT) {
+    const int i = line / H, k = line % H;
+    C x[N];
+#pragma unroll
+    for (int j = 0; j < N; ++j) x[j] = s[(i * N + j) * H + k];
+    fft<float, N, -1>(x);
+#pragma unroll
+    for (int j = 0; j < N; ++j) s[(i * N + j) * H + k] = x[j];
+  }
+  __syncthreads();
+  for (int line = tid; line < N * H; line += NT) {
+    const int j = line / H, k = line % H;
+    C x[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) x[i] = s[(i * N + j) * H + k];
+    fft<float, N, -1>(x);
+    // b2 / V, then the inverse along i
+#pragma unroll
+    for (int i = 0; i < N; ++i) x[i] = cscale(x[i], (float)b2[(i * N + j) * N + k] * (1.f / V));
+    fft<float, N, +1>(x);
+#pragma unroll
+    for (int i = 0; i < N; ++i) s[(i * N + j) * H + k] = x[i];
+  }
+  __syncthreads();
+  for (int line = tid; line < N * H; line += NT) {
+    const int i = line / H, k = line % H;
+    C x[N];
+#pragma unroll
+    for (int j = 0; j < N; ++j) x[j] = s[(i * N + j) * H + k];
+    fft<float, N, +1>(x);
+#pragma unroll
+    for (int j = 0; j < N; ++j) s[(i * N + j) * H + k] = x[j];
+  }
+  __syncthreads();
+  // complex-to-real inverse along k
+  for (int line = tid; line < N * N; line += NT) {
+    C x[N];
+#pragma unroll
+    for (int k = 0; k < H; ++k) x[k] = s[line * H + k];
+#pragma unroll
+    for (int k = H; k < N; ++k) {
+      const C c = s[line * H + (N - k)];
+      x[k] = mk<C>(c.x, -c.y);
+    }
+    fft<float, N, +1>(x);
+#pragma unroll
+    for (int k = 0; k < N; ++k) nu[soa_ix(upt, ldim, elem, (int64_t)line * N + k, V, soasz)] = (TB)(prefac * x[k].x);
+  }
+}
+
+template <typename TB, int N>
+cudaError_t launch_loss_rate(const dgfs_vhs* h, const void* f, void* nu, long long ldim, int nupts, int neles,
+                             int soasz, const int* gate, cudaStream_t st) {
+  const size_t smem = (size_t)N * N * (N / 2 + 1) * sizeof(cx<float>);
+  static bool attr[64];
+  const auto fn = loss_rate_kernel<TB, N>;
+  if (h->device >= 0 && h->device < 64 && !attr[h->device]) {
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr[h->device] = true;
+  }
+  fn<<<(unsigned)(nupts * neles), 256, smem, st>>>((const TB*)f, (TB*)nu, ldim, nupts, neles, soasz,
+                                                  (const TB*)h->b2, (float)h->prefac, gate);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+extern "C" int dgfs_vhs_loss_rate(dgfs_vhs* h, const void* f, void* nu, int nupts, int neles, long long ldim,
+                                  int soasz, const int* gate, void* stream) {
+  clear_error();
+  if (!h) return set_error(DGFS_ERR_INVALID, "null handle");
+  if (!f || !nu) return set_error(DGFS_ERR_INVALID, "null bank pointer");
+  if (nupts < 1 || neles < 1 || soasz < 1) return set_error(DGFS_ERR_INVALID, "bad bank shape");
+  const long long nblk = (neles + soasz - 1) / soasz;
+  if (ldim < nblk * soasz * (long long)h->V) return set_error(DGFS_ERR_INVALID, "ldim too small");
+  if ((long long)nupts * neles > 0x7fffffffLL) return set_error(DGFS_ERR_UNSUPPORTED, "too many points");
+  int dev = -1;
+  cudaGetDevice(&dev);
+  if (dev != h->device)
+    return set_error(DGFS_ERR_INVALID, "handle built on device %d used on device %d", h->device, dev);
+  const size_t esz = h->prec == 64 ? 8 : 4;
+  const char* fb = (const char*)f;
+  const char* nb = (const char*)nu;
+  const size_t bytes = (size_t)nupts * (size_t)ldim * esz;
+  if (fb < nb + bytes && nb < fb + bytes) return set_error(DGFS_ERR_INVALID, "f and nu overlap");
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = cudaErrorInvalidValue;
+#define LR(TB, NN) e = launch_loss_rate<TB, NN>(h, f, nu, ldim, nupts, neles, soasz, gate, st)
+  if (h->prec == 64) {
+    switch (h->N) {
+      case 8: LR(double, 8); break;
+      case 16: LR(double, 16); break;
+      case 24: LR(double, 24); break;
+      case 32: LR(double, 32); break;
+      default: return set_error(DGFS_ERR_UNSUPPORTED, "Nv=%d", h->N);
+    }
+  } else {
+    switch (h->N) {
+      case 8: LR(float, 8); break;
+      case 16: LR(float, 16); break;
+      case 24: LR(float, 24); break;
+      case 32: LR(float, 32); break;
+      default: return set_error(DGFS_ERR_UNSUPPORTED, "Nv=%d", h->N);
+    }
+  }
+#undef LR
+  if (e != cudaSuccess) return set_error(DGFS_ERR_CUDA, "loss-rate launch: %s", cudaGetErrorString(e));
+  return DGFS_OK;
+}

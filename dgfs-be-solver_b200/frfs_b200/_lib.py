@@ -45,6 +45,8 @@ _SIGS = {
     'dgfs_vhs_apply_list': (c_int, [c_void_p, c_void_p, c_void_p, c_int,
                                     c_int, c_ll, c_int, c_void_p, c_void_p,
                                     c_int, c_void_p]),
+    'dgfs_vhs_loss_rate': (c_int, [c_void_p, c_void_p, c_void_p, c_int,
+                                   c_int, c_ll, c_int, c_void_p, c_void_p]),
     'dgfs_vhs_info': (c_int, [c_void_p, ct.POINTER(c_int),
                               ct.POINTER(c_int), ct.POINTER(c_int),
                               ct.POINTER(c_int)]),

@@ -13,12 +13,15 @@ Per solution point:
 3. the degree >= 2 coefficients are divided by the deviation size
    s = max(eps, 1e-3) and log(s) is appended; an MLP (256 -> 512 -> 512 ->
    512 -> 256, tanh, with a linear skip from the input; BF16 weights, FP32
-   accumulation) predicts the windowed Hermite coefficients of Q(f) divided
-   by prefac rho^2 T^{gamma/2} s (near equilibrium Q is linear in f - M, so
-   both sides are O(1) whatever the distance from equilibrium);
-4. Q is rebuilt on the velocity grid (windowed coefficients mapped back by
-   the inverse windowed Gram matrix) and projected in FP64 onto zero mass,
-   momentum and energy moments.
+   accumulation) predicts the windowed Hermite coefficients of the gain
+   deviation G - nu M = Q + nu (f - M) (nu the collision frequency, M the
+   local Maxwellian) divided by prefac rho^2 T^{gamma/2} s: it is smooth
+   even where f jumps at a diffuse wall, and near equilibrium it is linear
+   in f - M, so both sides are O(1) whatever the distance from equilibrium;
+4. nu(c) is computed exactly (two 3D transforms per point), Q = (G - nu M)
+   - nu (f - M) is rebuilt on the velocity grid (windowed coefficients
+   mapped back by the inverse windowed Gram matrix) and projected in FP64
+   onto zero mass, momentum and energy moments.
 
 A point uses the surrogate when its non-equilibrium measure eps (the norm of
 its Hermite coefficients of degree >= 2, a local Knudsen indicator: Grad's
@@ -43,13 +46,13 @@ c_int, c_ll, c_double, c_float, c_void_p = (ct.c_int, ct.c_longlong,
                                             ct.c_double, ct.c_float,
                                             ct.c_void_p)
 _lib.declare('dgfs_hermite_embed', c_int,
-             [c_int, c_void_p, c_void_p, c_int, c_int, c_ll, c_int, c_double,
-              c_double, c_double, c_double, c_void_p, c_void_p, c_void_p,
-              c_void_p, c_void_p])
+             [c_int, c_void_p, c_void_p, c_void_p, c_int, c_int, c_ll, c_int,
+              c_double, c_double, c_double, c_double, c_void_p, c_void_p,
+              c_void_p, c_void_p, c_void_p])
 _lib.declare('dgfs_hermite_reconstruct', c_int,
              [c_int, c_void_p, c_void_p, c_void_p, c_int, c_int, c_ll, c_int,
               c_double, c_double, c_double, c_double, c_void_p, c_void_p,
-              c_void_p, c_void_p])
+              c_void_p, c_void_p, c_void_p, c_void_p])
 _lib.declare('dgfs_surrogate_gate', c_int,
              [c_int, c_void_p, c_float, c_void_p, c_void_p, c_void_p,
               c_void_p])
@@ -310,8 +313,28 @@ class VHSSurrogate:
         return self.backend.stream
 
     # -- features ------------------------------------------------------------
-    def embed(self, fbank, qbank=None, out=None):
-        """Features X, targets B (when qbank), frame mom, measure eps."""
+    def nu_bank(self, fbank):
+        """Workspace bank for the collision frequency nu(c)."""
+        key = ('nu',) + tuple(fbank.ioshape)
+        b = self.ws._bufs.get(key)
+        if b is None:
+            b = self.ws._bufs[key] = self.backend.matrix(fbank.ioshape)
+        return b
+
+    def loss_rate(self, fbank, nubank, gate=None):
+        """nu(c) at the points with gate != 0 (all when gate is None)."""
+        nupts, _, neles = fbank.ioshape
+        _, ldim, _ = fbank.traits
+        _lib.check(_lib.load().dgfs_vhs_loss_rate(
+            self.sm._h, fbank._as_parameter_, nubank._as_parameter_, nupts,
+            neles, ldim, self.backend.soasz, _p(gate), self._s),
+            'dgfs_vhs_loss_rate')
+        return nubank
+
+    def embed(self, fbank, qbank=None, out=None, nubank=None):
+        """Features X, targets B (when qbank: coefficients of Q, or of the
+        gain deviation Q + nu (f - M) when nubank is given), frame mom,
+        measure eps."""
         nupts, _, neles = fbank.ioshape
         npts = nupts*neles
         _, ldim, _ = fbank.traits
@@ -326,7 +349,8 @@ class VHSSurrogate:
             X, B, mom, eps = out
         _lib.check(_lib.load().dgfs_hermite_embed(
             self.backend.precision, fbank._as_parameter_,
-            qbank._as_parameter_ if qbank else None, nupts, neles, ldim,
+            qbank._as_parameter_ if qbank else None,
+            nubank._as_parameter_ if nubank else None, nupts, neles, ldim,
             self.vm.Nv(), self.vm.L(), self.vm.cw(), self.sm.prefactor,
             self.sm._gamma, _p(X), _p(B), _p(mom), _p(eps), self._s),
             'dgfs_hermite_embed')
@@ -355,8 +379,10 @@ class VHSSurrogate:
         return self._scale(B, eps, 0, NMODES, inverse=inverse)
 
     def embed_scaled(self, fbank, qbank):
-        """Training pair rows (scaled features, scaled targets) and eps."""
-        X, B, _, eps = self.embed(fbank, qbank)
+        """Training pair rows (scaled features, scaled gain-deviation
+        targets) and eps."""
+        nu = self.loss_rate(fbank, self.nu_bank(fbank))
+        X, B, _, eps = self.embed(fbank, qbank, nubank=nu)
         return self.scale_features(X, eps), self.scale_targets(B, eps), eps
 
     def set_normalisation(self, X, B):
@@ -441,13 +467,14 @@ class VHSSurrogate:
         _lib.check(lib.dgfs_surrogate_gate(npts, _p(eps), thr, _p(gate),
                                            _p(plain), _p(nplain), self._s),
                    'dgfs_surrogate_gate')
+        nu = self.loss_rate(fbank, self.nu_bank(fbank), gate)
         Bp = self.scale_targets(self.predict(X), eps, inverse=True)
         _lib.check(lib.dgfs_hermite_reconstruct(
             self.backend.precision, _p(Bp), _p(mom), _p(gate), nupts, neles,
             ldim, self.vm.Nv(), self.vm.L(), self.vm.cw(),
             self.sm.prefactor, self.sm._gamma, _p(self.ginv),
-            _p(self.gwinv), qbank._as_parameter_, self._s),
-            'dgfs_hermite_reconstruct')
+            _p(self.gwinv), fbank._as_parameter_, nu._as_parameter_,
+            qbank._as_parameter_, self._s), 'dgfs_hermite_reconstruct')
         _lib.check(lib.dgfs_vhs_apply_list(
             self.sm._h, fbank._as_parameter_, qbank._as_parameter_, nupts,
             neles, ldim, self.backend.soasz, _p(plain), _p(nplain), npts,
@@ -456,8 +483,8 @@ class VHSSurrogate:
         return gate
 
     # kernels one collide() launches: embed, 2 scale, gate (+ counter
-    # reset), 2 affine, 5 GEMMs, reconstruct, plain list
-    launches_per_collide = 13
+    # reset), loss rate, 2 affine, 5 GEMMs, reconstruct, plain list
+    launches_per_collide = 14
 
     def residual_check(self, fbank, qbank, scratch, sample=16, seed=0):
         """Plain Q at a random sample of the last call's surrogate points

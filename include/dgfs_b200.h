@@ -113,6 +113,17 @@ DGFS_API int dgfs_vhs_apply_list(dgfs_vhs* h, const void* f, void* Q, int nupts,
                                  const int* pts, const int* count,
                                  int max_points, void* stream);
 
+/* Collision frequency nu(c) = prefactor Re IFFT(b2 FFT(f) / V)(c), the loss
+ * rate of Q = prefactor (gain - f Re IFFT(b2 F)) (vhs-gll.mako:209-220,
+ * 246-266), into a bank of the same layout and precision, at the points
+ * with gate[pt] != 0 (all when gate is NULL).  Computed in FP32 whatever
+ * the precision (two 3D transforms per point).  Used by the learned
+ * surrogate, which keeps the loss term exact; no counterpart in the
+ * reference. */
+DGFS_API int dgfs_vhs_loss_rate(dgfs_vhs* h, const void* f, void* nu,
+                                int nupts, int neles, long long ldim,
+                                int soasz, const int* gate, void* stream);
+
 /* Launch geometry chosen by the handle (for reporting and tuning). */
 DGFS_API int dgfs_vhs_info(const dgfs_vhs* h, int* cluster, int* threads,
                   int* smem_bytes, int* max_clusters);
@@ -259,30 +270,35 @@ DGFS_API int dgfs_moments(int precision, const void* f, int nupts, int neles,
  * descending); window chi(c^) = erfc((|c^| - 4)/0.4)/2.  Feature row
  * X[pt][256]: a_k = cw/rho sum_v chi f phi_k(c^_v) (k < 220), sqrt(T)/L,
  * ux/L, uy/L, uz/L, zeros.  Target row B[pt][256]:
- * b_k = cw sum_v chi Q phi_k(c^_v) / (prefactor rho^2 T^{gamma/2}).  mom[pt][5]
+ * b_k = cw sum_v chi g phi_k(c^_v) / (prefactor rho^2 T^{gamma/2}), g = Q,
+ * or g = Q + nu (f - M) (the gain deviation G - nu M, M the local
+ * Maxwellian) when the collision-frequency bank nu is given.  mom[pt][5]
  * = rho, ux, uy, uz, T; eps[pt] = |a_k, degree >= 2| (non-equilibrium
  * measure).  Nv <= 32, soasz 32.  All pointers are device pointers; point
  * id pt = upt*neles + elem.
  * ---------------------------------------------------------------------- */
 DGFS_API int dgfs_hermite_embed(int precision, const void* f, const void* Q,
-                                int nupts, int neles, long long ldim, int Nv,
-                                double L, double cw, double prefactor,
-                                double gamma, float* X, float* B, double* mom,
-                                float* eps, void* stream);
+                                const void* nu, int nupts, int neles,
+                                long long ldim, int Nv, double L, double cw,
+                                double prefactor, double gamma, float* X,
+                                float* B, double* mom, float* eps,
+                                void* stream);
 
-/* Q(c) = prefactor rho^2 T^{gamma/2} T^{-3/2} pi^{-3/2} e^{-|c^|^2}
+/* g(c) = prefactor rho^2 T^{gamma/2} T^{-3/2} pi^{-3/2} e^{-|c^|^2}
  * sum_k d_k phi_k(c^) with d = gwinv B[pt] (gwinv: 220x220 row-major
  * inverse of the windowed Gram matrix int chi W phi_k phi_l dc^; NULL uses
- * d = B[pt]), then the FP64 projection onto zero mass, momentum and energy
- * with the 5x5 inverse Gram matrix ginv of (1, c, |c|^2) on the grid;
- * written only where gate[pt] != 0 (all points when gate is NULL). */
+ * d = B[pt]); Q = g, or Q = g - nu (f - M) when the banks f and nu are
+ * given; then the FP64 projection onto zero mass, momentum and energy with
+ * the 5x5 inverse Gram matrix ginv of (1, c, |c|^2) on the grid; written
+ * only where gate[pt] != 0 (all points when gate is NULL). */
 DGFS_API int dgfs_hermite_reconstruct(int precision, const float* B,
                                       const double* mom, const int* gate,
                                       int nupts, int neles, long long ldim,
                                       int Nv, double L, double cw,
                                       double prefactor, double gamma,
                                       const double* ginv, const double* gwinv,
-                                      void* Q, void* stream);
+                                      const void* f, const void* nu, void* Q,
+                                      void* stream);
 
 /* gate[pt] = eps[pt] < threshold; the other points are appended to
  * plain[0 .. *nplain) (unordered) for dgfs_vhs_apply_list. */

@@ -82,8 +82,16 @@ def basis(cv, u, T, deg=DEG):
                      for m in modes(deg)])                      # (nmodes, V)
 
 
-def embed(f, cv, cw, L, Q=None, prefac=1.0, gamma=0.0):
-    """Features x (256), frame (rho, u, T), eps and (if Q) targets b (256)."""
+def local_maxwellian(cv, rho, u, T):
+    ch2 = np.sum(((cv - u[:, None])/np.sqrt(T))**2, axis=0)
+    return rho*T**-1.5*np.pi**-1.5*np.exp(-ch2)
+
+
+def embed(f, cv, cw, L, Q=None, prefac=1.0, gamma=0.0, nu=None):
+    """Features x (256), frame (rho, u, T), eps and (if Q) targets b (256)
+    of g = Q, or of the gain deviation g = Q + nu (f - M) given the
+    collision frequency nu (M the local Maxwellian)."""
+    f = np.asarray(f, np.float64)
     rho, u, T = frame(f, cv, cw)
     Phi = basis(cv, u, T)
     chi = window(cv, u, T)
@@ -96,16 +104,21 @@ def embed(f, cv, cw, L, Q=None, prefac=1.0, gamma=0.0):
     eps = np.sqrt(np.sum(a[deg >= 2]**2))
     b = None
     if Q is not None:
+        g = np.asarray(Q, np.float64)
+        if nu is not None:
+            g = g + np.asarray(nu, np.float64)*(
+                f - local_maxwellian(cv, rho, u, T))
         b = np.zeros(256)
-        b[:len(a)] = Phi @ (chi*np.asarray(Q, np.float64))*cw/(
-            prefac*rho*rho*T**(0.5*gamma))
+        b[:len(a)] = Phi @ (chi*g)*cw/(prefac*rho*rho*T**(0.5*gamma))
     return x, (rho, u, T), eps, b
 
 
-def reconstruct(b, mom, cv, prefac=1.0, gamma=0.0, Gw=None):
+def reconstruct(b, mom, cv, prefac=1.0, gamma=0.0, Gw=None, f=None,
+                nu=None):
     """Q from windowed coefficients b: d = Gw^{-1} b (Gw = window_gram();
-    None: d = b), Q = prefac rho^2 T^{gamma/2} T^{-3/2} W(c^) sum d_k phi_k,
-    then the conservation projection."""
+    None: d = b), g = prefac rho^2 T^{gamma/2} T^{-3/2} W(c^) sum d_k phi_k,
+    Q = g (or g - nu (f - M) given f and nu), then the conservation
+    projection."""
     rho, u, T = mom
     Phi = basis(cv, u, T)
     ch2 = np.sum(((cv - u[:, None])/np.sqrt(T))**2, axis=0)
@@ -114,6 +127,9 @@ def reconstruct(b, mom, cv, prefac=1.0, gamma=0.0, Gw=None):
     if Gw is not None:
         d = np.linalg.solve(Gw, d)
     Q = prefac*rho*rho*T**(0.5*gamma)*T**-1.5*W*(d @ Phi)
+    if nu is not None:
+        Q = Q - np.asarray(nu, np.float64)*(
+            np.asarray(f, np.float64) - local_maxwellian(cv, rho, u, T))
     return project_conservative(Q, cv)
 
 

@@ -64,10 +64,13 @@ def test_embed_matches_oracle(precision):
     q = random_states(cv, nupts*neles, seed=4).reshape(nupts, neles, -1)
     fb, qb = _bank(be, f), _bank(be, q)
     sur = VHSSurrogate(sm)
+    nub = sur.loss_rate(fb, be.matrix(fb.ioshape))
     X, B, mom, eps = sur.embed(fb, qb)
+    _, Bg, _, _ = sur.embed(fb, qb, nubank=nub)
     torch.cuda.synchronize()
-    X, B, mom, eps = (t.cpu().numpy() for t in (X, B, mom, eps))
+    X, B, Bg, mom, eps = (t.cpu().numpy() for t in (X, B, Bg, mom, eps))
     fu, qu = fb.get().astype(np.float64), qb.get().astype(np.float64)
+    nu = nub.get().astype(np.float64)
     for u in range(nupts):
         for e in range(neles):
             pt = u*neles + e
@@ -78,6 +81,36 @@ def test_embed_matches_oracle(precision):
             assert rel_err(X[pt], x) < 1e-5
             assert rel_err(B[pt], b) < 1e-5
             assert abs(eps[pt] - ep) < 1e-5*ep
+            _, _, _, bg = osur.embed(
+                fu[u, :, e], cv, cw, vm.L(), Q=qu[u, :, e],
+                prefac=sm.prefactor, gamma=sm._gamma, nu=nu[u, :, e])
+            assert rel_err(Bg[pt], bg) < 1e-5
+
+
+@pytest.mark.parametrize('precision', ['double', 'single'])
+@pytest.mark.parametrize('name', ['relax0d-n16', 'couette-n24',
+                                  'channel-n32'])
+def test_loss_rate_matches_oracle(precision, name):
+    """nu(c) = prefac Re IFFT(b2 FFT(f)/V), computed in FP32: 2e-6 of
+    max nu; the gated call leaves the other points untouched."""
+    be, vm, sm = _model(precision, name)
+    from helpers import oracle_for
+    ovm, pre, prefac = oracle_for(config(name, precision))
+    nupts, neles = 1, 3
+    f = random_states(vm.cv(), nupts*neles, seed=9).reshape(nupts, neles, -1)
+    fb = _bank(be, f)
+    sur = VHSSurrogate(sm)
+    gate = torch.tensor([1, 0, 1], dtype=torch.int32, device=be.device)
+    nub = sur.loss_rate(fb, be.matrix(fb.ioshape), gate)
+    torch.cuda.synchronize()
+    nu = nub.get()
+    fu = fb.get().astype(np.float64)
+    for e in range(neles):
+        if e == 1:
+            assert np.all(nu[0, :, e] == 0)
+            continue
+        _, lo = ovhs.vhs_Q_gain_loss(fu[0, :, e], ovm, pre, prefac)
+        assert rel_err(nu[0, :, e], lo.real) < 2e-6
 
 
 @pytest.mark.parametrize('precision', ['double', 'single'])
@@ -101,13 +134,18 @@ def test_reconstruct_matches_oracle_and_gate(precision):
     d_gate = torch.tensor(gate, device=dev)
     Gw = osur.window_gram()
     d_gwinv = torch.tensor(np.linalg.inv(Gw).ravel(), device=dev)
+    fh = random_states(cv, npts, seed=12).reshape(nupts, neles, -1)
+    nh = np.abs(random_states(cv, npts, seed=13)).reshape(nupts, neles, -1)
+    fb, nb = _bank(be, fh), _bank(be, 20*nh)
     _lib.check(_lib.load().dgfs_hermite_reconstruct(
         be.precision, d_b.data_ptr(), d_mom.data_ptr(), d_gate.data_ptr(),
         nupts, neles, out.traits[1], vm.Nv(), vm.L(), vm.cw(), sm.prefactor,
         sm._gamma, sur.ginv.data_ptr(), d_gwinv.data_ptr(),
-        out._as_parameter_, be.stream), 'dgfs_hermite_reconstruct')
+        fb._as_parameter_, nb._as_parameter_, out._as_parameter_,
+        be.stream), 'dgfs_hermite_reconstruct')
     torch.cuda.synchronize()
     Q = out.get()
+    fu, nuu = fb.get().astype(np.float64), nb.get().astype(np.float64)
     tol = 1e-10 if precision == 'double' else 2e-6
     for pt in range(npts):
         u, e = divmod(pt, neles)
@@ -116,7 +154,8 @@ def test_reconstruct_matches_oracle_and_gate(precision):
             continue
         Qo = osur.reconstruct(Bp[pt].astype(np.float64),
                               (mom[pt, 0], mom[pt, 1:4], mom[pt, 4]), cv,
-                              sm.prefactor, sm._gamma, Gw=Gw)
+                              sm.prefactor, sm._gamma, Gw=Gw, f=fu[u, :, e],
+                              nu=nuu[u, :, e])
         assert rel_err(Q[u, :, e], Qo) < tol
 
 
