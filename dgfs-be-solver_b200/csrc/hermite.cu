@@ -13,7 +13,9 @@
 //               polynomials reach 1e4..1e6 at the corners of the velocity
 //               box, where f and Q hold only round-off; the window keeps that
 //               noise out of the coefficients
-//   embedding   a_k = (1/rho) cw sum_v chi f(c_v) phi_k(c^_v)
+//   embedding   a_k = (1/rho) cw sum_v chi (f - M)(c_v) phi_k(c^_v), M the
+//               local Maxwellian rho T^{-3/2} W(c^) (zero for a Maxwellian
+//               up to round-off, whatever the window)
 //   target      b_k = cw sum_v chi g(c_v) phi_k(c^_v) / (prefac rho^2 T^{gamma/2})
 //               with g = Q, or, given the collision frequency nu (Q = G -
 //               nu f), the gain deviation g = G - nu M = Q + nu (f - M), M
@@ -123,6 +125,10 @@ template <typename T> struct BankField {
   const T* g;
   __device__ double operator()(long long ix, double) const { return (double)g[ix]; }
 };
+template <typename T> struct DevField {  // f - M
+  const T* f;
+  __device__ double operator()(long long ix, double Mv) const { return (double)f[ix] - Mv; }
+};
 template <typename T> struct GainDevField {
   const T *q, *nu, *f;
   __device__ double operator()(long long ix, double Mv) const {
@@ -177,9 +183,9 @@ __device__ void project_modes(const Field& g, int upt, int e, const FrameArgs& a
   __syncthreads();
 }
 
-// Features X[pt][256] (a_k, then sqrt(T)/L and u/L), frame mom[pt][5],
-// non-equilibrium measure eps[pt] = |a_k, degree >= 2|, and optionally the
-// targets B[pt][256] of a collision bank Q.
+// Features X[pt][256] (a_k of f - M, then sqrt(T)/L and u/L), frame
+// mom[pt][5], non-equilibrium measure eps[pt] = |a_k, degree >= 2|, and
+// optionally the targets B[pt][256] of a collision bank Q.
 template <typename T>
 __global__ void __launch_bounds__(kThreads) embed_kernel(const T* __restrict__ f, const T* __restrict__ Q,
                                                          const T* __restrict__ nu,
@@ -203,7 +209,7 @@ __global__ void __launch_bounds__(kThreads) embed_kernel(const T* __restrict__ f
   basis_tables(a, mom, H);
   __syncthreads();
 
-  project_modes(BankField<T>{f}, upt, e, a, mom, H, t1, t2, coef);
+  project_modes(DevField<T>{f}, upt, e, a, mom, H, t1, t2, coef);
   const double rho = mom[0];
   double ne = 0;
   for (int k = threadIdx.x; k < kFeat; k += kThreads) {

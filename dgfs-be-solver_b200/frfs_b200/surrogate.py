@@ -5,13 +5,14 @@ fallback and judge (no counterpart in the reference).
 Per solution point:
 
 1. FP64 moments rho, u, T define a local frame c^ = (c - u)/sqrt(T);
-2. the distribution is embedded as 220 Hermite coefficients (total degree
-   <= 9) in that frame, taken under the radial window erfc((|c^| - 4)/0.4)/2
+2. the deviation f - M from the local Maxwellian is embedded as 220
+   Hermite coefficients (total degree <= 9) in that frame, taken under the
+   radial window erfc((|c^| - 4)/0.4)/2
    (the polynomials would otherwise amplify the round-off that f and Q hold
    at the corners of the velocity box), plus sqrt(T)/L and u/L (256
    features);
 3. the degree >= 2 coefficients are divided by the deviation size
-   s = max(eps, 1e-3) and log(s) is appended; an MLP (256 -> 512 -> 512 ->
+   s = max(eps, 1e-4) and log(s) is appended; an MLP (256 -> 512 -> 512 ->
    512 -> 256, tanh, with a linear skip from the input; BF16 weights, FP32
    accumulation) predicts the windowed Hermite coefficients of the gain
    deviation G - nu M = Q + nu (f - M) (nu the collision frequency, M the
@@ -81,7 +82,7 @@ NFEAT = 256
 NMODES = 220
 WIDTH = 512
 DEG = 9
-EPS0 = 1e-3     # floor of the deviation scale (the window alone gives 7e-4)
+EPS0 = 1e-4     # floor of the deviation scale s = max(eps, EPS0)
 LOGCOL = 224    # feature column that carries log(max(eps, EPS0))
 WIN_R, WIN_W = 4.0, 0.4       # the kernels' window erfc((|c^| - 4)/0.4)/2
 
@@ -562,14 +563,35 @@ def random_uniform_state(vm, rng, bimodal):
 
 
 def random_point_states(vm, n, rng):
-    """n positive distributions spanning far from and near equilibrium:
-    two-Maxwellian mixtures (random weights, velocities in the unit ball,
-    temperatures in [0.5, 3]) and anisotropic Gaussians (one temperature per
-    axis), with densities in [0.5, 2]; shape (n, V)."""
+    """n distributions spanning far from and near equilibrium: Maxwellians
+    times 1 + a random degree 2..4 Hermite polynomial of relative size
+    1e-3 .. 5e-2 (log-uniform), two-Maxwellian mixtures (random weights,
+    velocities in the unit ball, temperatures in [0.5, 3]) and anisotropic
+    Gaussians (one temperature per axis), with densities in [0.5, 2];
+    shape (n, V)."""
     cv = vm.cv()
     out = np.empty((n, cv.shape[1]))
+    modes = hermite_modes()
     for i in range(n):
-        if rng.uniform() < 0.6:
+        kind = rng.uniform()
+        if kind < 0.35:
+            # near equilibrium: a random Maxwellian times 1 + a random
+            # degree 2..4 Hermite polynomial of size 1e-3 .. 5e-2
+            rho, T, u = 1.0, rng.uniform(0.5, 3.0), _ball(rng)
+            ch = (cv - u[:, None])/np.sqrt(T)
+            y = np.sqrt(2.0)*ch
+            P = [np.ones_like(y), y]
+            for k in range(1, 4):
+                P.append((y*P[k] - np.sqrt(k)*P[k - 1])/np.sqrt(k + 1))
+            h = np.zeros(cv.shape[1])
+            for (a, b, c) in modes:
+                if 2 <= a + b + c <= 4:
+                    h += rng.standard_normal()*P[a][0]*P[b][1]*P[c][2]
+            m = np.exp(-np.sum(ch*ch, axis=0))/(np.pi*T)**1.5
+            h *= 10**rng.uniform(-3, np.log10(0.05))/np.sqrt(
+                np.sum(m*h*h)/np.sum(m))
+            f = m*(1 + h)
+        elif kind < 0.75:
             w = rng.uniform(0.2, 0.8)
             f = 0.0
             for wk in (w, 1 - w):

@@ -267,8 +267,9 @@ DGFS_API int dgfs_moments(int precision, const void* f, int nupts, int neles,
  * Per point: FP64 frame rho, u, T (the formulas of dgfs_moments);
  * c^ = (c - u)/sqrt(T); phi_n(x) = He_n(sqrt(2) x)/sqrt(n!); 220 modes
  * (i, j, k), i + j + k <= 9, ordered by degree, then i, then j (both
- * descending); window chi(c^) = erfc((|c^| - 4)/0.4)/2.  Feature row
- * X[pt][256]: a_k = cw/rho sum_v chi f phi_k(c^_v) (k < 220), sqrt(T)/L,
+ * descending); window chi(c^) = erfc((|c^| - 4)/0.4)/2; M the local
+ * Maxwellian rho T^{-3/2} pi^{-3/2} e^{-|c^|^2}.  Feature row X[pt][256]:
+ * a_k = cw/rho sum_v chi (f - M) phi_k(c^_v) (k < 220), sqrt(T)/L,
  * ux/L, uy/L, uz/L, zeros.  Target row B[pt][256]:
  * b_k = cw sum_v chi g phi_k(c^_v) / (prefactor rho^2 T^{gamma/2}), g = Q,
  * or g = Q + nu (f - M) (the gain deviation G - nu M, M the local

@@ -88,14 +88,16 @@ def local_maxwellian(cv, rho, u, T):
 
 
 def embed(f, cv, cw, L, Q=None, prefac=1.0, gamma=0.0, nu=None):
-    """Features x (256), frame (rho, u, T), eps and (if Q) targets b (256)
-    of g = Q, or of the gain deviation g = Q + nu (f - M) given the
-    collision frequency nu (M the local Maxwellian)."""
+    """Features x (256: windowed coefficients of (f - M)/rho, sqrt(T)/L,
+    u/L), frame (rho, u, T), eps and (if Q) targets b (256) of g = Q, or of
+    the gain deviation g = Q + nu (f - M) given the collision frequency nu
+    (M the local Maxwellian)."""
     f = np.asarray(f, np.float64)
     rho, u, T = frame(f, cv, cw)
     Phi = basis(cv, u, T)
     chi = window(cv, u, T)
-    a = Phi @ (chi*np.asarray(f, np.float64))*cw/rho
+    M = local_maxwellian(cv, rho, u, T)
+    a = Phi @ (chi*(f - M))*cw/rho
     x = np.zeros(256)
     x[:len(a)] = a
     x[len(a)] = np.sqrt(T)/L
@@ -106,8 +108,7 @@ def embed(f, cv, cw, L, Q=None, prefac=1.0, gamma=0.0, nu=None):
     if Q is not None:
         g = np.asarray(Q, np.float64)
         if nu is not None:
-            g = g + np.asarray(nu, np.float64)*(
-                f - local_maxwellian(cv, rho, u, T))
+            g = g + np.asarray(nu, np.float64)*(f - M)
         b = np.zeros(256)
         b[:len(a)] = Phi @ (chi*g)*cw/(prefac*rho*rho*T**(0.5*gamma))
     return x, (rho, u, T), eps, b
