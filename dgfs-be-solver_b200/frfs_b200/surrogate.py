@@ -12,7 +12,7 @@ Per solution point:
    at the corners of the velocity box), plus sqrt(T)/L and u/L (256
    features);
 3. the degree >= 2 coefficients are divided by the deviation size
-   s = max(eps, 1e-4) and log(s) is appended; an MLP (256 -> 512 -> 512 ->
+   s = max(eps, 1e-3) and log(s) is appended; an MLP (256 -> 512 -> 512 ->
    512 -> 256, tanh, with a linear skip from the input; BF16 weights, FP32
    accumulation) predicts the windowed Hermite coefficients of the gain
    deviation G - nu M = Q + nu (f - M) (nu the collision frequency, M the
@@ -82,7 +82,8 @@ NFEAT = 256
 NMODES = 220
 WIDTH = 512
 DEG = 9
-EPS0 = 1e-4     # floor of the deviation scale s = max(eps, EPS0)
+EPS0 = 1e-3     # floor of the deviation scale s = max(eps, EPS0); below it
+                # Q is dominated by the operator's aliasing, not by f - M
 LOGCOL = 224    # feature column that carries log(max(eps, EPS0))
 WIN_R, WIN_W = 4.0, 0.4       # the kernels' window erfc((|c^| - 4)/0.4)/2
 
@@ -563,9 +564,11 @@ def random_uniform_state(vm, rng, bimodal):
 
 
 def random_point_states(vm, n, rng):
-    """n distributions spanning far from and near equilibrium: Maxwellians
-    times 1 + a random degree 2..4 Hermite polynomial of relative size
-    1e-3 .. 5e-2 (log-uniform), two-Maxwellian mixtures (random weights,
+    """n distributions spanning far from and near equilibrium: pairs of
+    slightly different Maxwellians on either side of a random plane (the
+    jump a diffuse wall leaves in f), Maxwellians times 1 + a random degree
+    2..4 Hermite polynomial of relative size 1e-3 .. 5e-2 (log-uniform),
+    two-Maxwellian mixtures (random weights,
     velocities in the unit ball, temperatures in [0.5, 3]) and anisotropic
     Gaussians (one temperature per axis), with densities in [0.5, 2];
     shape (n, V)."""
@@ -574,7 +577,22 @@ def random_point_states(vm, n, rng):
     modes = hermite_modes()
     for i in range(n):
         kind = rng.uniform()
-        if kind < 0.35:
+        if kind < 0.25:
+            # a diffuse-wall-like state: two Maxwellians that differ by a
+            # small random amount, one on each side of a random plane
+            # through the mean velocity
+            T, u = rng.uniform(0.5, 3.0), _ball(rng)
+            amp = 10**rng.uniform(-3, -0.5)
+            T2 = T*(1 + amp*rng.standard_normal())
+            u2 = u + amp*np.sqrt(T)*rng.standard_normal(3)
+            n = rng.standard_normal(3)
+            n /= np.linalg.norm(n)
+            side = np.sum((cv - u[:, None])*n[:, None], axis=0) > 0
+            m1 = np.exp(-np.sum((cv - u[:, None])**2, axis=0)/T)/(np.pi*T)**1.5
+            m2 = np.exp(-np.sum((cv - u2[:, None])**2, axis=0)/T2) \
+                / (np.pi*T2)**1.5
+            f = np.where(side, m1, m2*(1 + amp*rng.standard_normal()))
+        elif kind < 0.5:
             # near equilibrium: a random Maxwellian times 1 + a random
             # degree 2..4 Hermite polynomial of size 1e-3 .. 5e-2
             rho, T, u = 1.0, rng.uniform(0.5, 3.0), _ball(rng)
@@ -591,7 +609,7 @@ def random_point_states(vm, n, rng):
             h *= 10**rng.uniform(-3, np.log10(0.05))/np.sqrt(
                 np.sum(m*h*h)/np.sum(m))
             f = m*(1 + h)
-        elif kind < 0.75:
+        elif kind < 0.8:
             w = rng.uniform(0.2, 0.8)
             f = 0.0
             for wk in (w, 1 - w):
@@ -611,17 +629,18 @@ def random_point_states(vm, n, rng):
 class Harvester:
     """Collects the scaled (features, targets) of every (f, Q) pair it is
     called with (installed as ``system.collide_hook``), keeping points with
-    eps < eps_max."""
+    eps_min <= eps < eps_max (below EPS0 the target is the operator's
+    aliasing, which the features cannot predict)."""
 
-    def __init__(self, sur, eps_max):
+    def __init__(self, sur, eps_max, eps_min=EPS0):
         self.sur = sur
-        self.eps_max = eps_max
+        self.eps_max, self.eps_min = eps_max, eps_min
         self.X, self.B = [], []
         self.seen = 0
 
     def __call__(self, fbank, qbank):
         X, B, eps = self.sur.embed_scaled(fbank, qbank)
-        keep = eps < self.eps_max
+        keep = (eps < self.eps_max) & (eps >= self.eps_min)
         self.X.append(X[keep])
         self.B.append(B[keep])
         self.seen += eps.numel()
