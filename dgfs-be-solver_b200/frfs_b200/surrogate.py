@@ -26,7 +26,10 @@ Per solution point:
 
 A point uses the surrogate when its non-equilibrium measure eps (the norm of
 its Hermite coefficients of degree >= 2, a local Knudsen indicator: Grad's
-expansion deviates from the Maxwellian at O(Kn)) is below the threshold;
+expansion deviates from the Maxwellian at O(Kn)) is below the threshold and
+the velocity grid resolves its local Maxwellian ((L - |u_axis|) >=
+3.5 sqrt(T); beyond that the plain operator's own truncation error, which
+the features do not see, dominates Q);
 every other point runs the plain operator through a device point list, with
 no host round trip.  ``residual_check`` re-evaluates a sample of surrogate
 points with the plain operator and reports their relative error, which the
@@ -55,8 +58,8 @@ _lib.declare('dgfs_hermite_reconstruct', c_int,
               c_double, c_double, c_double, c_double, c_void_p, c_void_p,
               c_void_p, c_void_p, c_void_p, c_void_p])
 _lib.declare('dgfs_surrogate_gate', c_int,
-             [c_int, c_void_p, c_float, c_void_p, c_void_p, c_void_p,
-              c_void_p])
+             [c_int, c_void_p, c_float, c_void_p, c_double, c_double,
+              c_void_p, c_void_p, c_void_p, c_void_p])
 _lib.declare('dgfs_mlp_gemm', c_int,
              [c_int, c_int, c_int, c_void_p, c_ll, c_ll, c_void_p, c_int,
               c_ll, c_ll, c_void_p, c_void_p, c_void_p, c_ll, c_int, c_int,
@@ -85,6 +88,8 @@ DEG = 9
 EPS0 = 1e-3     # floor of the deviation scale s = max(eps, EPS0); below it
                 # Q is dominated by the operator's aliasing, not by f - M
 LOGCOL = 224    # feature column that carries log(max(eps, EPS0))
+RMIN = 3.5      # resolved frames: (L - |u_axis|) >= RMIN sqrt(T) (the local
+                # Maxwellian's mass outside the velocity box is ~e^-12)
 WIN_R, WIN_W = 4.0, 0.4       # the kernels' window erfc((|c^| - 4)/0.4)/2
 
 
@@ -384,8 +389,15 @@ class VHSSurrogate:
         """Training pair rows (scaled features, scaled gain-deviation
         targets) and eps."""
         nu = self.loss_rate(fbank, self.nu_bank(fbank))
-        X, B, _, eps = self.embed(fbank, qbank, nubank=nu)
-        return self.scale_features(X, eps), self.scale_targets(B, eps), eps
+        X, B, mom, eps = self.embed(fbank, qbank, nubank=nu)
+        return (self.scale_features(X, eps), self.scale_targets(B, eps), eps,
+                mom)
+
+    def resolved(self, mom):
+        """Frames whose local Maxwellian the velocity grid resolves (the
+        gate's condition)."""
+        umax = mom[:, 1:4].abs().max(dim=1).values
+        return (self.vm.L() - umax) >= RMIN*mom[:, 4].sqrt()
 
     def set_normalisation(self, X, B):
         """Per-feature standardisation from training data.  Features that
@@ -466,7 +478,8 @@ class VHSSurrogate:
         gate = ws.get('gate', (npts,), torch.int32)
         plain = ws.get('plain', (npts,), torch.int32)
         nplain = ws.get('nplain', (1,), torch.int32)
-        _lib.check(lib.dgfs_surrogate_gate(npts, _p(eps), thr, _p(gate),
+        _lib.check(lib.dgfs_surrogate_gate(npts, _p(eps), thr, _p(mom),
+                                           self.vm.L(), RMIN, _p(gate),
                                            _p(plain), _p(nplain), self._s),
                    'dgfs_surrogate_gate')
         nu = self.loss_rate(fbank, self.nu_bank(fbank), gate)
@@ -630,7 +643,7 @@ class Harvester:
     """Collects the scaled (features, targets) of every (f, Q) pair it is
     called with (installed as ``system.collide_hook``), keeping points with
     eps_min <= eps < eps_max (below EPS0 the target is the operator's
-    aliasing, which the features cannot predict)."""
+    aliasing, which the features cannot predict) and a resolved frame."""
 
     def __init__(self, sur, eps_max, eps_min=EPS0):
         self.sur = sur
@@ -639,8 +652,9 @@ class Harvester:
         self.seen = 0
 
     def __call__(self, fbank, qbank):
-        X, B, eps = self.sur.embed_scaled(fbank, qbank)
-        keep = (eps < self.eps_max) & (eps >= self.eps_min)
+        X, B, eps, mom = self.sur.embed_scaled(fbank, qbank)
+        keep = (eps < self.eps_max) & (eps >= self.eps_min) & \
+            self.sur.resolved(mom)
         self.X.append(X[keep])
         self.B.append(B[keep])
         self.seen += eps.numel()

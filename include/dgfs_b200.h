@@ -301,9 +301,12 @@ DGFS_API int dgfs_hermite_reconstruct(int precision, const float* B,
                                       const void* f, const void* nu, void* Q,
                                       void* stream);
 
-/* gate[pt] = eps[pt] < threshold; the other points are appended to
- * plain[0 .. *nplain) (unordered) for dgfs_vhs_apply_list. */
+/* gate[pt] = eps[pt] < threshold and, when the frames mom are given, the
+ * local Maxwellian resolved by the grid of half width L:
+ * min over axes of (L - |u_axis|) >= rmin sqrt(T); the other points are
+ * appended to plain[0 .. *nplain) (unordered) for dgfs_vhs_apply_list. */
 DGFS_API int dgfs_surrogate_gate(int npts, const float* eps, float threshold,
+                                 const double* mom, double L, double rmin,
                                  int* gate, int* plain, int* nplain,
                                  void* stream);
 

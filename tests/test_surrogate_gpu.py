@@ -168,12 +168,19 @@ def test_gate_builds_the_plain_list():
     plain = torch.full((1000,), -1, dtype=torch.int32, device=dev)
     n = torch.empty(1, dtype=torch.int32, device=dev)
     s = torch.cuda.current_stream().cuda_stream
+    mom = np.c_[np.ones(1000), rng.uniform(-1, 1, (1000, 3)),
+                rng.uniform(0.5, 3, 1000)]
+    d_mom = torch.tensor(mom, device=dev)
+    L, rmin = 5.5, 3.5
     _lib.check(_lib.load().dgfs_surrogate_gate(
-        1000, e.data_ptr(), 0.05, gate.data_ptr(), plain.data_ptr(),
-        n.data_ptr(), s), 'dgfs_surrogate_gate')
+        1000, e.data_ptr(), 0.05, d_mom.data_ptr(), L, rmin,
+        gate.data_ptr(), plain.data_ptr(), n.data_ptr(), s),
+        'dgfs_surrogate_gate')
     torch.cuda.synchronize()
     g = gate.cpu().numpy()
-    assert np.array_equal(g, (eps < np.float32(0.05)).astype(np.int32))
+    res = (L - np.abs(mom[:, 1:4]).max(axis=1)) >= rmin*np.sqrt(mom[:, 4])
+    assert 0 < res.sum() < 1000
+    assert np.array_equal(g, ((eps < np.float32(0.05)) & res).astype(np.int32))
     k = int(n.item())
     assert k == int(np.sum(g == 0))
     assert sorted(plain.cpu().numpy()[:k]) == list(np.nonzero(g == 0)[0])
@@ -317,8 +324,9 @@ def test_training_reduces_loss():
 
 def test_collide_routes_points_and_conserves():
     """threshold 0: every point takes the plain operator (bit-identical to
-    fs_all); threshold huge: every point takes the network and its Q has
-    zero mass, momentum and energy; in between the routing follows eps."""
+    fs_all); threshold huge: every resolved point takes the network and its
+    Q has zero mass, momentum and energy; in between the routing follows
+    eps."""
     be, vm, sm = _model('single')
     cv = vm.cv()
     nupts, neles = 3, 12
@@ -336,25 +344,29 @@ def test_collide_routes_points_and_conserves():
     assert int(g.sum()) == 0
     assert np.array_equal(out.get(), ref.get())
 
+    _, _, mom, eps = sur.embed(fb)
+    e = eps.cpu().numpy()
+    res = sur.resolved(mom).cpu().numpy()
+    assert res.sum() >= npts - 4
     out2 = be.matrix(fb.ioshape)
-    g = sur.collide(fb, out2, threshold=1e30)
+    g = sur.collide(fb, out2, threshold=1e30).cpu().numpy()
     torch.cuda.synchronize()
-    assert int(g.sum()) == npts
+    assert np.array_equal(g, res.astype(np.int32))
     Q = out2.get().astype(np.float64)
     phi = np.vstack([np.ones(cv.shape[1]), cv, np.sum(cv*cv, axis=0)])
     for u in range(nupts):
-        for e in range(neles):
-            m = phi @ Q[u, :, e]
-            scale = np.abs(phi) @ np.abs(Q[u, :, e])
+        for el in range(neles):
+            if not g[u*neles + el]:
+                continue
+            m = phi @ Q[u, :, el]
+            scale = np.abs(phi) @ np.abs(Q[u, :, el])
             assert np.all(np.abs(m) < 1e-5*scale)
 
-    _, _, _, eps = sur.embed(fb)
-    e = eps.cpu().numpy()
     thr = float(np.median(e))
     out3 = be.matrix(fb.ioshape)
     g = sur.collide(fb, out3, threshold=thr).cpu().numpy()
     torch.cuda.synchronize()
-    assert np.array_equal(g, (e < np.float32(thr)).astype(np.int32))
+    assert np.array_equal(g, ((e < np.float32(thr)) & res).astype(np.int32))
     Q3, Qr, Q2 = out3.get(), ref.get(), out2.get()
     for pt in range(npts):
         u, el = divmod(pt, neles)
