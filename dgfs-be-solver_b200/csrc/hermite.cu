@@ -265,7 +265,8 @@ __global__ void __launch_bounds__(kThreads) reconstruct_kernel(const float* __re
   double* r1 = sm;                    // [kP][kP][N]   (i, j, K)
   double* r2 = sm + kP * kP * N;      // [kP][N][N]    (i, J, K)
   if (threadIdx.x < 5) mom[threadIdx.x] = mom_in[(long long)pt * 5 + threadIdx.x];
-  for (int k = threadIdx.x; k < kModes; k += kThreads) bw[k] = (double)Bp[(long long)pt * kFeat + k];
+  const bool zero = gate && gate[pt] == 2;  // relaxation only: G - nu M = 0
+  for (int k = threadIdx.x; k < kModes; k += kThreads) bw[k] = zero ? 0.0 : (double)Bp[(long long)pt * kFeat + k];
   __syncthreads();
   // d = Gw^{-1} b (windowed coefficients to expansion coefficients)
   for (int k = threadIdx.x; k < kModes; k += kThreads) {
@@ -339,16 +340,17 @@ __global__ void __launch_bounds__(kThreads) reconstruct_kernel(const float* __re
   }
 }
 
-// gate[pt] = eps[pt] < threshold and, given the frames mom, the local
-// Maxwellian resolved by the grid: min_axis (L - |u_axis|)/sqrt(T) >= rmin;
-// points that fail go to the plain list (order irrelevant: every point is
-// independent)
-__global__ void gate_kernel(int npts, const float* __restrict__ eps, float threshold,
+// gate[pt] = 1 when eps[pt] < threshold (2 when also eps[pt] < eps_zero:
+// the reconstruction then takes G - nu M = 0) and, given the frames mom,
+// the local Maxwellian is resolved by the grid:
+// min_axis (L - |u_axis|)/sqrt(T) >= rmin; gate 0 points go to the plain
+// list (order irrelevant: every point is independent)
+__global__ void gate_kernel(int npts, const float* __restrict__ eps, float threshold, float eps_zero,
                             const double* __restrict__ mom, double L, double rmin, int* __restrict__ gate,
                             int* __restrict__ plain, int* __restrict__ nplain) {
   const int pt = blockIdx.x * blockDim.x + threadIdx.x;
   if (pt >= npts) return;
-  int g = (eps[pt] < threshold) ? 1 : 0;
+  int g = (eps[pt] < threshold) ? (eps[pt] < eps_zero ? 2 : 1) : 0;
   if (mom) {
     const double* m = mom + (long long)pt * 5;
     const double umax = fmax(fabs(m[1]), fmax(fabs(m[2]), fabs(m[3])));
@@ -455,14 +457,15 @@ extern "C" int dgfs_hermite_reconstruct(int precision, const float* B, const dou
   return DGFS_OK;
 }
 
-extern "C" int dgfs_surrogate_gate(int npts, const float* eps, float threshold, const double* mom, double L,
-                                   double rmin, int* gate, int* plain, int* nplain, void* stream) {
+extern "C" int dgfs_surrogate_gate(int npts, const float* eps, float threshold, float eps_zero,
+                                   const double* mom, double L, double rmin, int* gate, int* plain, int* nplain,
+                                   void* stream) {
   dgfs::clear_error();
   if (npts < 1 || !eps || !gate || !plain || !nplain) return dgfs::set_error(DGFS_ERR_INVALID, "bad arguments");
   cudaError_t e = cudaMemsetAsync(nplain, 0, sizeof(int), (cudaStream_t)stream);
   if (e != cudaSuccess) return dgfs::set_error(DGFS_ERR_CUDA, "gate counter reset: %s", cudaGetErrorString(e));
-  gate_kernel<<<(npts + 255) / 256, 256, 0, (cudaStream_t)stream>>>(npts, eps, threshold, mom, L, rmin, gate,
-                                                                     plain, nplain);
+  gate_kernel<<<(npts + 255) / 256, 256, 0, (cudaStream_t)stream>>>(npts, eps, threshold, eps_zero, mom, L, rmin,
+                                                                     gate, plain, nplain);
   e = cudaGetLastError();
   return e == cudaSuccess ? DGFS_OK : dgfs::set_error(DGFS_ERR_CUDA, "gate launch: %s", cudaGetErrorString(e));
 }

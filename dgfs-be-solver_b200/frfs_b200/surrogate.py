@@ -30,8 +30,9 @@ expansion deviates from the Maxwellian at O(Kn)) is below the threshold and
 the velocity grid resolves its local Maxwellian ((L - |u_axis|) >=
 3.5 sqrt(T); beyond that the plain operator's own truncation error, which
 the features do not see, dominates Q);
-every other point runs the plain operator through a device point list, with
-no host round trip.  ``residual_check`` re-evaluates a sample of surrogate
+below eps = 1e-3 (where the plain Q is the operator's aliasing) the
+network is skipped and Q = -nu (f - M).  Every other point runs the plain
+operator through a device point list, with no host round trip.  ``residual_check`` re-evaluates a sample of surrogate
 points with the plain operator and reports their relative error, which the
 caller compares with its tolerance to fall back to the plain operator.
 
@@ -58,8 +59,8 @@ _lib.declare('dgfs_hermite_reconstruct', c_int,
               c_double, c_double, c_double, c_double, c_void_p, c_void_p,
               c_void_p, c_void_p, c_void_p, c_void_p])
 _lib.declare('dgfs_surrogate_gate', c_int,
-             [c_int, c_void_p, c_float, c_void_p, c_double, c_double,
-              c_void_p, c_void_p, c_void_p, c_void_p])
+             [c_int, c_void_p, c_float, c_float, c_void_p, c_double,
+              c_double, c_void_p, c_void_p, c_void_p, c_void_p])
 _lib.declare('dgfs_mlp_gemm', c_int,
              [c_int, c_int, c_int, c_void_p, c_ll, c_ll, c_void_p, c_int,
               c_ll, c_ll, c_void_p, c_void_p, c_void_p, c_ll, c_int, c_int,
@@ -478,10 +479,10 @@ class VHSSurrogate:
         gate = ws.get('gate', (npts,), torch.int32)
         plain = ws.get('plain', (npts,), torch.int32)
         nplain = ws.get('nplain', (1,), torch.int32)
-        _lib.check(lib.dgfs_surrogate_gate(npts, _p(eps), thr, _p(mom),
-                                           self.vm.L(), RMIN, _p(gate),
-                                           _p(plain), _p(nplain), self._s),
-                   'dgfs_surrogate_gate')
+        _lib.check(lib.dgfs_surrogate_gate(npts, _p(eps), thr, EPS0,
+                                           _p(mom), self.vm.L(), RMIN,
+                                           _p(gate), _p(plain), _p(nplain),
+                                           self._s), 'dgfs_surrogate_gate')
         nu = self.loss_rate(fbank, self.nu_bank(fbank), gate)
         Bp = self.scale_targets(self.predict(X), eps, inverse=True)
         _lib.check(lib.dgfs_hermite_reconstruct(
@@ -577,9 +578,10 @@ def random_uniform_state(vm, rng, bimodal):
 
 
 def random_point_states(vm, n, rng):
-    """n distributions spanning far from and near equilibrium: pairs of
-    slightly different Maxwellians on either side of a random plane (the
-    jump a diffuse wall leaves in f), Maxwellians times 1 + a random degree
+    """n distributions spanning far from and near equilibrium: wall fronts
+    (the gas Maxwellian on one side of a random plane, another Maxwellian on
+    the other, as the particles a diffuse wall emits leave it), Maxwellians
+    times 1 + a random degree
     2..4 Hermite polynomial of relative size 1e-3 .. 5e-2 (log-uniform),
     two-Maxwellian mixtures (random weights,
     velocities in the unit ball, temperatures in [0.5, 3]) and anisotropic
@@ -590,22 +592,26 @@ def random_point_states(vm, n, rng):
     modes = hermite_modes()
     for i in range(n):
         kind = rng.uniform()
-        if kind < 0.25:
-            # a diffuse-wall-like state: two Maxwellians that differ by a
-            # small random amount, one on each side of a random plane
-            # through the mean velocity
+        if kind < 0.3:
+            # a wall front: the gas Maxwellian on one side of a random plane,
+            # a different Maxwellian (another velocity, temperature and
+            # density, as a diffuse wall emits) on the other; the plane
+            # sits between half a thermal speed behind and three ahead of
+            # the mean velocity
             T, u = rng.uniform(0.5, 3.0), _ball(rng)
-            amp = 10**rng.uniform(-3, -0.5)
-            T2 = T*(1 + amp*rng.standard_normal())
-            u2 = u + amp*np.sqrt(T)*rng.standard_normal(3)
+            amp = 10**rng.uniform(-3, 0)
             n = rng.standard_normal(3)
             n /= np.linalg.norm(n)
-            side = np.sum((cv - u[:, None])*n[:, None], axis=0) > 0
+            T2 = T*np.clip(1 + amp*rng.standard_normal(), 0.5, 2.0)
+            u2 = u + amp*np.sqrt(T)*rng.standard_normal(3)
+            r2 = np.clip(1 + amp*rng.standard_normal(), 0.3, 3.0)
+            cut = np.sqrt(T)*rng.uniform(-0.5, 3.0)
+            side = np.sum((cv - u[:, None])*n[:, None], axis=0) > cut
             m1 = np.exp(-np.sum((cv - u[:, None])**2, axis=0)/T)/(np.pi*T)**1.5
             m2 = np.exp(-np.sum((cv - u2[:, None])**2, axis=0)/T2) \
                 / (np.pi*T2)**1.5
-            f = np.where(side, m1, m2*(1 + amp*rng.standard_normal()))
-        elif kind < 0.5:
+            f = np.where(side, r2*m2, m1)
+        elif kind < 0.55:
             # near equilibrium: a random Maxwellian times 1 + a random
             # degree 2..4 Hermite polynomial of size 1e-3 .. 5e-2
             rho, T, u = 1.0, rng.uniform(0.5, 3.0), _ball(rng)

@@ -109,7 +109,7 @@ def time_sweep(fn, reps, device):
 
 
 def run_study(ini, device='cuda:0', runs=5, steps=100, nsteps=200,
-              epochs=20, batch=1024, lr=1e-3, threshold=0.05, eps_max=0.2,
+              epochs=60, batch=1024, lr=1e-3, threshold=0.05, eps_max=0.2,
               check_every=50, tol=5e-3, reps=10, sphdesign=None, seed=1,
               max_pairs=200000, relax_points=576, relax_steps=100,
               relax_dt=0.005, log=None):
@@ -167,7 +167,9 @@ def run_study(ini, device='cuda:0', runs=5, steps=100, nsteps=200,
     out = scratch[0]
     t_plain = time_sweep(lambda: s32.sm.fs_all(fin, out), reps, device)
     t_sur = time_sweep(lambda: sur.collide(fin, out), reps, device)
-    gfrac = float(sur._last[0].float().mean())
+    g = sur._last[0]
+    gfrac = float((g != 0).float().mean())
+    gzero = float((g == 2).float().mean())
     eps = sur._last[1].cpu().numpy()
     return {
         'points': npts, 'pairs': npairs, 'pairs_solver': npairs_solver,
@@ -180,7 +182,7 @@ def run_study(ini, device='cuda:0', runs=5, steps=100, nsteps=200,
         'err_plain_fp32': errs(r32, u32, T32),
         'err_gate_without_network': errs(rz, uz, Tz),
         'residual_checks': chk,
-        'gate_fraction': gfrac,
+        'gate_fraction': gfrac, 'relaxation_only_fraction': gzero,
         'eps_quantiles': [float(q) for q in
                           np.quantile(eps, [0.1, 0.5, 0.9, 0.99])],
         'plain_ms_per_sweep': t_plain, 'surrogate_ms_per_sweep': t_sur,

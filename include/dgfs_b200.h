@@ -301,14 +301,16 @@ DGFS_API int dgfs_hermite_reconstruct(int precision, const float* B,
                                       const void* f, const void* nu, void* Q,
                                       void* stream);
 
-/* gate[pt] = eps[pt] < threshold and, when the frames mom are given, the
- * local Maxwellian resolved by the grid of half width L:
- * min over axes of (L - |u_axis|) >= rmin sqrt(T); the other points are
- * appended to plain[0 .. *nplain) (unordered) for dgfs_vhs_apply_list. */
+/* gate[pt] = 1 where eps[pt] < threshold (2 where also eps[pt] < eps_zero:
+ * dgfs_hermite_reconstruct then uses zero coefficients, i.e. Q = -nu (f - M)
+ * when nu is given) and, when the frames mom are given, the local
+ * Maxwellian is resolved by the grid of half width L: min over axes of
+ * (L - |u_axis|) >= rmin sqrt(T); gate 0 points are appended to
+ * plain[0 .. *nplain) (unordered) for dgfs_vhs_apply_list. */
 DGFS_API int dgfs_surrogate_gate(int npts, const float* eps, float threshold,
-                                 const double* mom, double L, double rmin,
-                                 int* gate, int* plain, int* nplain,
-                                 void* stream);
+                                 float eps_zero, const double* mom, double L,
+                                 double rmin, int* gate, int* plain,
+                                 int* nplain, void* stream);
 
 /* Scale-free surrogate rows, in place on X[M][ld]: columns [c0, c1) are
  * divided (inverse != 0: multiplied) by s = max(eps[m], eps0); forward
