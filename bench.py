@@ -12,7 +12,10 @@ SSP-RK2 solver step (default ``--mode step``: two collision sweeps over every
 solution point, two DG residuals with their boundary updates, one CUDA graph
 per stage) or one collision sweep alone (``--mode collide``: a single
 persistent launch of the fused VHS kernel).  The metric is Q(f) evaluations
-per second, whole job; the line also carries the DG step time.
+per second, whole job; the line also carries the DG step time and, at N=1
+on the Couette workload, the learned surrogate's run (``surrogate``: pairs
+harvested from the solver, training, rho/u/T errors against the plain FP64
+solution after 200 steps, evaluations per second plain vs surrogate).
 
 Multi-GPU (torchrun): every rank runs its own copy of the workload (the
 collision is independent per point, no data-path collective), so scaling is
@@ -58,6 +61,10 @@ def _parse():
                     help='VHS launch shape index (default: autotune)')
     ap.add_argument('--graphs', type=int, default=1,
                     help='CUDA graph per SSP-RK2 stage (--mode step)')
+    ap.add_argument('--surrogate', type=int, default=-1,
+                    help='train and judge the learned surrogate in this run '
+                         '(-1: on for couette-n24 at N=1)')
+    ap.add_argument('--surrogate-steps', type=int, default=200)
     return ap.parse_args()
 
 
@@ -383,13 +390,22 @@ def run_b200(args):
         stream.cuda_stream), 'dgfs_probe_fma_peak')
     flops_pt = sm.flops_per_point()
     achieved = flops_pt*npts/(vhs_ms*1e-3)/1e12
+    # DRAM bytes of one sweep from the committed ncu capture of the same
+    # launch (profiles/vhs_push_couette_n24_f32.md): f in + Q out, the
+    # tables stay in L2
+    traffic = 35.5e6 if (args.workload == 'couette-n24' and prec == 32) \
+        else None
     roof = {'bound': 'fp32-simt' if prec == 32 else 'fp64-simt',
             'achieved': achieved, 'peak': tf.value, 'unit': 'TFLOP/s',
             'frac': achieved/tf.value,
             'peak_source': 'measured in this run: FMA loop on every SM '
                            '(dgfs_probe_fma_peak)',
             'flops_per_point': flops_pt, 'launch_ms': vhs_ms,
-            'traffic': None, 'kernel': 'vhs_cluster_kernel'}
+            'traffic': traffic,
+            'traffic_source': 'ncu dram__bytes_read.sum + write.sum, '
+                              'profiles/vhs_push_couette_n24_f32.md'
+            if traffic else None,
+            'kernel': 'vhs_push_kernel / vhs_cluster_kernel (autotuned)'}
     extra = {}
     if args.mode == 'step':
         extra['dg_step_ms'] = ms_per_step
@@ -420,6 +436,19 @@ def run_b200(args):
             'kernels': 'dg_interp_kernel + dg_residual_kernel'}
     launch = sm.launch_info()
 
+    sur = None
+    want_sur = args.surrogate if args.surrogate >= 0 else int(
+        args.workload == 'couette-n24' and world == 1 and
+        args.mode == 'step')
+    if want_sur and world == 1:
+        # learned surrogate: harvested from the solver, trained with the
+        # project's kernels, judged against the plain FP64 solution
+        from frfs_b200 import workloads
+        from frfs_b200.surrogate_study import run_study
+        sur = run_study(workloads.WORKLOADS[args.workload],
+                        device=be.device, nsteps=args.surrogate_steps,
+                        sphdesign=SPHDESIGN)
+
     if rank == 0:
         cb = None
         if world == 1 and not args.no_cpu_baseline:
@@ -440,6 +469,8 @@ def run_b200(args):
                          'ms_by_variant': tune['all_ms']},
         }
         line.update(extra)
+        if sur is not None:
+            line['surrogate'] = sur
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
