@@ -13,6 +13,7 @@
 #include "../../include/dgfs_b200.h"
 #include "dgfs_internal.h"
 #include "vhs_push.cuh"
+#include "vhs_cube.cuh"
 
 namespace dgfs {
 
@@ -122,6 +123,40 @@ template <typename T, int N, int C, int MINB> static VhsVariant make_push() {
   return v;
 }
 
+template <int N> static cudaError_t launch_cube(const VhsArgs<float>& a, int nctas, cudaStream_t s) {
+  using G = CubeGeom<N>;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nctas, 1, 1);
+  cfg.blockDim = dim3(G::NT, 1, 1);
+  cfg.dynamicSmemBytes = G::SMEM_CX * sizeof(cx<float>);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 1;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, vhs_cube_kernel<N>, a);
+}
+
+// single-CTA kernel (FP32; kind 2 in dgfs_vhs_variant_kind)
+template <int N> static VhsVariant make_cube() {
+  using G = CubeGeom<N>;
+  VhsVariant v{};
+  v.prec = 32;
+  v.N = N;
+  v.C = 1;
+  v.db = 0;
+  v.push = 2;
+  v.minb = 1;
+  v.threads = G::NT;
+  v.smem = G::SMEM_CX * sizeof(cx<float>);
+  v.fn = (const void*)vhs_cube_kernel<N>;
+  v.launch32 = launch_cube<N>;
+  return v;
+}
+
 // Compiled launch shapes: (precision, N, cluster size, double-buffered
 // exchange, minimum CTAs per SM for the register budget).  The first entry
 // of each (precision, N) family is the default; the autotuner times the rest.
@@ -134,6 +169,8 @@ static const std::vector<VhsVariant>& variants() {
       make_push<float, 16, 4, 4>(),             make_push<float, 24, 8, 2>(),
       make_push<float, 24, 4, 1>(),             make_push<float, 24, 12, 3>(),
       make_push<float, 32, 16, 2>(),            make_push<float, 32, 8, 1>(),
+      make_cube<8>(),                           make_cube<16>(),
+      make_cube<24>(),
       make_variant<double, 8, 1, true, 4>(),    make_variant<double, 8, 2, true, 8>(),
       make_variant<double, 16, 4, true, 2>(),   make_variant<double, 16, 2, true, 1>(),
       make_variant<double, 16, 4, false, 3>(),

@@ -1,0 +1,431 @@
+// Single-CTA fast-spectral VHS kernel for FP32 and N <= 24: the whole N^3
+// problem of one point lives in one CTA's shared memory, so no transform
+// crosses SMs, and the transform count is nearly halved by an exact
+// restatement that uses the reality of f.
+//
+// The reference (frfs/solvers/dgfs/scattering.py:227-286, vhs-gll.mako)
+// computes per radial node p and direction q
+//     t3 = IFFT(cos a F), t4 = IFFT(sin a F),  S = t3^2 + t4^2 (complex),
+// with F = FFT(f)/V and a(l) = fac_p s_q.l, then
+//     Q = prefac (Re IFFT(sum_p w1_p FFT(sum_q S)) - f Re IFFT(b2 F)).
+// w1_p and b2 depend on |l| only, and the index grid maps -l onto itself up
+// to the Nyquist index (l0 holds -N/2 but not +N/2), so both are even on the
+// grid: Re IFFT(w FFT(S)) = IFFT(w FFT(Re S)) and only Re S matters.
+// Let l' = -l (mod N).  Real f gives F(l') = conj F(l), and
+// a(l') = -a(l) - theta(l), theta = fac_p N sum over the axes where l sits on
+// the Nyquist index of s_q[axis] (theta = 0 off those planes).  Splitting
+// cos a F and sin a F into parts that are even and odd under l -> l'
+// (conjugated) gives exactly
+//     Re S = Re(R^2) + Re(Nq^2),
+//     R  = IFFT(m F),  m = (cos a + cos(a+th) + sin a + sin(a+th)) / 2,
+//     Nq = IFFT(n F),  n = (cos a - cos(a+th) + sin a - sin(a+th)) / 2,
+// where n vanishes off the three Nyquist planes, so Nq is three 2D
+// transforms broadcast along one axis with a (-1)^x sign:
+//     Nq(x) = (-1)^x1 T1(x2,x3) + (-1)^x2 T2(x1,x3) + (-1)^x3 T3(x1,x2).
+// Off the Nyquist planes m = cos a + sin a: one complex transform per (p, q)
+// instead of two.  Per point: 1 + Nrho M + Nrho + 1 full transforms plus
+// the 2D ones (reference: 3 Nrho M + 3).  The last transform packs the two
+// real results: IFFT(fC + i b2 F) = Re QG + i Re Lf (fC and b2 F are
+// conjugate-even).
+//
+// Layout (shared memory, complex float): F for k3 <= N/2 ([N][N][N/2+1]),
+// the work cube as N^2 lines of N+1 (padding keeps line-parallel accesses
+// free of bank conflicts), the three Nyquist planes, the axis phases.
+// The gain spectrum fC accumulates in a global (L2-resident) slice per CTA.
+// Main threads own two lines per pass; NQ extra threads transform the
+// Nyquist planes during the first two passes of every (p, q).
+#pragma once
+
+#include "vhs_kernel.cuh"
+
+namespace dgfs {
+
+template <int N> struct CubeGeom {
+  static constexpr int H = N / 2 + 1;
+  static constexpr int NN = N * N;
+  static constexpr int LP = N + 1;                      // padded line stride
+  static constexpr int NM = NN / 2;                     // main threads (2 lines)
+  static constexpr int NQ = ((3 * N + 31) / 32) * 32;   // Nyquist-plane threads
+  static constexpr int NT = NM + NQ;
+  static constexpr int V = N * N * N;
+  static constexpr int PHS = 3 * N + 4;                 // one phase slot
+  static constexpr int OFF_F = 0;                       // [N][N][H]
+  static constexpr int OFF_W = OFF_F + NN * H;          // [NN][LP]
+  static constexpr int OFF_T = OFF_W + NN * LP;         // [3][N][LP]
+  static constexpr int OFF_PH = OFF_T + 3 * N * LP;     // [2][PHS]
+  static constexpr int SMEM_CX = OFF_PH + 2 * PHS;
+  static_assert(NM % 32 == 0, "main threads must fill warps");
+};
+
+template <int N>
+__global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsArgs<float> a) {
+  using G = CubeGeom<N>;
+  using C = cx<float>;
+  constexpr int H = G::H, NN = G::NN, LP = G::LP, NM = G::NM, V = G::V, PHS = G::PHS, NT = G::NT;
+  constexpr int NY = N / 2;
+
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* const sF = reinterpret_cast<C*>(smem_raw) + G::OFF_F;
+  C* const sW = reinterpret_cast<C*>(smem_raw) + G::OFF_W;
+  C* const sT1 = reinterpret_cast<C*>(smem_raw) + G::OFF_T;
+  C* const sT2 = sT1 + N * LP;
+  C* const sT3 = sT2 + N * LP;
+  C* const sPh = reinterpret_cast<C*>(smem_raw) + G::OFF_PH;
+  __shared__ double sRed[5][NT / 32];
+  __shared__ double sLam[5];
+
+  const int tid = threadIdx.x;
+  const bool is_main = tid < NM;
+  const int tq = tid - NM;
+  C* const fcg = a.fc + (size_t)blockIdx.x * V;
+  const float invV = 1.f / (float)V;
+  const int npq = a.P * a.M;
+
+  // axis phases e^{i fac_p s_q[ax] l0[k]} of (p, q), and
+  // Theta_ax = e^{i fac_p N s_q[ax]} = conj(e^{i fac_p s_q[ax] l0[N/2]})^2
+  auto load_phases = [&](int pq, int slot) {
+    const C* src = a.phase + (size_t)pq * 3 * N;
+    C* dst = sPh + slot * PHS;
+    for (int i = tid; i < 3 * N; i += NT) dst[i] = src[i];
+    if (tid < 3) {
+      const C e = src[tid * N + NY];
+      const C ce = mk<C>(e.x, -e.y);
+      dst[3 * N + tid] = cmul(ce, ce);
+    }
+  };
+  // F at (k1, k2, k3) from the half spectrum
+  auto Fat = [&](int k1, int k2, int k3) -> C {
+    if (k3 <= NY) return sF[(k1 * N + k2) * H + k3];
+    const C c = sF[(((N - k1) % N) * N + (N - k2) % N) * H + (N - k3)];
+    return mk<C>(c.x, -c.y);
+  };
+
+  const int npts = a.pcount ? min(a.npts, *a.pcount) : a.npts;
+  for (int ip = blockIdx.x; ip < npts; ip += gridDim.x) {
+    const int pt = a.plist ? a.plist[a.pt0 + ip] : a.pt0 + ip;
+    if ((unsigned)pt >= (unsigned)(a.nupts * a.neles)) continue;  // uniform over the CTA
+    const int upt = pt / a.neles, elem = pt % a.neles;
+
+    // ---- F = FFT(f) / V, kept for k3 <= N/2 ---------------------------------
+    if (is_main) {
+#pragma unroll 1
+      for (int r = 0; r < 2; ++r) {
+        const int L = tid + r * NM;  // line (x1, x2) along x3
+        C x[N];
+#pragma unroll
+        for (int k = 0; k < N; ++k) x[k] = mk<C>(a.f[soa_ix(upt, a.ldim, elem, (int64_t)L * N + k, V, a.soasz)], 0.f);
+        fft<float, N, -1>(x);
+#pragma unroll
+        for (int k = 0; k < N; ++k) sW[L * LP + k] = x[k];
+      }
+    }
+    __syncthreads();
+    if (is_main) {
+#pragma unroll 1
+      for (int r = 0; r < 2; ++r) {
+        const int L = tid + r * NM, x1 = L / N, k3 = L % N;  // line (x1, k3) along x2
+        C x[N];
+#pragma unroll
+        for (int j = 0; j < N; ++j) x[j] = sW[(x1 * N + j) * LP + k3];
+        fft<float, N, -1>(x);
+#pragma unroll
+        for (int j = 0; j < N; ++j) sW[(x1 * N + j) * LP + k3] = x[j];
+      }
+    }
+    __syncthreads();
+    if (is_main) {
+#pragma unroll 1
+      for (int L = tid; L < N * H; L += NM) {
+        const int k2 = L / H, k3 = L % H;  // line (k2, k3) along x1, k3 <= N/2
+        C x[N];
+#pragma unroll
+        for (int i = 0; i < N; ++i) x[i] = sW[(i * N + k2) * LP + k3];
+        fft<float, N, -1>(x);
+#pragma unroll
+        for (int i = 0; i < N; ++i) sF[(i * N + k2) * H + k3] = cscale(x[i], invV);
+      }
+    }
+    load_phases(0, 0);
+    __syncthreads();
+
+    // ---- gain: fC = sum_p w1_p FFT(sum_q Re S_pq) ---------------------------
+    int slot = 0;
+#pragma unroll 1
+    for (int p = 0; p < a.P; ++p) {
+      float S0[N], S1[N];
+#pragma unroll
+      for (int k = 0; k < N; ++k) S0[k] = S1[k] = 0.f;
+#pragma unroll 1
+      for (int q = 0; q < a.M; ++q) {
+        const int pq = p * a.M + q;
+        const C* ph = sPh + slot * PHS;
+        const C th1 = ph[3 * N], th2 = ph[3 * N + 1], th3 = ph[3 * N + 2];
+        // pass 1: R lines (k1, k2) along k3 | Nyquist first axes
+        if (is_main) {
+#pragma unroll 1
+          for (int r = 0; r < 2; ++r) {
+            const int L = tid + r * NM, k1 = L / N, k2 = L % N;
+            const C E12 = cmul(ph[k1], ph[N + k2]);
+            const bool ny12 = (k1 == NY) || (k2 == NY);
+            C t12 = mk<C>(1.f, 0.f);
+            if (k1 == NY) t12 = th1;
+            if (k2 == NY) t12 = cmul(t12, th2);
+            C x[N];
+#pragma unroll
+            for (int k = 0; k < N; ++k) {
+              const C E = cmul(E12, ph[2 * N + k]);
+              float m;
+              if (k == NY) {
+                const C Et = cmul(E, cmul(t12, th3));
+                m = 0.5f * (E.x + Et.x + E.y + Et.y);
+              } else if (ny12) {
+                const C Et = cmul(E, t12);
+                m = 0.5f * (E.x + Et.x + E.y + Et.y);
+              } else {
+                m = E.x + E.y;
+              }
+              x[k] = cscale(Fat(k1, k2, k), m);
+            }
+            fft<float, N, +1>(x);
+#pragma unroll
+            for (int k = 0; k < N; ++k) sW[L * LP + k] = x[k];
+          }
+        } else if (tq < 3 * N) {
+          // n F on the Nyquist planes: plane 1 (k1 = N/2) lines over k3,
+          // plane 2 (k2 = N/2, k1 != N/2) lines over k3, plane 3 (k3 = N/2,
+          // k1, k2 != N/2) lines over k2
+          const int which = tq / N, j = tq % N;
+          C x[N];
+#pragma unroll
+          for (int k = 0; k < N; ++k) {
+            int k1, k2, k3;
+            bool on;
+            if (which == 0) {
+              k1 = NY; k2 = j; k3 = k; on = true;
+            } else if (which == 1) {
+              k1 = j; k2 = NY; k3 = k; on = (j != NY);
+            } else {
+              k1 = j; k2 = k; k3 = NY; on = (j != NY) && (k != NY);
+            }
+            C v = mk<C>(0.f, 0.f);
+            if (on) {
+              const C E = cmul(cmul(ph[k1], ph[N + k2]), ph[2 * N + k3]);
+              C t = mk<C>(1.f, 0.f);
+              if (k1 == NY) t = th1;
+              if (k2 == NY) t = cmul(t, th2);
+              if (k3 == NY) t = cmul(t, th3);
+              const C Et = cmul(E, t);
+              const float n = 0.5f * (E.x - Et.x + E.y - Et.y);
+              v = cscale(Fat(k1, k2, k3), n);
+            }
+            x[k] = v;
+          }
+          fft<float, N, +1>(x);
+          C* T = which == 0 ? sT1 : (which == 1 ? sT2 : sT3);
+#pragma unroll
+          for (int k = 0; k < N; ++k) T[j * LP + k] = x[k];
+        }
+        if (pq + 1 < npq) load_phases(pq + 1, slot ^ 1);
+        __syncthreads();
+        // pass 2: lines (k1, x3) along k2 | Nyquist second axes (columns)
+        if (is_main) {
+#pragma unroll 1
+          for (int r = 0; r < 2; ++r) {
+            const int L = tid + r * NM, k1 = L / N, x3 = L % N;
+            C x[N];
+#pragma unroll
+            for (int j = 0; j < N; ++j) x[j] = sW[(k1 * N + j) * LP + x3];
+            fft<float, N, +1>(x);
+#pragma unroll
+            for (int j = 0; j < N; ++j) sW[(k1 * N + j) * LP + x3] = x[j];
+          }
+        } else if (tq < 3 * N) {
+          const int which = tq / N, col = tq % N;
+          C* T = which == 0 ? sT1 : (which == 1 ? sT2 : sT3);
+          C x[N];
+#pragma unroll
+          for (int j = 0; j < N; ++j) x[j] = T[j * LP + col];
+          fft<float, N, +1>(x);
+#pragma unroll
+          for (int j = 0; j < N; ++j) T[j * LP + col] = x[j];
+        }
+        __syncthreads();
+        // pass 3: lines (x2, x3) along k1; S += Re R^2 + Re Nq^2
+        if (is_main) {
+#pragma unroll
+          for (int r = 0; r < 2; ++r) {
+            const int L = tid + r * NM, x2 = L / N, x3 = L % N;
+            C x[N];
+#pragma unroll
+            for (int i = 0; i < N; ++i) x[i] = sW[(i * N + x2) * LP + x3];
+            fft<float, N, +1>(x);
+            const C t1 = sT1[x2 * LP + x3];
+            const float s2 = (x2 & 1) ? -1.f : 1.f, s3 = (x3 & 1) ? -1.f : 1.f;
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+              const float s1 = (i & 1) ? -1.f : 1.f;
+              const C t2 = sT2[i * LP + x3], t3 = sT3[i * LP + x2];
+              const float nr = s1 * t1.x + s2 * t2.x + s3 * t3.x;
+              const float ni = s1 * t1.y + s2 * t2.y + s3 * t3.y;
+              const float v = x[i].x * x[i].x - x[i].y * x[i].y + nr * nr - ni * ni;
+              if (r == 0) S0[i] += v;
+              else S1[i] += v;
+            }
+          }
+        }
+        slot ^= 1;
+        __syncthreads();
+      }
+
+      // FFT(S_p): lines (x2, x3) along x1 straight from the accumulators
+      if (is_main) {
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+          const int L = tid + r * NM, x2 = L / N, x3 = L % N;
+          C x[N];
+#pragma unroll
+          for (int i = 0; i < N; ++i) x[i] = mk<C>(r == 0 ? S0[i] : S1[i], 0.f);
+          fft<float, N, -1>(x);
+#pragma unroll
+          for (int i = 0; i < N; ++i) sW[(i * N + x2) * LP + x3] = x[i];
+        }
+      }
+      __syncthreads();
+      if (is_main) {
+#pragma unroll 1
+        for (int r = 0; r < 2; ++r) {
+          const int L = tid + r * NM, k1 = L / N, x3 = L % N;
+          C x[N];
+#pragma unroll
+          for (int j = 0; j < N; ++j) x[j] = sW[(k1 * N + j) * LP + x3];
+          fft<float, N, -1>(x);
+#pragma unroll
+          for (int j = 0; j < N; ++j) sW[(k1 * N + j) * LP + x3] = x[j];
+        }
+      }
+      __syncthreads();
+      if (is_main) {
+        const float* w1 = a.w1 + (size_t)p * V;
+#pragma unroll 1
+        for (int r = 0; r < 2; ++r) {
+          const int L = tid + r * NM;  // line (k1, k2) along k3; v = L N + k3
+          C x[N];
+#pragma unroll
+          for (int k = 0; k < N; ++k) x[k] = sW[L * LP + k];
+          fft<float, N, -1>(x);
+          C* dst = fcg + (size_t)L * N;
+          const float* w = w1 + (size_t)L * N;
+#pragma unroll
+          for (int k = 0; k < N; ++k) {
+            const C add = cscale(x[k], w[k]);
+            dst[k] = p == 0 ? add : cadd(dst[k], add);
+          }
+        }
+      }
+      __syncthreads();
+    }
+
+    // ---- IFFT(fC + i b2 F) = Re QG + i Re Lf; Q = prefac (QG - f Lf) ---------
+    if (is_main) {
+#pragma unroll 1
+      for (int r = 0; r < 2; ++r) {
+        const int L = tid + r * NM, k1 = L / N, k2 = L % N;
+        C x[N];
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+          const C g = fcg[(size_t)L * N + k];
+          const C Fv = Fat(k1, k2, k);
+          const float b = a.b2[L * N + k];
+          x[k] = mk<C>(g.x - b * Fv.y, g.y + b * Fv.x);
+        }
+        fft<float, N, +1>(x);
+#pragma unroll
+        for (int k = 0; k < N; ++k) sW[L * LP + k] = x[k];
+      }
+    }
+    __syncthreads();
+    if (is_main) {
+#pragma unroll 1
+      for (int r = 0; r < 2; ++r) {
+        const int L = tid + r * NM, k1 = L / N, x3 = L % N;
+        C x[N];
+#pragma unroll
+        for (int j = 0; j < N; ++j) x[j] = sW[(k1 * N + j) * LP + x3];
+        fft<float, N, +1>(x);
+#pragma unroll
+        for (int j = 0; j < N; ++j) sW[(k1 * N + j) * LP + x3] = x[j];
+      }
+    }
+    __syncthreads();
+    double mom[5] = {0, 0, 0, 0, 0};
+    if (is_main) {
+#pragma unroll 1
+      for (int r = 0; r < 2; ++r) {
+        const int L = tid + r * NM, x2 = L / N, x3 = L % N;
+        C x[N];
+#pragma unroll
+        for (int i = 0; i < N; ++i) x[i] = sW[(i * N + x2) * LP + x3];
+        fft<float, N, +1>(x);
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+          const int64_t v = (int64_t)(i * N + x2) * N + x3;
+          const float fv = a.f[soa_ix(upt, a.ldim, elem, v, V, a.soasz)];
+          const float qq = a.prefac * (x[i].x - fv * x[i].y);
+          if (!a.project) {
+            a.Q[soa_ix(upt, a.ldim, elem, v, V, a.soasz)] = qq;
+            continue;
+          }
+          sW[(i * N + x2) * LP + x3].x = qq;  // this thread's own slot
+          {
+            const double c0 = a.cvec[v], c1 = a.cvec[V + v], c2 = a.cvec[2 * V + v];
+            const double d = (double)qq;
+            mom[0] += d;
+            mom[1] += d * c0;
+            mom[2] += d * c1;
+            mom[3] += d * c2;
+            mom[4] += d * (c0 * c0 + c1 * c1 + c2 * c2);
+          }
+        }
+      }
+    }
+    if (a.project) {  // uniform: every thread takes part in the reduction
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        double s = mom[k];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if ((tid & 31) == 0) sRed[k][tid >> 5] = s;
+      }
+      __syncthreads();
+      if (tid < 5) {
+        double s = 0;
+        for (int w = 0; w < NT / 32; ++w) s += sRed[tid][w];
+        sRed[tid][0] = s;
+      }
+      __syncthreads();
+      if (tid < 5) {
+        double l = 0;
+        for (int j = 0; j < 5; ++j) l += a.ginv[tid * 5 + j] * sRed[j][0];
+        sLam[tid] = l;
+      }
+      __syncthreads();
+    }
+    if (is_main && a.project) {
+#pragma unroll 1
+      for (int r = 0; r < 2; ++r) {
+        const int L = tid + r * NM, x2 = L / N, x3 = L % N;
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+          const int64_t v = (int64_t)(i * N + x2) * N + x3;
+          const double c0 = a.cvec[v], c1 = a.cvec[V + v], c2 = a.cvec[2 * V + v];
+          const float qq = (float)((double)sW[(i * N + x2) * LP + x3].x -
+                                   (sLam[0] + sLam[1] * c0 + sLam[2] * c1 + sLam[3] * c2 +
+                                    sLam[4] * (c0 * c0 + c1 * c1 + c2 * c2)));
+          a.Q[soa_ix(upt, a.ldim, elem, v, V, a.soasz)] = qq;
+        }
+      }
+    }
+    __syncthreads();  // the work cube and fC are reused by the next point
+  }
+}
+
+}  // namespace dgfs

@@ -143,7 +143,9 @@ DGFS_API int dgfs_vhs_variant_info(const dgfs_vhs* h, int idx, int* cluster,
 DGFS_API int dgfs_vhs_select(dgfs_vhs* h, int idx);
 
 /* 1 if launch shape idx exchanges by remote pushes (st.async into the
- * owner's shared memory, mbarrier completion), 0 if by remote loads. */
+ * owner's shared memory, mbarrier completion), 0 if by remote loads, 2 for
+ * the single-CTA kernel (FP32, Nv <= 24: the whole point in one CTA's
+ * shared memory, one complex transform per (p, q)). */
 DGFS_API int dgfs_vhs_variant_kind(const dgfs_vhs* h, int idx, int* push);
 
 /* Synchronise `stream`, then report and clear the kernel error flag: the

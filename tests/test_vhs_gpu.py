@@ -104,7 +104,7 @@ def test_range_and_single_agree_with_all():
 
 
 @pytest.mark.parametrize('name,precision', [
-    ('small-n8', 'double'), ('relax0d-n16', 'double'),
+    ('small-n8', 'double'), ('small-n8', 'single'), ('relax0d-n16', 'double'),
     ('relax0d-n16', 'single'), ('couette-n24', 'double'),
     ('couette-n24', 'single'), ('channel-n32', 'double'),
     ('channel-n32', 'single')])
@@ -116,19 +116,27 @@ def test_launch_shapes_agree(name, precision):
     be, vm, sm = _model(cfg)
     ovm, pre, prefac = oracle_for(cfg)
     f = random_states(vm.cv(), 3, seed=9).reshape(1, 3, -1)
-    outs = []
+    outs, kinds = [], []
     for i, v in enumerate(sm.variants()):
         sm.select(i)
         fin, fout = _bank(be, vm, f)
         sm.fs_all(fin, fout)
         sm.status()                     # no bounded wait gave up
         outs.append(fout.get())
-    Qo = ovhs.vhs_Q(fin.get()[0, :, 2].astype(np.float64), ovm, pre, prefac)
+        kinds.append(v['exchange'])
+    fu = fin.get().astype(np.float64)
+    Qo = [ovhs.vhs_Q(fu[0, :, e], ovm, pre, prefac) for e in range(3)]
     tol = FP64_TOL if precision == 'double' else FP32_TOL
-    assert rel_err(outs[0][0, :, 2], Qo) < tol
-    for o in outs[1:]:
-        assert rel_err(o, outs[0]) < (1e-13 if precision == 'double'
-                                      else 1e-6)
+    assert rel_err(outs[0][0, :, 2], Qo[2]) < tol
+    for o, k in zip(outs[1:], kinds[1:]):
+        if k == 'single-cta':
+            # another (exact) arithmetic restatement: checked against the
+            # oracle at every point
+            for e in range(3):
+                assert rel_err(o[0, :, e], Qo[e]) < tol
+        else:
+            assert rel_err(o, outs[0]) < (1e-13 if precision == 'double'
+                                          else 1e-6)
 
 
 @pytest.mark.parametrize('precision', ['double', 'single'])
@@ -180,3 +188,33 @@ def test_invalid_arguments_raise():
         sm.fs(fin, fin, 0, 0)           # in-place is rejected
     with pytest.raises(DgfsError):
         sm.fs_range(fin, fout, 1, 5)    # range past the bank
+
+
+@pytest.mark.parametrize('name', ['small-n8', 'relax0d-n16', 'couette-n24'])
+@pytest.mark.parametrize('project', [0, 1])
+def test_single_cta_kernel(name, project):
+    """The single-CTA FP32 kernel (whole point in one CTA, one complex
+    transform per (p, q) plus the Nyquist-plane corrections) against the
+    oracle at every point of a bank that spans two AoSoA blocks, with and
+    without the conservation projection."""
+    cfg = _cfg(name, 'single')
+    cfg.set('backend-b200', 'vhs-project', project)
+    be, vm, sm = _model(cfg)
+    idx = [i for i, v in enumerate(sm.variants())
+           if v['exchange'] == 'single-cta']
+    assert len(idx) == 1
+    sm.select(idx[0])
+    ovm, pre, prefac = oracle_for(cfg)
+    nupts, neles = 2, 37
+    f = random_states(vm.cv(), nupts*neles, seed=21).reshape(nupts, neles,
+                                                            -1)
+    fin, fout = _bank(be, vm, f)
+    sm.fs_all(fin, fout)
+    sm.status()
+    Qg, fu = fout.get(), fin.get().astype(np.float64)
+    for u in range(nupts):
+        for e in range(neles):
+            Qo = ovhs.vhs_Q(fu[u, :, e], ovm, pre, prefac)
+            if project:
+                Qo = ovhs.project_conservative(Qo, ovm['cv'])
+            assert rel_err(Qg[u, :, e], Qo) < FP32_TOL, (u, e)
