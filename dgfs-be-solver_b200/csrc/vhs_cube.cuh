@@ -82,15 +82,22 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
   const int npq = a.P * a.M;
 
   // axis phases e^{i fac_p s_q[ax] l0[k]} of (p, q), and
-  // Theta_ax = e^{i fac_p N s_q[ax]} = conj(e^{i fac_p s_q[ax] l0[N/2]})^2
-  auto load_phases = [&](int pq, int slot) {
-    const C* src = a.phase + (size_t)pq * 3 * N;
-    C* dst = sPh + slot * PHS;
-    for (int i = tid; i < 3 * N; i += NT) dst[i] = src[i];
-    if (tid < 3) {
-      const C e = src[tid * N + NY];
-      const C ce = mk<C>(e.x, -e.y);
-      dst[3 * N + tid] = cmul(ce, ce);
+  // Theta_ax = e^{i fac_p N s_q[ax]} = conj(e^{i fac_p s_q[ax] l0[N/2]})^2.
+  // Threads tid < 3N each carry one entry: fetched from L2 at the start of
+  // a pass (phase_fetch), stored to the other slot at its end
+  // (phase_store), so the load latency hides behind the pass.
+  static_assert(3 * N <= NT, "one phase entry per thread");
+  auto phase_fetch = [&](int pq) -> C {
+    return tid < 3 * N ? a.phase[(size_t)pq * 3 * N + tid] : mk<C>(0.f, 0.f);
+  };
+  auto phase_store = [&](C e, int slot) {
+    if (tid < 3 * N) {
+      C* dst = sPh + slot * PHS;
+      dst[tid] = e;
+      if (tid % N == NY) {
+        const C ce = mk<C>(e.x, -e.y);
+        dst[3 * N + tid / N] = cmul(ce, ce);
+      }
     }
   };
   // F at (k1, k2, k3) from the half spectrum
@@ -145,7 +152,7 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
         for (int i = 0; i < N; ++i) sF[(i * N + k2) * H + k3] = cscale(x[i], invV);
       }
     }
-    load_phases(0, 0);
+    phase_store(phase_fetch(0), 0);
     __syncthreads();
 
     // ---- gain: fC = sum_p w1_p FFT(sum_q Re S_pq) ---------------------------
@@ -160,30 +167,29 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
         const int pq = p * a.M + q;
         const C* ph = sPh + slot * PHS;
         const C th1 = ph[3 * N], th2 = ph[3 * N + 1], th3 = ph[3 * N + 2];
-        // pass 1: R lines (k1, k2) along k3 | Nyquist first axes
+        const C phn = pq + 1 < npq ? phase_fetch(pq + 1) : mk<C>(0.f, 0.f);
+        // pass 1: R lines (k1, k2) along k3 | Nyquist first axes.
+        // m = Re((E + E t)(1 - i)) / 2 with E = E1 E2 E3[k3] and t the
+        // Nyquist factor (1 off the planes): per line A = (E12 + E12 t12)
+        // (1 - i) / 2 (A3 on the k3 = N/2 plane), then m = Re(A E3[k3]).
         if (is_main) {
 #pragma unroll 1
           for (int r = 0; r < 2; ++r) {
             const int L = tid + r * NM, k1 = L / N, k2 = L % N;
             const C E12 = cmul(ph[k1], ph[N + k2]);
-            const bool ny12 = (k1 == NY) || (k2 == NY);
             C t12 = mk<C>(1.f, 0.f);
             if (k1 == NY) t12 = th1;
             if (k2 == NY) t12 = cmul(t12, th2);
+            const C E12t = cmul(E12, t12);
+            const C s0 = cadd(E12, E12t), s3 = cadd(E12, cmul(E12t, th3));
+            const C A = mk<C>(0.5f * (s0.x + s0.y), 0.5f * (s0.y - s0.x));
+            const C A3 = mk<C>(0.5f * (s3.x + s3.y), 0.5f * (s3.y - s3.x));
             C x[N];
 #pragma unroll
             for (int k = 0; k < N; ++k) {
-              const C E = cmul(E12, ph[2 * N + k]);
-              float m;
-              if (k == NY) {
-                const C Et = cmul(E, cmul(t12, th3));
-                m = 0.5f * (E.x + Et.x + E.y + Et.y);
-              } else if (ny12) {
-                const C Et = cmul(E, t12);
-                m = 0.5f * (E.x + Et.x + E.y + Et.y);
-              } else {
-                m = E.x + E.y;
-              }
+              const C e3 = ph[2 * N + k];
+              const C& Ak = k == NY ? A3 : A;
+              const float m = Ak.x * e3.x - Ak.y * e3.y;
               x[k] = cscale(Fat(k1, k2, k), m);
             }
             fft<float, N, +1>(x);
@@ -225,7 +231,7 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
 #pragma unroll
           for (int k = 0; k < N; ++k) T[j * LP + k] = x[k];
         }
-        if (pq + 1 < npq) load_phases(pq + 1, slot ^ 1);
+        if (pq + 1 < npq) phase_store(phn, slot ^ 1);
         __syncthreads();
         // pass 2: lines (k1, x3) along k2 | Nyquist second axes (columns)
         if (is_main) {
