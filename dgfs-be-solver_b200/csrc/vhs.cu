@@ -123,7 +123,7 @@ template <typename T, int N, int C, int MINB> static VhsVariant make_push() {
   return v;
 }
 
-template <int N> static cudaError_t launch_cube(const VhsArgs<float>& a, int nctas, cudaStream_t s) {
+template <int N, bool IL1> static cudaError_t launch_cube(const VhsArgs<float>& a, int nctas, cudaStream_t s) {
   using G = CubeGeom<N>;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(nctas, 1, 1);
@@ -137,23 +137,25 @@ template <int N> static cudaError_t launch_cube(const VhsArgs<float>& a, int nct
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, vhs_cube_kernel<N>, a);
+  return cudaLaunchKernelEx(&cfg, vhs_cube_kernel<N, IL1>, a);
 }
 
-// single-CTA kernel (FP32; kind 2 in dgfs_vhs_variant_kind)
-template <int N> static VhsVariant make_cube() {
+// single-CTA kernel (FP32; kind 2 in dgfs_vhs_variant_kind); IL1: the
+// first pass of every (p, q) transforms a thread's two lines together
+// (more ILP, more registers; db reports it)
+template <int N, bool IL1> static VhsVariant make_cube() {
   using G = CubeGeom<N>;
   VhsVariant v{};
   v.prec = 32;
   v.N = N;
   v.C = 1;
-  v.db = 0;
+  v.db = IL1 ? 1 : 0;
   v.push = 2;
   v.minb = 1;
   v.threads = G::NT;
   v.smem = G::SMEM_CX * sizeof(cx<float>);
-  v.fn = (const void*)vhs_cube_kernel<N>;
-  v.launch32 = launch_cube<N>;
+  v.fn = (const void*)vhs_cube_kernel<N, IL1>;
+  v.launch32 = launch_cube<N, IL1>;
   return v;
 }
 
@@ -169,8 +171,9 @@ static const std::vector<VhsVariant>& variants() {
       make_push<float, 16, 4, 4>(),             make_push<float, 24, 8, 2>(),
       make_push<float, 24, 4, 1>(),             make_push<float, 24, 12, 3>(),
       make_push<float, 32, 16, 2>(),            make_push<float, 32, 8, 1>(),
-      make_cube<8>(),                           make_cube<16>(),
-      make_cube<24>(),
+      make_cube<8, false>(),                    make_cube<16, false>(),
+      make_cube<24, false>(),                   make_cube<16, true>(),
+      make_cube<24, true>(),
       make_variant<double, 8, 1, true, 4>(),    make_variant<double, 8, 2, true, 8>(),
       make_variant<double, 16, 4, true, 2>(),   make_variant<double, 16, 2, true, 1>(),
       make_variant<double, 16, 4, false, 3>(),

@@ -57,7 +57,7 @@ template <int N> struct CubeGeom {
   static_assert(NM % 32 == 0, "main threads must fill warps");
 };
 
-template <int N>
+template <int N, bool IL1>
 __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsArgs<float> a) {
   using G = CubeGeom<N>;
   using C = cx<float>;
@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
         // m = Re((E + E t)(1 - i)) / 2 with E = E1 E2 E3[k3] and t the
         // Nyquist factor (1 off the planes): per line A = (E12 + E12 t12)
         // (1 - i) / 2 (A3 on the k3 = N/2 plane), then m = Re(A E3[k3]).
-        if (is_main) {
+        if (is_main && !IL1) {
 #pragma unroll 1
           for (int r = 0; r < 2; ++r) {
             const int L = tid + r * NM, k1 = L / N, k2 = L % N;
@@ -189,12 +189,43 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
             for (int k = 0; k < N; ++k) {
               const C e3 = ph[2 * N + k];
               const C& Ak = k == NY ? A3 : A;
-              const float m = Ak.x * e3.x - Ak.y * e3.y;
-              x[k] = cscale(Fat(k1, k2, k), m);
+              x[k] = cscale(Fat(k1, k2, k), Ak.x * e3.x - Ak.y * e3.y);
             }
             fft<float, N, +1>(x);
 #pragma unroll
             for (int k = 0; k < N; ++k) sW[L * LP + k] = x[k];
+          }
+        } else if (is_main) {  // IL1: both lines of the thread at once
+          auto coef = [&](int k1, int k2, C& A, C& A3) {
+            const C E12 = cmul(ph[k1], ph[N + k2]);
+            C t12 = mk<C>(1.f, 0.f);
+            if (k1 == NY) t12 = th1;
+            if (k2 == NY) t12 = cmul(t12, th2);
+            const C E12t = cmul(E12, t12);
+            const C s0 = cadd(E12, E12t), s3 = cadd(E12, cmul(E12t, th3));
+            A = mk<C>(0.5f * (s0.x + s0.y), 0.5f * (s0.y - s0.x));
+            A3 = mk<C>(0.5f * (s3.x + s3.y), 0.5f * (s3.y - s3.x));
+          };
+          const int L0 = tid, L1 = tid + NM;
+          const int a1 = L0 / N, a2 = L0 % N, b1 = L1 / N, b2 = L1 % N;
+          C Aa, Aa3, Ab, Ab3;
+          coef(a1, a2, Aa, Aa3);
+          coef(b1, b2, Ab, Ab3);
+          C x[N], y[N];
+#pragma unroll
+          for (int k = 0; k < N; ++k) {
+            const C e3 = ph[2 * N + k];
+            const C& A0 = k == NY ? Aa3 : Aa;
+            const C& B0 = k == NY ? Ab3 : Ab;
+            x[k] = cscale(Fat(a1, a2, k), A0.x * e3.x - A0.y * e3.y);
+            y[k] = cscale(Fat(b1, b2, k), B0.x * e3.x - B0.y * e3.y);
+          }
+          fft<float, N, +1>(x);
+          fft<float, N, +1>(y);
+#pragma unroll
+          for (int k = 0; k < N; ++k) {
+            sW[L0 * LP + k] = x[k];
+            sW[L1 * LP + k] = y[k];
           }
         } else if (tq < 3 * N) {
           // n F on the Nyquist planes: plane 1 (k1 = N/2) lines over k3,
@@ -233,17 +264,24 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
         }
         if (pq + 1 < npq) phase_store(phn, slot ^ 1);
         __syncthreads();
-        // pass 2: lines (k1, x3) along k2 | Nyquist second axes (columns)
+        // pass 2: lines (k1, x3) along k2, both lines of a thread at once |
+        // Nyquist second axes (columns)
         if (is_main) {
-#pragma unroll 1
-          for (int r = 0; r < 2; ++r) {
-            const int L = tid + r * NM, k1 = L / N, x3 = L % N;
-            C x[N];
+          const int L0 = tid, L1 = tid + NM;
+          C* w0 = sW + (L0 / N) * N * LP + L0 % N;
+          C* w1 = sW + (L1 / N) * N * LP + L1 % N;
+          C x[N], y[N];
 #pragma unroll
-            for (int j = 0; j < N; ++j) x[j] = sW[(k1 * N + j) * LP + x3];
-            fft<float, N, +1>(x);
+          for (int j = 0; j < N; ++j) {
+            x[j] = w0[j * LP];
+            y[j] = w1[j * LP];
+          }
+          fft<float, N, +1>(x);
+          fft<float, N, +1>(y);
 #pragma unroll
-            for (int j = 0; j < N; ++j) sW[(k1 * N + j) * LP + x3] = x[j];
+          for (int j = 0; j < N; ++j) {
+            w0[j * LP] = x[j];
+            w1[j * LP] = y[j];
           }
         } else if (tq < 3 * N) {
           const int which = tq / N, col = tq % N;
@@ -256,26 +294,36 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
           for (int j = 0; j < N; ++j) T[j * LP + col] = x[j];
         }
         __syncthreads();
-        // pass 3: lines (x2, x3) along k1; S += Re R^2 + Re Nq^2
+        // pass 3: lines (x2, x3) along k1, both lines at once;
+        // S += Re R^2 + Re Nq^2
         if (is_main) {
+          const int L0 = tid, L1 = tid + NM;
+          const int a2 = L0 / N, a3 = L0 % N, b2 = L1 / N, b3 = L1 % N;
+          C x[N], y[N];
 #pragma unroll
-          for (int r = 0; r < 2; ++r) {
-            const int L = tid + r * NM, x2 = L / N, x3 = L % N;
-            C x[N];
+          for (int i = 0; i < N; ++i) {
+            x[i] = sW[(i * N + a2) * LP + a3];
+            y[i] = sW[(i * N + b2) * LP + b3];
+          }
+          fft<float, N, +1>(x);
+          fft<float, N, +1>(y);
+          const C ta = sT1[a2 * LP + a3], tb = sT1[b2 * LP + b3];
+          const float sa2 = (a2 & 1) ? -1.f : 1.f, sa3 = (a3 & 1) ? -1.f : 1.f;
+          const float sb2 = (b2 & 1) ? -1.f : 1.f, sb3 = (b3 & 1) ? -1.f : 1.f;
 #pragma unroll
-            for (int i = 0; i < N; ++i) x[i] = sW[(i * N + x2) * LP + x3];
-            fft<float, N, +1>(x);
-            const C t1 = sT1[x2 * LP + x3];
-            const float s2 = (x2 & 1) ? -1.f : 1.f, s3 = (x3 & 1) ? -1.f : 1.f;
-#pragma unroll
-            for (int i = 0; i < N; ++i) {
-              const float s1 = (i & 1) ? -1.f : 1.f;
-              const C t2 = sT2[i * LP + x3], t3 = sT3[i * LP + x2];
-              const float nr = s1 * t1.x + s2 * t2.x + s3 * t3.x;
-              const float ni = s1 * t1.y + s2 * t2.y + s3 * t3.y;
-              const float v = x[i].x * x[i].x - x[i].y * x[i].y + nr * nr - ni * ni;
-              if (r == 0) S0[i] += v;
-              else S1[i] += v;
+          for (int i = 0; i < N; ++i) {
+            const float s1 = (i & 1) ? -1.f : 1.f;
+            {
+              const C t2 = sT2[i * LP + a3], t3 = sT3[i * LP + a2];
+              const float nr = s1 * ta.x + sa2 * t2.x + sa3 * t3.x;
+              const float ni = s1 * ta.y + sa2 * t2.y + sa3 * t3.y;
+              S0[i] += x[i].x * x[i].x - x[i].y * x[i].y + nr * nr - ni * ni;
+            }
+            {
+              const C t2 = sT2[i * LP + b3], t3 = sT3[i * LP + b2];
+              const float nr = s1 * tb.x + sb2 * t2.x + sb3 * t3.x;
+              const float ni = s1 * tb.y + sb2 * t2.y + sb3 * t3.y;
+              S1[i] += y[i].x * y[i].x - y[i].y * y[i].y + nr * nr - ni * ni;
             }
           }
         }
