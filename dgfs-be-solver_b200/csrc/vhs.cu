@@ -161,18 +161,20 @@ template <int N, bool IL1> static VhsVariant make_cube() {
 
 // Compiled launch shapes: (precision, N, cluster size, double-buffered
 // exchange, minimum CTAs per SM for the register budget).  The first entry
-// of each (precision, N) family is the default; the autotuner times the rest.
+// of each (precision, N) family is the default (FP32 N = 24: the single-CTA
+// kernel, 14 ms against 20 ms for the best cluster shape on 576 points);
+// the autotuner times the rest.
 static const std::vector<VhsVariant>& variants() {
   static const std::vector<VhsVariant> v = {
       make_push<double, 8, 1, 4>(),             make_push<double, 16, 4, 2>(),
       make_push<double, 16, 2, 1>(),            make_push<double, 24, 8, 1>(),
       make_push<double, 24, 12, 1>(),           make_push<double, 32, 16, 1>(),
       make_push<float, 8, 1, 4>(),              make_push<float, 16, 2, 2>(),
-      make_push<float, 16, 4, 4>(),             make_push<float, 24, 8, 2>(),
-      make_push<float, 24, 4, 1>(),             make_push<float, 24, 12, 3>(),
-      make_push<float, 32, 16, 2>(),            make_push<float, 32, 8, 1>(),
-      make_cube<8, false>(),                    make_cube<16, false>(),
-      make_cube<24, false>(),                   make_cube<16, true>(),
+      make_push<float, 16, 4, 4>(),             make_cube<24, false>(),
+      make_push<float, 24, 8, 2>(),             make_push<float, 24, 4, 1>(),
+      make_push<float, 24, 12, 3>(),            make_push<float, 32, 16, 2>(),
+      make_push<float, 32, 8, 1>(),             make_cube<8, false>(),
+      make_cube<16, false>(),                   make_cube<16, true>(),
       make_cube<24, true>(),
       make_variant<double, 8, 1, true, 4>(),    make_variant<double, 8, 2, true, 8>(),
       make_variant<double, 16, 4, true, 2>(),   make_variant<double, 16, 2, true, 1>(),

@@ -84,6 +84,12 @@ class DGFSVHSGLLScatteringModel(DGFSScatteringModel):
         self._qz = np.ascontiguousarray(vm.qz(), dtype=np.float64)
         self._qw = np.ascontiguousarray(vm.qw(), dtype=np.float64)
         self._sz = np.ascontiguousarray(vm.sz(), dtype=np.float64)
+        self._lib = _lib.load()
+        self._extra = []
+        self._h = self._create_handle(cluster)
+
+    def _create_handle(self, cluster=0):
+        vm = self.vm
         p = _lib.VhsParams(
             Nv=vm.Nv(), Nrho=vm.Nrho(), M=vm.M(),
             precision=self.backend.precision, L=vm.L(),
@@ -92,13 +98,29 @@ class DGFSVHSGLLScatteringModel(DGFSScatteringModel):
             prefactor=self._prefactor, gamma=self._gamma,
             project=self._project, cluster=cluster)
         h = ct.c_void_p()
-        lib = _lib.load()
-        _lib.check(lib.dgfs_vhs_create(ct.byref(p), ct.byref(h)),
+        _lib.check(self._lib.dgfs_vhs_create(ct.byref(p), ct.byref(h)),
                    'dgfs_vhs_create')
-        self._h = h
-        self._lib = lib
+        return h
+
+    def make_handle(self, exchange):
+        """A second operator handle on the same tables' parameters with the
+        first compiled launch shape of the given kind ('push', 'pull',
+        'single-cta') selected, e.g. a cluster shape for calls on a few
+        points (it spreads one point over several SMs).  Owned and freed by
+        this model; None when no shape of that kind is compiled."""
+        kinds = [v['exchange'] for v in self.variants()]
+        if exchange not in kinds:
+            return None
+        h = self._create_handle()
+        _lib.check(self._lib.dgfs_vhs_select(h, kinds.index(exchange)),
+                   'dgfs_vhs_select')
+        self._extra.append(h)
+        return h
 
     def __del__(self):
+        for h in getattr(self, '_extra', []):
+            self._lib.dgfs_vhs_destroy(h)
+        self._extra = []
         h = getattr(self, '_h', None)
         if h:
             self._lib.dgfs_vhs_destroy(h)

@@ -315,6 +315,9 @@ class VHSSurrogate:
                                   dtype=torch.float64, device=self.device)
         self.loss_history = []
         self._last = None
+        # the plain fallback runs on a few points: a cluster launch shape
+        # spreads each of them over several SMs
+        self._plain_h = sm.make_handle('push') or sm._h
 
     @property
     def _s(self):
@@ -492,7 +495,7 @@ class VHSSurrogate:
             _p(self.gwinv), fbank._as_parameter_, nu._as_parameter_,
             qbank._as_parameter_, self._s), 'dgfs_hermite_reconstruct')
         _lib.check(lib.dgfs_vhs_apply_list(
-            self.sm._h, fbank._as_parameter_, qbank._as_parameter_, nupts,
+            self._plain_h, fbank._as_parameter_, qbank._as_parameter_, nupts,
             neles, ldim, self.backend.soasz, _p(plain), _p(nplain), npts,
             self._s), 'dgfs_vhs_apply_list')
         self._last = (gate, eps)
