@@ -318,6 +318,7 @@ class VHSSurrogate:
         # the plain fallback runs on a few points: a cluster launch shape
         # spreads each of them over several SMs
         self._plain_h = sm.make_handle('push') or sm._h
+        self._side = None
 
     @property
     def _s(self):
@@ -486,6 +487,21 @@ class VHSSurrogate:
                                            _p(mom), self.vm.L(), RMIN,
                                            _p(gate), _p(plain), _p(nplain),
                                            self._s), 'dgfs_surrogate_gate')
+        # the plain fallback (few points, on cluster shapes that leave SMs
+        # idle) runs on a side stream beside the network path; both write
+        # disjoint points of qbank.  Event fork/join keeps it capturable.
+        main = torch.cuda.current_stream(self.device)
+        if self._side is None:
+            self._side = torch.cuda.Stream(device=self.device)
+            self._fork = torch.cuda.Event()
+            self._join = torch.cuda.Event()
+        self._fork.record(main)
+        self._side.wait_event(self._fork)
+        _lib.check(lib.dgfs_vhs_apply_list(
+            self._plain_h, fbank._as_parameter_, qbank._as_parameter_, nupts,
+            neles, ldim, self.backend.soasz, _p(plain), _p(nplain), npts,
+            self._side.cuda_stream), 'dgfs_vhs_apply_list')
+        self._join.record(self._side)
         nu = self.loss_rate(fbank, self.nu_bank(fbank), gate)
         Bp = self.scale_targets(self.predict(X), eps, inverse=True)
         _lib.check(lib.dgfs_hermite_reconstruct(
@@ -494,10 +510,7 @@ class VHSSurrogate:
             self.sm.prefactor, self.sm._gamma, _p(self.ginv),
             _p(self.gwinv), fbank._as_parameter_, nu._as_parameter_,
             qbank._as_parameter_, self._s), 'dgfs_hermite_reconstruct')
-        _lib.check(lib.dgfs_vhs_apply_list(
-            self._plain_h, fbank._as_parameter_, qbank._as_parameter_, nupts,
-            neles, ldim, self.backend.soasz, _p(plain), _p(nplain), npts,
-            self._s), 'dgfs_vhs_apply_list')
+        main.wait_event(self._join)
         self._last = (gate, eps)
         return gate
 
