@@ -337,9 +337,12 @@ def test_collide_routes_points_and_conserves():
                         random_states(cv, 8, seed=3)]).reshape(
                             nupts, neles, -1)
     fb = _bank(be, f)
-    ref = be.matrix(fb.ioshape)
-    sm.fs_all(fb, ref)
     sur = VHSSurrogate(sm, seed=0)
+    # the plain points must equal the fallback handle's own evaluation
+    ref = be.matrix(fb.ioshape)
+    _lib.check(_lib.load().dgfs_vhs_apply(
+        sur._plain_h, fb._as_parameter_, ref._as_parameter_, nupts, neles,
+        fb.traits[1], be.soasz, -1, 0, be.stream), 'dgfs_vhs_apply')
     out = be.matrix(fb.ioshape)
     g = sur.collide(fb, out, threshold=0.0)
     torch.cuda.synchronize()
