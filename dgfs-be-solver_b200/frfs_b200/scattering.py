@@ -102,18 +102,21 @@ class DGFSVHSGLLScatteringModel(DGFSScatteringModel):
                    'dgfs_vhs_create')
         return h
 
-    def make_handle(self, exchange):
-        """A second operator handle on the same tables' parameters with the
-        first compiled launch shape of the given kind ('push', 'pull',
-        'single-cta') selected, e.g. a cluster shape for calls on a few
-        points (it spreads one point over several SMs).  Owned and freed by
-        this model; None when no shape of that kind is compiled."""
-        kinds = [v['exchange'] for v in self.variants()]
-        if exchange not in kinds:
+    def make_handle(self, exchange, largest_cluster=False):
+        """A second operator handle on the same parameters with the first
+        compiled launch shape of the given kind ('push', 'pull',
+        'single-cta') selected -- or, with largest_cluster, the one of that
+        kind with the most CTAs per point, for calls on a few points (it
+        spreads each over the most SMs).  Owned and freed by this model;
+        None when no shape of that kind is compiled."""
+        vs = self.variants()
+        idx = [i for i, v in enumerate(vs) if v['exchange'] == exchange]
+        if not idx:
             return None
+        pick = max(idx, key=lambda i: (vs[i]['cluster'], -i)) \
+            if largest_cluster else idx[0]
         h = self._create_handle()
-        _lib.check(self._lib.dgfs_vhs_select(h, kinds.index(exchange)),
-                   'dgfs_vhs_select')
+        _lib.check(self._lib.dgfs_vhs_select(h, pick), 'dgfs_vhs_select')
         self._extra.append(h)
         return h
 
