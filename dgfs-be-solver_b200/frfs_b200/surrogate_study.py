@@ -42,11 +42,18 @@ class ZeroSurrogate(VHSSurrogate):
         return Bp
 
 
-def make_system(ini, precision, device, sphdesign=None, graphs=True):
+def make_system(ini, precision, device, sphdesign=None, graphs=True,
+                project=None):
+    """The workload's system; FP32 runs take the FP64 conservation
+    projection (the production single-precision mode), FP64 runs the plain
+    reference operator, unless ``project`` says otherwise."""
     cfg = Inifile(ini(precision=precision))
     if sphdesign:
         cfg.set('spherical-design-rule', 'path', sphdesign)
     cfg.set('backend-b200', 'cuda-graphs', '1' if graphs else '0')
+    if project is None:
+        project = precision == 'single'
+    cfg.set('backend-b200', 'vhs-project', '1' if project else '0')
     be = B200Backend(cfg, device=device)
     return DGFSSystem(be, cfg)
 
