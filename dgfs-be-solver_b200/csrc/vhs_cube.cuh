@@ -23,10 +23,8 @@
 // transforms broadcast along one axis with a (-1)^x sign:
 //     Nq(x) = (-1)^x1 T1(x2,x3) + (-1)^x2 T2(x1,x3) + (-1)^x3 T3(x1,x2).
 // Off the Nyquist planes m = cos a + sin a: one complex transform per (p, q)
-// instead of two.  Per point: 1 + Nrho M + Nrho + 1 full transforms plus
-// the 2D ones (reference: 3 Nrho M + 3).  The last transform packs the two
-// real results: IFFT(fC + i b2 F) = Re QG + i Re Lf (fC and b2 F are
-// conjugate-even).
+// instead of two.  Per point: 1 + Nrho M + Nrho + 2 full transforms plus
+// the 2D ones (reference: 3 Nrho M + 3).
 //
 // Layout (shared memory, complex float): F for k3 <= N/2 ([N][N][N/2+1]),
 // the work cube as N^2 lines of N+1 (padding keeps line-parallel accesses
@@ -379,38 +377,82 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
       __syncthreads();
     }
 
-    // ---- IFFT(fC + i b2 F) = Re QG + i Re Lf; Q = prefac (QG - f Lf) ---------
+    // ---- Q = prefac (Re IFFT(fC) - f IFFT(b2 F)) ----------------------------
+    // Two transforms: fC, summed from FP32 transforms of real fields, is
+    // conjugate-even only to round-off, and packing it with b2 F into one
+    // transform would leak that round-off into the loss term as a constant
+    // times f (a momentum error proportional to rho u).
+    auto pass23 = [&]() {  // passes along k2 (in place) then along k1
+      __syncthreads();
+      if (is_main) {
+        const int L0 = tid, L1 = tid + NM;
+        C* w0 = sW + (L0 / N) * N * LP + L0 % N;
+        C* w1 = sW + (L1 / N) * N * LP + L1 % N;
+        C x[N], y[N];
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+          x[j] = w0[j * LP];
+          y[j] = w1[j * LP];
+        }
+        fft<float, N, +1>(x);
+        fft<float, N, +1>(y);
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+          w0[j * LP] = x[j];
+          w1[j * LP] = y[j];
+        }
+      }
+      __syncthreads();
+    };
+    // Lf = IFFT(b2 F): b2 F is built conjugate-even from the half spectrum.
+    // F is not needed after this transform's first pass, so its storage
+    // takes the real Lf values (slot v of each thread's own lines).
+    float* const sLf = reinterpret_cast<float*>(sF);
+    static_assert(2 * NN * H >= V, "Lf fits in the spectrum storage");
     if (is_main) {
 #pragma unroll 1
       for (int r = 0; r < 2; ++r) {
         const int L = tid + r * NM, k1 = L / N, k2 = L % N;
         C x[N];
 #pragma unroll
-        for (int k = 0; k < N; ++k) {
-          const C g = fcg[(size_t)L * N + k];
-          const C Fv = Fat(k1, k2, k);
-          const float b = a.b2[L * N + k];
-          x[k] = mk<C>(g.x - b * Fv.y, g.y + b * Fv.x);
-        }
+        for (int k = 0; k < N; ++k) x[k] = cscale(Fat(k1, k2, k), a.b2[L * N + k]);
         fft<float, N, +1>(x);
 #pragma unroll
         for (int k = 0; k < N; ++k) sW[L * LP + k] = x[k];
       }
     }
-    __syncthreads();
+    pass23();
     if (is_main) {
-#pragma unroll 1
-      for (int r = 0; r < 2; ++r) {
-        const int L = tid + r * NM, k1 = L / N, x3 = L % N;
-        C x[N];
+      const int L0 = tid, L1 = tid + NM;
+      C x[N], y[N];
 #pragma unroll
-        for (int j = 0; j < N; ++j) x[j] = sW[(k1 * N + j) * LP + x3];
-        fft<float, N, +1>(x);
+      for (int i = 0; i < N; ++i) {
+        x[i] = sW[(i * N + L0 / N) * LP + L0 % N];
+        y[i] = sW[(i * N + L1 / N) * LP + L1 % N];
+      }
+      fft<float, N, +1>(x);
+      fft<float, N, +1>(y);
 #pragma unroll
-        for (int j = 0; j < N; ++j) sW[(k1 * N + j) * LP + x3] = x[j];
+      for (int i = 0; i < N; ++i) {
+        sLf[(i * N + L0 / N) * N + L0 % N] = x[i].x;
+        sLf[(i * N + L1 / N) * N + L1 % N] = y[i].x;
       }
     }
     __syncthreads();
+    // QG = Re IFFT(fC)
+    if (is_main) {
+#pragma unroll 1
+      for (int r = 0; r < 2; ++r) {
+        const int L = tid + r * NM;
+        C x[N];
+#pragma unroll
+        for (int k = 0; k < N; ++k) x[k] = fcg[(size_t)L * N + k];
+        fft<float, N, +1>(x);
+#pragma unroll
+        for (int k = 0; k < N; ++k) sW[L * LP + k] = x[k];
+      }
+    }
+    pass23();
     double mom[5] = {0, 0, 0, 0, 0};
     if (is_main) {
 #pragma unroll 1
@@ -424,7 +466,7 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
         for (int i = 0; i < N; ++i) {
           const int64_t v = (int64_t)(i * N + x2) * N + x3;
           const float fv = a.f[soa_ix(upt, a.ldim, elem, v, V, a.soasz)];
-          const float qq = a.prefac * (x[i].x - fv * x[i].y);
+          const float qq = a.prefac * (x[i].x - fv * sLf[v]);
           if (!a.project) {
             a.Q[soa_ix(upt, a.ldim, elem, v, V, a.soasz)] = qq;
             continue;
