@@ -382,24 +382,19 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
     // conjugate-even only to round-off, and packing it with b2 F into one
     // transform would leak that round-off into the loss term as a constant
     // times f (a momentum error proportional to rho u).
-    auto pass23 = [&]() {  // passes along k2 (in place) then along k1
+    auto pass23 = [&]() {  // the pass along k2, in place, between barriers
       __syncthreads();
       if (is_main) {
-        const int L0 = tid, L1 = tid + NM;
-        C* w0 = sW + (L0 / N) * N * LP + L0 % N;
-        C* w1 = sW + (L1 / N) * N * LP + L1 % N;
-        C x[N], y[N];
+#pragma unroll 1
+        for (int r = 0; r < 2; ++r) {
+          const int L = tid + r * NM;
+          C* w = sW + (L / N) * N * LP + L % N;
+          C x[N];
 #pragma unroll
-        for (int j = 0; j < N; ++j) {
-          x[j] = w0[j * LP];
-          y[j] = w1[j * LP];
-        }
-        fft<float, N, +1>(x);
-        fft<float, N, +1>(y);
+          for (int j = 0; j < N; ++j) x[j] = w[j * LP];
+          fft<float, N, +1>(x);
 #pragma unroll
-        for (int j = 0; j < N; ++j) {
-          w0[j * LP] = x[j];
-          w1[j * LP] = y[j];
+          for (int j = 0; j < N; ++j) w[j * LP] = x[j];
         }
       }
       __syncthreads();
@@ -423,19 +418,15 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
     }
     pass23();
     if (is_main) {
-      const int L0 = tid, L1 = tid + NM;
-      C x[N], y[N];
+#pragma unroll 1
+      for (int r = 0; r < 2; ++r) {
+        const int L = tid + r * NM, x2 = L / N, x3 = L % N;
+        C x[N];
 #pragma unroll
-      for (int i = 0; i < N; ++i) {
-        x[i] = sW[(i * N + L0 / N) * LP + L0 % N];
-        y[i] = sW[(i * N + L1 / N) * LP + L1 % N];
-      }
-      fft<float, N, +1>(x);
-      fft<float, N, +1>(y);
+        for (int i = 0; i < N; ++i) x[i] = sW[(i * N + x2) * LP + x3];
+        fft<float, N, +1>(x);
 #pragma unroll
-      for (int i = 0; i < N; ++i) {
-        sLf[(i * N + L0 / N) * N + L0 % N] = x[i].x;
-        sLf[(i * N + L1 / N) * N + L1 % N] = y[i].x;
+        for (int i = 0; i < N; ++i) sLf[(i * N + x2) * N + x3] = x[i].x;
       }
     }
     __syncthreads();
