@@ -30,8 +30,9 @@
 // the work cube as N^2 lines of N+1 (padding keeps line-parallel accesses
 // free of bank conflicts), the three Nyquist planes, the axis phases.
 // The gain spectrum fC accumulates in a global (L2-resident) slice per CTA.
-// Main threads own two lines per pass; NQ extra threads transform the
-// Nyquist planes during the first two passes of every (p, q).
+// Main threads own two lines per pass; NQ extra threads (at most two lines
+// each) transform the Nyquist planes during the first two passes of every
+// (p, q).
 #pragma once
 
 #include "vhs_kernel.cuh"
@@ -43,7 +44,7 @@ template <int N> struct CubeGeom {
   static constexpr int NN = N * N;
   static constexpr int LP = N + 1;                      // padded line stride
   static constexpr int NM = NN / 2;                     // main threads (2 lines)
-  static constexpr int NQ = ((3 * N + 31) / 32) * 32;   // Nyquist-plane threads
+  static constexpr int NQ = ((3 * N / 2 + 31) / 32) * 32;  // Nyquist threads, <= 2 lines each
   static constexpr int NT = NM + NQ;
   static constexpr int V = N * N * N;
   static constexpr int PHS = 3 * N + 4;                 // one phase slot
@@ -55,8 +56,15 @@ template <int N> struct CubeGeom {
   static_assert(NM % 32 == 0, "main threads must fill warps");
 };
 
+// register cap: the whole 64K register file shared by NT threads (rounded
+// down to a multiple of 8)
+template <int N> constexpr int cube_maxnreg() {
+  return (65536 / CubeGeom<N>::NT) / 8 * 8 > 255 ? 255 : (65536 / CubeGeom<N>::NT) / 8 * 8;
+}
+
 template <int N, bool IL1>
-__global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsArgs<float> a) {
+__global__ void __maxnreg__(cube_maxnreg<N>())
+    vhs_cube_kernel(const VhsArgs<float> a) {
   using G = CubeGeom<N>;
   using C = cx<float>;
   constexpr int H = G::H, NN = G::NN, LP = G::LP, NM = G::NM, V = G::V, PHS = G::PHS, NT = G::NT;
@@ -225,11 +233,13 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
             sW[L0 * LP + k] = x[k];
             sW[L1 * LP + k] = y[k];
           }
-        } else if (tq < 3 * N) {
+        } else {
           // n F on the Nyquist planes: plane 1 (k1 = N/2) lines over k3,
           // plane 2 (k2 = N/2, k1 != N/2) lines over k3, plane 3 (k3 = N/2,
           // k1, k2 != N/2) lines over k2
-          const int which = tq / N, j = tq % N;
+#pragma unroll 1
+          for (int line = tq; line < 3 * N; line += G::NQ) {
+          const int which = line / N, j = line % N;
           C x[N];
 #pragma unroll
           for (int k = 0; k < N; ++k) {
@@ -259,6 +269,7 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
           C* T = which == 0 ? sT1 : (which == 1 ? sT2 : sT3);
 #pragma unroll
           for (int k = 0; k < N; ++k) T[j * LP + k] = x[k];
+          }
         }
         if (pq + 1 < npq) phase_store(phn, slot ^ 1);
         __syncthreads();
@@ -281,15 +292,18 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
             w0[j * LP] = x[j];
             w1[j * LP] = y[j];
           }
-        } else if (tq < 3 * N) {
-          const int which = tq / N, col = tq % N;
-          C* T = which == 0 ? sT1 : (which == 1 ? sT2 : sT3);
-          C x[N];
+        } else {
+#pragma unroll 1
+          for (int line = tq; line < 3 * N; line += G::NQ) {
+            const int which = line / N, col = line % N;
+            C* T = which == 0 ? sT1 : (which == 1 ? sT2 : sT3);
+            C x[N];
 #pragma unroll
-          for (int j = 0; j < N; ++j) x[j] = T[j * LP + col];
-          fft<float, N, +1>(x);
+            for (int j = 0; j < N; ++j) x[j] = T[j * LP + col];
+            fft<float, N, +1>(x);
 #pragma unroll
-          for (int j = 0; j < N; ++j) T[j * LP + col] = x[j];
+            for (int j = 0; j < N; ++j) T[j * LP + col] = x[j];
+          }
         }
         __syncthreads();
         // pass 3: lines (x2, x3) along k1, both lines at once;
