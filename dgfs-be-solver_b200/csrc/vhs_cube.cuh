@@ -30,9 +30,8 @@
 // the work cube as N^2 lines of N+1 (padding keeps line-parallel accesses
 // free of bank conflicts), the three Nyquist planes, the axis phases.
 // The gain spectrum fC accumulates in a global (L2-resident) slice per CTA.
-// Main threads own two lines per pass; NQ extra threads (at most two lines
-// each) transform the Nyquist planes during the first two passes of every
-// (p, q).
+// Main threads own two lines per pass; NQ extra threads (one line each)
+// transform the Nyquist planes during the first two passes of every (p, q).
 #pragma once
 
 #include "vhs_kernel.cuh"
@@ -44,7 +43,7 @@ template <int N> struct CubeGeom {
   static constexpr int NN = N * N;
   static constexpr int LP = N + 1;                      // padded line stride
   static constexpr int NM = NN / 2;                     // main threads (2 lines)
-  static constexpr int NQ = ((3 * N / 2 + 31) / 32) * 32;  // Nyquist threads, <= 2 lines each
+  static constexpr int NQ = ((3 * N + 31) / 32) * 32;  // Nyquist threads, one line each
   static constexpr int NT = NM + NQ;
   static constexpr int V = N * N * N;
   static constexpr int PHS = 3 * N + 4;                 // one phase slot
@@ -56,15 +55,8 @@ template <int N> struct CubeGeom {
   static_assert(NM % 32 == 0, "main threads must fill warps");
 };
 
-// register cap: the whole 64K register file shared by NT threads (rounded
-// down to a multiple of 8)
-template <int N> constexpr int cube_maxnreg() {
-  return (65536 / CubeGeom<N>::NT) / 8 * 8 > 255 ? 255 : (65536 / CubeGeom<N>::NT) / 8 * 8;
-}
-
 template <int N, bool IL1>
-__global__ void __maxnreg__(cube_maxnreg<N>())
-    vhs_cube_kernel(const VhsArgs<float> a) {
+__global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsArgs<float> a) {
   using G = CubeGeom<N>;
   using C = cx<float>;
   constexpr int H = G::H, NN = G::NN, LP = G::LP, NM = G::NM, V = G::V, PHS = G::PHS, NT = G::NT;
