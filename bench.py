@@ -334,8 +334,10 @@ def run_b200(args):
     if args.variant >= 0:
         sm.select(args.variant)
         tune = {'variant': sm.variants()[args.variant], 'all_ms': {}}
+        tune_idx = args.variant
     else:
         tune = sm.autotune(fin, fout, cache=False)
+        tune_idx = getattr(sm, "_variant", 0)
 
     for _ in range(args.warmup):
         step()
@@ -391,10 +393,16 @@ def run_b200(args):
     flops_pt = sm.flops_per_point()
     achieved = flops_pt*npts/(vhs_ms*1e-3)/1e12
     # DRAM bytes of one sweep from the committed ncu capture of the same
-    # launch (profiles/vhs_push_couette_n24_f32.md): f in + Q out, the
-    # tables stay in L2
-    traffic = 35.5e6 if (args.workload == 'couette-n24' and prec == 32) \
-        else None
+    # launch: f in + Q out, the tables and the per-CTA gain spectrum stay in
+    # L2 (profiles/vhs_cube_couette_n24_f32.md, vhs_push_couette_n24_f32.md)
+    kind = None
+    try:
+        kind = sm.variants()[tune_idx]['exchange']
+    except Exception:
+        pass
+    traffic = None
+    if args.workload == 'couette-n24' and prec == 32:
+        traffic = {'single-cta': 42.9e6, 'push': 35.5e6}.get(kind)
     roof = {'bound': 'fp32-simt' if prec == 32 else 'fp64-simt',
             'achieved': achieved, 'peak': tf.value, 'unit': 'TFLOP/s',
             'frac': achieved/tf.value,
@@ -402,10 +410,12 @@ def run_b200(args):
                            '(dgfs_probe_fma_peak)',
             'flops_per_point': flops_pt, 'launch_ms': vhs_ms,
             'traffic': traffic,
-            'traffic_source': 'ncu dram__bytes_read.sum + write.sum, '
-                              'profiles/vhs_push_couette_n24_f32.md'
-            if traffic else None,
-            'kernel': 'vhs_push_kernel / vhs_cluster_kernel (autotuned)'}
+            'traffic_source': 'ncu dram__bytes_read.sum + write.sum of the '
+                              'same launch shape, profiles/' if traffic
+            else None,
+            'kernel': {'single-cta': 'vhs_cube_kernel',
+                       'push': 'vhs_push_kernel',
+                       'pull': 'vhs_cluster_kernel'}.get(kind, kind)}
     extra = {}
     if args.mode == 'step':
         extra['dg_step_ms'] = ms_per_step
