@@ -22,7 +22,7 @@ struct dgfs_dg {
   void* uf;        // flux-point scratch [F][ldim_f]
 };
 
-constexpr int kBcChunks = 64;  // velocity chunks of the wall-sum reduction
+constexpr int kBcChunks = 256;  // velocity chunks of the wall-sum reduction
 
 namespace {
 
@@ -317,8 +317,7 @@ extern "C" int dgfs_dg_updatebc(dgfs_dg* h, int v0, int nv, int reset, void* str
     a.nv = nv;
     dg_bcsum_kernel<float, 2><<<grid, 256, 0, s>>>(a, h->bfpt, h->bele, h->nb, h->cw, chunk, h->bcpart);
   }
-  dg_bcsum_finish_kernel<<<(h->nb + 255) / 256, 256, 0, s>>>(h->bkind, h->nb, nchunks, h->bcpart, h->bcvals,
-                                                              reset);
+  dg_bcsum_finish_kernel<<<(h->nb + 7) / 8, 256, 0, s>>>(h->bkind, h->nb, nchunks, h->bcpart, h->bcvals, reset);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_error(DGFS_ERR_CUDA, "DG boundary update launch: %s", cudaGetErrorString(e));
   return DGFS_OK;

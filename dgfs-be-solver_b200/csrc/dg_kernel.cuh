@@ -129,28 +129,38 @@ __global__ void __launch_bounds__(256) dg_bcsum_kernel(const DgArgs<T> a, const 
   }
 }
 
-// Pass 2: sum the chunks in a fixed order (deterministic) into bcvals.
+// Pass 2: one warp per boundary point sums the chunks into bcvals in a
+// fixed order (lane-strided partial sums, then a fixed butterfly), so the
+// result is the same on every run.
 __global__ void __launch_bounds__(256) dg_bcsum_finish_kernel(const int* __restrict__ bkind, int nb, int nchunks,
                                                              const double* __restrict__ partials,
                                                              double* __restrict__ bcvals, int reset) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= nb || bkind[b] != BC_WALL_DIFFUSE) return;
+  const int b = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (b >= nb || bkind[b] != BC_WALL_DIFFUSE) return;  // uniform per warp
   double r0 = 0.0, r1 = 0.0;
-  for (int c = 0; c < nchunks; ++c) {
+  for (int c = lane; c < nchunks; c += 32) {
     r0 += partials[((int64_t)c * nb + b) * 2];
     r1 += partials[((int64_t)c * nb + b) * 2 + 1];
   }
-  if (reset) {
-    bcvals[2 * b] = r0;
-    bcvals[2 * b + 1] = r1;
-  } else {
-    bcvals[2 * b] += r0;
-    bcvals[2 * b + 1] += r1;
+  for (int o = 16; o > 0; o >>= 1) {
+    r0 += __shfl_xor_sync(0xffffffffu, r0, o);
+    r1 += __shfl_xor_sync(0xffffffffu, r1, o);
+  }
+  if (lane == 0) {
+    if (reset) {
+      bcvals[2 * b] = r0;
+      bcvals[2 * b + 1] = r1;
+    } else {
+      bcvals[2 * b] += r0;
+      bcvals[2 * b + 1] += r1;
+    }
   }
 }
 
+// FP32: 4 CTAs per SM (<= 64 registers): the kernel is bound by the latency
+// of its dependent partner loads, so occupancy buys memory parallelism
 template <typename T, int U, int F, int D>
-__global__ void __launch_bounds__(256) dg_residual_kernel(const DgArgs<T> a, const DgOps<T, U, F, D> op) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1) dg_residual_kernel(const DgArgs<T> a, const DgOps<T, U, F, D> op) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = (int)(t & 31);
   const int64_t w = t >> 5;
