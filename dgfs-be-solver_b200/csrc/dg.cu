@@ -17,6 +17,7 @@ struct dgfs_dg {
   std::vector<double> m0, m132, m3;  // host copies (operators travel as params)
   void *smats, *rcpdjac, *nrm, *mag, *cvx, *cvy, *cvz, *guw, *gfw;
   int *part, *bkind, *bgroup, *bfpt, *bele, *grefl;
+  int64_t* pbase;  // [F][E] partner offsets in the flux bank at v = 0
   double* bcvals;
   double* bcpart;  // [kBcChunks][nb][2] partial wall sums
   void* uf;        // flux-point scratch [F][ldim_f]
@@ -81,6 +82,7 @@ template <typename T> DgArgs<T> make_args(const dgfs_dg* h) {
   a.nrm = (const T*)h->nrm;
   a.mag = (const T*)h->mag;
   a.part = h->part;
+  a.pbase = h->pbase;
   a.cvx = (const T*)h->cvx;
   a.cvy = (const T*)h->cvy;
   a.cvz = (const T*)h->cvz;
@@ -175,7 +177,8 @@ int check_range(const dgfs_dg* h, int v0, int nv) {
 void free_dg(dgfs_dg* h) {
   if (!h) return;
   void* ptrs[] = {h->smats, h->rcpdjac, h->nrm, h->mag, h->cvx, h->cvy, h->cvz, h->guw, h->gfw,
-                  h->part, h->bkind, h->bgroup, h->bfpt, h->bele, h->grefl, h->bcvals, h->bcpart, h->uf};
+                  h->part, h->pbase, h->bkind, h->bgroup, h->bfpt, h->bele, h->grefl, h->bcvals, h->bcpart,
+                  h->uf};
   for (void* q : ptrs) cudaFree(q);
   delete h;
 }
@@ -239,6 +242,18 @@ extern "C" int dgfs_dg_create(const dgfs_dg_params* p, dgfs_dg** out) {
   int rc = cudaGetDevice(&h->device) == cudaSuccess ? DGFS_OK : set_error(DGFS_ERR_CUDA, "no CUDA device");
   if (!rc) rc = h->prec == 64 ? upload_geom<double>(h, p) : upload_geom<float>(h, p);
   if (!rc) rc = upload_int(&h->part, p->partner, (size_t)F * E);
+  if (!rc) {
+    // partner offsets in the flux bank at v = 0: fr ldim_f + (er/32) V 32 + er%32
+    std::vector<int64_t> pb((size_t)F * E);
+    for (size_t i = 0; i < pb.size(); ++i) {
+      const int q = p->partner[i];
+      pb[i] = q < 0 ? -1
+                    : (int64_t)(q / E) * h->ldim_f + (int64_t)((q % E) >> 5) * h->V * 32 + ((q % E) & 31);
+    }
+    if (cudaMalloc((void**)&h->pbase, pb.size() * sizeof(int64_t)) != cudaSuccess ||
+        cudaMemcpy(h->pbase, pb.data(), pb.size() * sizeof(int64_t), cudaMemcpyHostToDevice) != cudaSuccess)
+      rc = set_error(DGFS_ERR_NOMEM, "partner offset upload failed");
+  }
   const int nb = h->nb ? h->nb : 1;
   std::vector<int> zeros(nb, 0);
   if (!rc) rc = upload_int(&h->bkind, h->nb ? p->bkind : zeros.data(), nb);

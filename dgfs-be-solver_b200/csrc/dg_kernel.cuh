@@ -47,6 +47,7 @@ template <typename T> struct DgArgs {
   const T* nrm;            // [F][D][E] unit outward normals
   const T* mag;            // [F][E]    |S^T n|
   const int* part;         // [F][E]    fpt_r*E + e_r, or -(b+1) for boundary b
+  const int64_t* pbase;    // [F][E]    partner's flux-bank offset at v = 0 (-1: boundary)
   const T* cvx;            // [V] velocity grid
   const T* cvy;
   const T* cvz;
@@ -157,10 +158,11 @@ __global__ void __launch_bounds__(256) dg_bcsum_finish_kernel(const int* __restr
   }
 }
 
-// FP32: 4 CTAs per SM (<= 64 registers): the kernel is bound by the latency
-// of its dependent partner loads, so occupancy buys memory parallelism
+// FP32: at least 2 CTAs per SM.  The kernel is bound by the latency of its
+// partner loads; they are issued together up front (precomputed offsets)
+// so that their latencies overlap
 template <typename T, int U, int F, int D>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1) dg_residual_kernel(const DgArgs<T> a, const DgOps<T, U, F, D> op) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) dg_residual_kernel(const DgArgs<T> a, const DgOps<T, U, F, D> op) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = (int)(t & 31);
   const int64_t w = t >> 5;
@@ -173,6 +175,15 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1) dg_residual_kerne
 #pragma unroll
   for (int i = 0; i < U; ++i) u[i] = a.u[aos32(i, a.ldim_u, e, v, a.V)];
   const T c[3] = {a.cvx[v], a.cvy[v], a.cvz[v]};
+
+  // partner values first: every load independent of the others, so their
+  // latencies overlap (offsets precomputed per (flux point, element))
+  T urv[F];
+#pragma unroll
+  for (int f = 0; f < F; ++f) {
+    const int64_t pb = a.pbase[(int64_t)f * E + e];
+    urv[f] = pb >= 0 ? a.uf[pb + (int64_t)v * 32] : T(0);
+  }
 
   // common normal fluxes at this element's flux points
   T fh[F];
@@ -190,8 +201,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1) dg_residual_kerne
     const int p = a.part[(int64_t)f * E + e];
     T ur;
     if (p >= 0) {
-      const int64_t fr = p / E, er = p % E;
-      ur = a.uf[aos32(fr, a.ldim_f, er, v, a.V)];
+      ur = urv[f];
     } else {
       const int b = -p - 1;
       const int kind = a.bkind[b], g = a.bgroup[b];
