@@ -119,7 +119,7 @@ def run_study(ini, device='cuda:0', runs=5, steps=100, nsteps=200,
               epochs=60, batch=1024, lr=1e-3, threshold=0.05, eps_max=0.2,
               check_every=50, tol=5e-3, reps=10, sphdesign=None, seed=1,
               max_pairs=200000, relax_points=576, relax_steps=100,
-              relax_dt=0.005, log=None):
+              relax_dt=0.005, extra_thresholds=None, log=None):
     t0 = time.time()
     say = log or (lambda *a: None)
     s32 = make_system(ini, 'single', device, sphdesign)
@@ -169,6 +169,19 @@ def run_study(ini, device='cuda:0', runs=5, steps=100, nsteps=200,
         return {'rho': rel_l2(r, r64), 'u': rel_l2(u, u64),
                 'T': rel_l2(T, T64)}
 
+    # the gate threshold: error and speed of the surrogate run at others
+    sweep = {}
+    for thr in (extra_thresholds or ()):
+        sur.threshold = thr
+        (rt, ut, Tt), it, _ = run_workload(s32, nsteps, sur)
+        ft, ot = s32.bank[it], scratch[0]
+        tp = time_sweep(lambda: s32.sm.fs_all(ft, ot), reps, device)
+        ts = time_sweep(lambda: sur.collide(ft, ot), reps, device)
+        sweep[str(thr)] = {'err': errs(rt, ut, Tt), 'speedup': tp/ts,
+                           'gate_fraction':
+                           float((sur._last[0] != 0).float().mean())}
+    sur.threshold = threshold
+
     # 4. throughput of one collision sweep on the surrogate run's final state
     fin = s32.bank[idx]
     out = scratch[0]
@@ -196,5 +209,6 @@ def run_study(ini, device='cuda:0', runs=5, steps=100, nsteps=200,
         'plain_evals_per_s': npts/(t_plain*1e-3),
         'surrogate_evals_per_s': npts/(t_sur*1e-3),
         'speedup': t_plain/t_sur,
+        'threshold_sweep': sweep,
         'wall_s': time.time() - t0,
     }
