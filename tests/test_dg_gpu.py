@@ -137,8 +137,7 @@ def test_ssp_rk2_steps_match_oracle(precision, graphs):
                 out[i, :, e] = ovhs.vhs_Q(x[i, :, e], ovm, pre, prefac)
         return out
 
-    uo = s.bank[1].get()*0 + u  # FP32 banks start from the rounded input
-    uo = s.bank[0].get().astype(np.float64) if False else uo
+    # FP32 banks start from the rounded input
     u0 = u.astype(np.float32).astype(np.float64) if precision == 'single' \
         else u
     for _ in range(2):
