@@ -457,7 +457,7 @@ def run_b200(args):
         from frfs_b200.surrogate_study import run_study
         sur = run_study(workloads.WORKLOADS[args.workload],
                         device=be.device, nsteps=args.surrogate_steps,
-                        sphdesign=SPHDESIGN)
+                        sphdesign=SPHDESIGN, extra_thresholds=(0.1, 0.2))
 
     if rank == 0:
         cb = None

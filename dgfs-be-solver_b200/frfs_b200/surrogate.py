@@ -595,6 +595,23 @@ def random_uniform_state(vm, rng, bimodal):
     return f*rho/(np.sum(f)*vm.cw())
 
 
+def random_near_state(vm, rng, dmin=10**-1.5):
+    """A spatially uniform Maxwellian at a log-uniform distance d in
+    [dmin, 1] from the nondimensional reference state (rho = 1, T = 1,
+    u = 0, the scales the velocity mesh is built on): u uniform in the ball
+    of radius d, log rho and log T uniform in [-0.7 d, 0.7 d].  The
+    parameters stay inside the ranges of random_uniform_state's box
+    (rho in [0.5, 2], T in [0.5, 2], |u| <= 1) but the mismatch between
+    gas and walls at the reference temperature covers every scale, so the
+    wall fronts the solver grows range from weak to strong."""
+    from frfs_b200.initcond import maxwellian_values
+    d = 10**rng.uniform(np.log10(dmin), 0.0)
+    u = d*_ball(rng)
+    T = float(np.exp(d*rng.uniform(-0.7, 0.7)))
+    rho = float(np.exp(d*rng.uniform(-0.7, 0.7)))
+    return maxwellian_values(vm, rho, T, u)
+
+
 def random_point_states(vm, n, rng):
     """n distributions spanning far from and near equilibrium: wall fronts
     (the gas Maxwellian on one side of a random plane, another Maxwellian on
@@ -696,10 +713,11 @@ def _subsample(X, B, max_pairs, seed):
 
 
 def harvest(system, stepper_cls, sur, runs, steps, seed=1, eps_max=0.2,
-            bimodal_every=3, max_pairs=None):
+            bimodal_every=3, max_pairs=None, near=False):
     """Run ``runs`` trajectories of ``steps`` steps of the plain solver from
     random uniform initial states (seeds seed .. seed+runs-1; every
-    ``bimodal_every``-th is a bimodal mixture) and collect the (f, Q(f))
+    ``bimodal_every``-th is a bimodal mixture; with ``near``, Maxwellians
+    near the reference state, random_near_state) and collect the (f, Q(f))
     pairs of every collide (a seeded random subset of ``max_pairs`` when
     given).  Returns X, B on the device."""
     h = Harvester(sur, eps_max)
@@ -710,8 +728,11 @@ def harvest(system, stepper_cls, sur, runs, steps, seed=1, eps_max=0.2,
     try:
         for r in range(runs):
             rng = np.random.default_rng(seed + r)
-            f = random_uniform_state(vm, rng, (r % bimodal_every) ==
-                                     bimodal_every - 1)
+            if near:
+                f = random_near_state(vm, rng)
+            else:
+                f = random_uniform_state(vm, rng, (r % bimodal_every) ==
+                                         bimodal_every - 1)
             system.bank[0].set(np.broadcast_to(f[None, :, None], shape))
             st = stepper_cls(system, system.cfg)
             st.use_graphs = False

@@ -6,12 +6,15 @@ it with the plain operator (no counterpart in the reference).
 
 1. harvest (f, Q(f)) pairs from the plain FP32 solver started from random
    uniform states (Maxwellians with rho in [0.5, 2], T in [0.5, 3],
-   |u| <= 1, and bimodal mixtures), and from space-homogeneous relaxations
-   of random per-point states (which cross every distance from
-   equilibrium);
+   |u| <= 1, and bimodal mixtures; and Maxwellians at a log-uniform
+   distance from the reference state, whose mismatch with the walls covers
+   weak to strong wall fronts), and from space-homogeneous relaxations of
+   random per-point states (which cross every distance from equilibrium);
 2. train the MLP with the project's kernels;
 3. run the workload from its own initial state: plain FP64 (the reference
-   solution), plain FP32, surrogate-assisted FP32 (with a sampled residual
+   solution; once more with the conservation projection, the solution the
+   projected surrogate output tends to), plain FP32, surrogate-assisted
+   FP32 (with a sampled residual
    check every ``check_every`` steps that drops the surrogate when it
    fails), the same without checks, and an ablation in which the gated
    points get Q = 0 (the gate without the network);
@@ -115,7 +118,8 @@ def time_sweep(fn, reps, device):
     return e0.elapsed_time(e1)/reps
 
 
-def run_study(ini, device='cuda:0', runs=5, steps=100, nsteps=200,
+def run_study(ini, device='cuda:0', runs=5, near_runs=10, steps=100,
+              nsteps=200,
               epochs=60, batch=1024, lr=1e-3, threshold=0.05, eps_max=0.2,
               check_every=50, tol=5e-3, reps=10, sphdesign=None, seed=1,
               max_pairs=200000, relax_points=576, relax_steps=100,
@@ -130,6 +134,12 @@ def run_study(ini, device='cuda:0', runs=5, steps=100, nsteps=200,
     th = time.time()
     X, B = harvest(s32, StdTVDRK2DGFSStepper, sur, runs, steps, seed=seed,
                    eps_max=eps_max, max_pairs=max_pairs)
+    if near_runs:
+        Xn, Bn = harvest(s32, StdTVDRK2DGFSStepper, sur, near_runs, steps,
+                         seed=seed + 1000, eps_max=eps_max,
+                         max_pairs=max_pairs, near=True)
+        X, B = torch.cat([X, Xn]), torch.cat([B, Bn])
+        del Xn, Bn
     npairs_solver = int(X.shape[0])
     if relax_steps:
         Xr, Br = harvest_relaxation(s32.sm, sur, relax_points, relax_steps,
@@ -157,6 +167,13 @@ def run_study(ini, device='cuda:0', runs=5, steps=100, nsteps=200,
     (r64, u64, T64), _, _ = run_workload(s64, nsteps)
     del s64
     torch.cuda.empty_cache()
+    # the same with the conservation projection: the surrogate's output is
+    # projected, so against this solution its error is that of the network
+    # and the gate alone, without the plain operator's own conservation error
+    s64 = make_system(ini, 'double', device, sphdesign, project=True)
+    (p64, v64, S64), _, _ = run_workload(s64, nsteps)
+    del s64
+    torch.cuda.empty_cache()
     (r32, u32, T32), _, _ = run_workload(s32, nsteps)
     zero = ZeroSurrogate(s32.sm, threshold=threshold)
     (rz, uz, Tz), _, _ = run_workload(s32, nsteps, zero)
@@ -169,18 +186,28 @@ def run_study(ini, device='cuda:0', runs=5, steps=100, nsteps=200,
         return {'rho': rel_l2(r, r64), 'u': rel_l2(u, u64),
                 'T': rel_l2(T, T64)}
 
+    def errs_proj(r, u, T):
+        return {'rho': rel_l2(r, p64), 'u': rel_l2(u, v64),
+                'T': rel_l2(T, S64)}
+
     # the gate threshold: error and speed of the surrogate run at others
     sweep = {}
     for thr in (extra_thresholds or ()):
-        sur.threshold = thr
+        sur.threshold = zero.threshold = thr
+        (ra, ua, Ta), _, _ = run_workload(s32, nsteps, zero)
         (rt, ut, Tt), it, _ = run_workload(s32, nsteps, sur)
         ft, ot = s32.bank[it], scratch[0]
         tp = time_sweep(lambda: s32.sm.fs_all(ft, ot), reps, device)
         ts = time_sweep(lambda: sur.collide(ft, ot), reps, device)
-        sweep[str(thr)] = {'err': errs(rt, ut, Tt), 'speedup': tp/ts,
+        sweep[str(thr)] = {'err': errs(rt, ut, Tt),
+                           'err_gate_without_network': errs(ra, ua, Ta),
+                           'err_vs_projected_fp64': errs_proj(rt, ut, Tt),
+                           'err_gate_without_network_vs_projected_fp64':
+                           errs_proj(ra, ua, Ta),
+                           'speedup': tp/ts,
                            'gate_fraction':
                            float((sur._last[0] != 0).float().mean())}
-    sur.threshold = threshold
+    sur.threshold = zero.threshold = threshold
 
     # 4. throughput of one collision sweep on the surrogate run's final state
     fin = s32.bank[idx]
@@ -195,12 +222,18 @@ def run_study(ini, device='cuda:0', runs=5, steps=100, nsteps=200,
         'points': npts, 'pairs': npairs, 'pairs_solver': npairs_solver,
         'train_loss_first': hist[0], 'train_loss_last': hist[-1],
         'harvest_s': t_harvest, 'train_s': t_train,
-        'epochs': epochs, 'runs': runs, 'steps_per_run': steps,
+        'epochs': epochs, 'runs': runs, 'near_runs': near_runs,
+        'steps_per_run': steps,
         'nsteps': nsteps, 'threshold': threshold,
         'err_surrogate': errs(rs, us, Ts),
         'err_surrogate_without_checks': errs(rn, un, Tn),
         'err_plain_fp32': errs(r32, u32, T32),
         'err_gate_without_network': errs(rz, uz, Tz),
+        'err_vs_projected_fp64': {
+            'surrogate_without_checks': errs_proj(rn, un, Tn),
+            'gate_without_network': errs_proj(rz, uz, Tz),
+            'plain_fp32': errs_proj(r32, u32, T32),
+            'plain_fp64_unprojected': errs_proj(r64, u64, T64)},
         'residual_checks': chk,
         'gate_fraction': gfrac, 'relaxation_only_fraction': gzero,
         'eps_quantiles': [float(q) for q in
