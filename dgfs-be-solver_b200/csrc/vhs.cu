@@ -215,6 +215,8 @@ struct dgfs_vhs {
   void* phase;   // cx<T> [P][M][3][N]
   void* w1;      // T [P][V]
   void* b2;      // T [V]
+  void* w1t;     // T [P][N][N*N] (w1 with the last axis outermost)
+  void* b2t;     // T [N][N*N]
   double* ginv;  // [25]
   double* cvec;  // [3][V]
   void* fc;      // scratch: gain spectrum, one N^3 complex slice per cluster
@@ -358,8 +360,19 @@ template <typename T> static int build_tables(dgfs_vhs* h, const dgfs_vhs_params
     }
     b2[v] = (T)bsum;
   }
+  // the same tables with the last axis outermost: a thread that owns line
+  // (k1, k2) reads element k3 at k3 N^2 + k1 N + k2, so a warp's 32 lines
+  // read 32 consecutive entries
+  std::vector<T> w1t((size_t)P * V), b2t(V);
+  for (int ip = 0; ip < P; ++ip)
+    for (int l = 0; l < N * N; ++l)
+      for (int k = 0; k < N; ++k) w1t[((size_t)ip * N + k) * N * N + l] = w1[(size_t)ip * V + (size_t)l * N + k];
+  for (int l = 0; l < N * N; ++l)
+    for (int k = 0; k < N; ++k) b2t[(size_t)k * N * N + l] = b2[(size_t)l * N + k];
   int rc;
-  if ((rc = upload(&h->phase, phase)) || (rc = upload(&h->w1, w1)) || (rc = upload(&h->b2, b2))) return rc;
+  if ((rc = upload(&h->phase, phase)) || (rc = upload(&h->w1, w1)) || (rc = upload(&h->b2, b2)) ||
+      (rc = upload(&h->w1t, w1t)) || (rc = upload(&h->b2t, b2t)))
+    return rc;
 
   if (h->project) {
     // velocity grid (frfs/solvers/dgfs/velocitymesh.py:73-85) and the Gram
@@ -386,6 +399,8 @@ static void free_handle(dgfs_vhs* h) {
   cudaFree(h->phase);
   cudaFree(h->w1);
   cudaFree(h->b2);
+  cudaFree(h->w1t);
+  cudaFree(h->b2t);
   cudaFree(h->ginv);
   cudaFree(h->cvec);
   cudaFree(h->fc);
@@ -571,6 +586,8 @@ static int vhs_launch(dgfs_vhs* h, const void* f, void* Q, int nupts, int neles,
     a.phase = (const double2*)h->phase;
     a.w1 = (const double*)h->w1;
     a.b2 = (const double*)h->b2;
+    a.w1t = (const double*)h->w1t;
+    a.b2t = (const double*)h->b2t;
     a.fc = (double2*)h->fc;
     a.err = h->err;
     a.plist = plist;
@@ -595,6 +612,8 @@ static int vhs_launch(dgfs_vhs* h, const void* f, void* Q, int nupts, int neles,
     a.phase = (const float2*)h->phase;
     a.w1 = (const float*)h->w1;
     a.b2 = (const float*)h->b2;
+    a.w1t = (const float*)h->w1t;
+    a.b2t = (const float*)h->b2t;
     a.fc = (float2*)h->fc;
     a.err = h->err;
     a.plist = plist;

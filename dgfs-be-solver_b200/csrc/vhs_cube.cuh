@@ -29,7 +29,10 @@
 // Layout (shared memory, complex float): F for k3 <= N/2 ([N][N][N/2+1]),
 // the work cube as N^2 lines of N+1 (padding keeps line-parallel accesses
 // free of bank conflicts), the three Nyquist planes, the axis phases.
-// The gain spectrum fC accumulates in a global (L2-resident) slice per CTA.
+// The gain spectrum fC accumulates in a global (L2-resident) slice per CTA,
+// stored with the last axis outermost so that the per-line accesses of a
+// warp are contiguous (w1 and b2 come in the same order, from their own
+// tables).
 // Main threads own two lines per pass; NQ extra threads (one line each)
 // transform the Nyquist planes during the first two passes of every (p, q).
 #pragma once
@@ -363,20 +366,30 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
       }
       __syncthreads();
       if (is_main) {
-        const float* w1 = a.w1 + (size_t)p * V;
+        const float* w1 = a.w1t + (size_t)p * V;
 #pragma unroll 1
         for (int r = 0; r < 2; ++r) {
-          const int L = tid + r * NM;  // line (k1, k2) along k3; v = L N + k3
+          const int L = tid + r * NM;  // line (k1, k2) along k3
+          // fC and w1 with the last axis outermost ([k3][L]): a warp's
+          // accesses are 32 consecutive entries.  All loads of the line are
+          // issued before its first store (fC and w1 could alias as far as
+          // the compiler knows, which would otherwise order each load after
+          // the previous store): one round trip per line, not one per entry.
           C x[N];
 #pragma unroll
           for (int k = 0; k < N; ++k) x[k] = sW[L * LP + k];
           fft<float, N, -1>(x);
-          C* dst = fcg + (size_t)L * N;
-          const float* w = w1 + (size_t)L * N;
 #pragma unroll
-          for (int k = 0; k < N; ++k) {
-            const C add = cscale(x[k], w[k]);
-            dst[k] = p == 0 ? add : cadd(dst[k], add);
+          for (int k = 0; k < N; ++k) x[k] = cscale(x[k], w1[k * NN + L]);
+          if (p > 0) {
+            C acc[N];
+#pragma unroll
+            for (int k = 0; k < N; ++k) acc[k] = fcg[k * NN + L];
+#pragma unroll
+            for (int k = 0; k < N; ++k) fcg[k * NN + L] = cadd(acc[k], x[k]);
+          } else {
+#pragma unroll
+            for (int k = 0; k < N; ++k) fcg[k * NN + L] = x[k];
           }
         }
       }
@@ -416,7 +429,7 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
         const int L = tid + r * NM, k1 = L / N, k2 = L % N;
         C x[N];
 #pragma unroll
-        for (int k = 0; k < N; ++k) x[k] = cscale(Fat(k1, k2, k), a.b2[L * N + k]);
+        for (int k = 0; k < N; ++k) x[k] = cscale(Fat(k1, k2, k), a.b2t[k * NN + L]);
         fft<float, N, +1>(x);
 #pragma unroll
         for (int k = 0; k < N; ++k) sW[L * LP + k] = x[k];
@@ -443,7 +456,7 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
         const int L = tid + r * NM;
         C x[N];
 #pragma unroll
-        for (int k = 0; k < N; ++k) x[k] = fcg[(size_t)L * N + k];
+        for (int k = 0; k < N; ++k) x[k] = fcg[k * NN + L];
         fft<float, N, +1>(x);
 #pragma unroll
         for (int k = 0; k < N; ++k) sW[L * LP + k] = x[k];
@@ -455,17 +468,24 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
 #pragma unroll 1
       for (int r = 0; r < 2; ++r) {
         const int L = tid + r * NM, x2 = L / N, x3 = L % N;
+        // bank entry of v = i N^2 + L is b0 + i st (v enters the AoSoA
+        // index linearly); f of this line is loaded first, every load
+        // issued before the first store of Q (which may alias f as far as
+        // the compiler knows)
+        const int64_t b0 = soa_ix(upt, a.ldim, elem, L, V, a.soasz), st = (int64_t)NN * a.soasz;
         C x[N];
 #pragma unroll
         for (int i = 0; i < N; ++i) x[i] = sW[(i * N + x2) * LP + x3];
         fft<float, N, +1>(x);
+        float fl[N];
+#pragma unroll
+        for (int i = 0; i < N; ++i) fl[i] = a.f[b0 + i * st];
 #pragma unroll
         for (int i = 0; i < N; ++i) {
           const int64_t v = (int64_t)(i * N + x2) * N + x3;
-          const float fv = a.f[soa_ix(upt, a.ldim, elem, v, V, a.soasz)];
-          const float qq = a.prefac * (x[i].x - fv * sLf[v]);
+          const float qq = a.prefac * (x[i].x - fl[i] * sLf[v]);
           if (!a.project) {
-            a.Q[soa_ix(upt, a.ldim, elem, v, V, a.soasz)] = qq;
+            a.Q[b0 + i * st] = qq;
             continue;
           }
           sW[(i * N + x2) * LP + x3].x = qq;  // this thread's own slot

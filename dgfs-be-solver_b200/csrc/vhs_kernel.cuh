@@ -55,6 +55,8 @@ template <typename T> struct VhsArgs {
   const cx<T>* phase;   // [P][M][3][N] exp(i fac_p s_q[axis] l0[k])
   const T* w1;          // [P][V]  (2 qw_p sw / V) b1_p(l)
   const T* b2;          // [V]
+  const T* w1t;         // [P][N][N*N] w1 with the last axis outermost: w1t[p][k3][k1 N + k2]
+  const T* b2t;         // [N][N*N]    b2 likewise (lane-contiguous for per-line access)
   cx<T>* fc;            // scratch [gridDim.x][N][NJ]: gain spectrum per CTA
   int* err;             // set to 1 when a bounded wait gives up
   const int* plist;     // optional device list of linear points (NULL: pt0 + i)
