@@ -50,8 +50,12 @@ template <int N> struct CubeGeom {
   static constexpr int NT = NM + NQ;
   static constexpr int V = N * N * N;
   static constexpr int PHS = 3 * N + 4;                 // one phase slot
-  static constexpr int OFF_F = 0;                       // [N][N][H]
-  static constexpr int OFF_W = OFF_F + NN * H;          // [NN][LP]
+  // F at (k1, k2, k3 <= N/2) sits at k1 FS + k2 H + k3: one padding entry
+  // per k1 slab makes lanes that differ in k1 (the Nyquist-plane lines)
+  // fall in different banks
+  static constexpr int FS = N * H + 1;
+  static constexpr int OFF_F = 0;                       // [N][FS]
+  static constexpr int OFF_W = OFF_F + N * FS;          // [NN][LP]
   static constexpr int OFF_T = OFF_W + NN * LP;         // [3][N][LP]
   static constexpr int OFF_PH = OFF_T + 3 * N * LP;     // [2][PHS]
   static constexpr int SMEM_CX = OFF_PH + 2 * PHS;
@@ -62,7 +66,7 @@ template <int N, bool IL1>
 __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsArgs<float> a) {
   using G = CubeGeom<N>;
   using C = cx<float>;
-  constexpr int H = G::H, NN = G::NN, LP = G::LP, NM = G::NM, V = G::V, PHS = G::PHS, NT = G::NT;
+  constexpr int H = G::H, NN = G::NN, LP = G::LP, NM = G::NM, V = G::V, PHS = G::PHS, NT = G::NT, FS = G::FS;
   constexpr int NY = N / 2;
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -103,8 +107,8 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
   };
   // F at (k1, k2, k3) from the half spectrum
   auto Fat = [&](int k1, int k2, int k3) -> C {
-    if (k3 <= NY) return sF[(k1 * N + k2) * H + k3];
-    const C c = sF[(((N - k1) % N) * N + (N - k2) % N) * H + (N - k3)];
+    if (k3 <= NY) return sF[k1 * FS + k2 * H + k3];
+    const C c = sF[((N - k1) % N) * FS + ((N - k2) % N) * H + (N - k3)];
     return mk<C>(c.x, -c.y);
   };
 
@@ -150,7 +154,7 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
         for (int i = 0; i < N; ++i) x[i] = sW[(i * N + k2) * LP + k3];
         fft<float, N, -1>(x);
 #pragma unroll
-        for (int i = 0; i < N; ++i) sF[(i * N + k2) * H + k3] = cscale(x[i], invV);
+        for (int i = 0; i < N; ++i) sF[i * FS + k2 * H + k3] = cscale(x[i], invV);
       }
     }
     phase_store(phase_fetch(0), 0);
@@ -231,39 +235,58 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
         } else {
           // n F on the Nyquist planes: plane 1 (k1 = N/2) lines over k3,
           // plane 2 (k2 = N/2, k1 != N/2) lines over k3, plane 3 (k3 = N/2,
-          // k1, k2 != N/2) lines over k2
+          // k1, k2 != N/2) lines over k2.  On a line only the phase of the
+          // running axis changes, so n = Re(D (1 - i)) / 2 with
+          // D = E (1 - t) becomes n = Re(A e[k]) with one coefficient A per
+          // line (A3 where k meets the Nyquist index of the running axis),
+          // as for the main lines.  Addresses and conjugation are selects,
+          // so lines of different planes share a warp without divergence.
 #pragma unroll 1
           for (int line = tq; line < 3 * N; line += G::NQ) {
-          const int which = line / N, j = line % N;
-          C x[N];
-#pragma unroll
-          for (int k = 0; k < N; ++k) {
-            int k1, k2, k3;
-            bool on;
+            const int which = line / N, j = line % N;
+            const bool p3 = which == 2;
+            C Eb, tb;
             if (which == 0) {
-              k1 = NY; k2 = j; k3 = k; on = true;
+              Eb = cmul(ph[NY], ph[N + j]);
+              tb = j == NY ? cmul(th1, th2) : th1;
             } else if (which == 1) {
-              k1 = j; k2 = NY; k3 = k; on = (j != NY);
+              Eb = cmul(ph[j], ph[N + NY]);
+              tb = th2;
             } else {
-              k1 = j; k2 = k; k3 = NY; on = (j != NY) && (k != NY);
+              Eb = cmul(ph[j], ph[2 * N + NY]);
+              tb = th3;
             }
-            C v = mk<C>(0.f, 0.f);
-            if (on) {
-              const C E = cmul(cmul(ph[k1], ph[N + k2]), ph[2 * N + k3]);
-              C t = mk<C>(1.f, 0.f);
-              if (k1 == NY) t = th1;
-              if (k2 == NY) t = cmul(t, th2);
-              if (k3 == NY) t = cmul(t, th3);
-              const C Et = cmul(E, t);
-              const float n = 0.5f * (E.x - Et.x + E.y - Et.y);
-              v = cscale(Fat(k1, k2, k3), n);
-            }
-            x[k] = v;
-          }
-          fft<float, N, +1>(x);
-          C* T = which == 0 ? sT1 : (which == 1 ? sT2 : sT3);
+            C B = cmul(Eb, mk<C>(1.f - tb.x, -tb.y));
+            const C tb3 = cmul(tb, th3);
+            C B3 = p3 ? mk<C>(0.f, 0.f) : cmul(Eb, mk<C>(1.f - tb3.x, -tb3.y));
+            if (which != 0 && j == NY) B = B3 = mk<C>(0.f, 0.f);
+            const C A = mk<C>(0.5f * (B.x + B.y), 0.5f * (B.y - B.x));
+            const C A3 = mk<C>(0.5f * (B3.x + B3.y), 0.5f * (B3.y - B3.x));
+            const C* ev = ph + (p3 ? N : 2 * N);
+            // element k at lo + k sl (k <= N/2, or every k on plane 3), else
+            // conj(sF[hi - k]) (the mirrored point)
+            const int jm = (N - j) % N;
+            const int lo = which == 0 ? NY * FS + j * H : (which == 1 ? j * FS + NY * H : j * FS + NY);
+            const int sl = p3 ? H : 1;
+            const int hi = (which == 0 ? NY * FS + jm * H : jm * FS + NY * H) + N;
+            C x[N];
 #pragma unroll
-          for (int k = 0; k < N; ++k) T[j * LP + k] = x[k];
+            for (int k = 0; k < N; ++k) {
+              C v;
+              if (k <= NY) {
+                v = sF[lo + k * sl];
+              } else {
+                const C c = sF[p3 ? lo + k * H : hi - k];
+                v = mk<C>(c.x, p3 ? c.y : -c.y);
+              }
+              const C& Ak = k == NY ? A3 : A;
+              const C e = ev[k];
+              x[k] = cscale(v, Ak.x * e.x - Ak.y * e.y);
+            }
+            fft<float, N, +1>(x);
+            C* T = which == 0 ? sT1 : (which == 1 ? sT2 : sT3);
+#pragma unroll
+            for (int k = 0; k < N; ++k) T[j * LP + k] = x[k];
           }
         }
         if (pq + 1 < npq) phase_store(phn, slot ^ 1);
@@ -422,7 +445,7 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
     // F is not needed after this transform's first pass, so its storage
     // takes the real Lf values (slot v of each thread's own lines).
     float* const sLf = reinterpret_cast<float*>(sF);
-    static_assert(2 * NN * H >= V, "Lf fits in the spectrum storage");
+    static_assert(2 * N * FS >= V, "Lf fits in the spectrum storage");
     if (is_main) {
 #pragma unroll 1
       for (int r = 0; r < 2; ++r) {
