@@ -11,7 +11,8 @@
 //   dgfs_mlp_mse     loss = mean over rows and the first n_used columns of
 //                    w_j (Y - T)^2, and dY
 //   dgfs_mlp_adam    Adam step on FP32 weights, refreshing the BF16 copy
-//   dgfs_mlp_affine  y = (x - mu) * inv_sigma per column (and the inverse)
+//   dgfs_mlp_affine  y = (x - mu) * inv_sigma per column (and the inverse);
+//                    dgfs_mlp_affine_rows gathers / scatters through a row list
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -21,57 +22,92 @@
 
 namespace {
 
-constexpr int BM = 64, BN = 64, BK = 16, NTH = 256;
+constexpr int NTH = 256;
 
 __device__ __forceinline__ float ld_b(const float* p) { return *p; }
 __device__ __forceinline__ float ld_b(const __nv_bfloat16* p) { return __bfloat162float(*p); }
 
-// C[m][n] (ldc) = act(sum_k A(m,k) B(k,n) + bias[n]) (+ C if accumulate)
-template <typename TB>
-__global__ void __launch_bounds__(NTH) gemm_kernel(int M, int N, int K, const float* __restrict__ A, long long sam,
-                                                  long long sak, const TB* __restrict__ B, long long sbk,
-                                                  long long sbn, const float* __restrict__ bias,
-                                                  float* __restrict__ Z, float* __restrict__ C, long long ldc,
-                                                  int act, int accumulate) {
+// C[m][n] (ldc) = act(sum_k A(m,k) B(k,n) + bias[n]) (+ C if accumulate);
+// BM x BN tile per CTA, TM x TN outputs per thread (256 threads), BK-deep
+// slices of K staged in shared memory (deeper slices for small tiles: fewer
+// round trips to L2 per output).  With mcount, only the first *mcount rows
+// exist (a count the device produced): tiles past it return at once.
+template <typename TB, int BM, int BN, int TM, int TN, int BK>
+__global__ void __launch_bounds__(NTH) gemm_kernel(int M, const int* __restrict__ mcount, int N, int K,
+                                                  const float* __restrict__ A, long long sam, long long sak,
+                                                  const TB* __restrict__ B, long long sbk, long long sbn,
+                                                  const float* __restrict__ bias, float* __restrict__ Z,
+                                                  float* __restrict__ C, long long ldc, int act, int accumulate) {
+  static_assert((BM / TM) * (BN / TN) == NTH, "one output block per thread");
   __shared__ float As[BK][BM + 4];
   __shared__ float Bs[BK][BN + 4];
-  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  constexpr int TX = BN / TN;
+  const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
   const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
-  float acc[4][4] = {};
-  for (int k0 = 0; k0 < K; k0 += BK) {
-    for (int t = threadIdx.x; t < BK * BM; t += NTH) {
+  if (mcount) M = min(M, *mcount);
+  if (m0 >= M) return;  // uniform over the CTA
+  float acc[TM][TN] = {};
+  // slices of K go through registers: every global load of a slice is
+  // issued before any of its shared-memory stores, and the next slice's
+  // loads before this slice's products (one round trip to L2 per slice,
+  // hidden behind the FMAs)
+  constexpr int LA = BK * BM / NTH, LB = BK * BN / NTH;
+  static_assert(LA * NTH == BK * BM && LB * NTH == BK * BN, "whole tiles per thread");
+  float ra[LA], rb[LB];
+  auto fetch = [&](int k0) {
+#pragma unroll
+    for (int u = 0; u < LA; ++u) {
       // consecutive threads walk k when A is row-major (sak == 1), m otherwise
+      const int t = threadIdx.x + u * NTH;
       const int kk = sak == 1 ? t % BK : t / BM, mm = sak == 1 ? t / BK : t % BM;
       const int m = m0 + mm, k = k0 + kk;
-      As[kk][mm] = (m < M && k < K) ? A[m * sam + k * sak] : 0.f;
+      ra[u] = (m < M && k < K) ? A[m * sam + k * sak] : 0.f;
     }
-    for (int t = threadIdx.x; t < BK * BN; t += NTH) {
+#pragma unroll
+    for (int u = 0; u < LB; ++u) {
+      const int t = threadIdx.x + u * NTH;
       const int kk = sbn == 1 ? t / BN : t % BK, nn = sbn == 1 ? t % BN : t / BK;
       const int n = n0 + nn, k = k0 + kk;
-      Bs[kk][nn] = (n < N && k < K) ? ld_b(B + k * sbk + n * sbn) : 0.f;
+      rb[u] = (n < N && k < K) ? ld_b(B + k * sbk + n * sbn) : 0.f;
+    }
+  };
+  fetch(0);
+  for (int k0 = 0; k0 < K; k0 += BK) {
+#pragma unroll
+    for (int u = 0; u < LA; ++u) {
+      const int t = threadIdx.x + u * NTH;
+      const int kk = sak == 1 ? t % BK : t / BM, mm = sak == 1 ? t / BK : t % BM;
+      As[kk][mm] = ra[u];
+    }
+#pragma unroll
+    for (int u = 0; u < LB; ++u) {
+      const int t = threadIdx.x + u * NTH;
+      const int kk = sbn == 1 ? t / BN : t % BK, nn = sbn == 1 ? t % BN : t / BK;
+      Bs[kk][nn] = rb[u];
     }
     __syncthreads();
+    if (k0 + BK < K) fetch(k0 + BK);
 #pragma unroll
     for (int kk = 0; kk < BK; ++kk) {
-      float a[4], b[4];
+      float a[TM], b[TN];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[kk][ty * 4 + i];
+      for (int i = 0; i < TM; ++i) a[i] = As[kk][ty * TM + i];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx * 4 + j];
+      for (int j = 0; j < TN; ++j) b[j] = Bs[kk][tx * TN + j];
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < TM; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+        for (int j = 0; j < TN; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
     }
     __syncthreads();
   }
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int m = m0 + ty * 4 + i;
+  for (int i = 0; i < TM; ++i) {
+    const int m = m0 + ty * TM + i;
     if (m >= M) continue;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int n = n0 + tx * 4 + j;
+    for (int j = 0; j < TN; ++j) {
+      const int n = n0 + tx * TN + j;
       if (n >= N) continue;
       float z = acc[i][j] + (bias ? bias[n] : 0.f);
       if (accumulate) z += C[m * ldc + n];
@@ -149,6 +185,19 @@ __global__ void affine_kernel(int M, int N, const float* __restrict__ X, const f
   }
 }
 
+// Row-list form: forward (inverse = 0) gathers Y[r] = (X[rows[r]] - mu) s,
+// inverse scatters Y[rows[r]] = X[r] / s + mu, for r < min(M, *count).
+__global__ void affine_rows_kernel(int M, int N, const int* __restrict__ rows, const int* __restrict__ count,
+                                   const float* __restrict__ X, const float* __restrict__ mu,
+                                   const float* __restrict__ s, float* __restrict__ Y, int inverse) {
+  const int m = min(M, *count);
+  for (int r = blockIdx.x; r < m; r += gridDim.x) {
+    const long long src = inverse ? r : rows[r], dst = inverse ? rows[r] : r;
+    for (int c = threadIdx.x; c < N; c += blockDim.x)
+      Y[dst * N + c] = inverse ? X[src * N + c] / s[c] + mu[c] : (X[src * N + c] - mu[c]) * s[c];
+  }
+}
+
 __global__ void f32_to_bf16_kernel(long long n, const float* __restrict__ x, __nv_bfloat16* __restrict__ y) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     y[i] = __float2bfloat16_rn(x[i]);
@@ -163,20 +212,41 @@ inline int launched(const char* what) {
 
 }  // namespace
 
+template <typename TB, int BM, int BN, int TM, int TN, int BK>
+static void gemm_launch(int M, const int* mcount, int N, int K, const float* A, long long sam, long long sak,
+                        const TB* B, long long sbk, long long sbn, const float* bias, float* Z, float* C,
+                        long long ldc, int act, int accumulate, cudaStream_t s) {
+  const dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
+  gemm_kernel<TB, BM, BN, TM, TN, BK><<<grid, NTH, 0, s>>>(M, mcount, N, K, A, sam, sak, B, sbk, sbn, bias, Z, C, ldc,
+                                                       act, accumulate);
+}
+
+template <typename TB>
+static void gemm_pick(int M, const int* mcount, int N, int K, const float* A, long long sam, long long sak,
+                      const TB* B, long long sbk, long long sbn, const float* bias, float* Z, float* C,
+                      long long ldc, int act, int accumulate, cudaStream_t s) {
+  // 64 x 64 tiles when they fill the GPU; 32 x 32 for short products and
+  // for row counts known only on the device (typically a few dozen rows)
+  const long long tiles64 = (long long)((M + 63) / 64) * ((N + 63) / 64);
+  if (!mcount && tiles64 >= 148)
+    gemm_launch<TB, 64, 64, 4, 4, 16>(M, mcount, N, K, A, sam, sak, B, sbk, sbn, bias, Z, C, ldc, act, accumulate, s);
+  else
+    gemm_launch<TB, 32, 32, 2, 2, 64>(M, mcount, N, K, A, sam, sak, B, sbk, sbn, bias, Z, C, ldc, act, accumulate, s);
+}
+
 extern "C" int dgfs_mlp_gemm(int M, int N, int K, const float* A, long long sam, long long sak, const void* B,
                              int b_bf16, long long sbk, long long sbn, const float* bias, float* Z, float* C,
-                             long long ldc, int act, int accumulate, void* stream) {
+                             long long ldc, int act, int accumulate, const int* mcount, void* stream) {
   dgfs::clear_error();
   if (M < 1 || N < 1 || K < 1 || !A || !B || !C) return dgfs::set_error(DGFS_ERR_INVALID, "bad GEMM arguments");
   if (act != 0 && act != 1) return dgfs::set_error(DGFS_ERR_INVALID, "act must be 0 or 1");
-  if ((M + BM - 1) / BM > 65535) return dgfs::set_error(DGFS_ERR_UNSUPPORTED, "M=%d too large", M);
-  const dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
+  if ((M + 31) / 32 > 65535) return dgfs::set_error(DGFS_ERR_UNSUPPORTED, "M=%d too large", M);
   if (b_bf16)
-    gemm_kernel<__nv_bfloat16><<<grid, NTH, 0, (cudaStream_t)stream>>>(
-        M, N, K, A, sam, sak, (const __nv_bfloat16*)B, sbk, sbn, bias, Z, C, ldc, act, accumulate);
+    gemm_pick<__nv_bfloat16>(M, mcount, N, K, A, sam, sak, (const __nv_bfloat16*)B, sbk, sbn, bias, Z, C, ldc,
+                             act, accumulate, (cudaStream_t)stream);
   else
-    gemm_kernel<float><<<grid, NTH, 0, (cudaStream_t)stream>>>(M, N, K, A, sam, sak, (const float*)B, sbk, sbn,
-                                                                bias, Z, C, ldc, act, accumulate);
+    gemm_pick<float>(M, mcount, N, K, A, sam, sak, (const float*)B, sbk, sbn, bias, Z, C, ldc, act, accumulate,
+                     (cudaStream_t)stream);
   return launched("gemm");
 }
 
@@ -220,6 +290,16 @@ extern "C" int dgfs_mlp_affine(int M, int N, const float* X, const float* mu, co
   if (M < 1 || N < 1 || !X || !mu || !inv_sigma || !Y) return dgfs::set_error(DGFS_ERR_INVALID, "bad arguments");
   affine_kernel<<<blocks_for((long long)M * N), 256, 0, (cudaStream_t)stream>>>(M, N, X, mu, inv_sigma, Y, inverse);
   return launched("affine");
+}
+
+extern "C" int dgfs_mlp_affine_rows(int M, int N, const int* rows, const int* count, const float* X,
+                                    const float* mu, const float* inv_sigma, float* Y, int inverse, void* stream) {
+  dgfs::clear_error();
+  if (M < 1 || N < 1 || !rows || !count || !X || !mu || !inv_sigma || !Y)
+    return dgfs::set_error(DGFS_ERR_INVALID, "bad arguments");
+  affine_rows_kernel<<<M < 1024 ? M : 1024, 256, 0, (cudaStream_t)stream>>>(M, N, rows, count, X, mu, inv_sigma, Y,
+                                                                           inverse);
+  return launched("affine_rows");
 }
 
 extern "C" int dgfs_f32_to_bf16(long long n, const float* x, void* y, void* stream) {

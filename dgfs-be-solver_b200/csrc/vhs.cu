@@ -221,6 +221,10 @@ struct dgfs_vhs {
   double* cvec;  // [3][V]
   void* fc;      // scratch: gain spectrum, one N^3 complex slice per cluster
   size_t fc_bytes;
+  void* fcp;     // single-CTA kernel: partial gain spectra of split points (4 slices per CTA)
+  size_t fcp_bytes;
+  int* pdone;    // ... and the chunk counters (2 per CTA, zero between launches)
+  int pdone_n;
   int* err;      // device flag: a bounded wait in the kernel gave up
 };
 
@@ -271,6 +275,30 @@ static int select_index(dgfs_vhs* h, int idx) {
     if (cudaMalloc(&h->fc, need) != cudaSuccess)
       return set_error(DGFS_ERR_NOMEM, "cudaMalloc(%zu) for the gain-spectrum scratch failed", need);
     h->fc_bytes = need;
+  }
+  if (v->push == 2) {
+    // a launch on few points splits them into radial-node chunks: up to 4
+    // items per CTA, each with its own partial-spectrum slice, and up to 2
+    // points per CTA with a chunk counter
+    const size_t needp = (size_t)4 * ncl * (size_t)h->N * h->N * h->N * esz;
+    if (needp > h->fcp_bytes) {
+      cudaFree(h->fcp);
+      h->fcp = nullptr;
+      h->fcp_bytes = 0;
+      if (cudaMalloc(&h->fcp, needp) != cudaSuccess)
+        return set_error(DGFS_ERR_NOMEM, "cudaMalloc(%zu) for the partial-spectrum scratch failed", needp);
+      h->fcp_bytes = needp;
+    }
+    if (2 * ncl > h->pdone_n) {
+      cudaFree(h->pdone);
+      h->pdone = nullptr;
+      h->pdone_n = 0;
+      if (cudaMalloc((void**)&h->pdone, (size_t)2 * ncl * sizeof(int)) != cudaSuccess)
+        return set_error(DGFS_ERR_NOMEM, "cudaMalloc for the chunk counters failed");
+      if (cudaMemset(h->pdone, 0, (size_t)2 * ncl * sizeof(int)) != cudaSuccess)
+        return set_error(DGFS_ERR_CUDA, "cudaMemset of the chunk counters failed");
+      h->pdone_n = 2 * ncl;
+    }
   }
   h->vidx = idx;
   h->var = v;
@@ -404,6 +432,8 @@ static void free_handle(dgfs_vhs* h) {
   cudaFree(h->ginv);
   cudaFree(h->cvec);
   cudaFree(h->fc);
+  cudaFree(h->fcp);
+  cudaFree(h->pdone);
   cudaFree(h->err);
   delete h;
 }
@@ -569,7 +599,9 @@ static int vhs_launch(dgfs_vhs* h, const void* f, void* Q, int nupts, int neles,
     return set_error(DGFS_ERR_INVALID, "handle built on device %d used on device %d", h->device, dev);
   if (npts == 0) return DGFS_OK;
 
-  const int ncl = npts < h->max_clusters ? npts : h->max_clusters;
+  // the single-CTA kernel may split a point over up to P CTAs
+  const long long want = h->var->push == 2 ? (long long)npts * h->P : npts;
+  const int ncl = want < h->max_clusters ? (int)want : h->max_clusters;
   cudaError_t e;
   if (h->prec == 64) {
     VhsArgs<double> a{};
@@ -615,6 +647,10 @@ static int vhs_launch(dgfs_vhs* h, const void* f, void* Q, int nupts, int neles,
     a.w1t = (const float*)h->w1t;
     a.b2t = (const float*)h->b2t;
     a.fc = (float2*)h->fc;
+    if (h->var->push == 2) {
+      a.fcp = (float2*)h->fcp;
+      a.pdone = h->pdone;
+    }
     a.err = h->err;
     a.plist = plist;
     a.pcount = pcount;

@@ -62,6 +62,23 @@ template <int N> struct CubeGeom {
   static_assert(NM % 32 == 0, "main threads must fill warps");
 };
 
+// Radial-node chunks per point.  A launch with few points would leave SMs
+// idle with one point per CTA, so each point's P radial nodes can be split
+// into P work items of one node each: cost ~ waves x (nodes per item x
+// (3 M + 3) + 3) passes (the 3: every item transforms f itself).  Only 1 or
+// P chunks: with one node per chunk the final sum over the chunks' slices
+// adds the nodes in the same order as the unsplit accumulation, so a point's
+// Q does not depend on the launch it is part of (bit for bit).  Items are
+// capped at 4 per CTA of the grid (the partial-spectrum scratch).  Every CTA
+// computes the same value.
+__device__ __forceinline__ int cube_chunks(int npts, int G, int P, int M) {
+  if (P < 2 || (long long)npts * P > 4LL * G) return 1;
+  const double per_node = 3.0 * M + 3.0;
+  const double whole = (double)((npts + G - 1) / G) * (P * per_node + 3.0);
+  const double split = (double)(((long long)npts * P + G - 1) / G) * (per_node + 3.0);
+  return split < whole ? P : 1;
+}
+
 template <int N, bool IL1>
 __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsArgs<float> a) {
   using G = CubeGeom<N>;
@@ -113,10 +130,29 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
   };
 
   const int npts = a.pcount ? min(a.npts, *a.pcount) : a.npts;
-  for (int ip = blockIdx.x; ip < npts; ip += gridDim.x) {
+  // work item = (point, chunk of radial nodes); with KP > 1 each chunk's
+  // partial gain spectrum goes to its own scratch slice and the CTA that
+  // finishes a point's last chunk (a counter per point) sums the slices and
+  // completes the point.  No CTA waits for another.
+  // The values that stay fixed over an item live in shared memory (s_kp;
+  // s_it = first and end radial node, upt, elem): read where needed, they
+  // hold no registers through the (p, q) loop.
+  __shared__ int s_last, s_kp, s_it[4];
+  const int nitems = npts * (a.pdone ? cube_chunks(npts, gridDim.x, a.P, a.M) : 1);
+  if (tid == 0) s_kp = a.pdone ? cube_chunks(npts, gridDim.x, a.P, a.M) : 1;
+  __syncthreads();
+  for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+    const int ip = item / s_kp;
     const int pt = a.plist ? a.plist[a.pt0 + ip] : a.pt0 + ip;
     if ((unsigned)pt >= (unsigned)(a.nupts * a.neles)) continue;  // uniform over the CTA
     const int upt = pt / a.neles, elem = pt % a.neles;
+    if (tid == 0) {
+      const int ch = item % s_kp;
+      s_it[0] = ch * a.P / s_kp;
+      s_it[1] = (ch + 1) * a.P / s_kp;
+      s_it[2] = upt;
+      s_it[3] = elem;
+    }
 
     // ---- F = FFT(f) / V, kept for k3 <= N/2 ---------------------------------
     if (is_main) {
@@ -157,13 +193,13 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
         for (int i = 0; i < N; ++i) sF[i * FS + k2 * H + k3] = cscale(x[i], invV);
       }
     }
-    phase_store(phase_fetch(0), 0);
+    phase_store(phase_fetch(s_it[0] * a.M), 0);
     __syncthreads();
 
     // ---- gain: fC = sum_p w1_p FFT(sum_q Re S_pq) ---------------------------
     int slot = 0;
 #pragma unroll 1
-    for (int p = 0; p < a.P; ++p) {
+    for (int p = s_it[0]; p < s_it[1]; ++p) {
       float S0[N], S1[N];
 #pragma unroll
       for (int k = 0; k < N; ++k) S0[k] = S1[k] = 0.f;
@@ -404,19 +440,30 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
           fft<float, N, -1>(x);
 #pragma unroll
           for (int k = 0; k < N; ++k) x[k] = cscale(x[k], w1[k * NN + L]);
-          if (p > 0) {
+          C* const fca = s_kp == 1 ? fcg : a.fcp + (size_t)item * V;
+          if (p > s_it[0]) {
             C acc[N];
 #pragma unroll
-            for (int k = 0; k < N; ++k) acc[k] = fcg[k * NN + L];
+            for (int k = 0; k < N; ++k) acc[k] = fca[k * NN + L];
 #pragma unroll
-            for (int k = 0; k < N; ++k) fcg[k * NN + L] = cadd(acc[k], x[k]);
+            for (int k = 0; k < N; ++k) fca[k * NN + L] = cadd(acc[k], x[k]);
           } else {
 #pragma unroll
-            for (int k = 0; k < N; ++k) fcg[k * NN + L] = x[k];
+            for (int k = 0; k < N; ++k) fca[k * NN + L] = x[k];
           }
         }
       }
       __syncthreads();
+    }
+
+    if (s_kp > 1) {
+      // publish this chunk's slice; the point's last chunk goes on
+      __threadfence();
+      __syncthreads();
+      if (tid == 0) s_last = atomicAdd(a.pdone + item / s_kp, 1) == s_kp - 1;
+      __syncthreads();
+      if (!s_last) continue;  // uniform over the CTA
+      __threadfence();
     }
 
     // ---- Q = prefac (Re IFFT(fC) - f IFFT(b2 F)) ----------------------------
@@ -478,8 +525,22 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
       for (int r = 0; r < 2; ++r) {
         const int L = tid + r * NM;
         C x[N];
+        if (s_kp == 1) {
 #pragma unroll
-        for (int k = 0; k < N; ++k) x[k] = fcg[k * NN + L];
+          for (int k = 0; k < N; ++k) x[k] = fcg[k * NN + L];
+        } else {
+          // the chunks' slices, summed in a fixed order (L2 reads: other
+          // CTAs wrote them)
+#pragma unroll
+          for (int k = 0; k < N; ++k) x[k] = mk<C>(0.f, 0.f);
+#pragma unroll 1
+          const int kp = s_kp, i0 = item - item % kp;
+          for (int c = 0; c < kp; ++c) {
+            const C* src = a.fcp + (size_t)(i0 + c) * V + L;
+#pragma unroll
+            for (int k = 0; k < N; ++k) x[k] = cadd(x[k], __ldcg(src + k * NN));
+          }
+        }
         fft<float, N, +1>(x);
 #pragma unroll
         for (int k = 0; k < N; ++k) sW[L * LP + k] = x[k];
@@ -495,7 +556,7 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
         // index linearly); f of this line is loaded first, every load
         // issued before the first store of Q (which may alias f as far as
         // the compiler knows)
-        const int64_t b0 = soa_ix(upt, a.ldim, elem, L, V, a.soasz), st = (int64_t)NN * a.soasz;
+        const int64_t b0 = soa_ix(s_it[2], a.ldim, s_it[3], L, V, a.soasz), st = (int64_t)NN * a.soasz;
         C x[N];
 #pragma unroll
         for (int i = 0; i < N; ++i) x[i] = sW[(i * N + x2) * LP + x3];
@@ -556,10 +617,11 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
           const float qq = (float)((double)sW[(i * N + x2) * LP + x3].x -
                                    (sLam[0] + sLam[1] * c0 + sLam[2] * c1 + sLam[3] * c2 +
                                     sLam[4] * (c0 * c0 + c1 * c1 + c2 * c2)));
-          a.Q[soa_ix(upt, a.ldim, elem, v, V, a.soasz)] = qq;
+          a.Q[soa_ix(s_it[2], a.ldim, s_it[3], v, V, a.soasz)] = qq;
         }
       }
     }
+    if (s_kp > 1 && tid == 0) a.pdone[item / s_kp] = 0;  // every chunk has counted: ready for the next launch
     __syncthreads();  // the work cube and fC are reused by the next point
   }
 }

@@ -57,14 +57,16 @@ _lib.declare('dgfs_hermite_embed', c_int,
 _lib.declare('dgfs_hermite_reconstruct', c_int,
              [c_int, c_void_p, c_void_p, c_void_p, c_int, c_int, c_ll, c_int,
               c_double, c_double, c_double, c_double, c_void_p, c_void_p,
-              c_void_p, c_void_p, c_void_p, c_void_p])
+              c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+              c_void_p])
 _lib.declare('dgfs_surrogate_gate', c_int,
              [c_int, c_void_p, c_float, c_float, c_void_p, c_double,
-              c_double, c_void_p, c_void_p, c_void_p, c_void_p])
+              c_double, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+              c_void_p])
 _lib.declare('dgfs_mlp_gemm', c_int,
              [c_int, c_int, c_int, c_void_p, c_ll, c_ll, c_void_p, c_int,
               c_ll, c_ll, c_void_p, c_void_p, c_void_p, c_ll, c_int, c_int,
-              c_void_p])
+              c_void_p, c_void_p])
 _lib.declare('dgfs_mlp_tanh_bwd', c_int, [c_ll, c_void_p, c_void_p,
                                           c_void_p, c_void_p])
 _lib.declare('dgfs_mlp_colsum', c_int, [c_int, c_int, c_void_p, c_ll,
@@ -77,6 +79,9 @@ _lib.declare('dgfs_mlp_adam', c_int, [c_ll, c_void_p, c_void_p, c_void_p,
                                       c_void_p])
 _lib.declare('dgfs_mlp_affine', c_int, [c_int, c_int, c_void_p, c_void_p,
                                         c_void_p, c_void_p, c_int, c_void_p])
+_lib.declare('dgfs_mlp_affine_rows', c_int,
+             [c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+              c_void_p, c_int, c_void_p])
 _lib.declare('dgfs_f32_to_bf16', c_int, [c_ll, c_void_p, c_void_p, c_void_p])
 _lib.declare('dgfs_surrogate_scale', c_int,
              [c_int, c_int, c_void_p, c_float, c_int, c_int, c_int, c_int,
@@ -200,13 +205,15 @@ class MLP:
                                             self._s), 'dgfs_f32_to_bf16')
 
     def _gemm(self, A, B, C, M, N, K, sam, sak, sbk, sbn, bf16, bias=None,
-              act=0, acc=0):
+              act=0, acc=0, mcount=None):
         _lib.check(_lib.load().dgfs_mlp_gemm(
             M, N, K, _p(A), sam, sak, _p(B), 1 if bf16 else 0, sbk, sbn,
-            _p(bias), None, _p(C), N, act, acc, self._s), 'dgfs_mlp_gemm')
+            _p(bias), None, _p(C), N, act, acc, _p(mcount), self._s),
+            'dgfs_mlp_gemm')
 
-    def forward(self, X, keep=False):
-        """Y = W4 tanh(W3 tanh(W2 tanh(W1 X + b1) + b2) + b3) + b4 + Ws X."""
+    def forward(self, X, keep=False, mcount=None):
+        """Y = W4 tanh(W3 tanh(W2 tanh(W1 X + b1) + b2) + b3) + b4 + Ws X.
+        With mcount (a device int), only the first *mcount rows."""
         B = X.shape[0]
         nin, wd, nout = self.nin, self.width, self.nout
         tag = 'train' if keep else 'infer'
@@ -215,16 +222,17 @@ class MLP:
         H3 = self.ws.get(tag + 'H3', (B, wd))
         Y = self.ws.get(tag + 'Y', (B, nout))
         wb, w = self.wb, self.w
+        mc = mcount
         self._gemm(X, wb['W1'], H1, B, wd, nin, nin, 1, wd, 1, True,
-                   w['b1'], act=1)
+                   w['b1'], act=1, mcount=mc)
         self._gemm(H1, wb['W2'], H2, B, wd, wd, wd, 1, wd, 1, True,
-                   w['b2'], act=1)
+                   w['b2'], act=1, mcount=mc)
         self._gemm(H2, wb['W3'], H3, B, wd, wd, wd, 1, wd, 1, True,
-                   w['b3'], act=1)
+                   w['b3'], act=1, mcount=mc)
         self._gemm(H3, wb['W4'], Y, B, nout, wd, wd, 1, nout, 1, True,
-                   w['b4'])
+                   w['b4'], mcount=mc)
         self._gemm(X, wb['Ws'], Y, B, nout, nin, nin, 1, nout, 1, True,
-                   acc=1)
+                   acc=1, mcount=mc)
         if keep:
             self._cache = (X, H1, H2, H3)
         return Y
@@ -315,11 +323,13 @@ class VHSSurrogate:
                                   dtype=torch.float64, device=self.device)
         self.loss_history = []
         self._last = None
-        # the plain fallback runs on a few points: the largest cluster
-        # launch shape spreads each of them over the most SMs (for 42 Couette
-        # points: 1.76 ms with 12 CTAs per point, 2.0 ms with 8, 3.0 ms on
-        # the single-CTA shape)
-        self._plain_h = sm.make_handle('push', largest_cluster=True) or sm._h
+        # the plain fallback runs on a few points: its own handle (it runs
+        # on a side stream) with the single-CTA kernel, which splits few
+        # points into one work item per radial node (42 Couette points:
+        # 0.4 ms), else the cluster shape that spreads a point over the most
+        # SMs
+        self._plain_h = (sm.make_handle('single-cta') or
+                         sm.make_handle('push', largest_cluster=True) or sm._h)
         self._side = None
 
     @property
@@ -459,13 +469,29 @@ class VHSSurrogate:
         self.loss_history += hist
         return hist
 
-    def predict(self, X):
+    def predict(self, X, rows=None, count=None):
+        """Predicted (scaled) targets for the rows of X; with a device row
+        list rows[0 .. *count), only those rows (gathered, evaluated,
+        scattered back; the other rows of the result are left as they
+        are)."""
         npts = X.shape[0]
-        Xn = self._affine(X, self.mu_x, self.is_x,
-                          out=self.ws.get('Xn', (npts, NFEAT)))
-        Yn = self.mlp.forward(Xn)
-        return self._affine(Yn, self.mu_y, self.is_y, inverse=True,
-                            out=self.ws.get('Bp', (npts, NFEAT)))
+        Bp = self.ws.get('Bp', (npts, NFEAT))
+        if rows is None:
+            Xn = self._affine(X, self.mu_x, self.is_x,
+                              out=self.ws.get('Xn', (npts, NFEAT)))
+            Yn = self.mlp.forward(Xn)
+            return self._affine(Yn, self.mu_y, self.is_y, inverse=True,
+                                out=Bp)
+        lib = _lib.load()
+        Xn = self.ws.get('Xn', (npts, NFEAT))
+        _lib.check(lib.dgfs_mlp_affine_rows(
+            npts, NFEAT, _p(rows), _p(count), _p(X), _p(self.mu_x),
+            _p(self.is_x), _p(Xn), 0, self._s), 'dgfs_mlp_affine_rows')
+        Yn = self.mlp.forward(Xn, mcount=count)
+        _lib.check(lib.dgfs_mlp_affine_rows(
+            npts, NFEAT, _p(rows), _p(count), _p(Yn), _p(self.mu_y),
+            _p(self.is_y), _p(Bp), 1, self._s), 'dgfs_mlp_affine_rows')
+        return Bp
 
     # -- use -----------------------------------------------------------------
     def collide(self, fbank, qbank, threshold=None):
@@ -485,10 +511,13 @@ class VHSSurrogate:
         gate = ws.get('gate', (npts,), torch.int32)
         plain = ws.get('plain', (npts,), torch.int32)
         nplain = ws.get('nplain', (1,), torch.int32)
+        net = ws.get('net', (npts,), torch.int32)
+        nnet = ws.get('nnet', (1,), torch.int32)
         _lib.check(lib.dgfs_surrogate_gate(npts, _p(eps), thr, EPS0,
                                            _p(mom), self.vm.L(), RMIN,
                                            _p(gate), _p(plain), _p(nplain),
-                                           self._s), 'dgfs_surrogate_gate')
+                                           _p(net), _p(nnet), self._s),
+                   'dgfs_surrogate_gate')
         # the plain fallback (few points, on cluster shapes that leave SMs
         # idle) runs on a side stream beside the network path; both write
         # disjoint points of qbank.  Event fork/join keeps it capturable.
@@ -505,20 +534,26 @@ class VHSSurrogate:
             self._side.cuda_stream), 'dgfs_vhs_apply_list')
         self._join.record(self._side)
         nu = self.loss_rate(fbank, self.nu_bank(fbank), gate)
-        Bp = self.scale_targets(self.predict(X), eps, inverse=True)
+        # the network runs on the gate-1 rows only
+        Bp = self.scale_targets(self.predict(X, net, nnet), eps,
+                                inverse=True)
+        work = ws.get('rwork', (nupts*(-(-neles//32))*32*(32*5 + NMODES),),
+                      torch.float64)
         _lib.check(lib.dgfs_hermite_reconstruct(
             self.backend.precision, _p(Bp), _p(mom), _p(gate), nupts, neles,
             ldim, self.vm.Nv(), self.vm.L(), self.vm.cw(),
             self.sm.prefactor, self.sm._gamma, _p(self.ginv),
             _p(self.gwinv), fbank._as_parameter_, nu._as_parameter_,
-            qbank._as_parameter_, self._s), 'dgfs_hermite_reconstruct')
+            qbank._as_parameter_, _p(net), _p(nnet), _p(work), self._s),
+            'dgfs_hermite_reconstruct')
         main.wait_event(self._join)
         self._last = (gate, eps)
         return gate
 
     # kernels one collide() launches: embed, 2 scale, gate (+ counter
-    # reset), loss rate, 2 affine, 5 GEMMs, reconstruct, plain list
-    launches_per_collide = 14
+    # resets), loss rate, 2 row-list affine, 5 GEMMs, reconstruct (+
+    # coefficients, 2 relaxation passes), plain list
+    launches_per_collide = 17
 
     def residual_check(self, fbank, qbank, scratch, sample=16, seed=0):
         """Plain Q at a random sample of the last call's surrogate points

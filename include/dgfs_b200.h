@@ -293,7 +293,14 @@ DGFS_API int dgfs_hermite_embed(int precision, const void* f, const void* Q,
  * d = B[pt]); Q = g, or Q = g - nu (f - M) when the banks f and nu are
  * given; then the FP64 projection onto zero mass, momentum and energy with
  * the 5x5 inverse Gram matrix ginv of (1, c, |c|^2) on the grid; written
- * only where gate[pt] != 0 (all points when gate is NULL). */
+ * only where gate[pt] != 0 (all points when gate is NULL).  Split mode,
+ * with gate, nu, the list rows[0 .. *nrows) of the gate-1 points (device
+ * memory, as dgfs_surrogate_gate's net list) and work (device memory of
+ * nupts * ceil(neles/32) * 32 * (32 * 5 + 220) doubles): the gate-1 points'
+ * coefficients are computed once and their velocity ranges split over 8
+ * CTAs each, the gate-2 points (B ignored, Q = -nu (f - M)) go to
+ * coalesced kernels that take the 32 points of an AoSoA block at a time,
+ * and the projection runs as one coalesced pass. */
 DGFS_API int dgfs_hermite_reconstruct(int precision, const float* B,
                                       const double* mom, const int* gate,
                                       int nupts, int neles, long long ldim,
@@ -301,18 +308,22 @@ DGFS_API int dgfs_hermite_reconstruct(int precision, const float* B,
                                       double prefactor, double gamma,
                                       const double* ginv, const double* gwinv,
                                       const void* f, const void* nu, void* Q,
-                                      void* stream);
+                                      const int* rows, const int* nrows,
+                                      double* work, void* stream);
 
 /* gate[pt] = 1 where eps[pt] < threshold (2 where also eps[pt] < eps_zero:
  * dgfs_hermite_reconstruct then uses zero coefficients, i.e. Q = -nu (f - M)
  * when nu is given) and, when the frames mom are given, the local
  * Maxwellian is resolved by the grid of half width L: min over axes of
  * (L - |u_axis|) >= rmin sqrt(T); gate 0 points are appended to
- * plain[0 .. *nplain) (unordered) for dgfs_vhs_apply_list. */
+ * plain[0 .. *nplain) (unordered) for dgfs_vhs_apply_list, and, when net
+ * and nnet are given, gate 1 points to net[0 .. *nnet) (the rows the
+ * network evaluates). */
 DGFS_API int dgfs_surrogate_gate(int npts, const float* eps, float threshold,
                                  float eps_zero, const double* mom, double L,
                                  double rmin, int* gate, int* plain,
-                                 int* nplain, void* stream);
+                                 int* nplain, int* net, int* nnet,
+                                 void* stream);
 
 /* Scale-free surrogate rows, in place on X[M][ld]: columns [c0, c1) are
  * divided (inverse != 0: multiplied) by s = max(eps[m], eps0); forward
@@ -325,12 +336,14 @@ DGFS_API int dgfs_surrogate_scale(int M, int ld, const float* eps, float eps0,
 
 /* Surrogate MLP kernels (FP32 accumulation; B operand FP32 or BF16):
  * C[m*ldc+n] = act(sum_k A[m*sam+k*sak] B[k*sbk+n*sbn] + bias[n]) (+ C),
- * act 0 identity, 1 tanh; Z (optional) receives the pre-activation. */
+ * act 0 identity, 1 tanh; Z (optional) receives the pre-activation.
+ * mcount (optional, device memory): only rows m < min(M, *mcount) are
+ * computed, for row counts the device produced (no host round trip). */
 DGFS_API int dgfs_mlp_gemm(int M, int N, int K, const float* A, long long sam,
                            long long sak, const void* B, int b_bf16,
                            long long sbk, long long sbn, const float* bias,
                            float* Z, float* C, long long ldc, int act,
-                           int accumulate, void* stream);
+                           int accumulate, const int* mcount, void* stream);
 /* dZ = dH (1 - H^2) */
 DGFS_API int dgfs_mlp_tanh_bwd(long long n, const float* H, const float* dH,
                                float* dZ, void* stream);
@@ -352,6 +365,13 @@ DGFS_API int dgfs_mlp_adam(long long n, float* w, void* wbf16, const float* g,
 DGFS_API int dgfs_mlp_affine(int M, int N, const float* X, const float* mu,
                              const float* inv_sigma, float* Y, int inverse,
                              void* stream);
+/* Through a device row list, for r < min(M, *count): Y[r] =
+ * (X[rows[r]] - mu) inv_sigma (gather), or with inverse Y[rows[r]] =
+ * X[r] / inv_sigma + mu (scatter); N columns, rows of N floats. */
+DGFS_API int dgfs_mlp_affine_rows(int M, int N, const int* rows,
+                                  const int* count, const float* X,
+                                  const float* mu, const float* inv_sigma,
+                                  float* Y, int inverse, void* stream);
 DGFS_API int dgfs_f32_to_bf16(long long n, const float* x, void* y,
                               void* stream);
 

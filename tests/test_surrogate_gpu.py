@@ -114,10 +114,15 @@ def test_loss_rate_matches_oracle(precision, name):
 
 
 @pytest.mark.parametrize('precision', ['double', 'single'])
-def test_reconstruct_matches_oracle_and_gate(precision):
+@pytest.mark.parametrize('coalesced', [False, True])
+def test_reconstruct_matches_oracle_and_gate(precision, coalesced):
+    """Per-point path for every gated point, or (coalesced) the split mode:
+    the gate-1 points from a device list (in any order; the count caps it),
+    the gate-2 points on the AoSoA kernels; 35 elements span two AoSoA
+    blocks."""
     be, vm, sm = _model(precision)
     cv = vm.cv()
-    nupts, neles = 2, 3
+    nupts, neles = 1, 35
     npts = nupts*neles
     rng = np.random.default_rng(8)
     deg = np.array([sum(t) for t in osur.modes()])
@@ -125,7 +130,8 @@ def test_reconstruct_matches_oracle_and_gate(precision):
     Bp[:, :NMODES] = rng.standard_normal((npts, NMODES))*0.5**deg
     mom = np.c_[rng.uniform(0.5, 2, npts), rng.uniform(-0.3, 0.3, (npts, 3)),
                 rng.uniform(0.7, 1.5, npts)]
-    gate = np.array([1, 0, 1, 1, 0, 1], np.int32)
+    gate = rng.choice([0, 1, 2, 2], npts).astype(np.int32)  # 2: loss term only
+    gate[:3] = (0, 1, 2)
     dev = be.device
     out = be.matrix((nupts, vm.vsize(), neles))
     sur = VHSSurrogate(sm)
@@ -137,12 +143,20 @@ def test_reconstruct_matches_oracle_and_gate(precision):
     fh = random_states(cv, npts, seed=12).reshape(nupts, neles, -1)
     nh = np.abs(random_states(cv, npts, seed=13)).reshape(nupts, neles, -1)
     fb, nb = _bank(be, fh), _bank(be, 20*nh)
+    work = torch.zeros(nupts*2*32*(32*5 + NMODES), dtype=torch.float64,
+                       device=dev)
+    net = np.nonzero(gate == 1)[0].astype(np.int32)
+    d_net = torch.tensor(np.r_[net[::-1], -7], dtype=torch.int32, device=dev)
+    d_nnet = torch.tensor([len(net)], dtype=torch.int32, device=dev)
     _lib.check(_lib.load().dgfs_hermite_reconstruct(
         be.precision, d_b.data_ptr(), d_mom.data_ptr(), d_gate.data_ptr(),
         nupts, neles, out.traits[1], vm.Nv(), vm.L(), vm.cw(), sm.prefactor,
         sm._gamma, sur.ginv.data_ptr(), d_gwinv.data_ptr(),
         fb._as_parameter_, nb._as_parameter_, out._as_parameter_,
-        be.stream), 'dgfs_hermite_reconstruct')
+        d_net.data_ptr() if coalesced else None,
+        d_nnet.data_ptr() if coalesced else None,
+        work.data_ptr() if coalesced else None, be.stream),
+        'dgfs_hermite_reconstruct')
     torch.cuda.synchronize()
     Q = out.get()
     fu, nuu = fb.get().astype(np.float64), nb.get().astype(np.float64)
@@ -152,7 +166,8 @@ def test_reconstruct_matches_oracle_and_gate(precision):
         if not gate[pt]:
             assert np.all(Q[u, :, e] == 0)
             continue
-        Qo = osur.reconstruct(Bp[pt].astype(np.float64),
+        b = Bp[pt].astype(np.float64)*(gate[pt] == 1)
+        Qo = osur.reconstruct(b,
                               (mom[pt, 0], mom[pt, 1:4], mom[pt, 4]), cv,
                               sm.prefactor, sm._gamma, Gw=Gw, f=fu[u, :, e],
                               nu=nuu[u, :, e])
@@ -167,6 +182,8 @@ def test_gate_builds_the_plain_list():
     gate = torch.empty(1000, dtype=torch.int32, device=dev)
     plain = torch.full((1000,), -1, dtype=torch.int32, device=dev)
     n = torch.empty(1, dtype=torch.int32, device=dev)
+    net = torch.full((1000,), -1, dtype=torch.int32, device=dev)
+    nn = torch.empty(1, dtype=torch.int32, device=dev)
     s = torch.cuda.current_stream().cuda_stream
     mom = np.c_[np.ones(1000), rng.uniform(-1, 1, (1000, 3)),
                 rng.uniform(0.5, 3, 1000)]
@@ -174,8 +191,8 @@ def test_gate_builds_the_plain_list():
     L, rmin = 5.5, 3.5
     _lib.check(_lib.load().dgfs_surrogate_gate(
         1000, e.data_ptr(), 0.05, 0.01, d_mom.data_ptr(), L, rmin,
-        gate.data_ptr(), plain.data_ptr(), n.data_ptr(), s),
-        'dgfs_surrogate_gate')
+        gate.data_ptr(), plain.data_ptr(), n.data_ptr(), net.data_ptr(),
+        nn.data_ptr(), s), 'dgfs_surrogate_gate')
     torch.cuda.synchronize()
     g = gate.cpu().numpy()
     res = (L - np.abs(mom[:, 1:4]).max(axis=1)) >= rmin*np.sqrt(mom[:, 4])
@@ -186,6 +203,37 @@ def test_gate_builds_the_plain_list():
     k = int(n.item())
     assert k == int(np.sum(g == 0))
     assert sorted(plain.cpu().numpy()[:k]) == list(np.nonzero(g == 0)[0])
+    k = int(nn.item())
+    assert k == int(np.sum(g == 1))
+    assert sorted(net.cpu().numpy()[:k]) == list(np.nonzero(g == 1)[0])
+
+
+def test_predict_on_a_row_list_matches_all_rows():
+    """The network evaluated on a device row list (gather, GEMMs capped
+    by a device count, scatter) gives the rows of the full evaluation bit
+    for bit and leaves the other rows alone."""
+    be, vm, sm = _model('single')
+    sur = VHSSurrogate(sm, seed=3)
+    dev = be.device
+    g = torch.Generator(device='cpu').manual_seed(0)
+    M = 300
+    X = torch.randn(M, NFEAT, generator=g).to(dev)
+    sur.mu_x = torch.randn(NFEAT, generator=g).to(dev)*0.1
+    sur.is_x = (1 + torch.rand(NFEAT, generator=g)).to(dev)
+    sur.mu_y = torch.randn(NFEAT, generator=g).to(dev)*0.1
+    sur.is_y = (1 + torch.rand(NFEAT, generator=g)).to(dev)
+    full = sur.predict(X).clone()
+    rows = torch.tensor([5, 17, 299, 0, 123, 64, 65, 250], dtype=torch.int32,
+                        device=dev)
+    count = torch.tensor([6], dtype=torch.int32, device=dev)
+    sur.ws.get('Bp', (M, NFEAT)).fill_(7.0)
+    part = sur.predict(X, rows, count)
+    torch.cuda.synchronize()
+    used = rows[:6].long()
+    assert torch.equal(part[used], full[used])
+    rest = torch.ones(M, dtype=torch.bool, device=dev)
+    rest[used] = False
+    assert torch.all(part[rest] == 7.0)
 
 
 @pytest.mark.parametrize('precision', ['double', 'single'])
