@@ -39,7 +39,7 @@ from frfs_b200.system import DGFSSystem
 class ZeroSurrogate(VHSSurrogate):
     """The gate without the network: gated points get Q = 0."""
 
-    def predict(self, X):
+    def predict(self, X, rows=None, count=None):
         Bp = self.ws.get('Bp0', (X.shape[0], X.shape[1]))
         Bp.zero_()
         return Bp
