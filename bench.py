@@ -402,7 +402,7 @@ def run_b200(args):
         pass
     traffic = None
     if args.workload == 'couette-n24' and prec == 32:
-        traffic = {'single-cta': 42.9e6, 'push': 35.5e6}.get(kind)
+        traffic = {'single-cta': 36.7e6, 'push': 35.5e6}.get(kind)
     roof = {'bound': 'fp32-simt' if prec == 32 else 'fp64-simt',
             'achieved': achieved, 'peak': tf.value, 'unit': 'TFLOP/s',
             'frac': achieved/tf.value,
