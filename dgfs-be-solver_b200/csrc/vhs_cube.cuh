@@ -137,11 +137,24 @@ __global__ void __launch_bounds__(CubeGeom<N>::NT, 1) vhs_cube_kernel(const VhsA
   // The values that stay fixed over an item live in shared memory (s_kp;
   // s_it = first and end radial node, upt, elem): read where needed, they
   // hold no registers through the (p, q) loop.
-  __shared__ int s_last, s_kp, s_it[4];
-  const int nitems = npts * (a.pdone ? cube_chunks(npts, gridDim.x, a.P, a.M) : 1);
-  if (tid == 0) s_kp = a.pdone ? cube_chunks(npts, gridDim.x, a.P, a.M) : 1;
+  __shared__ int s_last, s_kp, s_ni, s_ga, s_it[4];
+  {
+    const int kp = a.pdone ? cube_chunks(npts, gridDim.x, a.P, a.M) : 1;
+    const int nitems = npts * kp;
+    // as few CTAs as the number of waves needs (same makespan): the SMs
+    // left over stay free for kernels on other streams (the surrogate's
+    // network path runs beside its plain fallback)
+    const int waves = (nitems + gridDim.x - 1) / gridDim.x;
+    const int gactive = waves > 0 ? (nitems + waves - 1) / waves : 0;
+    if ((int)blockIdx.x >= gactive) return;  // uniform over the CTA, before any barrier
+    if (tid == 0) {
+      s_kp = kp;
+      s_ni = nitems;
+      s_ga = gactive;
+    }
+  }
   __syncthreads();
-  for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+  for (int item = blockIdx.x; item < s_ni; item += s_ga) {
     const int ip = item / s_kp;
     const int pt = a.plist ? a.plist[a.pt0 + ip] : a.pt0 + ip;
     if ((unsigned)pt >= (unsigned)(a.nupts * a.neles)) continue;  // uniform over the CTA
