@@ -15,7 +15,7 @@ struct dgfs_dg {
   long long ldim_u, ldim_f;
   double cw;
   std::vector<double> m0, m132, m3;  // host copies (operators travel as params)
-  void *smats, *rcpdjac, *nrm, *mag, *cvx, *cvy, *cvz, *guw, *gfw;
+  void *smats, *rcpdjac, *nrm, *mag, *cvx, *cvy, *cvz, *guw, *gfw, *bwall;
   int *part, *bkind, *bgroup, *bfpt, *bele, *grefl;
   int64_t* pbase;  // [F][E] partner offsets in the flux bank at v = 0
   double* bcvals;
@@ -67,6 +67,11 @@ template <typename T> int upload_geom(dgfs_dg* h, const dgfs_dg_params* p) {
   }
   if ((rc = upload_as<T>(&h->guw, uw.data(), uw.size()))) return rc;
   if ((rc = upload_as<T>(&h->gfw, fw.data(), fw.size()))) return rc;
+  // per-point wall states (cylinder walls); a neutral placeholder otherwise
+  const size_t nb = h->nb;
+  std::vector<double> bw(4 * (nb ? nb : 1), 1.0);
+  if (nb && p->bwall) std::memcpy(bw.data(), p->bwall, 4 * nb * sizeof(double));
+  if ((rc = upload_as<T>(&h->bwall, bw.data(), bw.size()))) return rc;
   return DGFS_OK;
 }
 
@@ -91,6 +96,7 @@ template <typename T> DgArgs<T> make_args(const dgfs_dg* h) {
   a.guw = (const T*)h->guw;
   a.gfw = (const T*)h->gfw;
   a.grefl = h->grefl;
+  a.bwall = (const T*)h->bwall;
   a.bcvals = h->bcvals;
   return a;
 }
@@ -176,7 +182,7 @@ int check_range(const dgfs_dg* h, int v0, int nv) {
 
 void free_dg(dgfs_dg* h) {
   if (!h) return;
-  void* ptrs[] = {h->smats, h->rcpdjac, h->nrm, h->mag, h->cvx, h->cvy, h->cvz, h->guw, h->gfw,
+  void* ptrs[] = {h->smats, h->rcpdjac, h->nrm, h->mag, h->cvx, h->cvy, h->cvz, h->guw, h->gfw, h->bwall,
                   h->part, h->pbase, h->bkind, h->bgroup, h->bfpt, h->bele, h->grefl, h->bcvals, h->bcpart,
                   h->uf};
   for (void* q : ptrs) cudaFree(q);
@@ -210,7 +216,9 @@ extern "C" int dgfs_dg_create(const dgfs_dg_params* p, dgfs_dg** out) {
       return set_error(DGFS_ERR_INVALID, "partner entry %d = %d out of range", i, q);
   }
   for (int b = 0; b < p->nbfpts; ++b) {
-    if (p->bkind[b] < 0 || p->bkind[b] > BC_WALL_SPECULAR) return set_error(DGFS_ERR_INVALID, "bad boundary kind");
+    if (p->bkind[b] < 0 || p->bkind[b] > BC_WALL_DIFFUSE_CYL) return set_error(DGFS_ERR_INVALID, "bad boundary kind");
+    if (p->bkind[b] == BC_WALL_DIFFUSE_CYL && (!p->bwall || !(p->bwall[4 * b + 3] > 0.0)))
+      return set_error(DGFS_ERR_INVALID, "cylinder wall point %d without a positive wall temperature", b);
     if (p->bgroup[b] < 0 || p->bgroup[b] >= p->ngroups) return set_error(DGFS_ERR_INVALID, "bad boundary group");
     if (p->bfpt[b] < 0 || p->bfpt[b] >= F || p->bele[b] < 0 || p->bele[b] >= E)
       return set_error(DGFS_ERR_INVALID, "bad boundary flux point");

@@ -22,7 +22,14 @@
 
 namespace dgfs {
 
-enum DgBcKind { BC_WALL_DIFFUSE = 0, BC_INLET = 1, BC_OUTLET = 2, BC_VANISH = 3, BC_WALL_SPECULAR = 4 };
+enum DgBcKind {
+  BC_WALL_DIFFUSE = 0,
+  BC_INLET = 1,
+  BC_OUTLET = 2,
+  BC_VANISH = 3,
+  BC_WALL_SPECULAR = 4,
+  BC_WALL_DIFFUSE_CYL = 5
+};
 
 template <typename T, int U, int F, int D> struct DgOps {
   T m0[F][U];
@@ -57,6 +64,7 @@ template <typename T> struct DgArgs {
   const T* guw;            // [ngroups][3]
   const T* gfw;            // [ngroups][V]
   const int* grefl;        // [ngroups][V]
+  const T* bwall;          // [nb][4] wall Ux, Uy, Uz, T per boundary point (cylinder wall)
   const double* bcvals;    // [nb][2]
 };
 
@@ -98,22 +106,31 @@ __global__ void __launch_bounds__(256) dg_bcsum_kernel(const DgArgs<T> a, const 
   const int vbeg = a.v0 + blockIdx.x * chunk;
   const int vend = min(a.v0 + a.nv, vbeg + chunk);
   double acc0 = 0.0, acc1 = 0.0;
-  if (b < nb && a.bkind[b] == BC_WALL_DIFFUSE) {
+  const int kind = b < nb ? a.bkind[b] : -1;
+  if (kind == BC_WALL_DIFFUSE || kind == BC_WALL_DIFFUSE_CYL) {
     const int j = bfpt[b], e = bele[b], g = a.bgroup[b];
-    double n[D], uw[D];
+    const bool cyl = kind == BC_WALL_DIFFUSE_CYL;
+    double n[D], uw[3], tw = 1.0;
 #pragma unroll
-    for (int d = 0; d < D; ++d) {
-      n[d] = (double)a.nrm[((int64_t)j * D + d) * a.neles + e];
-      uw[d] = (double)a.guw[g * 3 + d];
-    }
+    for (int d = 0; d < D; ++d) n[d] = (double)a.nrm[((int64_t)j * D + d) * a.neles + e];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) uw[d] = cyl ? (double)a.bwall[b * 4 + d] : (double)a.guw[g * 3 + d];
+    if (cyl) tw = (double)a.bwall[b * 4 + 3];
     for (int v = vbeg + vg; v < vend; v += 8) {
-      double fac = ((double)a.cvx[v] - uw[0]) * n[0];
-      if (D > 1) fac += ((double)a.cvy[v] - uw[1]) * n[1];
-      if (D > 2) fac += ((double)a.cvz[v] - uw[2]) * n[2];
-      if (fac >= 0.0)
+      const double dc[3] = {(double)a.cvx[v] - uw[0], (double)a.cvy[v] - uw[1], (double)a.cvz[v] - uw[2]};
+      const double dx = dc[0], dy = dc[1], dz = dc[2];
+      double fac = 0.0;
+#pragma unroll
+      for (int d = 0; d < D; ++d) fac += dc[d] * n[d];
+      if (fac >= 0.0) {
         acc0 += fac * (double)a.uf[aos32(j, a.ldim_f, e, v, a.V)] * cw;
-      else
-        acc1 += fac * (double)a.gfw[(int64_t)g * a.V + v] * cw;
+      } else {
+        // the cylinder wall's Maxwellian exp(-|c - U|^2 / T), unnormalised
+        // like the reference's (the ratio of the two sums normalises it;
+        // bcs/dgfs-wall-diffuse-cyl-update.mako)
+        const double fw = cyl ? exp(-(dx * dx + dy * dy + dz * dz) / tw) : (double)a.gfw[(int64_t)g * a.V + v];
+        acc1 += fac * fw * cw;
+      }
     }
   }
   s0[vg][bl] = acc0;
@@ -137,7 +154,7 @@ __global__ void __launch_bounds__(256) dg_bcsum_finish_kernel(const int* __restr
                                                              const double* __restrict__ partials,
                                                              double* __restrict__ bcvals, int reset) {
   const int b = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-  if (b >= nb || bkind[b] != BC_WALL_DIFFUSE) return;  // uniform per warp
+  if (b >= nb || (bkind[b] != BC_WALL_DIFFUSE && bkind[b] != BC_WALL_DIFFUSE_CYL)) return;  // uniform per warp
   double r0 = 0.0, r1 = 0.0;
   for (int c = lane; c < nchunks; c += 32) {
     r0 += partials[((int64_t)c * nb + b) * 2];
@@ -158,11 +175,13 @@ __global__ void __launch_bounds__(256) dg_bcsum_finish_kernel(const int* __restr
   }
 }
 
-// FP32: 4 CTAs per SM (<= 64 registers; measured 0.132 ms per Couette stage
-// against 0.145 ms at 2 CTAs per SM): the kernel is bound by the latency of
-// its partner loads, issued together up front from precomputed offsets
+// FP32 up to p = 2: 4 CTAs per SM (<= 64 registers; measured 0.132 ms per
+// Couette stage against 0.145 ms at 2 CTAs per SM): the kernel is bound by
+// the latency of its partner loads, issued together up front from
+// precomputed offsets.  p = 3 (16 solution and flux points) holds too many
+// values for 64 registers: no occupancy bound there.
 template <typename T, int U, int F, int D>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1) dg_residual_kernel(const DgArgs<T> a, const DgOps<T, U, F, D> op) {
+__global__ void __launch_bounds__(256, (sizeof(T) == 4 && U <= 9) ? 4 : 1) dg_residual_kernel(const DgArgs<T> a, const DgOps<T, U, F, D> op) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = (int)(t & 31);
   const int64_t w = t >> 5;
@@ -212,6 +231,19 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1) dg_residual_kerne
         if (fac < T(0)) {
           const T fw = a.gfw[(int64_t)g * a.V + v];
           ur = kind == BC_INLET ? fw : fw * (T)(-a.bcvals[2 * b] / a.bcvals[2 * b + 1]);
+        } else {
+          ur = ul;
+        }
+      } else if (kind == BC_WALL_DIFFUSE_CYL) {
+        // bcs/dgfs-wall-diffuse-cyl.mako: wall state of this boundary point
+        const T* w = a.bwall + (int64_t)b * 4;
+        const T dc[3] = {c[0] - w[0], c[1] - w[1], c[2] - w[2]};
+        T fac = dc[0] * n[0];
+#pragma unroll
+        for (int d = 1; d < D; ++d) fac = fma(dc[d], n[d], fac);
+        if (fac < T(0)) {
+          const T mx = exp(-(dc[0] * dc[0] + dc[1] * dc[1] + dc[2] * dc[2]) / w[3]);
+          ur = mx * (T)(-a.bcvals[2 * b] / a.bcvals[2 * b + 1]);
         } else {
           ur = ul;
         }

@@ -75,3 +75,45 @@ def initial_distribution(cfg, vm, nupts, neles, sect='soln-ics'):
              ((5*K - 3)/K + (1 - K)/(K*K)*cSqr))
         return np.broadcast_to(f[None, :, None], (nupts, V, neles)).copy()
     raise ValueError(f'unsupported initial condition type {kind!r}')
+
+
+_EXPR_FUNCS = {'exp': np.exp, 'log': np.log, 'sqrt': np.sqrt, 'sin': np.sin,
+               'cos': np.cos, 'tan': np.tan, 'tanh': np.tanh,
+               'atan2': np.arctan2, 'pow': np.power, 'fabs': np.abs,
+               'abs': np.abs, 'min': np.minimum, 'max': np.maximum}
+
+
+def eval_point_expr(cfg, sect, key, x, y, z=None):
+    """A boundary expression of frfs's config (``_exp_opts``,
+    frfs/solvers/dgfs/inters.py:155-171: the [constants], x, y, z for the
+    flux point's location, pi, abs) evaluated at the points (x, y[, z]).
+    The expression passes Inifile.getexpr's character whitelist (no
+    quotes, brackets or underscores), and is evaluated with no builtins."""
+    expr = cfg.getexpr(sect, key)
+    ns = dict(_EXPR_FUNCS)
+    if 'constants' in cfg.sections():
+        for k, v in cfg.items('constants').items():
+            try:
+                ns[k] = float(v)
+            except (TypeError, ValueError):
+                pass
+    x = np.asarray(x, dtype=np.float64)
+    ns.update(x=x, y=np.asarray(y, dtype=np.float64),
+              z=np.zeros_like(x) if z is None else np.asarray(z, np.float64),
+              pi=np.pi)
+    val = eval(expr, {'__builtins__': {}}, ns)
+    return np.broadcast_to(np.asarray(val, dtype=np.float64), x.shape).copy()
+
+
+def cylinder_wall_states(cfg, vm, sect, x, y):
+    """Nondimensional wall state (Ux, Uy, Uz, T) of a 'dgfs-wall-diffuse-cyl'
+    boundary at the flux points (x, y): the section's ux, uy, uz, T
+    expressions divided by u0 and T0 (inters.py:449-462); shape (n, 4)."""
+    out = np.empty((len(np.atleast_1d(x)), 4))
+    for i, k in enumerate(('ux', 'uy', 'uz')):
+        out[:, i] = eval_point_expr(cfg, sect, k, x, y)/vm.u0()
+    out[:, 3] = eval_point_expr(cfg, sect, 'T', x, y)/vm.T0()
+    if not np.all(out[:, 3] > 0):
+        raise ValueError(f'[{sect}] wall temperature must be positive')
+    return out
+

@@ -25,7 +25,8 @@ import numpy as np
 from frfs_b200 import _lib
 from frfs_b200 import mesh as meshmod
 from frfs_b200.elements import ElementGeometry
-from frfs_b200.initcond import MaxwellianSection, initial_distribution
+from frfs_b200.initcond import (MaxwellianSection, cylinder_wall_states,
+                                initial_distribution)
 from frfs_b200.scattering import DGFSScatteringModel, subclass_where
 from frfs_b200.shapes import QuadShape
 from frfs_b200.velocitymesh import DGFSVelocityMesh
@@ -45,7 +46,8 @@ class DgParams(ct.Structure):
                 ('partner', c_ip), ('cv', c_dp), ('cw', c_double),
                 ('nbfpts', c_int), ('bkind', c_ip), ('bgroup', c_ip),
                 ('bfpt', c_ip), ('bele', c_ip), ('ngroups', c_int),
-                ('guw', c_dp), ('gfw', c_dp), ('grefl', c_ip)]
+                ('guw', c_dp), ('gfw', c_dp), ('grefl', c_ip),
+                ('bwall', c_dp)]
 
 
 _lib.declare('dgfs_dg_create', c_int, [ct.POINTER(DgParams),
@@ -62,8 +64,13 @@ _lib.declare('dgfs_dg_bcvals', c_int, [c_void_p, c_dp, c_int])
 _lib.declare('dgfs_dg_fpts', c_int, [c_void_p, ct.POINTER(c_void_p),
                                      ct.POINTER(c_ll)])
 
+# frfs boundary types (frfs/solvers/dgfs/inters.py) -> kernel kinds; the
+# normal-shock inlet is the inlet with a zero velocity in its sign test
+# (bcs/dgfs-inlet-normalshock.mako), the cylinder wall a diffuse wall with a
+# wall state per boundary point
 BC_KINDS = {'dgfs-wall-diffuse': 0, 'dgfs-inlet': 1, 'dgfs-outlet': 2,
-            'dgfs-vanish': 3, 'dgfs-wall-specular': 4}
+            'dgfs-vanish': 3, 'dgfs-wall-specular': 4,
+            'dgfs-inlet-normalshock': 1, 'dgfs-wall-diffuse-cyl': 5}
 
 
 def _ptr(a, kind=c_dp):
@@ -153,6 +160,10 @@ class DGFSSystem:
                 ms = MaxwellianSection(cfg, vm, sect)
                 guw.append(ms.u)
                 gfw.append(ms.values)
+            elif btype == 'dgfs-inlet-normalshock':
+                ms = MaxwellianSection(cfg, vm, sect)
+                guw.append(np.zeros(3))
+                gfw.append(ms.values)
             else:
                 guw.append(np.zeros(3))
                 gfw.append(np.zeros(V))
@@ -180,6 +191,17 @@ class DGFSSystem:
         bele = np.array([e for _, _, e in bpts], dtype=np.int32)
         for b, (g, j, e) in enumerate(bpts):
             part[j, e] = -(b + 1)
+        # cylinder walls: the wall state at every boundary flux point
+        bwall = np.ones((max(len(bpts), 1), 4))
+        bwall[:, :3] = 0.0
+        for name, (g, btype) in self.bc_sections.items():
+            if btype != 'dgfs-wall-diffuse-cyl':
+                continue
+            idx = [b for b, (gb, _, _) in enumerate(bpts) if gb == g]
+            xy = np.array([geo.plocfpts[j, e] for _, j, e in
+                           (bpts[b] for b in idx)])
+            bwall[idx] = cylinder_wall_states(cfg, vm, f'soln-bcs-{name}',
+                                              xy[:, 0], xy[:, 1])
         if np.any(part == np.iinfo(np.int32).min):
             raise ValueError('mesh has flux points on no interface or '
                              'boundary')
@@ -197,7 +219,8 @@ class DGFSSystem:
             guw=d(np.array(guw).reshape(-1, 3)),
             gfw=d(np.array(gfw).reshape(-1, V)),
             grefl=np.ascontiguousarray(np.array(grefl).reshape(-1, V),
-                                       dtype=np.int32))
+                                       dtype=np.int32),
+            bwall=d(bwall))
         nrow, ldim, _ = self.bank[0].traits
         p = DgParams(
             precision=self.backend.precision, ndims=2, nupts=self.nupts,
@@ -210,7 +233,7 @@ class DGFSSystem:
             bgroup=_ptr(bgroup, c_ip), bfpt=_ptr(bfpt, c_ip),
             bele=_ptr(bele, c_ip), ngroups=len(bnames),
             guw=_ptr(keep['guw']), gfw=_ptr(keep['gfw']),
-            grefl=_ptr(keep['grefl'], c_ip))
+            grefl=_ptr(keep['grefl'], c_ip), bwall=_ptr(keep['bwall']))
         h = c_void_p()
         lib = _lib.load()
         _lib.check(lib.dgfs_dg_create(ct.byref(p), ct.byref(h)),

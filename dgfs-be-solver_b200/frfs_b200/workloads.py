@@ -20,6 +20,8 @@ couette-n24   64x1 quadrilateral strip, p=2, N=24, Nrho=12, M=16, omega=0.81,
               |cx| = |cy| = 5.27 on this strip (eigenvalues of the operator);
               1e-4 gives 0.034.  M=16 replaces the requested M=12: the tabulated
               symmetric designs hold 2M in {2,6,12,32,48,70,...} points only.
+cylinder-n32  quadrilateral O-grid around a cylinder, p=3, N=32, Nrho=16,
+              M=24, Mach-2 inflow, diffuse cylinder wall (cylinder_n32).
 channel-n32   48x24 quadrilaterals, p=2 (10368 points), N=32, Nrho=16, M=24,
               x-periodic, diffuse walls at y=+-1/4, Maxwellian times
               (1 + 0.01 xi) with xi ~ N(0,1) per velocity node and point;
@@ -204,8 +206,71 @@ uz = 0.0
     return ini
 
 
+def cylinder_n32(precision='single', ntheta=40, nr=16, order=3, Nv=32,
+                 Nrho=16, M=24, mach=2.0, dt=2e-4, tend=0.01):
+    """Cylinder in a Mach-2 crossflow on a
+    quadrilateral O-grid, p=3, N=32, Nrho=16, M=24 (M=32 has no tabulated
+    symmetric design; the 48-point rule of M=24 is the nearest).  Cylinder
+    of radius 0.5 with a diffuse isothermal wall (``dgfs-wall-diffuse-cyl``,
+    wall at rest, T_w = T_inf), far field at radius 4: Maxwellian inflow
+    on the upstream half, outflow on the downstream half; uniform freestream
+    initial state.  Speeds: the freestream speed is mach * sqrt(5/6) u0
+    (sound speed of a monatomic gas at T0 in units of u0 = sqrt(2 R T0)).
+
+    Full size is ntheta x nr ~ 20 000 elements (ntheta=160, nr=125: 320 000
+    points, 42 GB per FP32 bank); the default, 40 x 16 = 640 elements
+    (10 240 points), has the channel's point count.  dt = 2e-4 gives
+    |c| dt / h = 0.023 on the smallest default element (h = sqrt(area) =
+    0.072) at the corner speed of the velocity box (|c| = 8.2); the p=3
+    FR-DG operator with SSP-RK2 on O-grids is stable up to 0.055
+    (eigenvalues of the operator on 12x2 and 16x3 O-grids)."""
+    u0 = _u0()
+    uinf = float(mach*np.sqrt(5.0/6.0)*u0)
+    ini = _BASE.format(precision=precision, Nv=Nv, NvBatchSize=Nv**3,
+                       Nrho=Nrho, H0=1e-3, rho0=1.5e-3,
+                       molarMass0=_MOLAR_MASS, cmax=0.0, dev=6.0, M=M,
+                       omega=0.81, order=order, tend=tend, dt=dt)
+    ini += f"""
+[mesh]
+type = quad-ogrid
+ntheta = {ntheta}
+nr = {nr}
+r-in = 0.5
+r-out = 4.0
+stretch = 1.15
+
+[soln-ics]
+type = maxwellian
+rho = 1.5e-3
+T = 273.0
+ux = {uinf!r}
+uy = 0.0
+uz = 0.0
+
+[soln-bcs-cylinder]
+type = dgfs-wall-diffuse-cyl
+ux = 0.0
+uy = 0.0
+uz = 0.0
+T = 273.0
+
+[soln-bcs-inflow]
+type = dgfs-inlet
+rho = 1.5e-3
+T = 273.0
+ux = {uinf!r}
+uy = 0.0
+uz = 0.0
+
+[soln-bcs-outflow]
+type = dgfs-outlet
+"""
+    return ini
+
+
 WORKLOADS = {
     'relax0d-n16': relax0d_n16,
     'couette-n24': couette_n24,
     'channel-n32': channel_n32,
+    'cylinder-n32': cylinder_n32,
 }

@@ -188,6 +188,11 @@ typedef struct dgfs_dg dgfs_dg;
 #define DGFS_BC_OUTLET 2        /* dgfs-outlet        (inters.py:386-413)  */
 #define DGFS_BC_VANISH 3        /* dgfs-vanish        (inters.py:416-443)  */
 #define DGFS_BC_WALL_SPECULAR 4 /* dgfs-wall-specular (inters.py:232-309)  */
+#define DGFS_BC_WALL_DIFFUSE_CYL 5 /* dgfs-wall-diffuse-cyl (inters.py:446-492):
+                                      diffuse wall whose velocity and
+                                      temperature vary along it (bwall)     */
+/* dgfs-inlet-normalshock (inters.py:353-383) is DGFS_BC_INLET with a zero
+ * guw: the incoming half is selected by c.n alone. */
 
 typedef struct dgfs_dg_params {
   int precision;          /* 64 or 32                                       */
@@ -217,6 +222,9 @@ typedef struct dgfs_dg_params {
   const double* guw;      /* [ngroups][3] wall / inlet velocity             */
   const double* gfw;      /* [ngroups][nvars] wall / inlet Maxwellian       */
   const int* grefl;       /* [ngroups][nvars] specular reflection map, or NULL */
+  const double* bwall;    /* [nbfpts][4] (Ux, Uy, Uz, T) of the wall at each
+                             boundary flux point (nondimensional), read for
+                             DGFS_BC_WALL_DIFFUSE_CYL points; NULL if none  */
 } dgfs_dg_params;
 
 DGFS_API int dgfs_dg_create(const dgfs_dg_params* params, dgfs_dg** out);

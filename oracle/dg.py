@@ -16,7 +16,8 @@ restates the kernels that act on the distribution banks:
                                                 bccflux.mako:20-36, bcs/*.mako
   tdivtconf   R += M3 uf                        elements.py:85-88
   negdivconf  R = -R / |J|                      kernels/negdivconf.mako:11-13
-  update_bc   diffuse-wall flux sums            bcs/dgfs-wall-diffuse-update.mako:14-36
+  update_bc   diffuse-wall flux sums            bcs/dgfs-wall-diffuse-update.mako:14-36,
+                                                bcs/dgfs-wall-diffuse-cyl-update.mako
 
 Arrays: u (nupts, V, neles); uf (nfpts, V, neles).
 """
@@ -29,7 +30,10 @@ class DGOracle:
         """ops: dict M0, M132, M3; geo: dict smats (D,U,D,E), rcpdjac (U,E),
         nrm (F,E,D), mag (F,E), srtd [face][ele] -> fpt indices;
         con: (lhs, rhs) lists of (eidx, fidx); bcons: name -> [(eidx, fidx)];
-        cv (3, V); bcs: name -> dict(type=..., fw=(V,), uw=(3,))."""
+        cv (3, V); bcs: name -> dict(type=..., fw=(V,), uw=(3,)), and for
+        'dgfs-wall-diffuse-cyl' w = (npts, 4): the wall (Ux, Uy, Uz, T) at
+        each of the region's flux points in self.bpts order (may be set
+        after construction)."""
         self.M0, self.M132, self.M3 = ops['M0'], ops['M132'], ops['M3']
         self.smats, self.rcpdjac = geo['smats'], geo['rcpdjac']
         self.nrm, self.mag, self.srtd = geo['nrm'], geo['mag'], geo['srtd']
@@ -78,6 +82,16 @@ class DGOracle:
         if kind == 'dgfs-inlet':
             fac = sum((self.cv[i] - bc['uw'][i])*n[i] for i in range(D))
             return np.where(fac < 0, bc['fw'], ul)
+        if kind == 'dgfs-inlet-normalshock':
+            # bcs/dgfs-inlet-normalshock.mako: c.n selects the incoming half
+            fac = sum(self.cv[i]*n[i] for i in range(D))
+            return np.where(fac < 0, bc['fw'], ul)
+        if kind == 'dgfs-wall-diffuse-cyl':
+            # bcs/dgfs-wall-diffuse-cyl.mako: the wall state (Ux, Uy, Uz, T)
+            # of this boundary point, unnormalised Maxwellian
+            fac, mx = self._cyl_wall(bc['w'][k], n)
+            b0, b1 = self.bcvals[name][:, k]
+            return np.where(fac < 0, mx*(-b0/b1), ul)
         if kind == 'dgfs-outlet':
             return ul
         if kind == 'dgfs-vanish':
@@ -86,6 +100,13 @@ class DGOracle:
         if kind == 'dgfs-wall-specular':
             return ul[self.specular_map(name, j, e)]
         raise ValueError(kind)
+
+    def _cyl_wall(self, w, n):
+        """(c - U).n and exp(-|c - U|^2 / T) for a cylinder-wall point."""
+        D = self.ndims
+        dc = self.cv - np.asarray(w[:3]).reshape(3, 1)
+        fac = sum(dc[i]*n[i] for i in range(D))
+        return fac, np.exp(-np.sum(dc*dc, axis=0)/w[3])
 
     def specular_map(self, name, j, e):
         """Reflected-velocity index (frfs/solvers/dgfs/inters.py:244-275,
@@ -109,16 +130,21 @@ class DGOracle:
         D = self.ndims
         for name, pts in self.bpts.items():
             bc = self.bcs[name]
-            if bc['type'] != 'dgfs-wall-diffuse':
+            if bc['type'] not in ('dgfs-wall-diffuse', 'dgfs-wall-diffuse-cyl'):
                 continue
             for k, (j, e) in enumerate(pts):
                 n = self.nrm[j, e]
-                fac = sum((self.cv[i] - bc['uw'][i])*n[i] for i in range(D))
+                if bc['type'] == 'dgfs-wall-diffuse':
+                    fac = sum((self.cv[i] - bc['uw'][i])*n[i] for i in range(D))
+                    fw = bc['fw']
+                else:
+                    # bcs/dgfs-wall-diffuse-cyl-update.mako
+                    fac, fw = self._cyl_wall(bc['w'][k], n)
                 ul = uf[j, :, e]
                 self.bcvals[name][0, k] = np.sum(np.where(fac >= 0, fac*ul*self.cw,
                                                           0.0))
                 self.bcvals[name][1, k] = np.sum(np.where(fac < 0,
-                                                          fac*bc['fw']*self.cw,
+                                                          fac*fw*self.cw,
                                                           0.0))
 
     def comm_flux(self, uf):

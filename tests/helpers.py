@@ -101,9 +101,19 @@ def dg_setup(cfg, mesh):
             bcons[name] = [(int(r['eidx']), int(r['fidx'])) for r in mesh[k]]
             sect = f'soln-bcs-{name}'
             btype = cfg.get(sect, 'type')
-            if btype in ('dgfs-wall-diffuse', 'dgfs-inlet'):
+            if btype in ('dgfs-wall-diffuse', 'dgfs-inlet',
+                         'dgfs-inlet-normalshock'):
                 ms = MaxwellianSection(cfg, vm, sect)
                 bcs[name] = {'type': btype, 'fw': ms.values, 'uw': ms.u}
             else:
                 bcs[name] = {'type': btype, 'fw': None, 'uw': np.zeros(3)}
-    return DGOracle(ops, g, con, bcons, vm.cv(), vm.cw(), bcs), sh, geo, vm
+    dg = DGOracle(ops, g, con, bcons, vm.cv(), vm.cw(), bcs)
+    # cylinder walls: the config's wall expressions at the region's flux
+    # points (host-side input, evaluated by the product's expression reader)
+    from frfs_b200.initcond import cylinder_wall_states
+    for name, bc in bcs.items():
+        if bc['type'] == 'dgfs-wall-diffuse-cyl':
+            xy = np.array([geo.plocfpts[j, e] for j, e in dg.bpts[name]])
+            bc['w'] = cylinder_wall_states(cfg, vm, f'soln-bcs-{name}',
+                                           xy[:, 0], xy[:, 1])
+    return dg, sh, geo, vm
