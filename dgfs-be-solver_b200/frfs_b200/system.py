@@ -117,6 +117,10 @@ class DGFSSystem:
         shape = (self.nupts, V, self.neles)
         if initsoln is None:
             f0 = initial_distribution(cfg, vm, self.nupts, self.neles)
+        elif isinstance(initsoln, dict):
+            # a checkpoint (frfs's restart branch, system.py:79-112)
+            from frfs_b200.checkpoint import restart_bank
+            f0 = restart_bank(initsoln, cfg, V, self.mesh)
         else:
             f0 = np.asarray(initsoln).reshape(shape)
         mats = [backend.matrix(shape, f0 if i == 0 else None)

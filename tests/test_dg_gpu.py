@@ -197,3 +197,34 @@ def test_cylinder_steps_run():
     rho = s.moments(st._idxcurr)[..., 0]
     assert np.all(np.isfinite(rho))
     assert np.max(np.abs(rho - 1.0)) < 0.05, np.max(np.abs(rho - 1.0))
+
+
+def test_checkpoint_restart_continues_bit_for_bit(tmp_path):
+    """Write a checkpoint after two SSP-RK2 steps, run two more; a new
+    system restarted from the checkpoint reaches the same bank bit for
+    bit (frfs's restart path, __main__.py:228-242, system.py:79-112)."""
+    from frfs_b200 import checkpoint as ck
+    from frfs_b200.steppers import StdTVDRK2DGFSStepper
+    cfg, m = _cfg('single'), mgen.quad_box(2, 2, 0.0, 0.5, 0.0, 0.5,
+                                           periodic_x=True, jitter=0.1)
+    dg, sh, geo, vm = dg_setup(cfg, m)
+    u = _states(vm, sh.nupts, geo.neles, seed=6)
+    be, s = _system(cfg, m, u)
+    st = StdTVDRK2DGFSStepper(s, cfg)
+    st.dt = 1e-3
+    st.advance(2)
+    path = ck.write(str(tmp_path/'ck.npz'), s, st)
+    st.advance(2)
+    torch.cuda.synchronize()
+    want = s.bank[st._idxcurr].get()
+
+    rec = ck.read(path)
+    s2 = DGFSSystem(B200Backend(cfg, device='cuda:0'), cfg, mesh=m,
+                    initsoln=rec)
+    st2 = StdTVDRK2DGFSStepper(s2, cfg)
+    st2.dt = 1e-3
+    st2.tcurr, st2.nacptsteps = ck.restart_time(rec)
+    assert st2.nacptsteps == 2
+    st2.advance(2)
+    torch.cuda.synchronize()
+    assert np.array_equal(s2.bank[st2._idxcurr].get(), want)
