@@ -79,6 +79,8 @@ def restart_bank(initsoln, cfg, V, mesh=None):
     curr = QuadShape(cfg.getint('solver', 'order'))
     if soln.shape[0] != solnb.nupts or soln.shape[1] != V:
         raise RuntimeError('stored solution does not match its config')
+    if solnb.nupts == curr.nupts and np.allclose(solnb.upts, curr.upts):
+        return soln  # same basis: the stored values, exactly
     interp = solnb.ubasis.nodal_basis_at(curr.upts)
     out = interp @ soln.reshape(solnb.nupts, -1)
     return out.reshape(curr.nupts, V, soln.shape[2])
