@@ -96,10 +96,13 @@ def _workload_desc(args, cfg, npts):
 
 
 def _points_shape(cfg):
-    """(nupts, neles) of the workload's mesh (quad p=2: 9 points)."""
+    """(nupts, neles) of the workload's mesh ((p+1)^2 points per quad)."""
     order = cfg.getint('solver', 'order')
     if cfg.hasopt('mesh', 'nx'):
         neles = cfg.getint('mesh', 'nx')*cfg.getint('mesh', 'ny')
+        return (order + 1)**2, neles
+    if cfg.hasopt('mesh', 'ntheta'):
+        neles = cfg.getint('mesh', 'ntheta')*cfg.getint('mesh', 'nr')
         return (order + 1)**2, neles
     return 1, 1
 
