@@ -315,7 +315,9 @@ def run_b200(args):
         stepper = StdTVDRK2DGFSStepper(system, cfg)
         fin, fout = system.bank[0], system.bank[1]
         evals_per_step = 2*npts
-        launches_per_step = 8   # per stage: VHS, interp, wall sums, residual
+        # per stage: VHS, interp, residual, and the two boundary-sum
+        # kernels when the mesh has boundary flux points
+        launches_per_step = 2*(3 + (2 if len(system.bpts) else 0))
 
         def step():
             stepper.advance(1)
