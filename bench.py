@@ -62,7 +62,7 @@ def _parse():
     ap.add_argument('--graphs', type=int, default=1,
                     help='CUDA graph per SSP-RK2 stage (--mode step)')
     ap.add_argument('--surrogate', type=int, default=-1,
-                    help='train and judge the learned surrogate in this run '
+                    help='train and evaluate the learned surrogate in this run '
                          '(-1: on for couette-n24 at N=1)')
     ap.add_argument('--surrogate-steps', type=int, default=200)
     return ap.parse_args()
@@ -457,7 +457,7 @@ def run_b200(args):
         args.mode == 'step')
     if want_sur and world == 1:
         # learned surrogate: harvested from the solver, trained with the
-        # project's kernels, judged against the plain FP64 solution
+        # project's kernels, measured against the plain FP64 solution
         from frfs_b200 import workloads
         from frfs_b200.surrogate_study import run_study
         sur = run_study(workloads.WORKLOADS[args.workload],

@@ -1,6 +1,6 @@
 # -*- coding: utf-8 -*-
 """Learned collision surrogate with the plain fast-spectral operator as
-fallback and judge (no counterpart in the reference).
+fallback and error reference (no counterpart in the reference).
 
 Per solution point:
 

@@ -1,6 +1,6 @@
 # -*- coding: utf-8 -*-
-"""Train the collision surrogate on the solver's own trajectories and judge
-it with the plain operator (no counterpart in the reference).
+"""Train the collision surrogate on the solver's own trajectories and measure
+its error with the plain operator (no counterpart in the reference).
 
 ``run_study`` does, on one GPU:
 
