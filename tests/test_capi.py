@@ -41,3 +41,28 @@ def test_error_path_without_gpu_work():
     assert b'null' in lib.dgfs_last_error()
     assert lib.dgfs_vhs_apply(None, None, None, 1, 1, 1, 32, -1, 0,
                               None) == 1
+
+
+def test_surrogate_entry_points_validate_arguments_before_any_cuda_call():
+    """Host-side argument checks of the surrogate's entry points (no GPU
+    needed): each bad call returns an error code and a message."""
+    import frfs_b200.surrogate  # noqa: F401  (declares the signatures)
+    lib = _lib.load()
+    p = ct.c_void_p(8)
+    # reconstruct: null coefficient / moment / output arrays
+    assert lib.dgfs_hermite_reconstruct(32, None, p, None, 1, 1, 32*4096, 16,
+                                        5.0, 1.0, 1.0, 1.0, p, None, None,
+                                        None, p, None, None, None, None) != 0
+    # gate: a network list without its counter
+    assert lib.dgfs_surrogate_gate(4, p, 0.05, 1e-3, None, 5.0, 3.5, p, p,
+                                   p, p, None, None) != 0
+    assert b'bad arguments' in lib.dgfs_last_error()
+    # row-list affine without a count
+    assert lib.dgfs_mlp_affine_rows(4, 8, p, None, p, p, p, p, 0, None) != 0
+    # GEMM with an unknown activation
+    assert lib.dgfs_mlp_gemm(4, 4, 4, p, 4, 1, p, 0, 4, 1, None, None, p, 4,
+                             2, 0, None, None) != 0
+    assert b'act' in lib.dgfs_last_error()
+    # scale with the log column inside the scaled range
+    assert lib.dgfs_surrogate_scale(4, 256, p, 1e-3, 4, 220, 100, 0, p,
+                                    None) != 0
