@@ -127,22 +127,33 @@ class ClockSampler:
               'clocks_event_reasons.sw_thermal_slowdown,'
               'clocks_event_reasons.sw_power_cap')
 
-    def __init__(self, gpu_index):
+    def __init__(self, gpu_index, period_ms=50):
         self.idx = gpu_index
+        self.period_ms = period_ms
         self.proc = None
         self.lines = []
+        self._first = 0
 
-    def start(self):
+    def start(self, wait_s=5.0):
+        """Start sampling and wait (bounded) for the first sample, so that
+        the region timed after this call is covered; samples taken before
+        it are not counted."""
         try:
             self.proc = subprocess.Popen(
                 ['nvidia-smi', '-i', str(self.idx),
                  f'--query-gpu={self.FIELDS}', '--format=csv,noheader,nounits',
-                 '-lms', '200'], stdout=subprocess.PIPE,
+                 '-lms', str(self.period_ms)], stdout=subprocess.PIPE,
                 stderr=subprocess.DEVNULL, text=True)
             self._t = threading.Thread(target=self._read, daemon=True)
             self._t.start()
         except (OSError, ValueError):
             self.proc = None
+            return
+        t0 = time.time()
+        while (not self.lines and self.proc.poll() is None
+               and time.time() - t0 < wait_s):
+            time.sleep(0.005)
+        self._first = len(self.lines)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -151,12 +162,22 @@ class ClockSampler:
     def stop(self):
         if self.proc is None:
             return None
+        # samples of the timed region; if the region was shorter than one
+        # period, the first sample after it
+        n_end = len(self.lines)
+        if n_end == self._first:
+            t0 = time.time()
+            while (len(self.lines) == n_end and self.proc.poll() is None
+                   and time.time() - t0 < 1.0):
+                time.sleep(0.005)
+            n_end = min(len(self.lines), n_end + 1)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
         self._t.join(timeout=2)
+        self.lines = self.lines[self._first:n_end]
         sm, smax, reasons = [], 0.0, set()
         names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown',
                  'sw_power_cap']
