@@ -127,7 +127,7 @@ class ClockSampler:
               'clocks_event_reasons.sw_thermal_slowdown,'
               'clocks_event_reasons.sw_power_cap')
 
-    def __init__(self, gpu_index, period_ms=50):
+    def __init__(self, gpu_index, period_ms=200):
         self.idx = gpu_index
         self.period_ms = period_ms
         self.proc = None
