@@ -35,13 +35,20 @@ import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
-sys.path.insert(0, os.path.join(ROOT, 'dgfs-be-solver_b200'))
+PKG = os.path.join(ROOT, 'dgfs-be-solver_b200')
+sys.path.insert(0, PKG)
 sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
-SPHDESIGN = os.path.join(ROOT, 'tests', 'golden', 'sphericaldesign')
+SPHDESIGN = os.path.join(PKG, 'frfs_b200', 'data', 'sphericaldesign')
 METRIC = 'Q(f) evals/s'
+
+# DRAM bytes (read + write) per launch measured by ncu, keyed by (kernel,
+# workload, points, precision bits); only exact matches are reported
+TRAFFIC = {
+    ('vhs_cube_kernel', 'couette-n24', 576, 32): 36.7e6,
+}
 
 
 def _parse():
@@ -65,14 +72,23 @@ def _parse():
                     help='train and evaluate the learned surrogate in this run '
                          '(-1: on for couette-n24 at N=1)')
     ap.add_argument('--surrogate-steps', type=int, default=200)
+    ap.add_argument('--elements', type=int, nargs=2, default=None,
+                    metavar=('NX', 'NY'),
+                    help='mesh size override (quad box: nx ny; O-grid: '
+                         'ntheta nr), for small profiling cases')
     return ap.parse_args()
 
 
 def _cfg(args):
     from frfs_b200 import workloads
     from frfs_b200.inifile import Inifile
+    kw = {}
+    if args.elements:
+        a, b = args.elements
+        kw = ({'ntheta': a, 'nr': b} if args.workload.startswith('cylinder')
+              else {'nx': a, 'ny': b})
     cfg = Inifile(workloads.WORKLOADS[args.workload](
-        precision=args.precision))
+        precision=args.precision, **kw))
     cfg.set('spherical-design-rule', 'path', SPHDESIGN)
     cfg.set('backend-b200', 'vhs-project', int(args.project))
     return cfg
@@ -418,17 +434,18 @@ def run_b200(args):
         stream.cuda_stream), 'dgfs_probe_fma_peak')
     flops_pt = sm.flops_per_point()
     achieved = flops_pt*npts/(vhs_ms*1e-3)/1e12
-    # DRAM bytes of one sweep from the committed ncu capture of the same
-    # launch: f in + Q out, the tables and the per-CTA gain spectrum stay in
-    # L2 (profiles/vhs_cube_couette_n24_f32.md, vhs_push_couette_n24_f32.md)
+    # DRAM traffic of the launch is not measured by this run (it needs an
+    # ncu capture); it is reported only from a capture of this exact kernel,
+    # workload, size and precision (TRAFFIC), else null
     kind = None
     try:
         kind = sm.variants()[tune_idx]['exchange']
     except Exception:
         pass
-    traffic = None
-    if args.workload == 'couette-n24' and prec == 32:
-        traffic = {'single-cta': 36.7e6, 'push': 35.5e6}.get(kind)
+    kname = {'single-cta': 'vhs_cube_kernel', 'push': 'vhs_push_kernel',
+             'pull': 'vhs_cluster_kernel'}.get(kind, kind)
+    tkey = (kname, args.workload, npts, prec)
+    traffic = TRAFFIC.get(tkey)
     roof = {'bound': 'fp32-simt' if prec == 32 else 'fp64-simt',
             'achieved': achieved, 'peak': tf.value, 'unit': 'TFLOP/s',
             'frac': achieved/tf.value,
@@ -436,12 +453,11 @@ def run_b200(args):
                            '(dgfs_probe_fma_peak)',
             'flops_per_point': flops_pt, 'launch_ms': vhs_ms,
             'traffic': traffic,
-            'traffic_source': 'ncu dram__bytes_read.sum + write.sum of the '
-                              'same launch shape, profiles/' if traffic
-            else None,
-            'kernel': {'single-cta': 'vhs_cube_kernel',
-                       'push': 'vhs_push_kernel',
-                       'pull': 'vhs_cluster_kernel'}.get(kind, kind)}
+            'traffic_source': ('ncu dram__bytes_read.sum + '
+                               'dram__bytes_write.sum of this kernel, '
+                               'workload, size and precision') if traffic
+            else 'not captured for this kernel/workload/size/precision',
+            'kernel': kname}
     extra = {}
     if args.mode == 'step':
         extra['dg_step_ms'] = ms_per_step

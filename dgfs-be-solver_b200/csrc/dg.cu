@@ -14,7 +14,7 @@ struct dgfs_dg {
   int prec, D, U, F, V, E, nb, ngroups, device;
   long long ldim_u, ldim_f;
   double cw;
-  std::vector<double> m0, m132, m3;  // host copies (operators travel as params)
+  std::vector<double> m0, m132, m3, m12;  // host copies (operators travel as params)
   void *smats, *rcpdjac, *nrm, *mag, *cvx, *cvy, *cvz, *guw, *gfw, *bwall;
   int *part, *bkind, *bgroup, *bfpt, *bele, *grefl;
   int64_t* pbase;  // [F][E] partner offsets in the flux bank at v = 0
@@ -112,6 +112,13 @@ template <typename T, int U, int F, int D> DgOps<T, U, F, D> make_ops(const dgfs
   return o;
 }
 
+template <typename T, int U> DgMassOps<T, U> make_mass_ops(const dgfs_dg* h) {
+  DgMassOps<T, U> o;
+  for (int r = 0; r < U; ++r)
+    for (int i = 0; i < U; ++i) o.m12[r][i] = (T)h->m12[r * U + i];
+  return o;
+}
+
 inline unsigned grid_for(const dgfs_dg* h, int nv) {
   const long long nblk = (h->E + 31) / 32;
   return (unsigned)((nblk * nv * 32 + 255) / 256);
@@ -142,6 +149,17 @@ cudaError_t run_rhs(const dgfs_dg* h, const void* u, void* out, int v0, int nv, 
   a.v0 = v0;
   a.nv = nv;
   dg_residual_kernel<T, U, F, D><<<grid_for(h, nv), 256, 0, s>>>(a, make_ops<T, U, F, D>(h));
+  return cudaGetLastError();
+}
+
+template <typename T, int U, int F, int D>
+cudaError_t run_invmass(const dgfs_dg* h, const void* u, void* out, int v0, int nv, cudaStream_t s) {
+  DgArgs<T> a = make_args<T>(h);
+  a.u = (const T*)u;
+  a.out = (T*)out;
+  a.v0 = v0;
+  a.nv = nv;
+  dg_invmass_kernel<T, U><<<grid_for(h, nv), 256, 0, s>>>(a, make_mass_ops<T, U>(h));
   return cudaGetLastError();
 }
 
@@ -243,6 +261,7 @@ extern "C" int dgfs_dg_create(const dgfs_dg_params* p, dgfs_dg** out) {
   h->m0.assign(p->m0, p->m0 + F * U);
   h->m132.assign(p->m132, p->m132 + U * D * U);
   h->m3.assign(p->m3, p->m3 + U * F);
+  if (p->m12) h->m12.assign(p->m12, p->m12 + U * U);
   const size_t esz = h->prec == 64 ? 8 : 4;
   const long long row = nblk * 32 * (long long)h->V;
   const long long ldmod = 128 / (long long)esz;
@@ -365,6 +384,26 @@ extern "C" int dgfs_dg_rhs(dgfs_dg* h, const void* u, void* out, int v0, int nv,
     DG_DISPATCH(float, CALL);
 #undef CALL
   if (e != cudaSuccess) return set_error(DGFS_ERR_CUDA, "DG residual launch: %s", cudaGetErrorString(e));
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_dg_invmass(dgfs_dg* h, const void* u, void* out, int v0, int nv, void* stream) {
+  clear_error();
+  if (!h) return set_error(DGFS_ERR_INVALID, "null handle");
+  if (h->m12.empty()) return set_error(DGFS_ERR_INVALID, "handle created without the M12 operator");
+  int rc = check_bank(h, u, "solution");
+  if (!rc) rc = check_bank(h, out, "output");
+  if (!rc) rc = check_range(h, v0, nv);
+  if (rc) return rc;
+  if (out == u) return set_error(DGFS_ERR_INVALID, "output bank must differ from the solution bank");
+  cudaError_t e = cudaSuccess;
+#define CALL(P, U, F, D) e = run_invmass<P, U, F, D>(h, u, out, v0, nv, (cudaStream_t)stream)
+  if (h->prec == 64)
+    DG_DISPATCH(double, CALL);
+  else
+    DG_DISPATCH(float, CALL);
+#undef CALL
+  if (e != cudaSuccess) return set_error(DGFS_ERR_CUDA, "DG invmass launch: %s", cudaGetErrorString(e));
   return DGFS_OK;
 }
 

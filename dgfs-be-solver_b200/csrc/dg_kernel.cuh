@@ -68,6 +68,10 @@ template <typename T> struct DgArgs {
   const double* bcvals;    // [nb][2]
 };
 
+template <typename T, int U> struct DgMassOps {
+  T m12[U][U];
+};
+
 __device__ __forceinline__ int64_t aos32(int64_t row, int64_t ldim, int64_t e, int64_t v, int64_t V) {
   return row * ldim + ((e >> 5) * V + v) * 32 + (e & 31);
 }
@@ -89,6 +93,29 @@ __global__ void __launch_bounds__(256) dg_interp_kernel(const DgArgs<T> a, const
 #pragma unroll
     for (int i = 0; i < U; ++i) s = fma(op.m0[f][i], u[i], s);
     a.uf[aos32(f, a.ldim_f, e, v, a.V)] = s;
+  }
+}
+
+// out = M12 u at the solution points of velocities [v0, v0 + nv): the
+// 'invmass' kernel of DGFSElements (frfs/solvers/dgfs/elements.py:161-164),
+// M12 = V^T V with V the orthonormal basis at the solution points.
+template <typename T, int U>
+__global__ void __launch_bounds__(256) dg_invmass_kernel(const DgArgs<T> a, const DgMassOps<T, U> op) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = (int)(t & 31);
+  const int64_t w = t >> 5;
+  const int v = a.v0 + (int)(w % a.nv);
+  const int64_t e = (w / a.nv) * 32 + lane;
+  if (e >= a.neles) return;
+  T u[U];
+#pragma unroll
+  for (int i = 0; i < U; ++i) u[i] = a.u[aos32(i, a.ldim_u, e, v, a.V)];
+#pragma unroll
+  for (int r = 0; r < U; ++r) {
+    T s = T(0);
+#pragma unroll
+    for (int i = 0; i < U; ++i) s = fma(op.m12[r][i], u[i], s);
+    a.out[aos32(r, a.ldim_u, e, v, a.V)] = s;
   }
 }
 

@@ -519,6 +519,16 @@ extern "C" int dgfs_vhs_status(dgfs_vhs* h, void* stream, int* flag) {
   return DGFS_OK;
 }
 
+extern "C" int dgfs_vhs_check_wait(dgfs_vhs* h, long long limit_ns, void* stream) {
+  clear_error();
+  if (limit_ns < 0 || limit_ns > 10000000000ll) return set_error(DGFS_ERR_INVALID, "limit_ns=%lld outside [0, 1e10]", limit_ns);
+  if (!h) return noalloc_check_wait((unsigned long long)limit_ns, stream);
+  wait_check_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(h->err, (uint64_t)limit_ns);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(DGFS_ERR_CUDA, "wait check launch: %s", cudaGetErrorString(e));
+  return DGFS_OK;
+}
+
 extern "C" int dgfs_vhs_num_variants(const dgfs_vhs* h, int* count) {
   clear_error();
   if (!h || !count) return set_error(DGFS_ERR_INVALID, "null argument");

@@ -13,12 +13,16 @@
 // module, so with the CUDA runtime's lazy module loading only processes that
 // call this entry point hold it, on every GPU they call it on, until exit.
 // Host code cannot use the array's name as a device address: on each device
-// the first call looks its address up with cudaGetSymbolAddress (and uploads
-// the FFT twiddles and sets kernel attributes); that first call should come
-// before any stream capture.  Every call rebuilds the tables it needs and
-// zeroes the accumulators that must start at zero, but all calls share the
-// array: calls whose launches can overlap on the GPU (different streams
-// without ordering) race on it.
+// the first call looks its address up with cudaGetSymbolAddress, uploads the
+// FFT twiddles and clears the error flag, and the first call for each
+// (precision, Nv) sets that kernel's attributes; those first calls should
+// come before any stream capture.  The addresses are kept for the life of
+// the process: a cudaDeviceReset invalidates them and is not supported.
+// Every call rebuilds the tables it needs and zeroes the accumulators that
+// must start at zero, but all calls share the array: calls whose launches
+// can overlap on the GPU (different streams without ordering) race on it.
+// The kernel's bounded-wait flag also lives in the array; it is sticky until
+// dgfs_vhs_noalloc_status reads and clears it.
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -58,7 +62,6 @@ struct TableArgs {
   void* b2;      // T [V]
   double* cvec;  // [3][V]
   double* ginv_out;
-  int* err;
 };
 
 __device__ __forceinline__ double ref_sinc(double s) { return sin(s + 1e-15) / (s + 1e-15); }
@@ -102,7 +105,6 @@ template <typename T> __global__ void noalloc_tables_kernel(const TableArgs a) {
     }
   }
   if (tid < 25) a.ginv_out[tid] = a.ginv[tid];
-  if (tid == 0) *a.err = 0;
 }
 
 struct Shape {
@@ -153,15 +155,19 @@ const Shape& shape_for(int prec, int N) {
   return s[prec == 64 ? 1 : 0][N == 8 ? 0 : N == 16 ? 1 : N == 24 ? 2 : 3];
 }
 
-// Per-device set-up state: the array's device address and the resident
-// cluster count of each shape.
+// Per-device set-up state: the array's device address, and per (precision,
+// Nv) shape whether its attributes are set and its resident cluster count.
 struct DeviceState {
   bool ready;
   unsigned char* base;
+  bool shape_ready[2][4];
   int max_clusters[2][4];
 };
 std::mutex g_mutex;
 DeviceState g_dev[64];
+
+// The error flag sits at offset 0 of the array.
+int* flag_ptr(DeviceState* st) { return (int*)st->base; }
 
 int setup_device(int dev, DeviceState** out) {
   using ::dgfs::set_error;
@@ -190,34 +196,57 @@ int setup_device(int dev, DeviceState** out) {
   if ((e = cudaMemcpyToSymbol(dgfs::c_tw64, t64, sizeof(t64))) != cudaSuccess ||
       (e = cudaMemcpyToSymbol(dgfs::c_tw32, t32, sizeof(t32))) != cudaSuccess)
     return set_error(DGFS_ERR_CUDA, "twiddle upload: %s", cudaGetErrorString(e));
-  for (int pi = 0; pi < 2; ++pi)
-    for (int ni = 0; ni < 4; ++ni) {
-      const int N = ni == 0 ? 8 : ni == 1 ? 16 : ni == 2 ? 24 : 32;
-      const Shape& s = shape_for(pi ? 64 : 32, N);
-      if ((e = cudaFuncSetAttribute(s.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem)) != cudaSuccess ||
-          (s.C > 8 &&
-           (e = cudaFuncSetAttribute(s.fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) != cudaSuccess))
-        return set_error(DGFS_ERR_CUDA, "kernel attributes: %s", cudaGetErrorString(e));
-      cudaLaunchConfig_t cfg = {};
-      cfg.gridDim = dim3(s.C, 1, 1);
-      cfg.blockDim = dim3(s.threads, 1, 1);
-      cfg.dynamicSmemBytes = s.smem;
-      cudaLaunchAttribute attr[1];
-      attr[0].id = cudaLaunchAttributeClusterDimension;
-      attr[0].val.clusterDim.x = s.C;
-      attr[0].val.clusterDim.y = 1;
-      attr[0].val.clusterDim.z = 1;
-      cfg.attrs = attr;
-      cfg.numAttrs = 1;
-      int ncl = 0;
-      if ((e = cudaOccupancyMaxActiveClusters(&ncl, s.fn, &cfg)) != cudaSuccess || ncl < 1)
-        return set_error(DGFS_ERR_UNSUPPORTED, "cluster occupancy: %s", cudaGetErrorString(e));
-      st.max_clusters[pi][ni] = ncl;
-    }
+  if ((e = cudaMemset(base, 0, sizeof(int))) != cudaSuccess)
+    return set_error(DGFS_ERR_CUDA, "error flag reset: %s", cudaGetErrorString(e));
   st.base = (unsigned char*)base;
   st.ready = true;
   *out = &st;
   return DGFS_OK;
+}
+
+// Attributes and resident cluster count of one (precision, Nv) shape, set
+// up on its first use only, so a shape that cannot run on this device fails
+// the calls that need it and no others.
+int setup_shape(DeviceState* st, int pi, int ni) {
+  using ::dgfs::set_error;
+  std::lock_guard<std::mutex> lk(g_mutex);
+  if (st->shape_ready[pi][ni]) return DGFS_OK;
+  const int N = ni == 0 ? 8 : ni == 1 ? 16 : ni == 2 ? 24 : 32;
+  const Shape& s = shape_for(pi ? 64 : 32, N);
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(s.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem)) != cudaSuccess ||
+      (s.C > 8 && (e = cudaFuncSetAttribute(s.fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) != cudaSuccess))
+    return set_error(DGFS_ERR_CUDA, "kernel attributes (Nv=%d, precision %d): %s", N, pi ? 64 : 32,
+                     cudaGetErrorString(e));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(s.C, 1, 1);
+  cfg.blockDim = dim3(s.threads, 1, 1);
+  cfg.dynamicSmemBytes = s.smem;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = s.C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int ncl = 0;
+  if ((e = cudaOccupancyMaxActiveClusters(&ncl, s.fn, &cfg)) != cudaSuccess || ncl < 1)
+    return set_error(DGFS_ERR_UNSUPPORTED, "cluster of %d CTAs (Nv=%d, precision %d) cannot be scheduled: %s", s.C,
+                     N, pi ? 64 : 32, cudaGetErrorString(e));
+  st->max_clusters[pi][ni] = ncl;
+  st->shape_ready[pi][ni] = true;
+  return DGFS_OK;
+}
+
+cudaError_t launch_wait_check(int* flag, uint64_t limit_ns, cudaStream_t stream) {
+  dgfs::wait_check_kernel<<<1, 32, 0, stream>>>(flag, limit_ns);
+  return cudaGetLastError();
+}
+
+int current_state(DeviceState** st) {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) return ::dgfs::set_error(DGFS_ERR_CUDA, "no CUDA device");
+  return setup_device(dev, st);
 }
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -307,13 +336,14 @@ int run(const dgfs_vhs_params* p, DeviceState* st, const void* f, void* Q, int n
   ta.b2 = b2;
   ta.cvec = cvec;
   ta.ginv_out = ginv;
-  ta.err = err;
   const int work = P * M * 3 * N > V ? P * M * 3 * N : V;
   noalloc_tables_kernel<T><<<(work + 255) / 256, 256, 0, stream>>>(ta);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_error(DGFS_ERR_CUDA, "table kernel launch: %s", cudaGetErrorString(e));
 
   const int pi = sizeof(T) == 8 ? 1 : 0, ni = N == 8 ? 0 : N == 16 ? 1 : N == 24 ? 2 : 3;
+  int rc = setup_shape(st, pi, ni);
+  if (rc) return rc;
   const Shape& s = shape_for(p->precision, N);
   int ncl = st->max_clusters[pi][ni];
   if (ncl > fit) ncl = fit;
@@ -383,12 +413,40 @@ extern "C" int dgfs_vhs_apply_noalloc(const dgfs_vhs_params* p, const void* f, v
     pt0 = 0;
     npts = nupts * neles;
   }
-  int dev = -1;
-  if (cudaGetDevice(&dev) != cudaSuccess) return set_error(DGFS_ERR_CUDA, "no CUDA device");
   DeviceState* st = nullptr;
-  int rc = setup_device(dev, &st);
+  int rc = current_state(&st);
   if (rc) return rc;
   if (p->precision == 64)
     return run<double>(p, st, f, Q, nupts, neles, ldim, soasz, pt0, npts, (cudaStream_t)stream);
   return run<float>(p, st, f, Q, nupts, neles, ldim, soasz, pt0, npts, (cudaStream_t)stream);
+}
+
+namespace dgfs {
+int noalloc_check_wait(unsigned long long limit_ns, void* stream) {
+  DeviceState* st = nullptr;
+  int rc = current_state(&st);
+  if (rc) return rc;
+  const cudaError_t e = launch_wait_check(flag_ptr(st), (uint64_t)limit_ns, (cudaStream_t)stream);
+  if (e != cudaSuccess) return set_error(DGFS_ERR_CUDA, "wait check launch: %s", cudaGetErrorString(e));
+  return DGFS_OK;
+}
+}  // namespace dgfs
+
+extern "C" int dgfs_vhs_noalloc_status(void* stream, int* flag) {
+  using ::dgfs::set_error;
+  ::dgfs::clear_error();
+  if (!flag) return set_error(DGFS_ERR_INVALID, "null argument");
+  *flag = 0;
+  DeviceState* st = nullptr;
+  int rc = current_state(&st);
+  if (rc) return rc;
+  cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+  if (e != cudaSuccess) return set_error(DGFS_ERR_CUDA, "stream: %s", cudaGetErrorString(e));
+  int v = 0;
+  if ((e = cudaMemcpy(&v, flag_ptr(st), sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess ||
+      (v && (e = cudaMemset(flag_ptr(st), 0, sizeof(int))) != cudaSuccess))
+    return set_error(DGFS_ERR_CUDA, "error flag: %s", cudaGetErrorString(e));
+  *flag = v;
+  if (v) return set_error(DGFS_ERR_CUDA, "an allocation-free VHS launch gave up waiting for cluster data (flag %d)", v);
+  return DGFS_OK;
 }

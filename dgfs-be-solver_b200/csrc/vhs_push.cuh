@@ -10,10 +10,10 @@
 // split into arrive (after the last local read) and wait (just before the next
 // pushes), so its latency hides behind the next pencil FFTs.
 //
-// Every mbarrier wait is bounded (a few seconds of %globaltimer); on expiry
-// the kernel records an error flag in global memory and carries on, so all
-// cluster barriers are still reached and the launch always terminates; the
-// host turns the flag into an error (dgfs_vhs_status).
+// Every mbarrier wait is bounded (1 s of %globaltimer); on expiry the kernel
+// records an error flag in global memory and carries on, so all cluster
+// barriers are still reached and the launch always terminates; the host
+// turns the flag into an error (dgfs_vhs_status).
 #pragma once
 
 #include "vhs_kernel.cuh"
@@ -49,22 +49,48 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-// Wait for phase `parity` of `bar`, giving up after ~1 s (error flag set).
-// Once the flag is set every later wait of the launch returns at once, so a
-// failed exchange costs one timeout, not one per (p, q).
-__device__ __forceinline__ void mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err) {
+// Default limit of one bounded wait: 1 s of %globaltimer.
+constexpr uint64_t kWaitLimitNs = 1000000000ull;
+
+// Wait for phase `parity` of `bar`, giving up after `limit_ns`: the wait
+// that gives up sets the global flag `err` (read by the host) and the CTA's
+// shared flag `gave_up`; every later wait of that CTA returns at once, so a
+// failed exchange costs one timeout per CTA, not one per (p, q).  The global
+// flag is only written here, never read: a flag left set by an earlier
+// launch does not change how this launch waits.
+__device__ __forceinline__ void mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err, int* gave_up,
+                                                  uint64_t limit_ns = kWaitLimitNs) {
   if (mbar_try_wait(bar, parity)) return;
   const uint64_t t0 = globaltimer_ns();
   for (uint32_t i = 1;; ++i) {
     if (mbar_try_wait(bar, parity)) return;
     if ((i & 255u) == 0) {
-      if (*(volatile int*)err) return;
-      if (globaltimer_ns() - t0 > 1000000000ull) {
+      if (*(volatile int*)gave_up) return;
+      if (globaltimer_ns() - t0 > limit_ns) {
         atomicExch(err, 1);
+        *(volatile int*)gave_up = 1;
         return;
       }
     }
   }
+}
+
+// Failure-detection check of the bounded wait: one CTA waits on an mbarrier
+// that expects 16 bytes nothing will send, so the wait runs out after
+// `limit_ns` and sets `err`, exactly as a push exchange whose data never
+// arrives would.  Nothing else is touched; the launch ends after one timeout.
+__global__ void __launch_bounds__(32) wait_check_kernel(int* err, uint64_t limit_ns) {
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int gave_up;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    gave_up = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) mbar_expect_tx(&bar, 16);
+  __syncthreads();
+  mbar_wait_bounded(&bar, 0, err, &gave_up, limit_ns);
 }
 __device__ __forceinline__ void st_async(uint32_t raddr, float2 v, uint32_t rbar) {
   asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f32 [%0], {%1, %2}, [%3];" ::"r"(raddr),
@@ -147,6 +173,7 @@ __global__ void __launch_bounds__(PushGeom<N, C>::NT, MINB) vhs_push_kernel(cons
   CX* sS = sPl + 4 * BSZ;                    // [NS][N][RP]
   CX* sPh = sS + BSZ;                        // [2][3N]
   __shared__ __align__(8) uint64_t sBar[2];
+  __shared__ int sGaveUp;
   __shared__ double sRed[5][NT / 32];
   __shared__ double sMom[5];
 
@@ -173,10 +200,11 @@ __global__ void __launch_bounds__(PushGeom<N, C>::NT, MINB) vhs_push_kernel(cons
     cl_wait();  // every CTA is done reading this set from two exchanges ago
     if (active) push_pencil<T, N, C>(x, sPl + (set * 2 + which) * BSZ, &sBar[set], l2g, l3);
     if (tid == 0) mbar_expect_tx(&sBar[set], kPhaseBytes);
-    mbar_wait_bounded(&sBar[set], (uint32_t)((it >> 1) & 1), a.err);
+    mbar_wait_bounded(&sBar[set], (uint32_t)((it >> 1) & 1), a.err, &sGaveUp);
   };
 
   if (tid == 0) {
+    sGaveUp = 0;
     mbar_init(&sBar[0], 1);
     mbar_init(&sBar[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");

@@ -60,6 +60,8 @@ _SIGS = {
     'dgfs_vhs_apply_noalloc': (c_int, [ct.POINTER(VhsParams), c_void_p,
                                        c_void_p, c_int, c_int, c_ll, c_int,
                                        c_int, c_int, c_void_p]),
+    'dgfs_vhs_noalloc_status': (c_int, [c_void_p, ct.POINTER(c_int)]),
+    'dgfs_vhs_check_wait': (c_int, [c_void_p, c_ll, c_void_p]),
     'dgfs_moments': (c_int, [c_int, c_void_p, c_int, c_int, c_ll, c_int,
                              c_double, c_double, c_void_p, c_void_p]),
     'dgfs_probe_fma_peak': (c_int, [c_int, c_int, ct.POINTER(c_double),

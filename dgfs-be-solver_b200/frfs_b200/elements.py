@@ -12,22 +12,22 @@ pairs the two sides of an interface (frfs/nputil.py:fuzzysort).
 
 import numpy as np
 
+from frfs_b200.shapes import tol_runs
+
 
 def fuzzysort(arr, idx, dim=0, tol=1e-6):
-    """Sort ``idx`` by arr[dim], breaking ties within ``tol`` by the next
-    coordinate (frfs/nputil.py:fuzzysort)."""
-    arrd = arr[dim]
-    srtdidx = sorted(idx, key=arrd.__getitem__)
-    if len(srtdidx) > 1:
-        i, ix = 0, srtdidx[0]
-        for j, jx in enumerate(srtdidx[1:], start=1):
-            if arrd[jx] - arrd[ix] >= tol:
-                if j - i > 1:
-                    srtdidx[i:j] = fuzzysort(arr, srtdidx[i:j], dim + 1, tol)
-                i, ix = j, jx
-        if i != j:
-            srtdidx[i:] = fuzzysort(arr, srtdidx[i:], dim + 1, tol)
-    return srtdidx
+    """Order the points ``idx`` by coordinate ``dim``; points whose
+    coordinate agrees within ``tol`` (runs anchored at their first member,
+    as in ``clean``) are ordered among themselves by the next coordinate.
+    This is the face flux-point ordering frfs pairs interfaces with
+    (frfs/nputil.py:84-100)."""
+    key = arr[dim]
+    order = sorted(idx, key=key.__getitem__)
+    out = []
+    for i, j in tol_runs([key[k] for k in order], tol):
+        run = order[i:j]
+        out.extend(fuzzysort(arr, run, dim + 1, tol) if j - i > 1 else run)
+    return out
 
 
 class ElementGeometry:

@@ -31,48 +31,47 @@ import numpy as np
 from frfs_b200.quadratures import gauss_legendre, gauss_legendre_lobatto
 
 
+def tol_runs(vals, tol):
+    """Split an ascending sequence into runs: a run starts at the first
+    value not yet taken and holds every later value that exceeds it by less
+    than ``tol``.  Yields (start, stop) index pairs."""
+    vals = np.asarray(vals, dtype=float)
+    n, i = len(vals), 0
+    while i < n:
+        far = np.nonzero(vals[i + 1:] - vals[i] >= tol)[0]
+        j = i + 1 + int(far[0]) if far.size else n
+        yield i, j
+        i = j
+
+
 def clean(arr, tol=1e-10):
-    """frfs/nputil.py:clean: flush tiny entries, coalesce equal magnitudes."""
-    arr = np.array(arr, dtype=np.float64, copy=True)
-    arr[np.abs(arr) < tol] = 0
-    if arr.size > 1:
-        amfl = np.abs(arr.ravel())
-        amix = np.argsort(amfl, kind='quicksort')
-        i, ix = 0, amix[0]
-        for j, jx in enumerate(amix[1:], start=1):
-            if amfl[jx] - amfl[ix] >= tol:
-                if j - i > 1:
-                    amfl[amix[i:j]] = np.median(amfl[amix[i:j]])
-                i, ix = j, jx
-        if i != j:
-            amfl[amix[i:]] = np.median(amfl[amix[i:]])
-        arr = np.copysign(amfl, arr.ravel()).reshape(arr.shape)
-    return arr
+    """Post-processing frfs applies to every operator matrix
+    (frfs/nputil.py:24-52): entries of magnitude below ``tol`` become zero;
+    then the magnitudes, taken in ascending order, are grouped into runs
+    that stay within ``tol`` of their first member, every run of two or more
+    is replaced by its median, and the signs are restored."""
+    out = np.array(arr, dtype=np.float64, copy=True)
+    out[np.abs(out) < tol] = 0
+    mag = np.abs(out).ravel()
+    order = np.argsort(mag)
+    srt = mag[order]
+    for i, j in tol_runs(srt, tol):
+        if j - i > 1:
+            mag[order[i:j]] = np.median(srt[i:j])
+    return np.copysign(mag, out.ravel()).reshape(out.shape)
 
 
-def jacobi(n, a, b, z):
-    """P_0..P_n of the Jacobi family at z (frfs/polys.py:12-33)."""
-    j = [np.ones_like(z, dtype=float) if hasattr(z, '__len__') else 1.0]
-    if n >= 1:
-        j.append(((a + b + 2)*z + a - b)/2)
-    if n >= 2:
-        apb, bbmaa = a + b, b*b - a*a
-        for q in range(2, n + 1):
-            qapbpq, apbp2q = q*(apb + q), apb + 2*q
-            apbp2qm1, apbp2qm2 = apbp2q - 1, apbp2q - 2
-            aq = apbp2q*apbp2qm1/(2*qapbpq)
-            bq = apbp2qm1*bbmaa/(2*qapbpq*apbp2qm2)
-            cq = apbp2q*(a + q - 1)*(b + q - 1)/(qapbpq*apbp2qm2)
-            j.append((aq*z - bq)*j[-1] - cq*j[-2])
-    return j
-
-
-def jacobi_diff(n, a, b, z):
-    dj = [0.0]
-    if n >= 1:
-        dj.extend(jp*(i + a + b + 2)/2
-                  for i, jp in enumerate(jacobi(n - 1, a + 1, b + 1, z)))
-    return dj
+def legendre(nmax, x):
+    """Legendre polynomials P_0..P_nmax and their derivatives at x, from
+    Bonnet's recurrence (n + 1) P_{n+1} = (2n + 1) x P_n - n P_{n-1} and
+    P'_{n+1} = P'_{n-1} + (2n + 1) P_n (Abramowitz & Stegun 22.7.10 and
+    22.8.5 in differentiated form)."""
+    p = [1.0, x]
+    dp = [0.0, 1.0]
+    for n in range(1, nmax):
+        p.append(((2*n + 1)*x*p[n] - n*p[n - 1])/(n + 1))
+        dp.append(dp[n - 1] + (2*n + 1)*p[n])
+    return p[:nmax + 1], dp[:nmax + 1]
 
 
 class _Basis:
@@ -86,12 +85,13 @@ class _Basis:
             self.pts = self.pts.T
 
     def _leg(self, x):
-        sk = [sqrt(k + 0.5) for k in range(self.order)]
-        return [c*p for c, p in zip(sk, jacobi(self.order - 1, 0, 0, x))]
+        """sqrt(k + 1/2) P_k(x), k < order: orthonormal on [-1, 1]."""
+        p, _ = legendre(self.order - 1, x)
+        return [sqrt(k + 0.5)*v for k, v in enumerate(p)]
 
     def _dleg(self, x):
-        sk = [sqrt(k + 0.5) for k in range(self.order)]
-        return [c*p for c, p in zip(sk, jacobi_diff(self.order - 1, 0, 0, x))]
+        _, dp = legendre(self.order - 1, x)
+        return [sqrt(k + 0.5)*v for k, v in enumerate(dp)]
 
     def ortho_basis_at(self, pts):
         pts = np.atleast_2d(np.asarray(pts, dtype=float))
@@ -193,7 +193,17 @@ class QuadShape:
         coeffs = np.vstack(coeffs)
         return clean(np.dot(coeffs, self.ubasis.ortho_basis_at(self.upts)).T)
 
+    @property
+    def m12(self):
+        """V^T V, V the orthonormal basis at the solution points: the
+        operator of DGFSElements' 'invmass' kernel (frfs/shapes.py:164-166,
+        frfs/solvers/dgfs/elements.py:161-164)."""
+        vdm = self.ubasis.vdm
+        return (vdm.T @ vdm).reshape(self.nupts, -1)
+
     def opmat(self, expr):
+        if expr == 'M12':
+            return self.m12
         m0, m1, m2, m3 = self.m0, self.m1, self.m2, self.m3
         if expr == 'M0':
             return clean(m0)
@@ -205,4 +215,6 @@ class QuadShape:
             return clean(m3)
         if expr == 'M1 - M3*M2':
             return clean(m1 - m3 @ m2)
+        if expr == 'M12':
+            return self.m12
         raise ValueError(f'unsupported operator expression {expr!r}')

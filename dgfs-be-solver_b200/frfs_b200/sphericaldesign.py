@@ -8,7 +8,9 @@ files of the requested rule name and point count, the one of highest degree.
 
 Search order for the directory: the ``paths`` argument, then the
 ``DGFS_SPHDESIGN_PATH`` environment variable (os.pathsep separated), then
-the ``frfs`` package if it is importable.
+the tables shipped with this package (``data/sphericaldesign``: the
+Womersley symmetric designs of frfs/sphericaldesign/symmetric that the
+workloads use), then the ``frfs`` package if it is importable.
 """
 
 import os
@@ -16,6 +18,8 @@ import re
 
 import numpy as np
 
+DATA_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'data',
+                        'sphericaldesign')
 _PAT = re.compile(r'([a-zA-Z0-9\-~+]+)-ss(\d+)(?:-m(\d+))?\.txt$')
 
 
@@ -30,6 +34,7 @@ def _search_dirs(paths):
     env = os.environ.get('DGFS_SPHDESIGN_PATH')
     if env:
         dirs += env.split(os.pathsep)
+    dirs.append(DATA_DIR)
     try:
         import importlib.util
         spec = importlib.util.find_spec('frfs')

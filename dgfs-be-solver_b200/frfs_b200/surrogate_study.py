@@ -247,24 +247,6 @@ def run_study(ini, device='cuda:0', runs=5, near_runs=10, steps=100,
     }
 
 
-def profile_collide(ini, device='cuda:0', nsteps=200, sphdesign=None):
-    """One surrogate collision sweep on the workload's state after nsteps
-    plain steps, bracketed by cudaProfilerStart/Stop (for a profiler run
-    with --profile-from-start off); three unprofiled sweeps first."""
-    s = make_system(ini, 'single', device, sphdesign)
-    sur = VHSSurrogate(s.sm)
-    _, idx, _ = run_workload(s, nsteps)
-    fb = s.bank[idx]
-    qb = s.backend.matrix(fb.ioshape)
-    for _ in range(3):
-        sur.collide(fb, qb)
-    torch.cuda.synchronize(device)
-    torch.cuda.cudart().cudaProfilerStart()
-    sur.collide(fb, qb)
-    torch.cuda.synchronize(device)
-    torch.cuda.cudart().cudaProfilerStop()
-
-
 if __name__ == '__main__':
     import argparse
     import os
@@ -272,17 +254,11 @@ if __name__ == '__main__':
     from frfs_b200 import workloads
     ap = argparse.ArgumentParser(description=__doc__.split('\n')[0])
     ap.add_argument('--workload', default='couette-n24')
-    ap.add_argument('--profile-collide', action='store_true',
-                    help='one surrogate sweep inside a profiler range')
     ap.add_argument('--sphdesign', default=os.path.join(
-        os.path.dirname(__file__), '..', '..', 'tests', 'golden',
-        'sphericaldesign'))
+        os.path.dirname(__file__), 'data', 'sphericaldesign'))
     args = ap.parse_args()
     ini = workloads.WORKLOADS[args.workload]
     sph = os.path.abspath(args.sphdesign)
-    if args.profile_collide:
-        profile_collide(ini, sphdesign=sph)
-    else:
-        import json
-        print(json.dumps(run_study(ini, sphdesign=sph,
-                                   log=lambda m: print(m, flush=True))))
+    import json
+    print(json.dumps(run_study(ini, sphdesign=sph,
+                               log=lambda m: print(m, flush=True))))

@@ -7,6 +7,7 @@ the DGFS steppers and the ARS explicit stage call:
   collide(t, uinbank, foutbank)                       system.py:199-218
   updatebc(t, uinbank, foutbank, batch, varidx)       system.py:180-196
   rhs(t, uinbank, foutbank, batch, varidx)            system.py:140-177
+  invmass(uinbank, foutbank)                          system.py:221-231
 
 with the distribution banks addressed by register index
 (``eles_scal_upts_inb_full``, system.py:127-136).  ``collide`` evaluates
@@ -47,7 +48,7 @@ class DgParams(ct.Structure):
                 ('nbfpts', c_int), ('bkind', c_ip), ('bgroup', c_ip),
                 ('bfpt', c_ip), ('bele', c_ip), ('ngroups', c_int),
                 ('guw', c_dp), ('gfw', c_dp), ('grefl', c_ip),
-                ('bwall', c_dp)]
+                ('bwall', c_dp), ('m12', c_dp)]
 
 
 _lib.declare('dgfs_dg_create', c_int, [ct.POINTER(DgParams),
@@ -60,6 +61,8 @@ _lib.declare('dgfs_dg_updatebc', c_int, [c_void_p, c_int, c_int, c_int,
 _lib.declare('dgfs_dg_rhs', c_int, [c_void_p, c_void_p, c_void_p, c_int,
                                     c_int, c_double, c_void_p, c_double,
                                     c_void_p, c_double, c_void_p, c_void_p])
+_lib.declare('dgfs_dg_invmass', c_int, [c_void_p, c_void_p, c_void_p, c_int,
+                                        c_int, c_void_p])
 _lib.declare('dgfs_dg_bcvals', c_int, [c_void_p, c_dp, c_int])
 _lib.declare('dgfs_dg_fpts', c_int, [c_void_p, ct.POINTER(c_void_p),
                                      ct.POINTER(c_ll)])
@@ -214,7 +217,8 @@ class DGFSSystem:
         d = lambda x: np.ascontiguousarray(x, dtype=np.float64)
         self._keep = keep = dict(
             m0=d(sh.opmat('M0')), m132=d(sh.opmat('M1 - M3*M2')),
-            m3=d(sh.opmat('M3')), smats=d(geo.smat_at(sh.upts)),
+            m3=d(sh.opmat('M3')), m12=d(sh.opmat('M12')),
+            smats=d(geo.smat_at(sh.upts)),
             rcpdjac=d(geo.rcpdjac_at(sh.upts)),
             nrm=d(geo.norm_pnorm_fpts.transpose(0, 2, 1)),
             mag=d(geo.mag_pnorm_fpts),
@@ -237,7 +241,8 @@ class DGFSSystem:
             bgroup=_ptr(bgroup, c_ip), bfpt=_ptr(bfpt, c_ip),
             bele=_ptr(bele, c_ip), ngroups=len(bnames),
             guw=_ptr(keep['guw']), gfw=_ptr(keep['gfw']),
-            grefl=_ptr(keep['grefl'], c_ip), bwall=_ptr(keep['bwall']))
+            grefl=_ptr(keep['grefl'], c_ip), bwall=_ptr(keep['bwall']),
+            m12=_ptr(keep['m12']))
         h = c_void_p()
         lib = _lib.load()
         _lib.check(lib.dgfs_dg_create(ct.byref(p), ct.byref(h)),
@@ -308,6 +313,14 @@ class DGFSSystem:
             self._dg, u._as_parameter_, self.bank[out]._as_parameter_, v0,
             nv, alpha, ptr(A), beta, ptr(B), gamma, ptr(C), s),
             'dgfs_dg_rhs')
+
+    def invmass(self, uinbank, foutbank):
+        """bank[foutbank] = M12 bank[uinbank] at every solution point and
+        velocity (system.py:221-231, elements.py:161-164)."""
+        u, out = self.bank[uinbank], self.bank[foutbank]
+        _lib.check(self._lib.dgfs_dg_invmass(
+            self._dg, u._as_parameter_, out._as_parameter_, 0,
+            self.vm.vsize(), self.backend.stream), 'dgfs_dg_invmass')
 
     def moments(self, bankidx=None):
         """FP64 moments at every solution point of a bank, shape

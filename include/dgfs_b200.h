@@ -149,8 +149,8 @@ DGFS_API int dgfs_vhs_select(dgfs_vhs* h, int idx);
 DGFS_API int dgfs_vhs_variant_kind(const dgfs_vhs* h, int idx, int* push);
 
 /* Synchronise `stream`, then report and clear the kernel error flag: the
- * push kernels bound every wait on cluster data (a few seconds) and set the
- * flag instead of hanging.  Returns DGFS_ERR_CUDA when it was set. */
+ * push kernels bound every wait on cluster data (1 s) and set the flag
+ * instead of hanging.  Returns DGFS_ERR_CUDA when it was set. */
 DGFS_API int dgfs_vhs_status(dgfs_vhs* h, void* stream, int* flag);
 
 /* Allocation-free variant of dgfs_vhs_apply (no counterpart in the
@@ -163,13 +163,34 @@ DGFS_API int dgfs_vhs_status(dgfs_vhs* h, void* stream, int* flag);
  * of 24 MiB (held on every GPU that uses this entry point until the process
  * exits); it never calls cudaMalloc or cudaFree.  Limits: Nrho <= 32 and
  * M <= 128 (every such size, up to Nv = 32 in FP64 with the projection,
- * fits in the array); larger sizes are rejected with DGFS_ERR_INVALID.  The first call on a device sets it up (symbol address,
- * twiddles, kernel attributes) and should come before any stream capture.
- * All calls share the array: calls that can overlap on the GPU race. */
+ * fits in the array); larger sizes are rejected with DGFS_ERR_INVALID.
+ * The first call on a device sets it up (symbol address, twiddles, error
+ * flag) and the first call for each (precision, Nv) sets that kernel's
+ * attributes; those first calls should come before any stream capture.
+ * cudaDeviceReset invalidates the set-up and is not supported.  All calls
+ * share the array: calls that can overlap on the GPU race.  A bounded wait
+ * that gives up sets a flag in the array that stays set until
+ * dgfs_vhs_noalloc_status reads it. */
 DGFS_API int dgfs_vhs_apply_noalloc(const dgfs_vhs_params* params,
                                     const void* f, void* Q, int nupts,
                                     int neles, long long ldim, int soasz,
                                     int elem, int upt, void* stream);
+
+/* Synchronise `stream`, then report and clear the error flag of the
+ * allocation-free path (set by any earlier dgfs_vhs_apply_noalloc launch on
+ * the current device whose bounded wait gave up; a Q computed by such a
+ * launch is invalid).  Returns DGFS_ERR_CUDA with *flag = 1 when it was
+ * set.  No counterpart in the reference. */
+DGFS_API int dgfs_vhs_noalloc_status(void* stream, int* flag);
+
+/* Failure-detection check (no counterpart in the reference): one CTA runs
+ * the push kernels' bounded wait on an exchange whose 16 bytes never
+ * arrive, with a limit of limit_ns nanoseconds (0 .. 1e10), so the wait runs
+ * out and sets the error flag of h (reported by dgfs_vhs_status) or, with h
+ * NULL, the allocation-free path's flag (dgfs_vhs_noalloc_status).  The
+ * wait returns and the launch ends normally; nothing else is touched. */
+DGFS_API int dgfs_vhs_check_wait(dgfs_vhs* h, long long limit_ns,
+                                 void* stream);
 
 /* ------------------------------------------------------------------------
  * FR-DG advection residual over all velocities
@@ -225,6 +246,9 @@ typedef struct dgfs_dg_params {
   const double* bwall;    /* [nbfpts][4] (Ux, Uy, Uz, T) of the wall at each
                              boundary flux point (nondimensional), read for
                              DGFS_BC_WALL_DIFFUSE_CYL points; NULL if none  */
+  const double* m12;      /* [nupts][nupts] operator M12 = V^T V for
+                             dgfs_dg_invmass (frfs/shapes.py:164-166), or
+                             NULL                                           */
 } dgfs_dg_params;
 
 DGFS_API int dgfs_dg_create(const dgfs_dg_params* params, dgfs_dg** out);
@@ -250,6 +274,13 @@ DGFS_API int dgfs_dg_rhs(dgfs_dg* h, const void* u, void* out, int v0, int nv,
                          double alpha, const void* A, double beta,
                          const void* B, double gamma, const void* C,
                          void* stream);
+
+/* out = M12 u on velocities [v0, v0+nv): DGFSSystem.invmass
+ * (frfs/solvers/dgfs/system.py:221-231), the 'invmass' kernel of
+ * frfs/solvers/dgfs/elements.py:161-164.  Needs m12 at create time; out must
+ * differ from u. */
+DGFS_API int dgfs_dg_invmass(dgfs_dg* h, const void* u, void* out, int v0,
+                             int nv, void* stream);
 
 /* Copy the 2*nbfpts diffuse-wall sums to host memory (synchronous). */
 DGFS_API int dgfs_dg_bcvals(const dgfs_dg* h, double* host, int n);

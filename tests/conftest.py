@@ -10,7 +10,8 @@ for p in (ROOT, os.path.join(ROOT, 'dgfs-be-solver_b200')):
         sys.path.insert(0, p)
 
 GOLDEN = os.path.join(ROOT, 'tests', 'golden')
-SPHDESIGN = os.path.join(GOLDEN, 'sphericaldesign')
+SPHDESIGN = os.path.join(ROOT, 'dgfs-be-solver_b200', 'frfs_b200', 'data',
+                         'sphericaldesign')
 
 
 def pytest_configure(config):

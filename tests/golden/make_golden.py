@@ -14,17 +14,18 @@ modules.  This script uses that to record, from the reference's own code:
 * half-sphere spherical design sz, sw (velocitymesh.py:128-135,
   frfs/sphericaldesign/__init__.py:84-107) -- the tabulated Womersley designs
   used by the workloads are also copied, in their original text format, to
-  ``tests/golden/sphericaldesign/`` so that tests and benchmarks can load
-  them on machines without the reference;
+  the package's data folder ``frfs_b200/data/sphericaldesign/`` so that the
+  solver, tests and benchmarks can load them on machines without the
+  reference;
 * VHS prefactor and gamma (frfs/solvers/dgfs/scattering.py:50-65);
 * Maxwellian initial condition values (frfs/solvers/dgfs/initcond.py:39-116);
 * quadrilateral FR operator matrices M0, M1, M2, M3, M1-M3*M2 and the point
   sets (frfs/shapes.py:83-166,243-289) for p = 1, 2, 3.
 
-Run from the repository root with the reference checked out at
-``/root/reference``::
+Run from the repository root, with DGFS_REFERENCE naming the directory of a
+checkout of the reference::
 
-    python tests/golden/make_golden.py
+    DGFS_REFERENCE=<path to the checkout> python tests/golden/make_golden.py
 """
 
 import collections
@@ -38,7 +39,7 @@ import types
 
 import numpy as np
 
-REF = os.environ.get('DGFS_REFERENCE', '/root/reference')
+REF = os.environ.get('DGFS_REFERENCE')
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(ROOT, 'dgfs-be-solver_b200'))
@@ -149,7 +150,8 @@ def velocity_fixture(name, inistr, icmod, vmmod, scmod, Inifile, out,
     # Copy the spherical design table that this mesh loads
     npts = 2*vm.M()
     src = os.path.join(REF, 'frfs', 'sphericaldesign', 'symmetric')
-    dst = os.path.join(out, 'sphericaldesign')
+    dst = os.path.join(ROOT, 'dgfs-be-solver_b200', 'frfs_b200', 'data',
+                       'sphericaldesign')
     os.makedirs(dst, exist_ok=True)
     for f in os.listdir(src):
         if f.endswith(f'-m{npts:05d}.txt'):
@@ -237,6 +239,9 @@ flux-pts = gauss-legendre
 
 
 def main():
+    if not REF or not os.path.isdir(os.path.join(REF, 'frfs')):
+        sys.exit('set DGFS_REFERENCE to the directory of a checkout of the '
+                 'reference (it holds the frfs package)')
     _install_shims()
     vmmod = _load('frfs.solvers.dgfs.velocitymesh')
     icmod = _load('frfs.solvers.dgfs.initcond')

@@ -228,3 +228,21 @@ def test_checkpoint_restart_continues_bit_for_bit(tmp_path):
     st2.advance(2)
     torch.cuda.synchronize()
     assert np.array_equal(s2.bank[st2._idxcurr].get(), want)
+
+
+@pytest.mark.parametrize('precision', ['double', 'single'])
+@pytest.mark.parametrize('order', [1, 2, 3])
+def test_invmass_matches_reference_operator(precision, order):
+    """DGFSSystem.invmass (frfs/solvers/dgfs/system.py:221-231): the bank
+    times M12, with M12 taken from the reference's own shapes fixture."""
+    from conftest import GOLDEN
+    M12 = np.load(f'{GOLDEN}/ref_shape_quad_p{order}.npz')['M12']
+    cfg, m = _cfg(precision, order=order), _mesh(order)
+    dg, sh, geo, vm = dg_setup(cfg, m)
+    u = _states(vm, sh.nupts, geo.neles, seed=order + 10)
+    be, s = _system(cfg, m, u)
+    u_used = s.bank[0].get().astype(np.float64)
+    s.invmass(0, 2)
+    torch.cuda.synchronize()
+    ref = np.einsum('ij,jve->ive', M12, u_used)
+    assert rel_err(s.bank[2].get(), ref) < TOL[precision]

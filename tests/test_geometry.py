@@ -19,7 +19,7 @@ def test_quad_operators_match_reference(order):
     np.testing.assert_allclose(sh.fpts, g['fpts'], atol=1e-15)
     np.testing.assert_array_equal(sh.norm_fpts, g['norm_fpts'])
     for key, expr in [('M0', 'M0'), ('M1', 'M1'), ('M2', 'M2'), ('M3', 'M3'),
-                      ('M132', 'M1 - M3*M2')]:
+                      ('M132', 'M1 - M3*M2'), ('M12', 'M12')]:
         np.testing.assert_allclose(sh.opmat(expr), g[key], rtol=0,
                                    atol=2e-14, err_msg=key)
 

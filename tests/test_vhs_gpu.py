@@ -227,3 +227,30 @@ def test_single_cta_kernel(name, project):
         for u in range(nupts):
             for e in range(neles):
                 assert rel_err(Qg[u, :, e], Qo[u, e]) < FP32_TOL, (i, u, e)
+
+
+def test_bounded_wait_that_runs_out_is_reported():
+    """Failure detection without a GPU fault: the push kernels' bounded wait,
+    run with a 1 ms limit on an exchange whose bytes never arrive, gives up,
+    sets the handle's flag and returns; dgfs_vhs_status reports it once and
+    the context stays usable (the next evaluation matches the oracle)."""
+    import ctypes as ct
+    from frfs_b200 import _lib
+    cfg = _cfg('small-n8', 'double')
+    be, vm, sm = _model(cfg)
+    lib = _lib.load()
+    assert lib.dgfs_vhs_check_wait(sm._h, 1000000, be.stream) == 0
+    flag = ct.c_int(0)
+    assert lib.dgfs_vhs_status(sm._h, be.stream, ct.byref(flag)) == 2
+    assert flag.value == 1
+    assert b'gave up' in lib.dgfs_last_error()
+    assert lib.dgfs_vhs_status(sm._h, be.stream, ct.byref(flag)) == 0
+    assert flag.value == 0
+    assert lib.dgfs_vhs_check_wait(sm._h, -1, be.stream) == 1
+    ovm, pre, prefac = oracle_for(cfg)
+    f = random_states(vm.cv(), 1, seed=5).reshape(1, 1, -1)
+    fin, fout = _bank(be, vm, f)
+    sm.fs(fin, fout, 0, 0)
+    sm.status()
+    Qo = ovhs.vhs_Q(f[0, 0], ovm, pre, prefac)
+    assert rel_err(fout.get()[0, :, 0], Qo) < FP64_TOL
