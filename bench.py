@@ -17,9 +17,12 @@ on the Couette workload, the learned surrogate's run (``surrogate``: pairs
 harvested from the solver, training, rho/u/T errors against the plain FP64
 solution after 200 steps, evaluations per second plain vs surrogate).
 
-Multi-GPU (torchrun): every rank runs its own copy of the workload (the
-collision is independent per point, no data-path collective), so scaling is
-weak; the time is the max over ranks.
+Multi-GPU (torchrun, --mode step): the workload's domain is widened to N
+copies side by side along x and split into N spatial partitions, one per
+rank (weak scaling: every rank holds the single-GPU workload's elements);
+the ranks exchange the face values of their shared faces once per residual
+over NCCL (frfs's MPI interfaces) and the time is the max over ranks.  With
+--mode collide every rank evaluates its own copy (no exchange).
 
 ``--impl reference`` times the reference's algorithm on the host cores: the
 reference itself is PyCUDA/cuFFT-only (no CPU path) and cannot be imported on
@@ -79,7 +82,10 @@ def _parse():
     return ap.parse_args()
 
 
-def _cfg(args):
+def _cfg(args, world=1):
+    """The workload's config; with world > 1 (partitioned runs) the
+    domain is ``world`` copies of the workload laid side by side along x,
+    one per rank (weak scaling)."""
     from frfs_b200 import workloads
     from frfs_b200.inifile import Inifile
     kw = {}
@@ -87,6 +93,11 @@ def _cfg(args):
         a, b = args.elements
         kw = ({'ntheta': a, 'nr': b} if args.workload.startswith('cylinder')
               else {'nx': a, 'ny': b})
+    if world > 1:
+        if args.workload not in ('couette-n24', 'channel-n32'):
+            raise SystemExit(f'{args.workload}: partitioned runs are set up '
+                             'for couette-n24 and channel-n32')
+        kw['copies'] = world
     cfg = Inifile(workloads.WORKLOADS[args.workload](
         precision=args.precision, **kw))
     cfg.set('spherical-design-rule', 'path', SPHDESIGN)
@@ -94,8 +105,12 @@ def _cfg(args):
     return cfg
 
 
-def _workload_desc(args, cfg, npts):
+def _workload_desc(args, cfg, npts, world=1):
     return {
+        'parallelism': (f'{world} spatial partitions, NCCL face-value halo '
+                        'exchange' if world > 1 and args.mode == 'step'
+                        else f'{world} independent replicas' if world > 1
+                        else 'single GPU'),
         'workload': f'{args.workload}: DGFS fast-spectral VHS Q(f) at every '
                     f'solution point' + (' + FR-DG SSP-RK2 step'
                                          if args.mode == 'step' else ''),
@@ -111,12 +126,13 @@ def _workload_desc(args, cfg, npts):
     }
 
 
-def _points_shape(cfg):
-    """(nupts, neles) of the workload's mesh ((p+1)^2 points per quad)."""
+def _points_shape(cfg, world=1):
+    """(nupts, neles) of the workload's mesh ((p+1)^2 points per quad),
+    per rank when the mesh is split over ``world`` ranks."""
     order = cfg.getint('solver', 'order')
     if cfg.hasopt('mesh', 'nx'):
         neles = cfg.getint('mesh', 'nx')*cfg.getint('mesh', 'ny')
-        return (order + 1)**2, neles
+        return (order + 1)**2, neles//world
     if cfg.hasopt('mesh', 'ntheta'):
         neles = cfg.getint('mesh', 'ntheta')*cfg.getint('mesh', 'nr')
         return (order + 1)**2, neles
@@ -316,6 +332,47 @@ def _max_over_ranks(x, world, device):
     return float(t.item())
 
 
+def _fp64_line(args, stream, flush, fin32):
+    import torch
+    from frfs_b200 import _lib
+    from frfs_b200.backend import B200Backend
+    from frfs_b200.scattering import DGFSVHSGLLScatteringModel
+    from frfs_b200.velocitymesh import DGFSVelocityMesh
+    a = argparse.Namespace(**vars(args))
+    a.precision = 'double'
+    cfg = _cfg(a)
+    be = B200Backend(cfg, device=fin32.backend.device)
+    vm = DGFSVelocityMesh(be, cfg)
+    sm = DGFSVHSGLLScatteringModel(be, cfg, vm)
+    f = fin32.get().astype(np.float64)
+    fin = be.matrix(f.shape, f)
+    fout = be.matrix(f.shape)
+    npts = f.shape[0]*f.shape[2]
+    sm.fs_all(fin, fout)
+    sm.status()
+    ms = float(np.mean(_timed(lambda: sm.fs_all(fin, fout), 3, stream,
+                              flush)))
+    sm.status()
+    tf = _lib.c_double()
+    pms = _lib.ct.c_float()
+    _lib.check(_lib.load().dgfs_probe_fma_peak(
+        64, 1024, _lib.ct.byref(tf), _lib.ct.byref(pms), stream.cuda_stream),
+        'dgfs_probe_fma_peak')
+    achieved = sm.flops_per_point()*npts/(ms*1e-3)/1e12
+    kind = sm.variants()[getattr(sm, '_variant', 0)]['exchange']
+    torch.cuda.synchronize()
+    return {'metric': METRIC, 'value': npts/(ms*1e-3), 'unit': 'evals/s',
+            'dtype': 'f64', 'sweep_ms': ms, 'points': npts,
+            'kernel': {'push': 'vhs_push_kernel',
+                       'pull': 'vhs_cluster_kernel'}.get(kind, kind),
+            'roofline': {'bound': 'fp64-simt', 'achieved': achieved,
+                         'peak': tf.value, 'unit': 'TFLOP/s',
+                         'frac': achieved/tf.value,
+                         'peak_source': 'measured in this run: FP64 FMA '
+                                        'loop on every SM '
+                                        '(dgfs_probe_fma_peak)'}}
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
@@ -333,9 +390,10 @@ def run_b200(args):
     from frfs_b200.scattering import DGFSVHSGLLScatteringModel
     from frfs_b200.velocitymesh import DGFSVelocityMesh
 
-    cfg = _cfg(args)
+    part = world > 1 and args.mode == 'step'
+    cfg = _cfg(args, world if part else 1)
     be = B200Backend(cfg, device=f'cuda:{local}')
-    nupts, neles = _points_shape(cfg)
+    nupts, neles = _points_shape(cfg, world if part else 1)
     npts = nupts*neles
     stream = torch.cuda.current_stream()
     flush = torch.empty(256*1024*1024 // 4, dtype=torch.float32,
@@ -347,14 +405,26 @@ def run_b200(args):
         cfg.set('backend-b200', 'cuda-graphs', int(args.graphs))
         vm0 = DGFSVelocityMesh(None, cfg)
         f0 = _synthetic_f(vm0.cv(), nupts, neles, seed=rank)
-        system = DGFSSystem(be, cfg, initsoln=f0)
+        mesh, prank = None, 0
+        if part:
+            # spatial partitions: rank r runs part r of the widened mesh
+            # and exchanges face values with its neighbours over NCCL
+            from frfs_b200 import mesh as meshmod
+            from frfs_b200 import partition as pt
+            whole = meshmod.from_config(cfg)
+            mesh, _ = pt.partition_mesh(whole, pt.partition_elements(
+                whole['spt_quad_p0'], world))
+            prank = rank
+        system = DGFSSystem(be, cfg, mesh=mesh, prank=prank, initsoln=f0)
         vm, sm = system.vm, system.sm
         stepper = StdTVDRK2DGFSStepper(system, cfg)
         fin, fout = system.bank[0], system.bank[1]
         evals_per_step = 2*npts
-        # per stage: VHS, interp, residual, and the two boundary-sum
-        # kernels when the mesh has boundary flux points
-        launches_per_step = 2*(3 + (2 if len(system.bpts) else 0))
+        # per stage: VHS, interp, residual, the two boundary-sum kernels
+        # when the part has boundary flux points, the pack kernel when it
+        # has faces shared with other parts
+        launches_per_step = 2*(3 + (2 if len(system.bpts) else 0) +
+                               (1 if system.halo is not None else 0))
 
         def step():
             stepper.advance(1)
@@ -488,6 +558,11 @@ def run_b200(args):
             'kernels': 'dg_interp_kernel + dg_residual_kernel'}
     launch = sm.launch_info()
 
+    if rank == 0 and world == 1 and args.precision == 'single':
+        # the FP64 mode on the same points: one collision sweep in full
+        # double precision (the parity mode), against the FP64 FMA peak
+        extra['fp64'] = _fp64_line(args, stream, flush, fin)
+
     sur = None
     want_sur = args.surrogate if args.surrogate >= 0 else int(
         args.workload == 'couette-n24' and world == 1 and
@@ -512,7 +587,7 @@ def run_b200(args):
             'scaling': 'weak', 'vs_baseline': None,
             'dtype': 'f32' if prec == 32 else 'f64',
             'data': 'synthetic',
-            'config': _workload_desc(args, cfg, npts),
+            'config': _workload_desc(args, cfg, npts, world),
             'clocks': clk, 'e2e': e2e,
             'gpu_launches': args.steps*launches_per_step,
             'roofline': roof, 'cpu_baseline': cb,

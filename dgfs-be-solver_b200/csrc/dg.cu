@@ -11,19 +11,23 @@
 using namespace dgfs;
 
 struct dgfs_dg {
-  int prec, D, U, F, V, E, nb, ngroups, device;
+  int prec, D, U, F, V, E, nb, ngroups, device, nhalo, nsend;
   long long ldim_u, ldim_f;
   double cw;
   std::vector<double> m0, m132, m3, m12;  // host copies (operators travel as params)
   void *smats, *rcpdjac, *nrm, *mag, *cvx, *cvy, *cvz, *guw, *gfw, *bwall;
   int *part, *bkind, *bgroup, *bfpt, *bele, *grefl;
-  int64_t* pbase;  // [F][E] partner offsets in the flux bank at v = 0
   double* bcvals;
   double* bcpart;  // [kBcChunks][nb][2] partial wall sums
   void* uf;        // flux-point scratch [F][ldim_f]
+  void* geoblk;    // [nblk][32][GS] per-block geometry rows (T)
+  int64_t* pblk;   // [nblk][32][PS] partner offsets, boundary and halo codes
+  int *sfpt, *sele;  // [nsend] flux point and element of each send row
+  const void* halo;  // caller's [nhalo][V] received values (dgfs_dg_set_halo)
 };
 
 constexpr int kBcChunks = 256;  // velocity chunks of the wall-sum reduction
+constexpr int kVpt = 8;         // velocities per warp in the interp/residual kernels
 
 namespace {
 
@@ -75,6 +79,43 @@ template <typename T> int upload_geom(dgfs_dg* h, const dgfs_dg_params* p) {
   return DGFS_OK;
 }
 
+// Per-block geometry rows of the residual kernel (DgGeo layout): for each
+// element S[k][i][kk] = smats[i][k][kk][e], 1/|J| (zero padded), and
+// |S^T n| n at the flux points; partner codes: the partner's flux-bank
+// offset at v = 0 (interior), -1-b (boundary point b), -1-(nb+h) (halo row
+// h).  Lanes past the last element are zero.
+template <typename T, int U, int F, int D> int build_blocks(dgfs_dg* h, const dgfs_dg_params* p) {
+  using G = DgGeo<T, U, F, D>;
+  const int E = h->E;
+  const size_t nblk = (E + 31) / 32;
+  std::vector<T> g(nblk * 32 * G::GS, T(0));
+  std::vector<int64_t> pb(nblk * 32 * G::PS, 0);
+  for (int e = 0; e < E; ++e) {
+    T* row = g.data() + (size_t)e * G::GS;
+    for (int k = 0; k < U; ++k)
+      for (int i = 0; i < D; ++i)
+        for (int kk = 0; kk < D; ++kk)
+          row[G::OS + (k * D + i) * D + kk] = (T)p->smats[(((size_t)i * U + k) * D + kk) * E + e];
+    for (int k = 0; k < U; ++k) row[G::OR + k] = (T)p->rcpdjac[(size_t)k * E + e];
+    for (int f = 0; f < F; ++f)
+      for (int d = 0; d < D; ++d)
+        row[G::ON + f * D + d] = (T)(p->mag[(size_t)f * E + e] * p->nrm[((size_t)f * D + d) * E + e]);
+    int64_t* prow = pb.data() + (size_t)e * G::PS;
+    for (int f = 0; f < F; ++f) {
+      const int q = p->partner[(size_t)f * E + e];
+      prow[f] = q >= 0 ? (int64_t)(q / E) * h->ldim_f + (int64_t)((q % E) >> 5) * h->V * 32 + ((q % E) & 31)
+                       : (int64_t)q;
+    }
+  }
+  if (cudaMalloc(&h->geoblk, g.size() * sizeof(T)) != cudaSuccess ||
+      cudaMalloc((void**)&h->pblk, pb.size() * sizeof(int64_t)) != cudaSuccess)
+    return set_error(DGFS_ERR_NOMEM, "block geometry allocation failed");
+  if (cudaMemcpy(h->geoblk, g.data(), g.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(h->pblk, pb.data(), pb.size() * sizeof(int64_t), cudaMemcpyHostToDevice) != cudaSuccess)
+    return set_error(DGFS_ERR_CUDA, "block geometry upload: %s", cudaGetErrorString(cudaGetLastError()));
+  return DGFS_OK;
+}
+
 template <typename T> DgArgs<T> make_args(const dgfs_dg* h) {
   DgArgs<T> a{};
   a.V = h->V;
@@ -87,7 +128,6 @@ template <typename T> DgArgs<T> make_args(const dgfs_dg* h) {
   a.nrm = (const T*)h->nrm;
   a.mag = (const T*)h->mag;
   a.part = h->part;
-  a.pbase = h->pbase;
   a.cvx = (const T*)h->cvx;
   a.cvy = (const T*)h->cvy;
   a.cvz = (const T*)h->cvz;
@@ -98,6 +138,10 @@ template <typename T> DgArgs<T> make_args(const dgfs_dg* h) {
   a.grefl = h->grefl;
   a.bwall = (const T*)h->bwall;
   a.bcvals = h->bcvals;
+  a.nb = h->nb;
+  a.geoblk = (const T*)h->geoblk;
+  a.pblk = h->pblk;
+  a.halo = (const T*)h->halo;
   return a;
 }
 
@@ -124,13 +168,18 @@ inline unsigned grid_for(const dgfs_dg* h, int nv) {
   return (unsigned)((nblk * nv * 32 + 255) / 256);
 }
 
+// (element block, velocity chunk of 8 * kVpt) grid of the interp/residual
+inline dim3 grid_blk(const dgfs_dg* h, int nv) {
+  return dim3((unsigned)((h->E + 31) / 32), (unsigned)((nv + 8 * kVpt - 1) / (8 * kVpt)));
+}
+
 template <typename T, int U, int F, int D>
 cudaError_t run_interp(const dgfs_dg* h, const void* u, int v0, int nv, cudaStream_t s) {
   DgArgs<T> a = make_args<T>(h);
   a.u = (const T*)u;
   a.v0 = v0;
   a.nv = nv;
-  dg_interp_kernel<T, U, F, D><<<grid_for(h, nv), 256, 0, s>>>(a, make_ops<T, U, F, D>(h));
+  dg_interp_kernel<T, U, F, D, kVpt><<<grid_blk(h, nv), 256, 0, s>>>(a, make_ops<T, U, F, D>(h));
   return cudaGetLastError();
 }
 
@@ -148,7 +197,7 @@ cudaError_t run_rhs(const dgfs_dg* h, const void* u, void* out, int v0, int nv, 
   a.gamma = (T)gamma;
   a.v0 = v0;
   a.nv = nv;
-  dg_residual_kernel<T, U, F, D><<<grid_for(h, nv), 256, 0, s>>>(a, make_ops<T, U, F, D>(h));
+  dg_residual_kernel<T, U, F, D, kVpt><<<grid_blk(h, nv), 256, 0, s>>>(a, make_ops<T, U, F, D>(h));
   return cudaGetLastError();
 }
 
@@ -201,8 +250,8 @@ int check_range(const dgfs_dg* h, int v0, int nv) {
 void free_dg(dgfs_dg* h) {
   if (!h) return;
   void* ptrs[] = {h->smats, h->rcpdjac, h->nrm, h->mag, h->cvx, h->cvy, h->cvz, h->guw, h->gfw, h->bwall,
-                  h->part, h->pbase, h->bkind, h->bgroup, h->bfpt, h->bele, h->grefl, h->bcvals, h->bcpart,
-                  h->uf};
+                  h->part, h->bkind, h->bgroup, h->bfpt, h->bele, h->grefl, h->bcvals, h->bcpart,
+                  h->uf, h->geoblk, h->pblk, h->sfpt, h->sele};
   for (void* q : ptrs) cudaFree(q);
   delete h;
 }
@@ -228,11 +277,16 @@ extern "C" int dgfs_dg_create(const dgfs_dg_params* p, dgfs_dg** out) {
     return set_error(DGFS_ERR_INVALID, "bad boundary description");
   if (p->ngroups && (!p->guw || !p->gfw)) return set_error(DGFS_ERR_INVALID, "null boundary group data");
   const int U = p->nupts, F = p->nfpts, D = p->ndims, E = p->neles;
+  if (p->nhalo < 0 || p->nsend < 0 || (p->nsend && (!p->sfpt || !p->sele)))
+    return set_error(DGFS_ERR_INVALID, "bad partition halo description");
   for (int i = 0; i < F * E; ++i) {
     const int q = p->partner[i];
-    if (q >= 0 ? (long long)q >= (long long)F * E : (-q - 1) >= p->nbfpts)
+    if (q >= 0 ? (long long)q >= (long long)F * E : (long long)(-(long long)q - 1) >= (long long)p->nbfpts + p->nhalo)
       return set_error(DGFS_ERR_INVALID, "partner entry %d = %d out of range", i, q);
   }
+  for (int s = 0; s < p->nsend; ++s)
+    if (p->sfpt[s] < 0 || p->sfpt[s] >= F || p->sele[s] < 0 || p->sele[s] >= E)
+      return set_error(DGFS_ERR_INVALID, "bad send row %d", s);
   for (int b = 0; b < p->nbfpts; ++b) {
     if (p->bkind[b] < 0 || p->bkind[b] > BC_WALL_DIFFUSE_CYL) return set_error(DGFS_ERR_INVALID, "bad boundary kind");
     if (p->bkind[b] == BC_WALL_DIFFUSE_CYL && (!p->bwall || !(p->bwall[4 * b + 3] > 0.0)))
@@ -256,6 +310,8 @@ extern "C" int dgfs_dg_create(const dgfs_dg_params* p, dgfs_dg** out) {
   h->E = E;
   h->nb = p->nbfpts;
   h->ngroups = p->ngroups;
+  h->nhalo = p->nhalo;
+  h->nsend = p->nsend;
   h->ldim_u = p->ldim;
   h->cw = p->cw;
   h->m0.assign(p->m0, p->m0 + F * U);
@@ -270,16 +326,15 @@ extern "C" int dgfs_dg_create(const dgfs_dg_params* p, dgfs_dg** out) {
   if (!rc) rc = h->prec == 64 ? upload_geom<double>(h, p) : upload_geom<float>(h, p);
   if (!rc) rc = upload_int(&h->part, p->partner, (size_t)F * E);
   if (!rc) {
-    // partner offsets in the flux bank at v = 0: fr ldim_f + (er/32) V 32 + er%32
-    std::vector<int64_t> pb((size_t)F * E);
-    for (size_t i = 0; i < pb.size(); ++i) {
-      const int q = p->partner[i];
-      pb[i] = q < 0 ? -1
-                    : (int64_t)(q / E) * h->ldim_f + (int64_t)((q % E) >> 5) * h->V * 32 + ((q % E) & 31);
-    }
-    if (cudaMalloc((void**)&h->pbase, pb.size() * sizeof(int64_t)) != cudaSuccess ||
-        cudaMemcpy(h->pbase, pb.data(), pb.size() * sizeof(int64_t), cudaMemcpyHostToDevice) != cudaSuccess)
-      rc = set_error(DGFS_ERR_NOMEM, "partner offset upload failed");
+#define CALL(P, U_, F_, D_) rc = build_blocks<P, U_, F_, D_>(h, p)
+    if (h->prec == 64)
+      DG_DISPATCH(double, CALL);
+    else
+      DG_DISPATCH(float, CALL);
+#undef CALL
+  }
+  if (!rc && h->nsend) {
+    if ((rc = upload_int(&h->sfpt, p->sfpt, h->nsend)) == DGFS_OK) rc = upload_int(&h->sele, p->sele, h->nsend);
   }
   const int nb = h->nb ? h->nb : 1;
   std::vector<int> zeros(nb, 0);
@@ -374,6 +429,7 @@ extern "C" int dgfs_dg_rhs(dgfs_dg* h, const void* u, void* out, int v0, int nv,
   if (!rc) rc = check_range(h, v0, nv);
   if (rc) return rc;
   if (out == u) return set_error(DGFS_ERR_INVALID, "output bank must differ from the solution bank");
+  if (h->nhalo && !h->halo) return set_error(DGFS_ERR_INVALID, "partition faces without a halo buffer (dgfs_dg_set_halo)");
   if (!std::isfinite(alpha) || !std::isfinite(beta) || !std::isfinite(gamma))
     return set_error(DGFS_ERR_INVALID, "non-finite combination coefficient");
   cudaError_t e = cudaSuccess;
@@ -404,6 +460,35 @@ extern "C" int dgfs_dg_invmass(dgfs_dg* h, const void* u, void* out, int v0, int
     DG_DISPATCH(float, CALL);
 #undef CALL
   if (e != cudaSuccess) return set_error(DGFS_ERR_CUDA, "DG invmass launch: %s", cudaGetErrorString(e));
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_dg_pack(dgfs_dg* h, void* send, void* stream) {
+  clear_error();
+  if (!h) return set_error(DGFS_ERR_INVALID, "null handle");
+  if (!h->nsend) return DGFS_OK;
+  int rc = check_bank(h, send, "send");
+  if (rc) return rc;
+  const long long n = (long long)h->nsend * h->V;
+  const unsigned grid = (unsigned)((n + 255) / 256);
+  if (h->prec == 64)
+    dg_pack_kernel<double><<<grid, 256, 0, (cudaStream_t)stream>>>((const double*)h->uf, h->ldim_f, h->V, h->sfpt,
+                                                                    h->sele, h->nsend, (double*)send);
+  else
+    dg_pack_kernel<float><<<grid, 256, 0, (cudaStream_t)stream>>>((const float*)h->uf, h->ldim_f, h->V, h->sfpt,
+                                                                   h->sele, h->nsend, (float*)send);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(DGFS_ERR_CUDA, "DG pack launch: %s", cudaGetErrorString(e));
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_dg_set_halo(dgfs_dg* h, const void* recv) {
+  clear_error();
+  if (!h) return set_error(DGFS_ERR_INVALID, "null handle");
+  if (h->nhalo && !recv) return set_error(DGFS_ERR_INVALID, "null halo buffer");
+  int rc = recv ? check_bank(h, recv, "halo") : DGFS_OK;
+  if (rc) return rc;
+  h->halo = recv;
   return DGFS_OK;
 }
 

@@ -1,21 +1,32 @@
 // FR-DG advection residual over all discrete velocities.
 //
-// One thread per (velocity v, element e); a warp covers the 32 elements of
-// one AoSoA block at one velocity, so every bank access is a coalesced
-// 32-element row.  The element operators travel in the kernel parameters
-// (constant bank) and every loop over them is unrolled, so matrix entries are
-// FMA operands, not loads.
+// Banks are frfs's AoSoA(32) layout: value (row i, velocity v, element e) at
+// i*ldim + ((e/32)*V + v)*32 + e%32, so the 32 elements of one block at one
+// velocity form one coalesced 128-byte row.  A CTA of 256 threads takes one
+// 32-element block (lane = element) and a chunk of 8*VPT velocities (warp w
+// takes v = chunk + 8*it + w): consecutive warps read consecutive rows.  The
+// element operators travel in the kernel parameters (constant bank) and every
+// loop over them is unrolled, so matrix entries are FMA operands, not loads.
+// The residual stages the block's element geometry (metric terms, 1/|J|,
+// scaled normals, partner offsets) in shared memory once per CTA, one row of
+// GS values per lane read with 16-byte loads, and reuses it for every
+// velocity of the chunk.
 //
 //   dg_interp_kernel    uf = M0 u at the flux points (frfs/solvers/dgfs/
 //                        elements.py:55-59, 'disu')
 //   dg_bcsum_kernel     diffuse-wall sums over velocities in FP64
 //                        (kernels/bcs/dgfs-wall-diffuse-update.mako:14-36)
 //   dg_residual_kernel  R = -(1/|J|)[(M1 - M3 M2) F~ + M3 F^] with the upwind
-//                        common flux at every flux point (interfaces and
-//                        boundaries), fused with the Runge-Kutta combination
+//                        common flux at every flux point (interfaces,
+//                        boundaries and faces shared with another partition),
+//                        fused with the Runge-Kutta combination
 //                        out = a A + b B + g (R + C)
 //                        (elements.py:49-118, intcflux.mako, bccflux.mako,
-//                        rusanov.mako:46-50, negdivconf.mako, axnpby.mako)
+//                        mpicflux.mako, rusanov.mako:46-50, negdivconf.mako,
+//                        axnpby.mako)
+//   dg_pack_kernel      face values at the flux points on partition faces
+//                        into a send buffer (the 'pack' kernel of frfs's MPI
+//                        interfaces, inters.py:61-112)
 #pragma once
 
 #include "dgfs_common.cuh"
@@ -54,7 +65,6 @@ template <typename T> struct DgArgs {
   const T* nrm;            // [F][D][E] unit outward normals
   const T* mag;            // [F][E]    |S^T n|
   const int* part;         // [F][E]    fpt_r*E + e_r, or -(b+1) for boundary b
-  const int64_t* pbase;    // [F][E]    partner's flux-bank offset at v = 0 (-1: boundary)
   const T* cvx;            // [V] velocity grid
   const T* cvy;
   const T* cvz;
@@ -66,6 +76,29 @@ template <typename T> struct DgArgs {
   const int* grefl;        // [ngroups][V]
   const T* bwall;          // [nb][4] wall Ux, Uy, Uz, T per boundary point (cylinder wall)
   const double* bcvals;    // [nb][2]
+  int nb;                  // boundary flux points
+  // per element block: geometry rows [nblk][32][GS] and partner offsets
+  // [nblk][32][PS] (>= 0: flux-bank offset of the partner at v = 0;
+  // -1-b: boundary point b < nb; -1-(nb+h): row h of the halo)
+  const T* geoblk;
+  const int64_t* pblk;
+  const T* halo;           // [nhalo][V] partner face values from other partitions
+};
+
+// Shared-memory row of one element (T values): metric terms S[k][i][kk]
+// (k-major, D*D per solution point), 1/|J| (padded to a 16-byte multiple),
+// |S^T n| n at the flux points [F][D]; GS pads the row so that the 16-byte
+// loads of 8 consecutive lanes fall in distinct bank quads.  Partner offsets
+// [F] int64 per lane, padded to PS likewise.
+template <typename T, int U, int F, int D> struct DgGeo {
+  static constexpr int VW = 16 / (int)sizeof(T);
+  static constexpr int OS = 0, NS = U * D * D;
+  static constexpr int OR = NS, NR = ((U + VW - 1) / VW) * VW;
+  static constexpr int ON = OR + NR, NN = F * D;
+  static constexpr int G = ON + NN;
+  static constexpr int GS = sizeof(T) == 4 ? G + ((4 - G % 8) + 8) % 8 : G + ((2 - G % 4) + 4) % 4;
+  static constexpr int PS = F + ((2 - F % 4) + 4) % 4;
+  static_assert(NS % VW == 0 && NN % VW == 0, "16-byte sections");
 };
 
 template <typename T, int U> struct DgMassOps {
@@ -76,23 +109,30 @@ __device__ __forceinline__ int64_t aos32(int64_t row, int64_t ldim, int64_t e, i
   return row * ldim + ((e >> 5) * V + v) * 32 + (e & 31);
 }
 
-template <typename T, int U, int F, int D>
+template <typename T, int U, int F, int D, int VPT>
 __global__ void __launch_bounds__(256) dg_interp_kernel(const DgArgs<T> a, const DgOps<T, U, F, D> op) {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int lane = (int)(t & 31);
-  const int64_t w = t >> 5;
-  const int v = a.v0 + (int)(w % a.nv);
-  const int64_t e = (w / a.nv) * 32 + lane;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t e = (int64_t)blockIdx.x * 32 + lane;
   if (e >= a.neles) return;
-  T u[U];
+  const int vend = a.v0 + a.nv;
+  const int vbeg = a.v0 + (int)blockIdx.y * (8 * VPT) + w;
+#pragma unroll 1
+  for (int it = 0; it < VPT; ++it) {
+    const int v = vbeg + 8 * it;
+    if (v >= vend) break;
+    const int64_t o = ((int64_t)blockIdx.x * a.V + v) * 32 + lane;
+    T u[U];
+    const T* up = a.u + o;
 #pragma unroll
-  for (int i = 0; i < U; ++i) u[i] = a.u[aos32(i, a.ldim_u, e, v, a.V)];
+    for (int i = 0; i < U; ++i, up += a.ldim_u) u[i] = __ldg(up);
+    T* fp = a.uf + o;
 #pragma unroll
-  for (int f = 0; f < F; ++f) {
-    T s = T(0);
+    for (int f = 0; f < F; ++f, fp += a.ldim_f) {
+      T s = T(0);
 #pragma unroll
-    for (int i = 0; i < U; ++i) s = fma(op.m0[f][i], u[i], s);
-    a.uf[aos32(f, a.ldim_f, e, v, a.V)] = s;
+      for (int i = 0; i < U; ++i) s = fma(op.m0[f][i], u[i], s);
+      *fp = s;
+    }
   }
 }
 
@@ -202,118 +242,189 @@ __global__ void __launch_bounds__(256) dg_bcsum_finish_kernel(const int* __restr
   }
 }
 
-// FP32 up to p = 2: 4 CTAs per SM (<= 64 registers; measured 0.132 ms per
-// Couette stage against 0.145 ms at 2 CTAs per SM): the kernel is bound by
-// the latency of its partner loads, issued together up front from
-// precomputed offsets.  p = 3 (16 solution and flux points) holds too many
-// values for 64 registers: no occupancy bound there.
-template <typename T, int U, int F, int D>
-__global__ void __launch_bounds__(256, (sizeof(T) == 4 && U <= 9) ? 4 : 1) dg_residual_kernel(const DgArgs<T> a, const DgOps<T, U, F, D> op) {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int lane = (int)(t & 31);
-  const int64_t w = t >> 5;
-  const int v = a.v0 + (int)(w % a.nv);
-  const int64_t e = (w / a.nv) * 32 + lane;
-  if (e >= a.neles) return;
-  const int64_t E = a.neles;
+template <typename T> struct Vec16;
+template <> struct Vec16<float> { using type = float4; };
+template <> struct Vec16<double> { using type = double2; };
 
-  T u[U];
+// n 16-byte loads from shared memory into r[0 .. n*VW)
+template <typename T, int N> __device__ __forceinline__ void lds16(const T* src, T* r) {
+  using V4 = typename Vec16<T>::type;
+  constexpr int VW = 16 / (int)sizeof(T);
 #pragma unroll
-  for (int i = 0; i < U; ++i) u[i] = a.u[aos32(i, a.ldim_u, e, v, a.V)];
-  const T c[3] = {a.cvx[v], a.cvy[v], a.cvz[v]};
-
-  // partner values first: every load independent of the others, so their
-  // latencies overlap (offsets precomputed per (flux point, element))
-  T urv[F];
-#pragma unroll
-  for (int f = 0; f < F; ++f) {
-    const int64_t pb = a.pbase[(int64_t)f * E + e];
-    urv[f] = pb >= 0 ? a.uf[pb + (int64_t)v * 32] : T(0);
-  }
-
-  // common normal fluxes at this element's flux points
-  T fh[F];
-#pragma unroll
-  for (int f = 0; f < F; ++f) {
-    T ul = T(0);
-#pragma unroll
-    for (int i = 0; i < U; ++i) ul = fma(op.m0[f][i], u[i], ul);
-    T n[D];
-#pragma unroll
-    for (int d = 0; d < D; ++d) n[d] = a.nrm[((int64_t)f * D + d) * E + e];
-    T nc = n[0] * c[0];
-#pragma unroll
-    for (int d = 1; d < D; ++d) nc = fma(n[d], c[d], nc);
-    const int p = a.part[(int64_t)f * E + e];
-    T ur;
-    if (p >= 0) {
-      ur = urv[f];
+  for (int j = 0; j < N; ++j) {
+    const V4 q = reinterpret_cast<const V4*>(src)[j];
+    if constexpr (VW == 4) {
+      r[4 * j] = q.x; r[4 * j + 1] = q.y; r[4 * j + 2] = q.z; r[4 * j + 3] = q.w;
     } else {
-      const int b = -p - 1;
-      const int kind = a.bkind[b], g = a.bgroup[b];
-      if (kind == BC_WALL_DIFFUSE || kind == BC_INLET) {
-        T fac = (c[0] - a.guw[g * 3]) * n[0];
+      r[2 * j] = q.x; r[2 * j + 1] = q.y;
+    }
+  }
+}
+
+// Ghost value of boundary point b at velocity v (bccflux.mako with the
+// bcs/*.mako kinds); nmv = |S^T n| n, whose sign tests equal the unit
+// normal's; ul the interior face value.
+template <typename T, int D>
+__device__ __forceinline__ T dg_ghost(const DgArgs<T>& a, int b, int v, int64_t e, int f, const T* c, const T* nmv,
+                                   T nc, T ul) {
+  const int kind = a.bkind[b], g = a.bgroup[b];
+  if (kind == BC_WALL_DIFFUSE || kind == BC_INLET) {
+    T fac = (c[0] - a.guw[g * 3]) * nmv[0];
 #pragma unroll
-        for (int d = 1; d < D; ++d) fac = fma(c[d] - a.guw[g * 3 + d], n[d], fac);
-        if (fac < T(0)) {
-          const T fw = a.gfw[(int64_t)g * a.V + v];
-          ur = kind == BC_INLET ? fw : fw * (T)(-a.bcvals[2 * b] / a.bcvals[2 * b + 1]);
-        } else {
-          ur = ul;
-        }
-      } else if (kind == BC_WALL_DIFFUSE_CYL) {
-        // bcs/dgfs-wall-diffuse-cyl.mako: wall state of this boundary point
-        const T* w = a.bwall + (int64_t)b * 4;
-        const T dc[3] = {c[0] - w[0], c[1] - w[1], c[2] - w[2]};
-        T fac = dc[0] * n[0];
+    for (int d = 1; d < D; ++d) fac = fma(c[d] - a.guw[g * 3 + d], nmv[d], fac);
+    if (fac < T(0)) {
+      const T fw = a.gfw[(int64_t)g * a.V + v];
+      return kind == BC_INLET ? fw : fw * (T)(-a.bcvals[2 * b] / a.bcvals[2 * b + 1]);
+    }
+    return ul;
+  }
+  if (kind == BC_WALL_DIFFUSE_CYL) {
+    // bcs/dgfs-wall-diffuse-cyl.mako: wall state of this boundary point
+    const T* w = a.bwall + (int64_t)b * 4;
+    const T dc[3] = {c[0] - w[0], c[1] - w[1], c[2] - w[2]};
+    T fac = dc[0] * nmv[0];
 #pragma unroll
-        for (int d = 1; d < D; ++d) fac = fma(dc[d], n[d], fac);
-        if (fac < T(0)) {
-          const T mx = exp(-(dc[0] * dc[0] + dc[1] * dc[1] + dc[2] * dc[2]) / w[3]);
-          ur = mx * (T)(-a.bcvals[2 * b] / a.bcvals[2 * b + 1]);
-        } else {
-          ur = ul;
+    for (int d = 1; d < D; ++d) fac = fma(dc[d], nmv[d], fac);
+    if (fac < T(0)) {
+      const T mx = exp(-(dc[0] * dc[0] + dc[1] * dc[1] + dc[2] * dc[2]) / w[3]);
+      return mx * (T)(-a.bcvals[2 * b] / a.bcvals[2 * b + 1]);
+    }
+    return ul;
+  }
+  if (kind == BC_VANISH) return nc < T(0) ? T(0) : ul;
+  if (kind == BC_WALL_SPECULAR) {
+    const int vr = a.grefl[(int64_t)g * a.V + v];
+    return a.uf[aos32(f, a.ldim_f, e, vr, a.V)];
+  }
+  return ul;  // outlet
+}
+
+// FP32 up to p = 2 holds its working set in 80 registers (3 CTAs of 256 per
+// SM), FP32 p = 3 and FP64 up to p = 2 in 128 (2 per SM), FP64 p = 3 in 160.
+template <typename T, int U, int F, int D, int VPT>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? (U <= 9 ? 3 : 2) : (U <= 9 ? 2 : 1))
+    dg_residual_kernel(const DgArgs<T> a, const DgOps<T, U, F, D> op) {
+  using G = DgGeo<T, U, F, D>;
+  __shared__ __align__(16) T sg[32 * G::GS];
+  __shared__ __align__(16) int64_t sp[32 * G::PS];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  {
+    const T* gs = a.geoblk + (size_t)blockIdx.x * 32 * G::GS;
+    for (int i = threadIdx.x; i < 32 * G::GS; i += 256) sg[i] = gs[i];
+    const int64_t* ps = a.pblk + (size_t)blockIdx.x * 32 * G::PS;
+    for (int i = threadIdx.x; i < 32 * G::PS; i += 256) sp[i] = ps[i];
+  }
+  __syncthreads();
+  const int64_t e = (int64_t)blockIdx.x * 32 + lane;
+  if (e >= a.neles) return;
+  const T* gl = sg + lane * G::GS;
+  const int64_t* pl = sp + lane * G::PS;
+  const int vend = a.v0 + a.nv;
+  const int vbeg = a.v0 + (int)blockIdx.y * (8 * VPT) + w;
+
+#pragma unroll 1
+  for (int it = 0; it < VPT; ++it) {
+    const int v = vbeg + 8 * it;
+    if (v >= vend) break;
+    const int64_t o = ((int64_t)blockIdx.x * a.V + v) * 32 + lane;
+
+    // every bank value of this (v, e) first, so the loads overlap
+    T u[U];
+    {
+      const T* up = a.u + o;
+#pragma unroll
+      for (int i = 0; i < U; ++i, up += a.ldim_u) u[i] = __ldg(up);
+    }
+    T urv[F];
+#pragma unroll
+    for (int f = 0; f < F; f += 2) {
+      const longlong2 pb = reinterpret_cast<const longlong2*>(pl)[f / 2];
+      urv[f] = pb.x >= 0 ? a.uf[pb.x + (int64_t)v * 32] : T(0);
+      if (f + 1 < F) urv[f + 1] = pb.y >= 0 ? a.uf[pb.y + (int64_t)v * 32] : T(0);
+    }
+    const T c[3] = {__ldg(a.cvx + v), __ldg(a.cvy + v), __ldg(a.cvz + v)};
+
+    // R = (M1 - M3 M2) F~ + M3 F^, accumulated term by term so that only
+    // the U partial sums and u stay live
+    T R[U];
+#pragma unroll
+    for (int r = 0; r < U; ++r) R[r] = T(0);
+
+    // common normal fluxes |S^T n| F^ at this element's flux points
+    {
+      T nm[G::NN];
+#pragma unroll
+      for (int f = 0; f < F; ++f) {
+        // scaled normals fetched where first used (16 bytes at a time)
+        if ((f * D) % G::VW == 0) lds16<T, 1>(gl + G::ON + f * D, nm + f * D);
+        T ul = T(0);
+#pragma unroll
+        for (int i = 0; i < U; ++i) ul = fma(op.m0[f][i], u[i], ul);
+        const T* nmv = nm + f * D;
+        T nc = nmv[0] * c[0];
+#pragma unroll
+        for (int d = 1; d < D; ++d) nc = fma(nmv[d], c[d], nc);
+        T ur = urv[f];
+        const int64_t pb = pl[f];
+        if (pb < 0) {
+          const int b = (int)(-pb - 1);
+          ur = b >= a.nb ? a.halo[(int64_t)(b - a.nb) * a.V + v] : dg_ghost<T, D>(a, b, v, e, f, c, nmv, nc, ul);
         }
-      } else if (kind == BC_VANISH) {
-        ur = nc < T(0) ? T(0) : ul;
-      } else if (kind == BC_WALL_SPECULAR) {
-        const int vr = a.grefl[(int64_t)g * a.V + v];
-        ur = a.uf[aos32(f, a.ldim_f, e, vr, a.V)];
-      } else {
-        ur = ul;  // outlet
+        // upwind flux (rusanov.mako:46-50) with the scaled normal
+        const T fh = T(0.5) * nc * (ul + ur) + T(0.5) * fabs(nc) * (ul - ur);
+#pragma unroll
+        for (int r = 0; r < U; ++r) R[r] = fma(op.m3[r][f], fh, R[r]);
       }
     }
-    // upwind flux 0.5 (n.c)(ul + ur) + 0.5 |n.c| (ul - ur)  (rusanov.mako:46-50)
-    const T fn = T(0.5) * nc * (ul + ur) + T(0.5) * fabs(nc) * (ul - ur);
-    fh[f] = a.mag[(int64_t)f * E + e] * fn;
-  }
 
-  // transformed flux at the solution points F~_i = sum_k S_ik c_k u
-  T ft[D * U];
+    // transformed flux at the solution points F~_(i,k) = (sum_kk S_ik,kk c_kk) u_k
+    {
+      T sm[G::NS];
 #pragma unroll
-  for (int i = 0; i < D; ++i)
+      for (int k = 0; k < U; ++k)
 #pragma unroll
-    for (int k = 0; k < U; ++k) {
-      T s = T(0);
+        for (int i = 0; i < D; ++i) {
+          if (((k * D + i) * D) % G::VW == 0) lds16<T, 1>(gl + G::OS + (k * D + i) * D, sm + (k * D + i) * D);
+          T s = T(0);
 #pragma unroll
-      for (int kk = 0; kk < D; ++kk) s = fma(a.smats[(((int64_t)i * U + k) * D + kk) * E + e], c[kk], s);
-      ft[i * U + k] = s * u[k];
+          for (int kk = 0; kk < D; ++kk) s = fma(sm[(k * D + i) * D + kk], c[kk], s);
+          const T ft = s * u[k];
+#pragma unroll
+          for (int r = 0; r < U; ++r) R[r] = fma(op.m132[r][i * U + k], ft, R[r]);
+        }
     }
 
+    T rj[G::NR];
+    lds16<T, G::NR / G::VW>(gl + G::OR, rj);
+    const T* ap = a.A ? a.A + o : nullptr;
+    const T* bp = a.B ? a.B + o : nullptr;
+    const T* cp = a.Cq ? a.Cq + o : nullptr;
+    T* op_ = a.out + o;
 #pragma unroll
-  for (int r = 0; r < U; ++r) {
-    T s = T(0);
-#pragma unroll
-    for (int j = 0; j < D * U; ++j) s = fma(op.m132[r][j], ft[j], s);
-#pragma unroll
-    for (int f = 0; f < F; ++f) s = fma(op.m3[r][f], fh[f], s);
-    const T R = -a.rcpdjac[(int64_t)r * E + e] * s;
-    const int64_t o = aos32(r, a.ldim_u, e, v, a.V);
-    T res = a.gamma * (a.Cq ? R + a.Cq[o] : R);
-    if (a.A) res = fma(a.alpha, a.A[o], res);
-    if (a.B) res = fma(a.beta, a.B[o], res);
-    a.out[o] = res;
+    for (int r = 0; r < U; ++r) {
+      const T Rr = -rj[r] * R[r];
+      T res = a.gamma * (cp ? Rr + __ldg(cp) : Rr);
+      if (ap) res = fma(a.alpha, __ldg(ap), res);
+      if (bp) res = fma(a.beta, __ldg(bp), res);
+      *op_ = res;
+      op_ += a.ldim_u;
+      if (ap) ap += a.ldim_u;
+      if (bp) bp += a.ldim_u;
+      if (cp) cp += a.ldim_u;
+    }
   }
+}
+
+// send[s][v] = uf[sfpt[s]][v][sele[s]] for every velocity: the face values a
+// neighbouring partition needs, one row per shared flux point.
+template <typename T>
+__global__ void __launch_bounds__(256) dg_pack_kernel(const T* __restrict__ uf, int64_t ldim_f, int V,
+                                                     const int* __restrict__ sfpt, const int* __restrict__ sele,
+                                                     int nsend, T* __restrict__ send) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)nsend * V) return;
+  const int s = (int)(t / V), v = (int)(t % V);
+  send[t] = uf[aos32(sfpt[s], ldim_f, sele[s], v, V)];
 }
 
 }  // namespace dgfs

@@ -35,7 +35,10 @@ class BaseDGFSStepper:
         self.tcurr = cfg.getfloat(sect, 'tstart', 0.0)
         self.tend = cfg.getfloat(sect, 'tend', self.tcurr)
         self.nacptsteps = 0
-        self.use_graphs = cfg.getint('backend-b200', 'cuda-graphs', 0) == 1
+        # a partitioned system exchanges face values with torch.distributed
+        # point-to-point calls inside every stage; those stages run eagerly
+        self.use_graphs = (cfg.getint('backend-b200', 'cuda-graphs', 0) == 1
+                           and getattr(system, 'halo', None) is None)
         self._graphs = {}
         self._idxcurr = 0
         if len(system.bank) < self.nregs:

@@ -48,7 +48,8 @@ class DgParams(ct.Structure):
                 ('nbfpts', c_int), ('bkind', c_ip), ('bgroup', c_ip),
                 ('bfpt', c_ip), ('bele', c_ip), ('ngroups', c_int),
                 ('guw', c_dp), ('gfw', c_dp), ('grefl', c_ip),
-                ('bwall', c_dp), ('m12', c_dp)]
+                ('bwall', c_dp), ('m12', c_dp), ('nhalo', c_int),
+                ('nsend', c_int), ('sfpt', c_ip), ('sele', c_ip)]
 
 
 _lib.declare('dgfs_dg_create', c_int, [ct.POINTER(DgParams),
@@ -63,6 +64,8 @@ _lib.declare('dgfs_dg_rhs', c_int, [c_void_p, c_void_p, c_void_p, c_int,
                                     c_void_p, c_double, c_void_p, c_void_p])
 _lib.declare('dgfs_dg_invmass', c_int, [c_void_p, c_void_p, c_void_p, c_int,
                                         c_int, c_void_p])
+_lib.declare('dgfs_dg_pack', c_int, [c_void_p, c_void_p, c_void_p])
+_lib.declare('dgfs_dg_set_halo', c_int, [c_void_p, c_void_p])
 _lib.declare('dgfs_dg_bcvals', c_int, [c_void_p, c_dp, c_int])
 _lib.declare('dgfs_dg_fpts', c_int, [c_void_p, ct.POINTER(c_void_p),
                                      ct.POINTER(c_ll)])
@@ -99,14 +102,22 @@ class DGFSSystem:
     name = 'dgfs'
 
     def __init__(self, backend, cfg, mesh=None, nreg=3, initsoln=None,
-                 sphdesign_paths=None):
+                 sphdesign_paths=None, prank=0, halo_exchange=None):
+        """``mesh`` in frfs's dictionary form, whole (keys ``*_p0``) or
+        partitioned (``frfs_b200.partition.partition_mesh``), of which this
+        system runs part ``prank``.  A part with faces shared with other
+        parts exchanges their face values once per residual through
+        ``halo_exchange(send, recv, nbrs, counts)`` (default:
+        ``partition.exchange`` over torch.distributed, ranks = parts)."""
         self.backend = backend
         self.cfg = cfg
         self.vm = vm = DGFSVelocityMesh(backend, cfg, sphdesign_paths)
         self.mesh = mesh if mesh is not None else meshmod.from_config(cfg)
+        self.prank = int(prank)
+        self._sfx = f'_p{self.prank}'
         order = cfg.getint('solver', 'order')
         self.shape = sh = QuadShape(order)
-        spt = self.mesh['spt_quad_p0']
+        spt = self.mesh['spt_quad' + self._sfx]
         self.geo = geo = ElementGeometry(sh, spt)
         self.ndims = 2
         self.neles, self.nupts, self.nfpts = geo.neles, sh.nupts, sh.nfpts
@@ -137,6 +148,7 @@ class DGFSSystem:
 
         self.surrogate = None
         self.collide_hook = None
+        self.halo_exchange = halo_exchange
         self._build_dg()
 
     # -- DG handle ----------------------------------------------------------
@@ -144,7 +156,7 @@ class DGFSSystem:
         sh, geo, vm, cfg = self.shape, self.geo, self.vm, self.cfg
         E, F, V = self.neles, self.nfpts, vm.vsize()
         part = np.full((F, E), np.iinfo(np.int32).min, dtype=np.int64)
-        lhs, rhs = self.mesh['con_p0']
+        lhs, rhs = self.mesh['con' + self._sfx]
         srtd = geo.srtd_face_fpts
         for l, r in zip(lhs, rhs):
             el, fl, er, fr = int(l['eidx']), int(l['fidx']), int(r['eidx']), \
@@ -153,8 +165,9 @@ class DGFSSystem:
                 part[jl, el] = jr*E + er
                 part[jr, er] = jl*E + el
 
-        bnames = sorted(k[5:-3] for k in self.mesh
-                        if k.startswith('bcon_') and k.endswith('_p0'))
+        sfx = self._sfx
+        bnames = sorted(k[5:-len(sfx)] for k in self.mesh
+                        if k.startswith('bcon_') and k.endswith(sfx))
         bpts, guw, gfw, grefl, kinds = [], [], [], [], []
         self.bc_sections = {}
         for g, name in enumerate(bnames):
@@ -174,7 +187,7 @@ class DGFSSystem:
             else:
                 guw.append(np.zeros(3))
                 gfw.append(np.zeros(V))
-            recs = self.mesh[f'bcon_{name}_p0']
+            recs = self.mesh[f'bcon_{name}{sfx}']
             for rec in recs:
                 e, f = int(rec['eidx']), int(rec['fidx'])
                 for j in srtd[f][e]:
@@ -198,6 +211,14 @@ class DGFSSystem:
         bele = np.array([e for _, _, e in bpts], dtype=np.int32)
         for b, (g, j, e) in enumerate(bpts):
             part[j, e] = -(b + 1)
+        # faces shared with other parts: halo row h of the received values
+        from frfs_b200.partition import halo_rows
+        nbrs, counts, hrows = halo_rows(self.mesh, self.prank, srtd)
+        for h, (j, e) in enumerate(hrows):
+            part[j, e] = -(len(bpts) + 1 + h)
+        self.halo = (nbrs, counts) if hrows else None
+        sfpt = np.array([j for j, _ in hrows] or [0], dtype=np.int32)
+        sele = np.array([e for _, e in hrows] or [0], dtype=np.int32)
         # cylinder walls: the wall state at every boundary flux point
         bwall = np.ones((max(len(bpts), 1), 4))
         bwall[:, :3] = 0.0
@@ -242,12 +263,23 @@ class DGFSSystem:
             bele=_ptr(bele, c_ip), ngroups=len(bnames),
             guw=_ptr(keep['guw']), gfw=_ptr(keep['gfw']),
             grefl=_ptr(keep['grefl'], c_ip), bwall=_ptr(keep['bwall']),
-            m12=_ptr(keep['m12']))
+            m12=_ptr(keep['m12']), nhalo=len(hrows), nsend=len(hrows),
+            sfpt=_ptr(sfpt, c_ip), sele=_ptr(sele, c_ip))
+        keep['sfpt'], keep['sele'] = sfpt, sele
         h = c_void_p()
         lib = _lib.load()
         _lib.check(lib.dgfs_dg_create(ct.byref(p), ct.byref(h)),
                    'dgfs_dg_create')
         self._dg, self._lib = h, lib
+        if self.halo is not None:
+            import torch
+            tdt = torch.float64 if self.backend.precision == 64 else \
+                torch.float32
+            self.halo_send = torch.zeros((len(hrows), V), dtype=tdt,
+                                         device=self.backend.device)
+            self.halo_recv = torch.zeros_like(self.halo_send)
+            _lib.check(lib.dgfs_dg_set_halo(h, self.halo_recv.data_ptr()),
+                       'dgfs_dg_set_halo')
 
     def __del__(self):
         h = getattr(self, '_dg', None)
@@ -288,9 +320,26 @@ class DGFSSystem:
         s = self.backend.stream
         _lib.check(self._lib.dgfs_dg_interp(self._dg, u._as_parameter_, v0,
                                             nv, s), 'dgfs_dg_interp')
+        if self.halo is not None and v0 + nv == self.vm.vsize():
+            # face values of the shared faces to and from the neighbouring
+            # parts, once the last velocity slice is interpolated
+            # (inters.py:83-92: pack, send, recv; unpack is the residual's
+            # direct read of the received rows)
+            self.exchange_halo()
         _lib.check(self._lib.dgfs_dg_updatebc(self._dg, v0, nv,
                                               1 if v0 == 0 else 0, s),
                    'dgfs_dg_updatebc')
+
+    def exchange_halo(self):
+        """Pack this part's face values on shared faces and exchange them
+        with the neighbouring parts (all velocities)."""
+        _lib.check(self._lib.dgfs_dg_pack(self._dg, self.halo_send.data_ptr(),
+                                          self.backend.stream), 'dgfs_dg_pack')
+        nbrs, counts = self.halo
+        fn = self.halo_exchange
+        if fn is None:
+            from frfs_b200.partition import exchange as fn
+        fn(self.halo_send, self.halo_recv, nbrs, counts)
 
     def rhs(self, t, uinbank, foutbank, batch, varidx):
         """foutbank[slice] = -div F(uinbank[slice]) (system.py:140-177)."""

@@ -115,8 +115,10 @@ uz = 0.0
     return ini
 
 
-def couette_n24(precision='double', M=16, nele=64):
-    """1D/3V Couette slab as a 64x1 quad strip; BASELINE configuration 2."""
+def couette_n24(precision='double', M=16, nele=64, copies=1):
+    """1D/3V Couette slab as a 64x1 quad strip; BASELINE configuration 2.
+    ``copies`` > 1 widens the slab to that many slab widths (nele elements
+    each, the same element size) for weak scaling over partitions."""
     u0 = _u0()
     ini = _BASE.format(precision=precision, Nv=24, NvBatchSize=13824,
                        Nrho=12, H0=1e-3, rho0=1.5e-3,
@@ -125,10 +127,10 @@ def couette_n24(precision='double', M=16, nele=64):
     ini += f"""
 [mesh]
 type = quad-strip
-nx = {nele}
+nx = {nele*copies}
 ny = 1
-xlo = -0.5
-xhi = 0.5
+xlo = {-0.5*copies!r}
+xhi = {0.5*copies!r}
 ylo = 0.0
 yhi = {1.0/nele!r}
 periodic-y = 1
@@ -160,8 +162,11 @@ uz = 0.0
     return ini
 
 
-def channel_n32(precision='double', nx=48, ny=24, Nv=32, Nrho=16, M=24):
-    """2D/3V channel on 48x24 quads; BASELINE configuration 3."""
+def channel_n32(precision='double', nx=48, ny=24, Nv=32, Nrho=16, M=24,
+                copies=1):
+    """2D/3V channel on 48x24 quads; BASELINE configuration 3.  ``copies``
+    > 1 lengthens the periodic channel to that many channel lengths (nx
+    elements each) for weak scaling over partitions."""
     ini = _BASE.format(precision=precision, Nv=Nv, NvBatchSize=Nv**3,
                        Nrho=Nrho, H0=1e-3, rho0=1.5e-3,
                        molarMass0=_MOLAR_MASS, cmax=0.0, dev=5.0, M=M,
@@ -169,10 +174,10 @@ def channel_n32(precision='double', nx=48, ny=24, Nv=32, Nrho=16, M=24):
     ini += f"""
 [mesh]
 type = quad-box
-nx = {nx}
+nx = {nx*copies}
 ny = {ny}
-xlo = -0.5
-xhi = 0.5
+xlo = {-0.5*copies!r}
+xhi = {0.5*copies!r}
 ylo = -0.25
 yhi = 0.25
 periodic-x = 1

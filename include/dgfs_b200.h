@@ -249,6 +249,16 @@ typedef struct dgfs_dg_params {
   const double* m12;      /* [nupts][nupts] operator M12 = V^T V for
                              dgfs_dg_invmass (frfs/shapes.py:164-166), or
                              NULL                                           */
+  /* Faces shared with other partitions of the mesh (frfs's MPI interfaces,
+   * DGFSMPIInters, frfs/solvers/dgfs/inters.py:61-112): a flux point whose
+   * partner lives in another partition has partner = -(nbfpts + 1 + h), h
+   * the row of the halo buffer that receives the partner's face values
+   * (dgfs_dg_set_halo); the send rows list this partition's flux points
+   * that others need (dgfs_dg_pack).  Zero / NULL for a whole mesh.        */
+  int nhalo;              /* halo rows (received flux points)               */
+  int nsend;              /* send rows                                      */
+  const int* sfpt;        /* [nsend] flux point of each send row            */
+  const int* sele;        /* [nsend] element of each send row               */
 } dgfs_dg_params;
 
 DGFS_API int dgfs_dg_create(const dgfs_dg_params* params, dgfs_dg** out);
@@ -274,6 +284,18 @@ DGFS_API int dgfs_dg_rhs(dgfs_dg* h, const void* u, void* out, int v0, int nv,
                          double alpha, const void* A, double beta,
                          const void* B, double gamma, const void* C,
                          void* stream);
+
+/* Pack the current face values (dgfs_dg_interp) of the send rows for all
+ * velocities: send[s*nvars + v] = uf(sfpt[s], v, sele[s]), a device buffer
+ * of nsend*nvars values of the handle's precision (the 'pack' kernel of
+ * frfs's MPI interfaces, frfs/solvers/dgfs/inters.py:83-85).  The caller
+ * exchanges the rows with the neighbouring partitions (NCCL send/recv). */
+DGFS_API int dgfs_dg_pack(dgfs_dg* h, void* send, void* stream);
+
+/* Device buffer of nhalo*nvars received face values (row h = halo row h,
+ * all velocities), read by every later dgfs_dg_rhs; required when the
+ * handle has partition faces.  The buffer stays owned by the caller. */
+DGFS_API int dgfs_dg_set_halo(dgfs_dg* h, const void* recv);
 
 /* out = M12 u on velocities [v0, v0+nv): DGFSSystem.invmass
  * (frfs/solvers/dgfs/system.py:221-231), the 'invmass' kernel of

@@ -18,6 +18,8 @@ restates the kernels that act on the distribution banks:
   negdivconf  R = -R / |J|                      kernels/negdivconf.mako:11-13
   update_bc   diffuse-wall flux sums            bcs/dgfs-wall-diffuse-update.mako:14-36,
                                                 bcs/dgfs-wall-diffuse-cyl-update.mako
+  (faces shared with another partition are a boundary region of type 'mpi'
+  whose ghost values are the received partner values, kernels/mpicflux.mako)
 
 Arrays: u (nupts, V, neles); uf (nfpts, V, neles).
 """
@@ -99,6 +101,11 @@ class DGOracle:
             return np.where(fac < 0, 0.0, ul)
         if kind == 'dgfs-wall-specular':
             return ul[self.specular_map(name, j, e)]
+        if kind == 'mpi':
+            # a face shared with another partition: the partner's face value
+            # received from it (kernels/mpicflux.mako: the Riemann solve
+            # against the received ur, scaled by the local |S^T n|)
+            return bc['ur'][k]
         raise ValueError(kind)
 
     def _cyl_wall(self, w, n):
