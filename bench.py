@@ -513,6 +513,7 @@ def run_b200(args):
     except Exception:
         pass
     kname = {'single-cta': 'vhs_cube_kernel', 'push': 'vhs_push_kernel',
+             'pair': 'vhs_pair_kernel',
              'pull': 'vhs_cluster_kernel'}.get(kind, kind)
     tkey = (kname, args.workload, npts, prec)
     traffic = TRAFFIC.get(tkey)

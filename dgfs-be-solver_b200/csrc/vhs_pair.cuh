@@ -1,0 +1,557 @@
+// Two-CTA fast-spectral VHS kernel for FP32 and N = 32.
+//
+// The same exact restatement of the reference's operator as the single-CTA
+// kernel (vhs_cube.cuh: one complex transform R = IFFT(m F) per (p, q), the
+// Nyquist-plane term Nq as three 2D transforms, Re S = Re R^2 + Re Nq^2,
+// fC = sum_p w1_p FFT(S_p), Q = prefac (Re IFFT(fC) - f Re IFFT(b2 F))),
+// frfs/solvers/dgfs/scattering.py:227-286 and vhs-gll.mako:103-266), for a
+// grid that does not fit one SM: a thread-block cluster of two CTAs per
+// solution point, persistent over the bank.
+//
+// Data distribution (rank r of the pair):
+//   k-slab   CTA r owns the k1 values K_r (16 of them, closed under
+//            k1 -> -k1 mod 32, so a line's Hermitian mirror is local):
+//            K_0 = {0..7, 16, 25..31}, K_1 = {8..15, 17..24};
+//   x-slab   CTA r owns x2 in X_r = [16 r, 16 r + 16).
+// A 3D inverse transform runs along k3 on the lines (k1 in K_r, k2), along
+// k2 on the lines (k1 in K_r, x3), then along k1 on the lines (x2 in X_r,
+// x3).  Between the second and third passes each CTA pushes the half of its
+// k-slab that the other owns in x (16 complex values per line) straight into
+// the other CTA's shared memory with st.async, completing on its mbarrier;
+// the destination is the region the receiver has just read for its own
+// second pass, so one work cube per CTA suffices.  In the work cube W the
+// value (k1, x2, x3) of the third pass sits at row kinv(k1) * 32 +
+// 16 owner(k1) + x2 - 16 r.  Forward transforms (FFT(S_p)) run the passes in
+// the opposite order with the same exchange.  The spectrum F of the point
+// (k3 <= N/2, [k3][k1][k2]) and the gain spectrum fC live in the pair's
+// slice of a global scratch (L2 resident); S_p accumulates in shared memory.
+// Every mbarrier wait is bounded (the error flag of dgfs_vhs_status).
+//
+// Shared memory (complex float unless noted): W [16][32][33], S [32][16][32]
+// (float), the Nyquist planes T1..T3 [32][33], two phase slots.  352
+// threads: 256 main threads (two of the 512 lines of every pass each, one
+// after the other: a 32-point register FFT needs ~130 registers) and 96 that
+// transform the Nyquist planes during the first two passes of every (p, q).
+#pragma once
+
+#include "vhs_push.cuh"
+
+namespace dgfs {
+
+struct PairGeom {
+  static constexpr int N = 32, H = 17, NY = 16, NN = 1024, V = 32768;
+  static constexpr int LP = 33;              // padded line stride
+  static constexpr int NL = 512;             // lines of a pass
+  static constexpr int NM = 256;             // main threads (lines t and t + 256)
+  static constexpr int NQ = 96;              // Nyquist-plane threads
+  static constexpr int NT = NM + NQ;
+  static constexpr int PHS = 3 * N + 4;
+  static constexpr int OFF_W = 0;                        // [16][32][LP] cx
+  static constexpr int OFF_S = OFF_W + 16 * N * LP;      // [32][16][32] float = 8192 cx
+  static constexpr int OFF_T = OFF_S + 8192;             // [3][32][LP] cx
+  static constexpr int OFF_PH = OFF_T + 3 * N * LP;      // [2][PHS] cx
+  static constexpr int SMEM_CX = OFF_PH + 2 * PHS;
+  static constexpr int SLICE = H * NN;                   // cx per spectrum in the scratch
+  static constexpr uint32_t XBYTES = NL * 16 * 8;        // bytes one exchange brings in
+};
+
+// k1 ownership: K_0 = {0..7, 16, 25..31}, K_1 = {8..15, 17..24}
+__device__ __forceinline__ int pair_owner(int k1) { return (k1 <= 7 || k1 == 16 || k1 >= 25) ? 0 : 1; }
+__device__ __forceinline__ int pair_kinv(int k1) {
+  return k1 <= 7 ? k1 : k1 == 16 ? 8 : k1 >= 25 ? k1 - 16 : k1 <= 15 ? k1 - 8 : k1 - 9;
+}
+__device__ __forceinline__ int pair_kmap(int r, int l) {
+  return r == 0 ? (l <= 7 ? l : l == 8 ? 16 : l + 16) : (l <= 7 ? l + 8 : l + 9);
+}
+
+__device__ __forceinline__ void st_async_f2(uint32_t raddr, float2 v, uint32_t rbar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f32 [%0], {%1, %2}, [%3];" ::"r"(raddr),
+               "f"(v.x), "f"(v.y), "r"(rbar)
+               : "memory");
+}
+__device__ __forceinline__ void cl_sync() {
+  cl_arrive();
+  cl_wait();
+}
+
+// third-pass line (x2l = hi, x3 = lo) along k1 from the two halves
+__device__ __forceinline__ void pair_load3(float2 (&x)[32], const float2* sW, int hi, int lo) {
+  constexpr int N = PairGeom::N, LP = PairGeom::LP;
+#pragma unroll
+  for (int k1 = 0; k1 < N; ++k1) x[k1] = sW[(pair_kinv(k1) * N + 16 * pair_owner(k1) + hi) * LP + lo];
+}
+
+__global__ void __launch_bounds__(PairGeom::NT, 1) vhs_pair_kernel(const VhsArgs<float> a) {
+  using G = PairGeom;
+  using C = cx<float>;
+  constexpr int N = G::N, H = G::H, NY = G::NY, NN = G::NN, V = G::V, LP = G::LP, NM = G::NM, PHS = G::PHS;
+
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* const sW = reinterpret_cast<C*>(smem_raw) + G::OFF_W;
+  float* const sS = reinterpret_cast<float*>(reinterpret_cast<C*>(smem_raw) + G::OFF_S);
+  C* const sT1 = reinterpret_cast<C*>(smem_raw) + G::OFF_T;
+  C* const sT2 = sT1 + N * LP;
+  C* const sT3 = sT2 + N * LP;
+  C* const sPh = reinterpret_cast<C*>(smem_raw) + G::OFF_PH;
+  __shared__ __align__(8) uint64_t sBar;
+  __shared__ int sGaveUp;
+  __shared__ double sRed[5][G::NT / 32];
+  __shared__ double sMom[5];
+
+  cg::cluster_group cluster = cg::this_cluster();
+  const int r = (int)cluster.block_rank();
+  const int tid = threadIdx.x;
+  const bool is_main = tid < NM;
+  const int tq = tid - NM;
+  const int cid = blockIdx.x / 2, ncl = gridDim.x / 2;
+  // the pair's scratch: F [H][N][N] then fC [H][N][N] (fC doubles as the
+  // exchange buffer of the forward transform of f)
+  C* const Fg = a.fc + (size_t)cid * 2 * G::SLICE;
+  C* const fC = Fg + G::SLICE;
+  const float invV = 1.f / (float)V;
+  const int npq = a.P * a.M;
+  // a main thread's lines in every pass: L = tid + 256 h (h = 0, 1), with
+  // hi = L >> 5 (k1l, or x2l in the third pass) and lo = L & 31 (k2, x3)
+  const int lo = tid & 31, hi0 = tid >> 5;  // hi of line h: hi0 + 8 h
+  const uint32_t peer = (uint32_t)(r ^ 1);
+  const uint32_t rbar = cluster_addr(&sBar, peer);
+  const uint32_t rW = cluster_addr(sW, peer);
+  int xpar = 0;  // parity of the next exchange on sBar
+
+  if (tid == 0) {
+    sGaveUp = 0;
+    mbar_init(&sBar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  cl_sync();
+
+  // Second pass of an inverse transform (lines (k1l, x3 = lo) along k2) and
+  // the exchange: of the 32 outputs (index x2) of each line the 16 with x2
+  // in X_r stay, the others go to the peer, which keeps them at row
+  // k1l * 32 + 16 r + (x2 - 16 (1 - r)) of its work cube -- the region it
+  // has just read for its own second pass.  Nyquist threads run `nyq`
+  // (their own second pass) meanwhile.
+  auto pass2_exchange = [&](auto&& nyq) {
+    C out0[16];
+    if (is_main) {
+#pragma unroll 1
+      for (int h = 0; h < 2; ++h) {
+        const int hi = hi0 + 8 * h;
+        C x[N];
+#pragma unroll
+        for (int j = 0; j < N; ++j) x[j] = sW[(hi * N + j) * LP + lo];
+        fft<float, N, +1>(x);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) sW[(hi * N + 16 * r + j) * LP + lo] = r ? x[16 + j] : x[j];
+        if (h == 0) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) out0[j] = r ? x[j] : x[16 + j];
+        } else {
+          cl_sync();  // both CTAs have read their second-pass lines
+          if (tid == 0) mbar_expect_tx(&sBar, G::XBYTES);
+#pragma unroll
+          for (int hh = 0; hh < 2; ++hh) {
+            const int hj = hi0 + 8 * hh;
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              const uint32_t off = (uint32_t)(((hj * N + 16 * r + j) * LP + lo) * sizeof(C));
+              st_async_f2(rW + off, hh == 0 ? out0[j] : (r ? x[j] : x[16 + j]), rbar);
+            }
+          }
+        }
+      }
+    } else {
+      nyq();
+      cl_sync();
+    }
+    mbar_wait_bounded(&sBar, (uint32_t)xpar, a.err, &sGaveUp);
+    xpar ^= 1;
+  };
+
+  const int npts = a.pcount ? min(a.npts, *a.pcount) : a.npts;
+#pragma unroll 1
+  for (int ip = cid; ip < npts; ip += ncl) {
+    const int pt = a.plist ? a.plist[a.pt0 + ip] : a.pt0 + ip;
+    // listed ids come from device memory: both CTAs read the same entry and
+    // skip together, so the cluster barriers stay paired
+    if ((unsigned)pt >= (unsigned)(a.nupts * a.neles)) continue;
+    const int upt = pt / a.neles, elem = pt % a.neles;
+
+    // ---- F = FFT(f) / V into the scratch, k3 <= N/2 ------------------------
+    // lines (x1 = 16 r + hi, x2 = lo) along x3, then (x1l, k3) along x2
+    // (272 lines), then through the scratch to lines (k2, k3) along x1
+    if (is_main) {
+#pragma unroll 1
+      for (int h = 0; h < 2; ++h) {
+        const int hi = hi0 + 8 * h, x1 = 16 * r + hi;
+        const int64_t b0 = soa_ix(upt, a.ldim, elem, (int64_t)(x1 * N + lo) * N, V, a.soasz);
+        C x[N];
+#pragma unroll
+        for (int k = 0; k < N; ++k) x[k] = mk<C>(a.f[b0 + (int64_t)k * a.soasz], 0.f);
+        fft<float, N, -1>(x);
+#pragma unroll
+        for (int k = 0; k <= NY; ++k) sW[(hi * N + lo) * LP + k] = x[k];
+      }
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int t = tid; t < 16 * H; t += G::NT) {
+      const int x1l = t / H, k3 = t % H;
+      C x[N];
+#pragma unroll
+      for (int j = 0; j < N; ++j) x[j] = sW[(x1l * N + j) * LP + k3];
+      fft<float, N, -1>(x);
+      // exchange buffer [k3][x1][k2] (the fC slice, free until p = 0 ends)
+#pragma unroll
+      for (int j = 0; j < N; ++j) fC[(k3 * N + 16 * r + x1l) * N + j] = x[j];
+    }
+    cl_sync();  // the exchange buffer is complete (cluster-scope release/acquire)
+#pragma unroll 1
+    for (int t = tid; t < 16 * H; t += G::NT) {
+      const int k2 = 16 * r + t / H, k3 = t % H;
+      C x[N];
+#pragma unroll
+      for (int i = 0; i < N; ++i) x[i] = __ldcg(fC + (k3 * N + i) * N + k2);
+      fft<float, N, -1>(x);
+#pragma unroll
+      for (int i = 0; i < N; ++i) Fg[(k3 * N + i) * N + k2] = cscale(x[i], invV);
+    }
+    if (tid < 3 * N) {
+      const C e = a.phase[tid];
+      sPh[tid] = e;
+      if (tid % N == NY) sPh[3 * N + tid / N] = cmul(mk<C>(e.x, -e.y), mk<C>(e.x, -e.y));
+    }
+    cl_sync();  // F complete in the scratch; the exchange buffer may be reused
+
+    // F at (k1, k2, k3) from the half spectrum in the scratch (written by
+    // both CTAs: read through L2)
+    auto Fat = [&](int k1, int k2, int k3) -> C {
+      if (k3 <= NY) return __ldcg(Fg + (k3 * N + k1) * N + k2);
+      const C c = __ldcg(Fg + ((N - k3) * N + (N - k1) % N) * N + (N - k2) % N);
+      return mk<C>(c.x, -c.y);
+    };
+
+    int slot = 0;
+#pragma unroll 1
+    for (int p = 0; p < a.P; ++p) {
+#pragma unroll 1
+      for (int q = 0; q < a.M; ++q) {
+        const int pq = p * a.M + q;
+        const C* ph = sPh + slot * PHS;
+        const C th1 = ph[3 * N], th2 = ph[3 * N + 1], th3 = ph[3 * N + 2];
+        const C phn = (tid < 3 * N && pq + 1 < npq) ? a.phase[(size_t)(pq + 1) * 3 * N + tid] : mk<C>(0.f, 0.f);
+        // pass 1: lines (k1, k2 = lo) along k3 | Nyquist first axes
+        if (is_main) {
+#pragma unroll 1
+          for (int h = 0; h < 2; ++h) {
+            const int hi = hi0 + 8 * h, k1 = pair_kmap(r, hi), k2 = lo;
+            const C E12 = cmul(ph[k1], ph[N + k2]);
+            C t12 = mk<C>(1.f, 0.f);
+            if (k1 == NY) t12 = th1;
+            if (k2 == NY) t12 = cmul(t12, th2);
+            const C E12t = cmul(E12, t12);
+            const C s0 = cadd(E12, E12t), s3 = cadd(E12, cmul(E12t, th3));
+            const C A = mk<C>(0.5f * (s0.x + s0.y), 0.5f * (s0.y - s0.x));
+            const C A3 = mk<C>(0.5f * (s3.x + s3.y), 0.5f * (s3.y - s3.x));
+            C x[N];
+#pragma unroll
+            for (int k = 0; k < N; ++k) {
+              const C e3 = ph[2 * N + k];
+              const C& Ak = k == NY ? A3 : A;
+              x[k] = cscale(Fat(k1, k2, k), Ak.x * e3.x - Ak.y * e3.y);
+            }
+            fft<float, N, +1>(x);
+#pragma unroll
+            for (int k = 0; k < N; ++k) sW[(hi * N + k2) * LP + k] = x[k];
+          }
+        } else {
+          // n F on the Nyquist planes (vhs_cube.cuh): plane 1 (k1 = N/2)
+          // lines over k3, plane 2 (k2 = N/2) lines over k3, plane 3
+          // (k3 = N/2) lines over k2; one coefficient per line
+          const int which = tq / N, j = tq % N;
+          const bool p3 = which == 2;
+          C Eb, tb;
+          if (which == 0) {
+            Eb = cmul(ph[NY], ph[N + j]);
+            tb = j == NY ? cmul(th1, th2) : th1;
+          } else if (which == 1) {
+            Eb = cmul(ph[j], ph[N + NY]);
+            tb = th2;
+          } else {
+            Eb = cmul(ph[j], ph[2 * N + NY]);
+            tb = th3;
+          }
+          C B = cmul(Eb, mk<C>(1.f - tb.x, -tb.y));
+          const C tb3 = cmul(tb, th3);
+          C B3 = p3 ? mk<C>(0.f, 0.f) : cmul(Eb, mk<C>(1.f - tb3.x, -tb3.y));
+          if (which != 0 && j == NY) B = B3 = mk<C>(0.f, 0.f);
+          const C A = mk<C>(0.5f * (B.x + B.y), 0.5f * (B.y - B.x));
+          const C A3 = mk<C>(0.5f * (B3.x + B3.y), 0.5f * (B3.y - B3.x));
+          const C* ev = ph + (p3 ? N : 2 * N);
+          C x[N];
+#pragma unroll
+          for (int k = 0; k < N; ++k) {
+            const C v = which == 0 ? Fat(NY, j, k) : which == 1 ? Fat(j, NY, k) : Fat(j, k, NY);
+            const C& Ak = k == NY ? A3 : A;
+            const C e = ev[k];
+            x[k] = cscale(v, Ak.x * e.x - Ak.y * e.y);
+          }
+          fft<float, N, +1>(x);
+          C* T = which == 0 ? sT1 : (which == 1 ? sT2 : sT3);
+#pragma unroll
+          for (int k = 0; k < N; ++k) T[j * LP + k] = x[k];
+        }
+        __syncthreads();
+        if (tid < 3 * N && pq + 1 < npq) {
+          C* dst = sPh + (slot ^ 1) * PHS;
+          dst[tid] = phn;
+          if (tid % N == NY) dst[3 * N + tid / N] = cmul(mk<C>(phn.x, -phn.y), mk<C>(phn.x, -phn.y));
+        }
+        // pass 2 and the exchange | Nyquist second axes (all 32 columns of
+        // every plane; the third pass reads the rows of its own x2 half)
+        pass2_exchange([&]() {
+          const int which = tq / N, col = tq % N;
+          C* T = which == 0 ? sT1 : (which == 1 ? sT2 : sT3);
+          C x[N];
+#pragma unroll
+          for (int j = 0; j < N; ++j) x[j] = T[j * LP + col];
+          fft<float, N, +1>(x);
+#pragma unroll
+          for (int j = 0; j < N; ++j) T[j * LP + col] = x[j];
+        });
+        __syncthreads();  // the Nyquist columns are complete
+        // pass 3: lines (x2 = 16 r + hi, x3 = lo) along k1;
+        // S += Re R^2 + Re Nq^2
+        if (is_main) {
+#pragma unroll 1
+          for (int h = 0; h < 2; ++h) {
+            const int hi = hi0 + 8 * h, x2 = 16 * r + hi, x3 = lo;
+            C x[N];
+            pair_load3(x, sW, hi, lo);
+            fft<float, N, +1>(x);
+            const C t1 = sT1[x2 * LP + x3];
+            const float s2 = (x2 & 1) ? -1.f : 1.f, s3 = (x3 & 1) ? -1.f : 1.f;
+            float* Sl = sS + hi * N + x3;
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+              const float s1 = (i & 1) ? -1.f : 1.f;
+              const C t2 = sT2[i * LP + x3], t3 = sT3[i * LP + x2];
+              const float nr = s1 * t1.x + s2 * t2.x + s3 * t3.x;
+              const float ni = s1 * t1.y + s2 * t2.y + s3 * t3.y;
+              const float v = x[i].x * x[i].x - x[i].y * x[i].y + nr * nr - ni * ni;
+              Sl[i * 16 * N] = q == 0 ? v : Sl[i * 16 * N] + v;
+            }
+          }
+        }
+        slot ^= 1;
+        __syncthreads();
+      }
+
+      // ---- fC += w1_p FFT(S_p) ----------------------------------------------
+      // lines (x2l, x3) along x1 from S, the exchange to k-slabs, lines
+      // (k1l, x3) along x2, lines (k1l, k2) along x3 into fC (k3 <= N/2).
+      // An output k1 of a first-pass line is local when owned, else pushed
+      // to the peer's row kinv(k1) * 32 + x2.
+      cl_sync();  // the peer has finished its third pass (its W is free)
+      if (tid == 0) mbar_expect_tx(&sBar, G::XBYTES);
+      if (is_main) {
+#pragma unroll 1
+        for (int h = 0; h < 2; ++h) {
+          const int hi = hi0 + 8 * h, x2 = 16 * r + hi;
+          C x[N];
+          const float* Sl = sS + hi * N + lo;
+#pragma unroll
+          for (int i = 0; i < N; ++i) x[i] = mk<C>(Sl[i * 16 * N], 0.f);
+          fft<float, N, -1>(x);
+#pragma unroll
+          for (int k1 = 0; k1 < N; ++k1) {
+            const int row = pair_kinv(k1) * N + x2;
+            if (pair_owner(k1) == r) {
+              sW[row * LP + lo] = x[k1];
+            } else {
+              st_async_f2(rW + (uint32_t)((row * LP + lo) * sizeof(C)), x[k1], rbar);
+            }
+          }
+        }
+      }
+      mbar_wait_bounded(&sBar, (uint32_t)xpar, a.err, &sGaveUp);
+      xpar ^= 1;
+      __syncthreads();
+      if (is_main) {
+#pragma unroll 1
+        for (int h = 0; h < 2; ++h) {
+          const int hi = hi0 + 8 * h;
+          C x[N];
+#pragma unroll
+          for (int j = 0; j < N; ++j) x[j] = sW[(hi * N + j) * LP + lo];
+          fft<float, N, -1>(x);
+#pragma unroll
+          for (int j = 0; j < N; ++j) sW[(hi * N + j) * LP + lo] = x[j];
+        }
+      }
+      __syncthreads();
+      if (is_main) {
+        const float* w1 = a.w1t + (size_t)p * V;
+#pragma unroll 1
+        for (int h = 0; h < 2; ++h) {
+          const int hi = hi0 + 8 * h, k1 = pair_kmap(r, hi), k2 = lo, L = k1 * N + k2;
+          C x[N];
+#pragma unroll
+          for (int k = 0; k < N; ++k) x[k] = sW[(hi * N + k2) * LP + k];
+          fft<float, N, -1>(x);
+#pragma unroll
+          for (int k = 0; k <= NY; ++k) x[k] = cscale(x[k], __ldg(w1 + k * NN + L));
+          if (p > 0) {
+            // read-modify-write in chunks of 6 (the loads of a chunk issued
+            // together; fewer live registers than the whole line)
+#pragma unroll
+            for (int k0 = 0; k0 <= NY; k0 += 6) {
+              C acc[6];
+#pragma unroll
+              for (int k = k0; k < k0 + 6 && k <= NY; ++k) acc[k - k0] = fC[k * NN + L];
+#pragma unroll
+              for (int k = k0; k < k0 + 6 && k <= NY; ++k) fC[k * NN + L] = cadd(acc[k - k0], x[k]);
+            }
+          } else {
+#pragma unroll
+            for (int k = 0; k <= NY; ++k) fC[k * NN + L] = x[k];
+          }
+        }
+      }
+      __syncthreads();
+    }
+
+    // ---- Q = prefac (Re IFFT(fC) - f Re IFFT(b2 F)) ----------------------------
+    // Two inverse transforms over the half spectra (each line's mirror is in
+    // this CTA's k-slab): Lf into S, then the gain and Q into S.
+#pragma unroll 1
+    for (int t = 0; t < 2; ++t) {
+      if (is_main) {
+#pragma unroll 1
+        for (int h = 0; h < 2; ++h) {
+          const int hi = hi0 + 8 * h, k1 = pair_kmap(r, hi), k2 = lo, L = k1 * N + k2;
+          const int m1 = (N - k1) % N, m2 = (N - k2) % N;
+          C x[N];
+#pragma unroll
+          for (int k = 0; k < N; ++k) {
+            if (t == 0) {
+              x[k] = cscale(Fat(k1, k2, k), __ldg(a.b2t + k * NN + L));
+            } else if (k <= NY) {
+              x[k] = fC[k * NN + L];
+            } else {
+              const C c = fC[(N - k) * NN + m1 * N + m2];
+              x[k] = mk<C>(c.x, -c.y);
+            }
+          }
+          fft<float, N, +1>(x);
+#pragma unroll
+          for (int k = 0; k < N; ++k) sW[(hi * N + k2) * LP + k] = x[k];
+        }
+      }
+      __syncthreads();
+      pass2_exchange([]() {});
+      if (is_main) {
+#pragma unroll 1
+        for (int h = 0; h < 2; ++h) {
+          const int hi = hi0 + 8 * h;
+          C x[N];
+          pair_load3(x, sW, hi, lo);
+          fft<float, N, +1>(x);
+          float* Sl = sS + hi * N + lo;
+          if (t == 0) {
+#pragma unroll
+            for (int i = 0; i < N; ++i) Sl[i * 16 * N] = x[i].x;
+          } else {
+            // x2 = 16 r + hi, x3 = lo: bank entries v = i N^2 + x2 N + x3
+            const int64_t b0 = soa_ix(upt, a.ldim, elem, (int64_t)(16 * r + hi) * N + lo, V, a.soasz);
+            const int64_t st = (int64_t)NN * a.soasz;
+#pragma unroll
+            for (int i0 = 0; i0 < N; i0 += 8) {
+              float fl[8];
+#pragma unroll
+              for (int i = 0; i < 8; ++i) fl[i] = a.f[b0 + (i0 + i) * st];
+#pragma unroll
+              for (int i = 0; i < 8; ++i)
+                Sl[(i0 + i) * 16 * N] = a.prefac * (x[i0 + i].x - fl[i] * Sl[(i0 + i) * 16 * N]);
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+
+    // write Q (this CTA's x2 half), with the optional FP64 projection onto
+    // zero mass, momentum and energy over both halves
+    double lam[5] = {0, 0, 0, 0, 0};
+    if (a.project) {
+      double mom[5] = {0, 0, 0, 0, 0};
+      if (is_main) {
+#pragma unroll 1
+        for (int h = 0; h < 2; ++h) {
+          const int hi = hi0 + 8 * h;
+          const float* Sl = sS + hi * N + lo;
+#pragma unroll 4
+          for (int i = 0; i < N; ++i) {
+            const int64_t v = (int64_t)(i * N + 16 * r + hi) * N + lo;
+            const double d = (double)Sl[i * 16 * N];
+            const double c0 = a.cvec[v], c1 = a.cvec[V + v], c2 = a.cvec[2 * V + v];
+            mom[0] += d;
+            mom[1] += d * c0;
+            mom[2] += d * c1;
+            mom[3] += d * c2;
+            mom[4] += d * (c0 * c0 + c1 * c1 + c2 * c2);
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        double s = mom[k];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if ((tid & 31) == 0) sRed[k][tid >> 5] = s;
+      }
+      __syncthreads();
+      if (tid < 5) {
+        double s = 0;
+        for (int w = 0; w < G::NT / 32; ++w) s += sRed[tid][w];
+        sMom[tid] = s;
+      }
+      cl_sync();  // both halves' moments in place
+      double mt[5];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) mt[k] = sMom[k] + cluster.map_shared_rank(sMom, (int)peer)[k];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        double s = 0;
+#pragma unroll
+        for (int j = 0; j < 5; ++j) s += a.ginv[k * 5 + j] * mt[j];
+        lam[k] = s;
+      }
+    }
+    if (is_main) {
+#pragma unroll 1
+      for (int h = 0; h < 2; ++h) {
+        const int hi = hi0 + 8 * h;
+        const float* Sl = sS + hi * N + lo;
+        const int64_t b0 = soa_ix(upt, a.ldim, elem, (int64_t)(16 * r + hi) * N + lo, V, a.soasz);
+        const int64_t st = (int64_t)NN * a.soasz;
+#pragma unroll 4
+        for (int i = 0; i < N; ++i) {
+          float qq = Sl[i * 16 * N];
+          if (a.project) {
+            const int64_t v = (int64_t)(i * N + 16 * r + hi) * N + lo;
+            const double c0 = a.cvec[v], c1 = a.cvec[V + v], c2 = a.cvec[2 * V + v];
+            qq = (float)((double)qq - (lam[0] + lam[1] * c0 + lam[2] * c1 + lam[3] * c2 +
+                                       lam[4] * (c0 * c0 + c1 * c1 + c2 * c2)));
+          }
+          a.Q[b0 + i * st] = qq;
+        }
+      }
+    }
+    // the next point rewrites the scratch, S and the moments: both CTAs done
+    cl_sync();
+  }
+  cl_sync();  // no CTA leaves while the peer may still address its memory
+}
+
+}  // namespace dgfs

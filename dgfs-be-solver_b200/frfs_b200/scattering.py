@@ -198,7 +198,8 @@ class DGFSVHSGLLScatteringModel(DGFSScatteringModel):
             _lib.check(self._lib.dgfs_vhs_variant_kind(self._h, i,
                                                        ct.byref(k)),
                        'dgfs_vhs_variant_kind')
-            d['exchange'] = {0: 'pull', 1: 'push', 2: 'single-cta'}[k.value]
+            d['exchange'] = {0: 'pull', 1: 'push', 2: 'single-cta',
+                             3: 'pair'}[k.value]
             out.append(d)
         return out
 

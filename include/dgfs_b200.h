@@ -145,7 +145,10 @@ DGFS_API int dgfs_vhs_select(dgfs_vhs* h, int idx);
 /* 1 if launch shape idx exchanges by remote pushes (st.async into the
  * owner's shared memory, mbarrier completion), 0 if by remote loads, 2 for
  * the single-CTA kernel (FP32, Nv <= 24: the whole point in one CTA's
- * shared memory, one complex transform per (p, q)). */
+ * shared memory, one complex transform per (p, q)), 3 for the two-CTA
+ * kernel (FP32, Nv = 32: the same transforms on a pair of CTAs that swap
+ * half of the work cube through distributed shared memory once per
+ * transform). */
 DGFS_API int dgfs_vhs_variant_kind(const dgfs_vhs* h, int idx, int* push);
 
 /* Synchronise `stream`, then report and clear the kernel error flag: the

@@ -128,13 +128,13 @@ def test_launch_shapes_agree(name, precision):
     Qo = [ovhs.vhs_Q(fu[0, :, e], ovm, pre, prefac) for e in range(3)]
     tol = FP64_TOL if precision == 'double' else FP32_TOL
     # the cluster shapes share one arithmetic (agree to round-off); the
-    # single-CTA shapes use another exact restatement: every shape is
+    # single-CTA and two-CTA shapes use another exact restatement: every shape is
     # checked against the oracle, cluster shapes also against each other
     first = None
     for o, k in zip(outs, kinds):
         for e in range(3):
             assert rel_err(o[0, :, e], Qo[e]) < tol
-        if k == 'single-cta':
+        if k in ('single-cta', 'pair'):
             continue
         if first is None:
             first = o
@@ -254,3 +254,34 @@ def test_bounded_wait_that_runs_out_is_reported():
     sm.status()
     Qo = ovhs.vhs_Q(f[0, 0], ovm, pre, prefac)
     assert rel_err(fout.get()[0, :, 0], Qo) < FP64_TOL
+
+
+@pytest.mark.parametrize('project', [0, 1])
+def test_pair_kernel_bank(project):
+    """The two-CTA kernel (FP32, N = 32, the default there) on a bank of
+    10 points over two AoSoA rows, with and without the FP64 projection,
+    against the oracle point by point; a second launch on the same banks
+    gives the same values (the per-pair scratch is rewritten per point)."""
+    cfg = config('channel-n32', 'single', Nrho=4, M=6)
+    cfg.set('backend-b200', 'vhs-project', project)
+    be, vm, sm = _model(cfg)
+    assert sm.variants()[0]['exchange'] == 'pair'
+    ovm, pre, prefac = oracle_for(cfg)
+    nupts, neles = 2, 5
+    f = random_states(vm.cv(), nupts*neles, seed=13).reshape(nupts, neles, -1)
+    fin, fout = _bank(be, vm, f)
+    sm.fs_all(fin, fout)
+    sm.status()
+    Qg = fout.get()
+    _, fout2 = _bank(be, vm, f)
+    sm.fs_all(fin, fout2)
+    sm.status()
+    np.testing.assert_array_equal(Qg, fout2.get())
+    fu = fin.get().astype(np.float64)
+    cv = vm.cv()
+    for u in range(nupts):
+        for e in range(neles):
+            Qo = ovhs.vhs_Q(fu[u, :, e], ovm, pre, prefac)
+            if project:
+                Qo = ovhs.project_conservative(Qo, cv)
+            assert rel_err(Qg[u, :, e], Qo) < FP32_TOL, (u, e)
