@@ -160,11 +160,11 @@ template <int N, bool IL1> static VhsVariant make_cube() {
   return v;
 }
 
-static cudaError_t launch_pair(const VhsArgs<float>& a, int nclusters, cudaStream_t s) {
+template <int LPT> static cudaError_t launch_pair(const VhsArgs<float>& a, int nclusters, cudaStream_t s) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(nclusters * 2, 1, 1);
-  cfg.blockDim = dim3(PairGeom::NT, 1, 1);
-  cfg.dynamicSmemBytes = PairGeom::SMEM_CX * sizeof(cx<float>);
+  cfg.blockDim = dim3(PairGeom<LPT>::NT, 1, 1);
+  cfg.dynamicSmemBytes = PairGeom<LPT>::SMEM_CX * sizeof(cx<float>);
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -173,22 +173,23 @@ static cudaError_t launch_pair(const VhsArgs<float>& a, int nclusters, cudaStrea
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, vhs_pair_kernel, a);
+  return cudaLaunchKernelEx(&cfg, vhs_pair_kernel<LPT>, a);
 }
 
-// two-CTA kernel (FP32, N = 32; kind 3 in dgfs_vhs_variant_kind)
-static VhsVariant make_pair() {
+// two-CTA kernel (FP32, N = 32; kind 3 in dgfs_vhs_variant_kind); LPT
+// lines per main thread and pass (db reports LPT - 1)
+template <int LPT> static VhsVariant make_pair() {
   VhsVariant v{};
   v.prec = 32;
   v.N = 32;
   v.C = 2;
-  v.db = 0;
+  v.db = LPT - 1;
   v.push = 3;
   v.minb = 1;
-  v.threads = PairGeom::NT;
-  v.smem = PairGeom::SMEM_CX * sizeof(cx<float>);
-  v.fn = (const void*)vhs_pair_kernel;
-  v.launch32 = launch_pair;
+  v.threads = PairGeom<LPT>::NT;
+  v.smem = PairGeom<LPT>::SMEM_CX * sizeof(cx<float>);
+  v.fn = (const void*)vhs_pair_kernel<LPT>;
+  v.launch32 = launch_pair<LPT>;
   return v;
 }
 
@@ -205,7 +206,8 @@ static const std::vector<VhsVariant>& variants() {
       make_push<float, 8, 1, 4>(),              make_push<float, 16, 2, 2>(),
       make_push<float, 16, 4, 4>(),             make_cube<24, false>(),
       make_push<float, 24, 8, 2>(),             make_push<float, 24, 4, 1>(),
-      make_push<float, 24, 12, 3>(),            make_pair(),
+      make_push<float, 24, 12, 3>(),            make_pair<2>(),
+      make_pair<1>(),
       make_push<float, 32, 16, 2>(),
       make_push<float, 32, 8, 1>(),             make_cube<8, false>(),
       make_cube<16, false>(),                   make_cube<16, true>(),
@@ -303,7 +305,7 @@ static int select_index(dgfs_vhs* h, int idx) {
   const size_t esz = h->prec == 64 ? 16 : 8;
   // gain-spectrum scratch: one N^3 complex slice per cluster, or for the
   // two-CTA kernel the half spectra of F and fC
-  const size_t need = v->push == 3 ? (size_t)ncl * 2 * PairGeom::SLICE * esz
+  const size_t need = v->push == 3 ? (size_t)ncl * 2 * PairGeom<1>::SLICE * esz
                                    : (size_t)ncl * v->C * (size_t)h->N * h->N * h->N / v->C * esz;
   if (need > h->fc_bytes) {
     cudaFree(h->fc);

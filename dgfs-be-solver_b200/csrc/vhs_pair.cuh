@@ -38,12 +38,17 @@
 
 namespace dgfs {
 
-struct PairGeom {
+// LPT: lines of a pass per main thread.  LPT = 2: 256 main threads (lines
+// t and t + 256, one after the other, 168 registers) and 96 threads for the
+// Nyquist planes; LPT = 1: 512 threads at 128 registers, the first 96 of
+// which also take the Nyquist lines.
+template <int LPT> struct PairGeom {
   static constexpr int N = 32, H = 17, NY = 16, NN = 1024, V = 32768;
   static constexpr int LP = 33;              // padded line stride
   static constexpr int NL = 512;             // lines of a pass
-  static constexpr int NM = 256;             // main threads (lines t and t + 256)
-  static constexpr int NQ = 96;              // Nyquist-plane threads
+  static constexpr int NM = NL / LPT;        // main threads
+  static constexpr int HS = 16 / LPT;        // step of a thread's line index hi
+  static constexpr int NQ = LPT == 2 ? 96 : 0;  // threads for the Nyquist planes only
   static constexpr int NT = NM + NQ;
   static constexpr int PHS = 3 * N + 4;
   static constexpr int OFF_W = 0;                        // [16][32][LP] cx
@@ -76,13 +81,15 @@ __device__ __forceinline__ void cl_sync() {
 
 // third-pass line (x2l = hi, x3 = lo) along k1 from the two halves
 __device__ __forceinline__ void pair_load3(float2 (&x)[32], const float2* sW, int hi, int lo) {
-  constexpr int N = PairGeom::N, LP = PairGeom::LP;
+  constexpr int N = 32, LP = 33;
 #pragma unroll
   for (int k1 = 0; k1 < N; ++k1) x[k1] = sW[(pair_kinv(k1) * N + 16 * pair_owner(k1) + hi) * LP + lo];
 }
 
-__global__ void __launch_bounds__(PairGeom::NT, 1) vhs_pair_kernel(const VhsArgs<float> a) {
-  using G = PairGeom;
+template <int LPT>
+__global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const VhsArgs<float> a) {
+  using G = PairGeom<LPT>;
+  constexpr int HS = G::HS;
   using C = cx<float>;
   constexpr int N = G::N, H = G::H, NY = G::NY, NN = G::NN, V = G::V, LP = G::LP, NM = G::NM, PHS = G::PHS;
 
@@ -102,7 +109,9 @@ __global__ void __launch_bounds__(PairGeom::NT, 1) vhs_pair_kernel(const VhsArgs
   const int r = (int)cluster.block_rank();
   const int tid = threadIdx.x;
   const bool is_main = tid < NM;
-  const int tq = tid - NM;
+  // the Nyquist lines: own threads (LPT = 2) or the first 96 main threads
+  const bool has_nyq = G::NQ > 0 ? !is_main : tid < 3 * N;
+  const int tq = G::NQ > 0 ? tid - NM : tid;
   const int cid = blockIdx.x / 2, ncl = gridDim.x / 2;
   // the pair's scratch: F [H][N][N] then fC [H][N][N] (fC doubles as the
   // exchange buffer of the forward transform of f)
@@ -110,9 +119,9 @@ __global__ void __launch_bounds__(PairGeom::NT, 1) vhs_pair_kernel(const VhsArgs
   C* const fC = Fg + G::SLICE;
   const float invV = 1.f / (float)V;
   const int npq = a.P * a.M;
-  // a main thread's lines in every pass: L = tid + 256 h (h = 0, 1), with
+  // a main thread's lines in every pass: L = tid + NM h (h < LPT), with
   // hi = L >> 5 (k1l, or x2l in the third pass) and lo = L & 31 (k2, x3)
-  const int lo = tid & 31, hi0 = tid >> 5;  // hi of line h: hi0 + 8 h
+  const int lo = tid & 31, hi0 = tid >> 5;  // hi of line h: hi0 + HS h
   const uint32_t peer = (uint32_t)(r ^ 1);
   const uint32_t rbar = cluster_addr(&sBar, peer);
   const uint32_t rW = cluster_addr(sW, peer);
@@ -133,36 +142,36 @@ __global__ void __launch_bounds__(PairGeom::NT, 1) vhs_pair_kernel(const VhsArgs
   // has just read for its own second pass.  Nyquist threads run `nyq`
   // (their own second pass) meanwhile.
   auto pass2_exchange = [&](auto&& nyq) {
-    C out0[16];
+    if (has_nyq) nyq();
     if (is_main) {
+      C outp[LPT > 1 ? 16 : 1];  // outgoing half of line 0 while line 1 runs (LPT = 2)
 #pragma unroll 1
-      for (int h = 0; h < 2; ++h) {
-        const int hi = hi0 + 8 * h;
+      for (int h = 0; h < LPT; ++h) {
+        const int hi = hi0 + HS * h;
         C x[N];
 #pragma unroll
         for (int j = 0; j < N; ++j) x[j] = sW[(hi * N + j) * LP + lo];
         fft<float, N, +1>(x);
 #pragma unroll
         for (int j = 0; j < 16; ++j) sW[(hi * N + 16 * r + j) * LP + lo] = r ? x[16 + j] : x[j];
-        if (h == 0) {
+        if (h < LPT - 1) {
 #pragma unroll
-          for (int j = 0; j < 16; ++j) out0[j] = r ? x[j] : x[16 + j];
+          for (int j = 0; j < 16; ++j) outp[j % (LPT > 1 ? 16 : 1)] = r ? x[j] : x[16 + j];
         } else {
           cl_sync();  // both CTAs have read their second-pass lines
           if (tid == 0) mbar_expect_tx(&sBar, G::XBYTES);
 #pragma unroll
-          for (int hh = 0; hh < 2; ++hh) {
-            const int hj = hi0 + 8 * hh;
+          for (int hh = 0; hh < LPT; ++hh) {
+            const int hj = hi0 + HS * hh;
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
               const uint32_t off = (uint32_t)(((hj * N + 16 * r + j) * LP + lo) * sizeof(C));
-              st_async_f2(rW + off, hh == 0 ? out0[j] : (r ? x[j] : x[16 + j]), rbar);
+              st_async_f2(rW + off, hh < LPT - 1 ? outp[j % (LPT > 1 ? 16 : 1)] : (r ? x[j] : x[16 + j]), rbar);
             }
           }
         }
       }
     } else {
-      nyq();
       cl_sync();
     }
     mbar_wait_bounded(&sBar, (uint32_t)xpar, a.err, &sGaveUp);
@@ -183,8 +192,8 @@ __global__ void __launch_bounds__(PairGeom::NT, 1) vhs_pair_kernel(const VhsArgs
     // (272 lines), then through the scratch to lines (k2, k3) along x1
     if (is_main) {
 #pragma unroll 1
-      for (int h = 0; h < 2; ++h) {
-        const int hi = hi0 + 8 * h, x1 = 16 * r + hi;
+      for (int h = 0; h < LPT; ++h) {
+        const int hi = hi0 + HS * h, x1 = 16 * r + hi;
         const int64_t b0 = soa_ix(upt, a.ldim, elem, (int64_t)(x1 * N + lo) * N, V, a.soasz);
         C x[N];
 #pragma unroll
@@ -244,8 +253,8 @@ __global__ void __launch_bounds__(PairGeom::NT, 1) vhs_pair_kernel(const VhsArgs
         // pass 1: lines (k1, k2 = lo) along k3 | Nyquist first axes
         if (is_main) {
 #pragma unroll 1
-          for (int h = 0; h < 2; ++h) {
-            const int hi = hi0 + 8 * h, k1 = pair_kmap(r, hi), k2 = lo;
+          for (int h = 0; h < LPT; ++h) {
+            const int hi = hi0 + HS * h, k1 = pair_kmap(r, hi), k2 = lo;
             const C E12 = cmul(ph[k1], ph[N + k2]);
             C t12 = mk<C>(1.f, 0.f);
             if (k1 == NY) t12 = th1;
@@ -265,7 +274,8 @@ __global__ void __launch_bounds__(PairGeom::NT, 1) vhs_pair_kernel(const VhsArgs
 #pragma unroll
             for (int k = 0; k < N; ++k) sW[(hi * N + k2) * LP + k] = x[k];
           }
-        } else {
+        }
+        if (has_nyq) {
           // n F on the Nyquist planes (vhs_cube.cuh): plane 1 (k1 = N/2)
           // lines over k3, plane 2 (k2 = N/2) lines over k3, plane 3
           // (k3 = N/2) lines over k2; one coefficient per line
@@ -320,13 +330,12 @@ __global__ void __launch_bounds__(PairGeom::NT, 1) vhs_pair_kernel(const VhsArgs
 #pragma unroll
           for (int j = 0; j < N; ++j) T[j * LP + col] = x[j];
         });
-        __syncthreads();  // the Nyquist columns are complete
         // pass 3: lines (x2 = 16 r + hi, x3 = lo) along k1;
         // S += Re R^2 + Re Nq^2
         if (is_main) {
 #pragma unroll 1
-          for (int h = 0; h < 2; ++h) {
-            const int hi = hi0 + 8 * h, x2 = 16 * r + hi, x3 = lo;
+          for (int h = 0; h < LPT; ++h) {
+            const int hi = hi0 + HS * h, x2 = 16 * r + hi, x3 = lo;
             C x[N];
             pair_load3(x, sW, hi, lo);
             fft<float, N, +1>(x);
@@ -357,8 +366,8 @@ __global__ void __launch_bounds__(PairGeom::NT, 1) vhs_pair_kernel(const VhsArgs
       if (tid == 0) mbar_expect_tx(&sBar, G::XBYTES);
       if (is_main) {
 #pragma unroll 1
-        for (int h = 0; h < 2; ++h) {
-          const int hi = hi0 + 8 * h, x2 = 16 * r + hi;
+        for (int h = 0; h < LPT; ++h) {
+          const int hi = hi0 + HS * h, x2 = 16 * r + hi;
           C x[N];
           const float* Sl = sS + hi * N + lo;
 #pragma unroll
@@ -380,8 +389,8 @@ __global__ void __launch_bounds__(PairGeom::NT, 1) vhs_pair_kernel(const VhsArgs
       __syncthreads();
       if (is_main) {
 #pragma unroll 1
-        for (int h = 0; h < 2; ++h) {
-          const int hi = hi0 + 8 * h;
+        for (int h = 0; h < LPT; ++h) {
+          const int hi = hi0 + HS * h;
           C x[N];
 #pragma unroll
           for (int j = 0; j < N; ++j) x[j] = sW[(hi * N + j) * LP + lo];
@@ -394,8 +403,8 @@ __global__ void __launch_bounds__(PairGeom::NT, 1) vhs_pair_kernel(const VhsArgs
       if (is_main) {
         const float* w1 = a.w1t + (size_t)p * V;
 #pragma unroll 1
-        for (int h = 0; h < 2; ++h) {
-          const int hi = hi0 + 8 * h, k1 = pair_kmap(r, hi), k2 = lo, L = k1 * N + k2;
+        for (int h = 0; h < LPT; ++h) {
+          const int hi = hi0 + HS * h, k1 = pair_kmap(r, hi), k2 = lo, L = k1 * N + k2;
           C x[N];
 #pragma unroll
           for (int k = 0; k < N; ++k) x[k] = sW[(hi * N + k2) * LP + k];
@@ -429,8 +438,8 @@ __global__ void __launch_bounds__(PairGeom::NT, 1) vhs_pair_kernel(const VhsArgs
     for (int t = 0; t < 2; ++t) {
       if (is_main) {
 #pragma unroll 1
-        for (int h = 0; h < 2; ++h) {
-          const int hi = hi0 + 8 * h, k1 = pair_kmap(r, hi), k2 = lo, L = k1 * N + k2;
+        for (int h = 0; h < LPT; ++h) {
+          const int hi = hi0 + HS * h, k1 = pair_kmap(r, hi), k2 = lo, L = k1 * N + k2;
           const int m1 = (N - k1) % N, m2 = (N - k2) % N;
           C x[N];
 #pragma unroll
@@ -453,8 +462,8 @@ __global__ void __launch_bounds__(PairGeom::NT, 1) vhs_pair_kernel(const VhsArgs
       pass2_exchange([]() {});
       if (is_main) {
 #pragma unroll 1
-        for (int h = 0; h < 2; ++h) {
-          const int hi = hi0 + 8 * h;
+        for (int h = 0; h < LPT; ++h) {
+          const int hi = hi0 + HS * h;
           C x[N];
           pair_load3(x, sW, hi, lo);
           fft<float, N, +1>(x);
@@ -488,8 +497,8 @@ __global__ void __launch_bounds__(PairGeom::NT, 1) vhs_pair_kernel(const VhsArgs
       double mom[5] = {0, 0, 0, 0, 0};
       if (is_main) {
 #pragma unroll 1
-        for (int h = 0; h < 2; ++h) {
-          const int hi = hi0 + 8 * h;
+        for (int h = 0; h < LPT; ++h) {
+          const int hi = hi0 + HS * h;
           const float* Sl = sS + hi * N + lo;
 #pragma unroll 4
           for (int i = 0; i < N; ++i) {
@@ -530,8 +539,8 @@ __global__ void __launch_bounds__(PairGeom::NT, 1) vhs_pair_kernel(const VhsArgs
     }
     if (is_main) {
 #pragma unroll 1
-      for (int h = 0; h < 2; ++h) {
-        const int hi = hi0 + 8 * h;
+      for (int h = 0; h < LPT; ++h) {
+        const int hi = hi0 + HS * h;
         const float* Sl = sS + hi * N + lo;
         const int64_t b0 = soa_ix(upt, a.ldim, elem, (int64_t)(16 * r + hi) * N + lo, V, a.soasz);
         const int64_t st = (int64_t)NN * a.soasz;

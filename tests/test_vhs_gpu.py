@@ -257,15 +257,18 @@ def test_bounded_wait_that_runs_out_is_reported():
 
 
 @pytest.mark.parametrize('project', [0, 1])
-def test_pair_kernel_bank(project):
-    """The two-CTA kernel (FP32, N = 32, the default there) on a bank of
-    10 points over two AoSoA rows, with and without the FP64 projection,
-    against the oracle point by point; a second launch on the same banks
-    gives the same values (the per-pair scratch is rewritten per point)."""
+@pytest.mark.parametrize('variant', [0, 1])
+def test_pair_kernel_bank(project, variant):
+    """The two-CTA kernel (FP32, N = 32, the default there; both thread
+    layouts) on a bank of 10 points over two AoSoA rows, with and without
+    the FP64 projection, against the oracle point by point; a second launch
+    on the same banks gives the same values (the per-pair scratch is
+    rewritten per point)."""
     cfg = config('channel-n32', 'single', Nrho=4, M=6)
     cfg.set('backend-b200', 'vhs-project', project)
     be, vm, sm = _model(cfg)
-    assert sm.variants()[0]['exchange'] == 'pair'
+    assert sm.variants()[variant]['exchange'] == 'pair'
+    sm.select(variant)
     ovm, pre, prefac = oracle_for(cfg)
     nupts, neles = 2, 5
     f = random_states(vm.cv(), nupts*neles, seed=13).reshape(nupts, neles, -1)
