@@ -304,8 +304,8 @@ static int select_index(dgfs_vhs* h, int idx) {
   if (rc) return rc;
   const size_t esz = h->prec == 64 ? 16 : 8;
   // gain-spectrum scratch: one N^3 complex slice per cluster, or for the
-  // two-CTA kernel the half spectra of F and fC
-  const size_t need = v->push == 3 ? (size_t)ncl * 2 * PairGeom<1>::SLICE * esz
+  // two-CTA kernel the half spectra of F and fC and the staging buffers
+  const size_t need = v->push == 3 ? (size_t)ncl * PairGeom<1>::SCRATCH * esz
                                    : (size_t)ncl * v->C * (size_t)h->N * h->N * h->N / v->C * esz;
   if (need > h->fc_bytes) {
     cudaFree(h->fc);

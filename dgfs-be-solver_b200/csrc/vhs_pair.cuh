@@ -15,17 +15,20 @@
 //   x-slab   CTA r owns x2 in X_r = [16 r, 16 r + 16).
 // A 3D inverse transform runs along k3 on the lines (k1 in K_r, k2), along
 // k2 on the lines (k1 in K_r, x3), then along k1 on the lines (x2 in X_r,
-// x3).  Between the second and third passes each CTA pushes the half of its
-// k-slab that the other owns in x (16 complex values per line) straight into
-// the other CTA's shared memory with st.async, completing on its mbarrier;
-// the destination is the region the receiver has just read for its own
-// second pass, so one work cube per CTA suffices.  In the work cube W the
-// value (k1, x2, x3) of the third pass sits at row kinv(k1) * 32 +
-// 16 owner(k1) + x2 - 16 r.  Forward transforms (FFT(S_p)) run the passes in
-// the opposite order with the same exchange.  The spectrum F of the point
-// (k3 <= N/2, [k3][k1][k2]) and the gain spectrum fC live in the pair's
-// slice of a global scratch (L2 resident); S_p accumulates in shared memory.
-// Every mbarrier wait is bounded (the error flag of dgfs_vhs_status).
+// x3).  Between the second and third passes each CTA hands the half of its
+// k-slab that the other owns in x (16 complex values per line) to the other
+// through a staging buffer in the pair's global scratch (L2 resident):
+// coalesced 8-byte stores, one cluster barrier (release/acquire at cluster
+// scope), coalesced L2 loads straight into the third pass's registers.
+// Measured per (p, q), this moves the 64 KB a CTA sends about three times
+// faster than remote shared-memory stores (st.async into the peer's work
+// cube, an earlier form of this kernel).  The staging buffers alternate
+// between consecutive exchanges, so the barrier of one exchange also tells a
+// CTA that the peer has finished reading the buffer it is about to refill.
+// Forward transforms (FFT(S_p)) run the passes in the opposite order with
+// the same exchange.  The spectrum F of the point (k3 <= N/2, [k3][k1][k2])
+// and the gain spectrum fC live in the pair's slice of the scratch too; S_p
+// accumulates in shared memory.
 //
 // Shared memory (complex float unless noted): W [16][32][33], S [32][16][32]
 // (float), the Nyquist planes T1..T3 [32][33], two phase slots.  352
@@ -57,7 +60,9 @@ template <int LPT> struct PairGeom {
   static constexpr int OFF_PH = OFF_T + 3 * N * LP;      // [2][PHS] cx
   static constexpr int SMEM_CX = OFF_PH + 2 * PHS;
   static constexpr int SLICE = H * NN;                   // cx per spectrum in the scratch
-  static constexpr uint32_t XBYTES = NL * 16 * 8;        // bytes one exchange brings in
+  static constexpr int XSLAB = 16 * 16 * N;              // cx per staging buffer [k1l][j][x3]
+  // scratch per pair: F, fC, then [2 CTAs][2 alternating buffers] staging
+  static constexpr int SCRATCH = 2 * SLICE + 4 * XSLAB;
 };
 
 // k1 ownership: K_0 = {0..7, 16, 25..31}, K_1 = {8..15, 17..24}
@@ -69,21 +74,21 @@ __device__ __forceinline__ int pair_kmap(int r, int l) {
   return r == 0 ? (l <= 7 ? l : l == 8 ? 16 : l + 16) : (l <= 7 ? l + 8 : l + 9);
 }
 
-__device__ __forceinline__ void st_async_f2(uint32_t raddr, float2 v, uint32_t rbar) {
-  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f32 [%0], {%1, %2}, [%3];" ::"r"(raddr),
-               "f"(v.x), "f"(v.y), "r"(rbar)
-               : "memory");
-}
 __device__ __forceinline__ void cl_sync() {
   cl_arrive();
   cl_wait();
 }
 
-// third-pass line (x2l = hi, x3 = lo) along k1 from the two halves
-__device__ __forceinline__ void pair_load3(float2 (&x)[32], const float2* sW, int hi, int lo) {
+// third-pass line (x2l = hi, x3 = lo) along k1: the k1 of this CTA from its
+// work cube (row kinv(k1) * 32 + x2, x2 = 16 r + hi), the others from the
+// peer's staging buffer ([kinv(k1)][hi][lo], written before the barrier)
+__device__ __forceinline__ void pair_load3(float2 (&x)[32], const float2* sW, const float2* xpeer, int r, int hi,
+                                           int lo) {
   constexpr int N = 32, LP = 33;
 #pragma unroll
-  for (int k1 = 0; k1 < N; ++k1) x[k1] = sW[(pair_kinv(k1) * N + 16 * pair_owner(k1) + hi) * LP + lo];
+  for (int k1 = 0; k1 < N; ++k1)
+    x[k1] = pair_owner(k1) == r ? sW[(pair_kinv(k1) * N + 16 * r + hi) * LP + lo]
+                                : __ldcg(xpeer + (pair_kinv(k1) * 16 + hi) * N + lo);
 }
 
 template <int LPT>
@@ -100,8 +105,6 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
   C* const sT2 = sT1 + N * LP;
   C* const sT3 = sT2 + N * LP;
   C* const sPh = reinterpret_cast<C*>(smem_raw) + G::OFF_PH;
-  __shared__ __align__(8) uint64_t sBar;
-  __shared__ int sGaveUp;
   __shared__ double sRed[5][G::NT / 32];
   __shared__ double sMom[5];
 
@@ -115,25 +118,18 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
   const int cid = blockIdx.x / 2, ncl = gridDim.x / 2;
   // the pair's scratch: F [H][N][N] then fC [H][N][N] (fC doubles as the
   // exchange buffer of the forward transform of f)
-  C* const Fg = a.fc + (size_t)cid * 2 * G::SLICE;
+  C* const Fg = a.fc + (size_t)cid * G::SCRATCH;
   C* const fC = Fg + G::SLICE;
+  C* const Xs = fC + G::SLICE;  // staging: [rank][buffer][k1l][j][x3]
   const float invV = 1.f / (float)V;
   const int npq = a.P * a.M;
   // a main thread's lines in every pass: L = tid + NM h (h < LPT), with
   // hi = L >> 5 (k1l, or x2l in the third pass) and lo = L & 31 (k2, x3)
   const int lo = tid & 31, hi0 = tid >> 5;  // hi of line h: hi0 + HS h
   const uint32_t peer = (uint32_t)(r ^ 1);
-  const uint32_t rbar = cluster_addr(&sBar, peer);
-  const uint32_t rW = cluster_addr(sW, peer);
-  int xpar = 0;  // parity of the next exchange on sBar
-
-  if (tid == 0) {
-    sGaveUp = 0;
-    mbar_init(&sBar, 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
-  cl_sync();
+  int xb = 0;  // staging buffer of the next exchange
+  auto xmine = [&](int b) { return Xs + (size_t)(r * 2 + b) * G::XSLAB; };
+  auto xpeer = [&](int b) { return (const C*)(Xs + (size_t)((r ^ 1) * 2 + b) * G::XSLAB); };
 
   // Second pass of an inverse transform (lines (k1l, x3 = lo) along k2) and
   // the exchange: of the 32 outputs (index x2) of each line the 16 with x2
@@ -141,10 +137,15 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
   // k1l * 32 + 16 r + (x2 - 16 (1 - r)) of its work cube -- the region it
   // has just read for its own second pass.  Nyquist threads run `nyq`
   // (their own second pass) meanwhile.
-  auto pass2_exchange = [&](auto&& nyq) {
+  // Second pass of an inverse transform (lines (k1l, x3 = lo) along k2) and
+  // the exchange: of the 32 outputs (index x2) of each line the 16 with x2
+  // in X_r stay in the work cube, the others go to this CTA's staging buffer
+  // [k1l][x2 - 16 (1 - r)][x3] for the peer.  Nyquist threads run `nyq`
+  // (their own second pass) meanwhile.  Returns the buffer to read.
+  auto pass2_exchange = [&](auto&& nyq) -> int {
     if (has_nyq) nyq();
     if (is_main) {
-      C outp[LPT > 1 ? 16 : 1];  // outgoing half of line 0 while line 1 runs (LPT = 2)
+      C* const xs = xmine(xb);
 #pragma unroll 1
       for (int h = 0; h < LPT; ++h) {
         const int hi = hi0 + HS * h;
@@ -153,31 +154,17 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
         for (int j = 0; j < N; ++j) x[j] = sW[(hi * N + j) * LP + lo];
         fft<float, N, +1>(x);
 #pragma unroll
-        for (int j = 0; j < 16; ++j) sW[(hi * N + 16 * r + j) * LP + lo] = r ? x[16 + j] : x[j];
-        if (h < LPT - 1) {
-#pragma unroll
-          for (int j = 0; j < 16; ++j) outp[j % (LPT > 1 ? 16 : 1)] = r ? x[j] : x[16 + j];
-        } else {
-          cl_sync();  // both CTAs have read their second-pass lines
-          if (tid == 0) mbar_expect_tx(&sBar, G::XBYTES);
-#pragma unroll
-          for (int hh = 0; hh < LPT; ++hh) {
-            const int hj = hi0 + HS * hh;
-#pragma unroll
-            for (int j = 0; j < 16; ++j) {
-              const uint32_t off = (uint32_t)(((hj * N + 16 * r + j) * LP + lo) * sizeof(C));
-              st_async_f2(rW + off, hh < LPT - 1 ? outp[j % (LPT > 1 ? 16 : 1)] : (r ? x[j] : x[16 + j]), rbar);
-            }
-          }
+        for (int j = 0; j < 16; ++j) {
+          sW[(hi * N + 16 * r + j) * LP + lo] = r ? x[16 + j] : x[j];
+          __stcg(xs + (hi * 16 + j) * N + lo, r ? x[j] : x[16 + j]);
         }
       }
-    } else {
-      cl_sync();
     }
-    mbar_wait_bounded(&sBar, (uint32_t)xpar, a.err, &sGaveUp);
-    xpar ^= 1;
+    cl_sync();  // both halves staged (cluster-scope release / acquire)
+    const int b = xb;
+    xb ^= 1;
+    return b;
   };
-
   const int npts = a.pcount ? min(a.npts, *a.pcount) : a.npts;
 #pragma unroll 1
   for (int ip = cid; ip < npts; ip += ncl) {
@@ -320,7 +307,7 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
         }
         // pass 2 and the exchange | Nyquist second axes (all 32 columns of
         // every plane; the third pass reads the rows of its own x2 half)
-        pass2_exchange([&]() {
+        const int xr = pass2_exchange([&]() {
           const int which = tq / N, col = tq % N;
           C* T = which == 0 ? sT1 : (which == 1 ? sT2 : sT3);
           C x[N];
@@ -337,7 +324,7 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
           for (int h = 0; h < LPT; ++h) {
             const int hi = hi0 + HS * h, x2 = 16 * r + hi, x3 = lo;
             C x[N];
-            pair_load3(x, sW, hi, lo);
+            pair_load3(x, sW, xpeer(xr), r, hi, lo);
             fft<float, N, +1>(x);
             const C t1 = sT1[x2 * LP + x3];
             const float s2 = (x2 & 1) ? -1.f : 1.f, s3 = (x3 & 1) ? -1.f : 1.f;
@@ -362,9 +349,8 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
       // (k1l, x3) along x2, lines (k1l, k2) along x3 into fC (k3 <= N/2).
       // An output k1 of a first-pass line is local when owned, else pushed
       // to the peer's row kinv(k1) * 32 + x2.
-      cl_sync();  // the peer has finished its third pass (its W is free)
-      if (tid == 0) mbar_expect_tx(&sBar, G::XBYTES);
       if (is_main) {
+        C* const xs = xmine(xb);
 #pragma unroll 1
         for (int h = 0; h < LPT; ++h) {
           const int hi = hi0 + HS * h, x2 = 16 * r + hi;
@@ -375,25 +361,23 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
           fft<float, N, -1>(x);
 #pragma unroll
           for (int k1 = 0; k1 < N; ++k1) {
-            const int row = pair_kinv(k1) * N + x2;
-            if (pair_owner(k1) == r) {
-              sW[row * LP + lo] = x[k1];
-            } else {
-              st_async_f2(rW + (uint32_t)((row * LP + lo) * sizeof(C)), x[k1], rbar);
-            }
+            if (pair_owner(k1) == r) sW[(pair_kinv(k1) * N + x2) * LP + lo] = x[k1];
+            else __stcg(xs + (pair_kinv(k1) * 16 + hi) * N + lo, x[k1]);
           }
         }
       }
-      mbar_wait_bounded(&sBar, (uint32_t)xpar, a.err, &sGaveUp);
-      xpar ^= 1;
-      __syncthreads();
+      cl_sync();  // both halves staged
+      const int xr = xb;
+      xb ^= 1;
       if (is_main) {
 #pragma unroll 1
         for (int h = 0; h < LPT; ++h) {
           const int hi = hi0 + HS * h;
+          const C* xp = xpeer(xr);
           C x[N];
 #pragma unroll
-          for (int j = 0; j < N; ++j) x[j] = sW[(hi * N + j) * LP + lo];
+          for (int j = 0; j < N; ++j)
+            x[j] = (j >> 4) == r ? sW[(hi * N + j) * LP + lo] : __ldcg(xp + (hi * 16 + (j & 15)) * N + lo);
           fft<float, N, -1>(x);
 #pragma unroll
           for (int j = 0; j < N; ++j) sW[(hi * N + j) * LP + lo] = x[j];
@@ -459,13 +443,13 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
         }
       }
       __syncthreads();
-      pass2_exchange([]() {});
+      const int xr = pass2_exchange([]() {});
       if (is_main) {
 #pragma unroll 1
         for (int h = 0; h < LPT; ++h) {
           const int hi = hi0 + HS * h;
           C x[N];
-          pair_load3(x, sW, hi, lo);
+          pair_load3(x, sW, xpeer(xr), r, hi, lo);
           fft<float, N, +1>(x);
           float* Sl = sS + hi * N + lo;
           if (t == 0) {
