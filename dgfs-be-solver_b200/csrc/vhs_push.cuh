@@ -79,7 +79,7 @@ __device__ __forceinline__ void mbar_wait_bounded(uint64_t* bar, uint32_t parity
 // that expects 16 bytes nothing will send, so the wait runs out after
 // `limit_ns` and sets `err`, exactly as a push exchange whose data never
 // arrives would.  Nothing else is touched; the launch ends after one timeout.
-__global__ void __launch_bounds__(32) wait_check_kernel(int* err, uint64_t limit_ns) {
+static __global__ void __launch_bounds__(32) wait_check_kernel(int* err, uint64_t limit_ns) {
   __shared__ __align__(8) uint64_t bar;
   __shared__ int gave_up;
   if (threadIdx.x == 0) {

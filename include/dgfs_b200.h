@@ -196,6 +196,51 @@ DGFS_API int dgfs_vhs_check_wait(dgfs_vhs* h, long long limit_ns,
                                  void* stream);
 
 /* ------------------------------------------------------------------------
+ * Binary-mixture VSS collision operator
+ *
+ * Replaces: DGFSBiVSSGLLScatteringModel (frfs/solvers/dgfsbi/
+ * scattering.py:44-330): one handle per ordered species pair (p, q) holds
+ * the pair's precomputation (scattering.py:172-198, vss-gll.mako:31-93);
+ * dgfs_vss_apply evaluates Qij (scattering.py:227-315).  fs(elem, upt,
+ * f_0, f_1, Q_0, Q_1) of the reference is Q_p = sum_q Q(f_p, f_q): apply
+ * the pair (p, 0) without and (p, 1) with accumulation.
+ * ---------------------------------------------------------------------- */
+typedef struct dgfs_vss dgfs_vss;
+
+typedef struct dgfs_vss_params {
+  int Nv;             /* velocity points per direction (8, 16, 24, 32)      */
+  int Nrho;           /* Gauss radial nodes                                 */
+  int M;              /* full-sphere directions of the transforms           */
+  int Mpre;           /* full-sphere directions of the precomputation       */
+  int precision;      /* 64 or 32 (Nv = 32: 32 only)                        */
+  double L;           /* velocity domain half width                         */
+  const double* qz;   /* [Nrho] radial nodes on [0, R] (dgfsbi/velocitymesh.py:137-140) */
+  const double* qw;   /* [Nrho] radial weights                              */
+  const double* sz;   /* [M*3] full-sphere design (sw = 4 pi / M)           */
+  const double* szpre;/* [Mpre*3] design of the precomputation              */
+  double mp, mq;      /* nondimensional masses of species p and q           */
+  double alpha;       /* VSS scattering exponent (eta = alpha - 1)          */
+  double omega;       /* viscosity exponent (gamma = 2 (1 - omega))         */
+  double prefactor;   /* the pair's prefactor (scattering.py:64-87)         */
+} dgfs_vss_params;
+
+DGFS_API int dgfs_vss_create(const dgfs_vss_params* params, dgfs_vss** out);
+DGFS_API int dgfs_vss_destroy(dgfs_vss* h);
+
+/* Q(f_p, f_q) for one point (elem >= 0) or every point of a bank (elem < 0,
+ * one persistent launch); fp, fq, Q device banks of the handle's precision
+ * in the AoSoA layout of dgfs_vhs_apply (fp may equal fq; Q overlaps
+ * neither); accumulate != 0 adds to Q instead of overwriting it. */
+DGFS_API int dgfs_vss_apply(dgfs_vss* h, const void* fp, const void* fq,
+                            void* Q, int nupts, int neles, long long ldim,
+                            int soasz, int elem, int upt, int accumulate,
+                            void* stream);
+
+/* Synchronise `stream`, then report and clear the kernel's bounded-wait
+ * error flag (DGFS_ERR_CUDA when a wait gave up). */
+DGFS_API int dgfs_vss_status(dgfs_vss* h, void* stream, int* flag);
+
+/* ------------------------------------------------------------------------
  * FR-DG advection residual over all velocities
  *
  * Replaces: the element/interface kernels behind DGFSSystem.rhs and

@@ -91,3 +91,24 @@ def test_equilibrium(setup):
     Qne = vss.vss_Q([g1, g2], mesh, pre, params)
     for a, b in zip(Qeq, Qne):
         assert np.max(np.abs(a)) < 1e-2*np.max(np.abs(b))
+
+
+def test_product_mixture_mesh_matches_oracle():
+    """frfs_b200.mixture's mesh (the product side of dgfsbi/velocitymesh.py)
+    equals the oracle's restatement."""
+    import sys
+    sys.path.insert(0, __import__('os').path.dirname(__file__))
+    from test_vss_gpu import mixture_config
+    from frfs_b200.mixture import DGFSBiVelocityMesh
+    cfg = mixture_config('double', Nv=24, Nrho=12)
+    vm = DGFSBiVelocityMesh(None, cfg)
+    mesh = vss.mixture_mesh(24, 12, vm.sz(), [39.96e-3, 83.8e-3], H0=1e-3,
+                            T0=273.0, rho0=1.5e-3, molarMass0=39.96e-3,
+                            cmax=0.0, Tmax=273.0, dev=5.0)
+    for k in ('L', 'S', 'R', 'cw'):
+        assert getattr(vm, k)() == pytest.approx(mesh[k], rel=1e-15) \
+            if hasattr(vm, k) else True
+    np.testing.assert_allclose(vm.qz(), mesh['qz'], rtol=1e-15)
+    np.testing.assert_allclose(vm.qw(), mesh['qw'], rtol=1e-14)
+    np.testing.assert_array_equal(vm.cv(), mesh['cv'])
+    assert vm.masses() == pytest.approx(mesh['masses'], rel=1e-15)
