@@ -130,7 +130,10 @@ template <typename T> int upload_cx(void** dst, const std::vector<std::complex<d
 // scattering.py:172-198): with l the index grid (0..N/2-1, -N/2..-1 per
 // axis, I slowest), fac_x = pi / L qz_x and the full-sphere designs sz (M
 // directions, sw = 4 pi / M) and szpre (Mpre, swpre = 4 pi / Mpre):
-//   B[y][y'] = (1 + sz_y . szpre_y')^eta           (clipped at 0)
+//   B[y][y'] = (1 + sz_y . szpre_y')^eta           (1 + cos below 1e-12 in
+//              magnitude is the exact 0 of an antipodal pair of the
+//              symmetric designs: rounding leaves +-1e-16 there, where pow
+//              would give NaN or up to (1e-16)^eta)
 //   b_xy(l)  = swpre qz_x^(gamma+2) sum_y' B[y][y'] e^{-i mq/(mp+mq) fac_x szpre_y'.l}
 //   c(l)     = sum_x qw_x sw swpre qz_x^(gamma+2) sum_y sum_y' B[y][y'] e^{-i fac_x szpre_y'.l}
 // and the weight of computeQG, w_x = qw_x sw / V, folded into b_xy.
@@ -158,6 +161,7 @@ template <typename T> int build(dgfs_vss* h, const dgfs_vss_params* p) {
     for (int y2 = 0; y2 < Mp; ++y2) {
       double d = 1.0;
       for (int ax = 0; ax < 3; ++ax) d += p->sz[y * 3 + ax] * p->szpre[y2 * 3 + ax];
+      if (std::fabs(d) < 1e-12) d = 0.0;
       B[(size_t)y * Mp + y2] = std::pow(d > 0.0 ? d : 0.0, eta);
     }
   // szpre_y' . l for every grid point

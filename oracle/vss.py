@@ -6,9 +6,10 @@ the per-pair parameters and precomputation
 (scattering.py:227-330 with the kernels of
 frfs/solvers/dgfsbi/kernels/scattering/vss-gll.mako).
 
-Test infrastructure only (see ``oracle/__init__.py``); no product kernel
-evaluates this operator.  Conventions as the VHS oracle: cuFFT's
-unnormalised forward/inverse transforms, velocity index I slowest.
+Test infrastructure only (see ``oracle/__init__.py``): the checker of the
+product's VSS kernel (tests/test_vss_gpu.py).  Conventions as the VHS
+oracle: cuFFT's unnormalised forward/inverse transforms, velocity index I
+slowest.
 """
 
 from math import gamma as _gammafn
@@ -86,10 +87,14 @@ def vss_precompute(mesh, params, szpre):
     for pq, prm in params.items():
         mp, mq = masses[int(pq[0])], masses[int(pq[1])]
         mpq = mq/(mp + mq)
-        # (1 + cos)^eta; antipodal pairs of a symmetric design give
-        # 1 + cos = -1e-16 in floating point, where the reference's pow
-        # would return NaN: clipped at 0 here
-        B = np.maximum(1. + sz @ szpre.T, 0.0)**prm['eta']    # (M, Mpre)
+        # (1 + cos)^eta (vss-gll.mako:74-76); for the antipodal pairs of a
+        # symmetric design 1 + cos is 0 mathematically but +-1e-16 after
+        # rounding, where the reference's pow gives NaN (negative) or up to
+        # (1e-16)^eta (positive) depending on the summation order: values
+        # below 1e-12 in magnitude are taken as the exact 0
+        d = 1. + sz @ szpre.T
+        d[np.abs(d) < 1e-12] = 0.0
+        B = np.maximum(d, 0.0)**prm['eta']                     # (M, Mpre)
         b = np.empty((P, M, V), dtype=np.complex128)
         c = np.zeros(V, dtype=np.complex128)
         for x in range(P):
