@@ -416,6 +416,13 @@ def run_b200(args):
                 whole['spt_quad_p0'], world))
             prank = rank
         system = DGFSSystem(be, cfg, mesh=mesh, prank=prank, initsoln=f0)
+        if part:
+            # every rank joins one collective before the first
+            # point-to-point exchange (NCCL communicator set-up)
+            dist.barrier()
+        # residual launch shape: timed on this mesh, fastest kept (setup,
+        # not timed; bank 1 is scratch before the first step)
+        dg_tune = system.autotune_dg(0, 1)
         vm, sm = system.vm, system.sm
         stepper = StdTVDRK2DGFSStepper(system, cfg)
         fin, fout = system.bank[0], system.bank[1]
@@ -556,7 +563,9 @@ def run_b200(args):
             'peak_source': 'MEASURED_PEAKS.json hbm_gbs' if peaks
             else 'fallback 6650 GB/s',
             'bytes_per_launch': dg_bytes, 'launch_ms': dg_ms,
-            'kernels': 'dg_interp_kernel + dg_residual_kernel'}
+            'kernels': 'dg_interp_kernel + dg_residual_kernel',
+            'residual_shape': system.dg_variants()[system._dg_shape],
+            'ms_by_shape': dg_tune}
     launch = sm.launch_info()
 
     if rank == 0 and world == 1 and args.precision == 'single':

@@ -12,6 +12,7 @@ using namespace dgfs;
 
 struct dgfs_dg {
   int prec, D, U, F, V, E, nb, ngroups, device, nhalo, nsend;
+  int shape;  // residual launch shape (kDgShapes)
   long long ldim_u, ldim_f;
   double cw;
   std::vector<double> m0, m132, m3, m12;  // host copies (operators travel as params)
@@ -27,7 +28,16 @@ struct dgfs_dg {
 };
 
 constexpr int kBcChunks = 256;  // velocity chunks of the wall-sum reduction
-constexpr int kVpt = 8;         // velocities per warp in the interp/residual kernels
+constexpr int kVpt = 8;         // velocities per warp in the interp kernel
+
+// Residual launch shapes: (velocities per warp, prefetch of the RK terms,
+// CTAs per SM of the register budget); MB 0 = the precision's default
+// (3 for FP32 p <= 2, 2 for FP32 p = 3 and FP64 p <= 2, 1 for FP64 p = 3).
+struct DgShape {
+  int vpt, pf, mb;
+};
+constexpr DgShape kDgShapes[] = {{8, 0, 0}, {8, 1, 0}, {8, 1, 2}, {16, 1, 2}, {4, 0, 0}};
+constexpr int kDgNumShapes = sizeof(kDgShapes) / sizeof(kDgShapes[0]);
 
 namespace {
 
@@ -184,6 +194,19 @@ cudaError_t run_interp(const dgfs_dg* h, const void* u, int v0, int nv, cudaStre
 }
 
 template <typename T, int U, int F, int D>
+constexpr int dg_default_mb() {
+  return sizeof(T) == 4 ? (U <= 9 ? 3 : 2) : (U <= 9 ? 2 : 1);
+}
+
+template <typename T, int U, int F, int D, int VPT, int PF, int MB>
+cudaError_t launch_rhs(const dgfs_dg* h, const DgArgs<T>& a, int nv, cudaStream_t s) {
+  constexpr int mb = MB ? MB : dg_default_mb<T, U, F, D>();
+  const dim3 grid((unsigned)((h->E + 31) / 32), (unsigned)((nv + 8 * VPT - 1) / (8 * VPT)));
+  dg_residual_kernel<T, U, F, D, VPT, PF, mb><<<grid, 256, 0, s>>>(a, make_ops<T, U, F, D>(h));
+  return cudaGetLastError();
+}
+
+template <typename T, int U, int F, int D>
 cudaError_t run_rhs(const dgfs_dg* h, const void* u, void* out, int v0, int nv, double alpha, const void* A,
                     double beta, const void* B, double gamma, const void* C, cudaStream_t s) {
   DgArgs<T> a = make_args<T>(h);
@@ -197,8 +220,13 @@ cudaError_t run_rhs(const dgfs_dg* h, const void* u, void* out, int v0, int nv, 
   a.gamma = (T)gamma;
   a.v0 = v0;
   a.nv = nv;
-  dg_residual_kernel<T, U, F, D, kVpt><<<grid_blk(h, nv), 256, 0, s>>>(a, make_ops<T, U, F, D>(h));
-  return cudaGetLastError();
+  switch (h->shape) {
+    case 1: return launch_rhs<T, U, F, D, 8, 1, 0>(h, a, nv, s);
+    case 2: return launch_rhs<T, U, F, D, 8, 1, 2>(h, a, nv, s);
+    case 3: return launch_rhs<T, U, F, D, 16, 1, 2>(h, a, nv, s);
+    case 4: return launch_rhs<T, U, F, D, 4, 0, 0>(h, a, nv, s);
+    default: return launch_rhs<T, U, F, D, 8, 0, 0>(h, a, nv, s);
+  }
 }
 
 template <typename T, int U, int F, int D>
@@ -489,6 +517,32 @@ extern "C" int dgfs_dg_set_halo(dgfs_dg* h, const void* recv) {
   int rc = recv ? check_bank(h, recv, "halo") : DGFS_OK;
   if (rc) return rc;
   h->halo = recv;
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_dg_num_variants(const dgfs_dg* h, int* count) {
+  clear_error();
+  if (!h || !count) return set_error(DGFS_ERR_INVALID, "null argument");
+  *count = kDgNumShapes;
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_dg_variant_info(const dgfs_dg* h, int idx, int* vpt, int* prefetch, int* min_ctas_per_sm) {
+  clear_error();
+  if (!h || !vpt || !prefetch || !min_ctas_per_sm) return set_error(DGFS_ERR_INVALID, "null argument");
+  if (idx < 0 || idx >= kDgNumShapes) return set_error(DGFS_ERR_INVALID, "variant %d outside 0..%d", idx, kDgNumShapes - 1);
+  const DgShape& sh = kDgShapes[idx];
+  *vpt = sh.vpt;
+  *prefetch = sh.pf;
+  *min_ctas_per_sm = sh.mb ? sh.mb : (h->prec == 32 ? (h->U <= 9 ? 3 : 2) : (h->U <= 9 ? 2 : 1));
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_dg_select(dgfs_dg* h, int idx) {
+  clear_error();
+  if (!h) return set_error(DGFS_ERR_INVALID, "null handle");
+  if (idx < 0 || idx >= kDgNumShapes) return set_error(DGFS_ERR_INVALID, "variant %d outside 0..%d", idx, kDgNumShapes - 1);
+  h->shape = idx;
   return DGFS_OK;
 }
 

@@ -299,10 +299,14 @@ __device__ __forceinline__ T dg_ghost(const DgArgs<T>& a, int b, int v, int64_t 
   return ul;  // outlet
 }
 
-// FP32 up to p = 2 holds its working set in 80 registers (3 CTAs of 256 per
-// SM), FP32 p = 3 and FP64 up to p = 2 in 128 (2 per SM), FP64 p = 3 in 160.
-template <typename T, int U, int F, int D, int VPT>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? (U <= 9 ? 3 : 2) : (U <= 9 ? 2 : 1))
+// Launch shapes (the autotuner's choice, dgfs_dg_select): VPT velocities per
+// warp and CTA chunk; PF = 1 loads the Runge-Kutta terms A, B, C of an
+// iteration together with u, before the flux work, as one combination
+// K = a A + b B + g C (U more registers); MB CTAs of 256 per SM the
+// register budget is compiled for (FP32 p <= 2 needs 80 registers at
+// PF = 0, FP32 p = 3 and FP64 p <= 2 128, FP64 p = 3 160).
+template <typename T, int U, int F, int D, int VPT, int PF, int MB>
+__global__ void __launch_bounds__(256, MB)
     dg_residual_kernel(const DgArgs<T> a, const DgOps<T, U, F, D> op) {
   using G = DgGeo<T, U, F, D>;
   __shared__ __align__(16) T sg[32 * G::GS];
@@ -334,6 +338,17 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? (U <= 9 ? 3 : 2) : (U <=
       const T* up = a.u + o;
 #pragma unroll
       for (int i = 0; i < U; ++i, up += a.ldim_u) u[i] = __ldg(up);
+    }
+    T K[PF ? U : 1];
+    if constexpr (PF != 0) {
+#pragma unroll
+      for (int r = 0; r < U; ++r) {
+        const int64_t ro = o + (int64_t)r * a.ldim_u;
+        T k = a.Cq ? a.gamma * __ldg(a.Cq + ro) : T(0);
+        if (a.A) k = fma(a.alpha, __ldg(a.A + ro), k);
+        if (a.B) k = fma(a.beta, __ldg(a.B + ro), k);
+        K[r] = k;
+      }
     }
     T urv[F];
 #pragma unroll
@@ -396,21 +411,27 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? (U <= 9 ? 3 : 2) : (U <=
 
     T rj[G::NR];
     lds16<T, G::NR / G::VW>(gl + G::OR, rj);
-    const T* ap = a.A ? a.A + o : nullptr;
-    const T* bp = a.B ? a.B + o : nullptr;
-    const T* cp = a.Cq ? a.Cq + o : nullptr;
-    T* op_ = a.out + o;
+    if constexpr (PF != 0) {
+      T* op_ = a.out + o;
 #pragma unroll
-    for (int r = 0; r < U; ++r) {
-      const T Rr = -rj[r] * R[r];
-      T res = a.gamma * (cp ? Rr + __ldg(cp) : Rr);
-      if (ap) res = fma(a.alpha, __ldg(ap), res);
-      if (bp) res = fma(a.beta, __ldg(bp), res);
-      *op_ = res;
-      op_ += a.ldim_u;
-      if (ap) ap += a.ldim_u;
-      if (bp) bp += a.ldim_u;
-      if (cp) cp += a.ldim_u;
+      for (int r = 0; r < U; ++r, op_ += a.ldim_u) *op_ = fma(a.gamma, -rj[r] * R[r], K[r]);
+    } else {
+      const T* ap = a.A ? a.A + o : nullptr;
+      const T* bp = a.B ? a.B + o : nullptr;
+      const T* cp = a.Cq ? a.Cq + o : nullptr;
+      T* op_ = a.out + o;
+#pragma unroll
+      for (int r = 0; r < U; ++r) {
+        const T Rr = -rj[r] * R[r];
+        T res = a.gamma * (cp ? Rr + __ldg(cp) : Rr);
+        if (ap) res = fma(a.alpha, __ldg(ap), res);
+        if (bp) res = fma(a.beta, __ldg(bp), res);
+        *op_ = res;
+        op_ += a.ldim_u;
+        if (ap) ap += a.ldim_u;
+        if (bp) bp += a.ldim_u;
+        if (cp) cp += a.ldim_u;
+      }
     }
   }
 }

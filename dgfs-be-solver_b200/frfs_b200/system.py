@@ -66,6 +66,10 @@ _lib.declare('dgfs_dg_invmass', c_int, [c_void_p, c_void_p, c_void_p, c_int,
                                         c_int, c_void_p])
 _lib.declare('dgfs_dg_pack', c_int, [c_void_p, c_void_p, c_void_p])
 _lib.declare('dgfs_dg_set_halo', c_int, [c_void_p, c_void_p])
+_lib.declare('dgfs_dg_num_variants', c_int, [c_void_p, c_ip])
+_lib.declare('dgfs_dg_variant_info', c_int, [c_void_p, c_int, c_ip, c_ip,
+                                             c_ip])
+_lib.declare('dgfs_dg_select', c_int, [c_void_p, c_int])
 _lib.declare('dgfs_dg_bcvals', c_int, [c_void_p, c_dp, c_int])
 _lib.declare('dgfs_dg_fpts', c_int, [c_void_p, ct.POINTER(c_void_p),
                                      ct.POINTER(c_ll)])
@@ -149,6 +153,7 @@ class DGFSSystem:
         self.surrogate = None
         self.collide_hook = None
         self.halo_exchange = halo_exchange
+        self._dg_shape = 0
         self._build_dg()
 
     # -- DG handle ----------------------------------------------------------
@@ -370,6 +375,53 @@ class DGFSSystem:
         _lib.check(self._lib.dgfs_dg_invmass(
             self._dg, u._as_parameter_, out._as_parameter_, 0,
             self.vm.vsize(), self.backend.stream), 'dgfs_dg_invmass')
+
+    # -- residual launch shapes (the autotuner's knob) -------------------------
+    def dg_variants(self):
+        """Compiled residual launch shapes: velocities per warp, whether
+        the Runge-Kutta terms are loaded ahead of the flux work, CTAs per SM
+        of the register budget."""
+        n = c_int()
+        _lib.check(self._lib.dgfs_dg_num_variants(self._dg, ct.byref(n)),
+                   'dgfs_dg_num_variants')
+        out = []
+        for i in range(n.value):
+            v = [c_int() for _ in range(3)]
+            _lib.check(self._lib.dgfs_dg_variant_info(
+                self._dg, i, *[ct.byref(x) for x in v]),
+                'dgfs_dg_variant_info')
+            out.append(dict(vpt=v[0].value, prefetch=v[1].value,
+                            min_ctas_per_sm=v[2].value))
+        return out
+
+    def select_dg(self, idx):
+        _lib.check(self._lib.dgfs_dg_select(self._dg, int(idx)),
+                   'dgfs_dg_select')
+        self._dg_shape = int(idx)
+
+    def autotune_dg(self, uin=0, out=1, reps=3):
+        """Time every residual launch shape on a full Runge-Kutta stage of
+        bank ``uin`` into bank ``out`` (overwritten: call before stepping)
+        and keep the fastest; returns {shape index: ms}."""
+        import torch
+        dev = self.backend.device
+        ms = {}
+        for i in range(len(self.dg_variants())):
+            self.select_dg(i)
+            stage = lambda: self.rk_stage(uin, out, 0.5, uin, 0.5, uin, 1e-4,
+                                          uin, interp=(i == 0))
+            stage()
+            torch.cuda.synchronize(dev)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                stage()
+            e1.record()
+            e1.synchronize()
+            ms[i] = e0.elapsed_time(e1)/reps
+        self.select_dg(min(ms, key=ms.get))
+        return ms
 
     def moments(self, bankidx=None):
         """FP64 moments at every solution point of a bank, shape

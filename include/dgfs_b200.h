@@ -352,6 +352,16 @@ DGFS_API int dgfs_dg_set_halo(dgfs_dg* h, const void* recv);
 DGFS_API int dgfs_dg_invmass(dgfs_dg* h, const void* u, void* out, int v0,
                              int nv, void* stream);
 
+/* Launch shapes of the residual kernel (the autotuner's knob): count; per
+ * index the velocities per warp, whether the Runge-Kutta terms are loaded
+ * ahead of the flux work, and the CTAs per SM the register budget was
+ * compiled for; dgfs_dg_select sets the shape of later dgfs_dg_rhs calls
+ * (index 0 by default).  No counterpart in the reference. */
+DGFS_API int dgfs_dg_num_variants(const dgfs_dg* h, int* count);
+DGFS_API int dgfs_dg_variant_info(const dgfs_dg* h, int idx, int* vpt,
+                                  int* prefetch, int* min_ctas_per_sm);
+DGFS_API int dgfs_dg_select(dgfs_dg* h, int idx);
+
 /* Copy the 2*nbfpts diffuse-wall sums to host memory (synchronous). */
 DGFS_API int dgfs_dg_bcvals(const dgfs_dg* h, double* host, int n);
 

@@ -138,3 +138,48 @@ def test_partitioned_residual_equals_whole_mesh_residual(world):
     assert sorted(out.keys()) == list(range(world))
     for r in range(world):
         assert out[r] < 1e-13, (r, out[r])
+
+
+@pytest.mark.parametrize('workload,world', [('couette-n24', 2),
+                                            ('couette-n24', 8),
+                                            ('channel-n32', 2),
+                                            ('channel-n32', 4),
+                                            ('channel-n32', 8)])
+def test_weak_scaled_bench_partitions(workload, world):
+    """bench.py's multi-GPU set-up: the workload widened to `world` copies
+    along x splits into `world` parts of exactly the single-GPU workload's
+    element count, every part has the shared faces of a strip (two
+    neighbours, one for the walled Couette slab's end parts) and its halo
+    rows pair up with its neighbours' rows."""
+    import argparse
+    import importlib.util
+    import os
+    from conftest import ROOT
+    spec = importlib.util.spec_from_file_location(
+        'bench', os.path.join(ROOT, 'bench.py'))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    args = argparse.Namespace(workload=workload, precision='single',
+                              project=1, elements=None)
+    cfg1 = bench._cfg(args, 1)
+    cfg = bench._cfg(args, world)
+    nupts, neles = bench._points_shape(cfg, world)
+    assert (nupts, neles) == bench._points_shape(cfg1, 1)
+    whole = mgen.from_config(cfg)
+    pm, glob = pt.partition_mesh(whole, pt.partition_elements(
+        whole['spt_quad_p0'], world))
+    from frfs_b200.elements import ElementGeometry
+    from frfs_b200.shapes import QuadShape
+    sh = QuadShape(cfg.getint('solver', 'order'))
+    rows = {}
+    for k in range(world):
+        assert len(glob[k]) == neles
+        geo = ElementGeometry(sh, pm[f'spt_quad_p{k}'])
+        nbrs, counts, hr = pt.halo_rows(pm, k, geo.srtd_face_fpts)
+        periodic = workload == 'channel-n32'
+        want = 2 if (periodic or 0 < k < world - 1) else 1
+        assert len(set(nbrs)) == min(want, world - 1)
+        rows[k] = dict(zip(nbrs, counts))
+    for k in rows:
+        for s, n in rows[k].items():
+            assert rows[s][k] == n
