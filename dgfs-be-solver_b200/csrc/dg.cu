@@ -28,7 +28,7 @@ struct dgfs_dg {
 };
 
 constexpr int kBcChunks = 256;  // velocity chunks of the wall-sum reduction
-constexpr int kVpt = 8;         // velocities per warp in the interp kernel
+constexpr int kVpt = 8;         // velocities per warp in the interp kernel (largest)
 
 // Residual launch shapes: (velocities per warp, prefetch of the RK terms,
 // CTAs per SM of the register budget); MB 0 = the precision's default
@@ -36,7 +36,7 @@ constexpr int kVpt = 8;         // velocities per warp in the interp kernel
 struct DgShape {
   int vpt, pf, mb;
 };
-constexpr DgShape kDgShapes[] = {{8, 0, 0}, {8, 1, 0}, {8, 1, 2}, {16, 1, 2}, {4, 0, 0}};
+constexpr DgShape kDgShapes[] = {{8, 0, 0}, {8, 1, 0}, {8, 1, 2}, {16, 1, 2}, {4, 0, 0}, {4, 1, 0}, {2, 1, 0}};
 constexpr int kDgNumShapes = sizeof(kDgShapes) / sizeof(kDgShapes[0]);
 
 namespace {
@@ -189,7 +189,16 @@ cudaError_t run_interp(const dgfs_dg* h, const void* u, int v0, int nv, cudaStre
   a.u = (const T*)u;
   a.v0 = v0;
   a.nv = nv;
-  dg_interp_kernel<T, U, F, D, kVpt><<<grid_blk(h, nv), 256, 0, s>>>(a, make_ops<T, U, F, D>(h));
+  // the interp kernel takes the velocity chunk of the selected residual
+  // shape (small meshes: more CTAs)
+  const int vs = kDgShapes[h->shape].vpt, vpt = vs <= 2 ? 2 : vs <= 4 ? 4 : kVpt;
+  const dim3 grid((unsigned)((h->E + 31) / 32), (unsigned)((nv + 8 * vpt - 1) / (8 * vpt)));
+  if (vpt <= 2)
+    dg_interp_kernel<T, U, F, D, 2><<<grid, 256, 0, s>>>(a, make_ops<T, U, F, D>(h));
+  else if (vpt <= 4)
+    dg_interp_kernel<T, U, F, D, 4><<<grid, 256, 0, s>>>(a, make_ops<T, U, F, D>(h));
+  else
+    dg_interp_kernel<T, U, F, D, kVpt><<<grid, 256, 0, s>>>(a, make_ops<T, U, F, D>(h));
   return cudaGetLastError();
 }
 
@@ -225,6 +234,8 @@ cudaError_t run_rhs(const dgfs_dg* h, const void* u, void* out, int v0, int nv, 
     case 2: return launch_rhs<T, U, F, D, 8, 1, 2>(h, a, nv, s);
     case 3: return launch_rhs<T, U, F, D, 16, 1, 2>(h, a, nv, s);
     case 4: return launch_rhs<T, U, F, D, 4, 0, 0>(h, a, nv, s);
+    case 5: return launch_rhs<T, U, F, D, 4, 1, 0>(h, a, nv, s);
+    case 6: return launch_rhs<T, U, F, D, 2, 1, 0>(h, a, nv, s);
     default: return launch_rhs<T, U, F, D, 8, 0, 0>(h, a, nv, s);
   }
 }
