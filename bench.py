@@ -75,6 +75,13 @@ def _parse():
                     help='train and evaluate the learned surrogate in this run '
                          '(-1: on for couette-n24 at N=1)')
     ap.add_argument('--surrogate-steps', type=int, default=200)
+    ap.add_argument('--initial', default='synthetic',
+                    choices=['synthetic', 'workload'],
+                    help='step mode: synthetic noisy Maxwellians or the '
+                         "workload's own initial condition")
+    ap.add_argument('--e2e', type=int, default=1,
+                    help='0: skip the end-to-end measurement (banks too '
+                         'large for a pinned host copy)')
     ap.add_argument('--elements', type=int, nargs=2, default=None,
                     metavar=('NX', 'NY'),
                     help='mesh size override (quad box: nx ny; O-grid: '
@@ -404,7 +411,11 @@ def run_b200(args):
         from frfs_b200.system import DGFSSystem
         cfg.set('backend-b200', 'cuda-graphs', int(args.graphs))
         vm0 = DGFSVelocityMesh(None, cfg)
-        f0 = _synthetic_f(vm0.cv(), nupts, neles, seed=rank)
+        # synthetic noisy Maxwellians, or (--initial workload) the
+        # workload's own initial condition, filled on the device when it is
+        # uniform in space (banks too large for a host copy)
+        f0 = (_synthetic_f(vm0.cv(), nupts, neles, seed=rank)
+              if args.initial == 'synthetic' else None)
         mesh, prank = None, 0
         if part:
             # spatial partitions: rank r runs part r of the widened mesh
@@ -478,26 +489,30 @@ def run_b200(args):
 
     # end to end through the public API: pinned host distribution ->
     # device, the step, device -> pinned host result, all timed
-    src_bank = fin
-    dst_bank = fin if args.mode == 'step' else fout
-    hin = torch.empty(src_bank.data.numel(), dtype=src_bank.data.dtype,
-                      pin_memory=True)
-    hin.copy_(src_bank.data.cpu())
-    hout = torch.empty_like(hin, pin_memory=True)
+    e2e = None
+    if args.e2e:
+        src_bank = fin
+        dst_bank = fin if args.mode == 'step' else fout
+        hin = torch.empty(src_bank.data.numel(), dtype=src_bank.data.dtype,
+                          pin_memory=True)
+        hin.copy_(src_bank.data.cpu())
+        hout = torch.empty_like(hin, pin_memory=True)
 
-    def e2e_step():
-        src_bank.data.copy_(hin, non_blocking=True)
-        step()
-        hout.copy_(dst_bank.data, non_blocking=True)
-    for _ in range(2):
-        e2e_step()
-    torch.cuda.synchronize()
-    te = _max_over_ranks(float(np.sum(_timed(e2e_step, args.steps, stream,
-                                               flush))), world, be.device)
-    e2e = {'value': world*evals_per_step*args.steps/(te*1e-3),
-           'unit': 'evals/s',
-           'h2d_bytes_per_step': int(hin.numel()*hin.element_size()),
-           'd2h_bytes_per_step': int(hout.numel()*hout.element_size())}
+        def e2e_step():
+            src_bank.data.copy_(hin, non_blocking=True)
+            step()
+            hout.copy_(dst_bank.data, non_blocking=True)
+        for _ in range(2):
+            e2e_step()
+        torch.cuda.synchronize()
+        te = _max_over_ranks(float(np.sum(_timed(e2e_step, args.steps,
+                                                   stream, flush))),
+                             world, be.device)
+        e2e = {'value': world*evals_per_step*args.steps/(te*1e-3),
+               'unit': 'evals/s',
+               'h2d_bytes_per_step': int(hin.numel()*hin.element_size()),
+               'd2h_bytes_per_step': int(hout.numel()*hout.element_size())}
+        del hin, hout
 
     # dominant kernel: the fused VHS launch, timed alone on the same bank
     prec = 64 if args.precision == 'double' else 32
@@ -568,7 +583,8 @@ def run_b200(args):
             'ms_by_shape': dg_tune}
     launch = sm.launch_info()
 
-    if rank == 0 and world == 1 and args.precision == 'single':
+    if rank == 0 and world == 1 and args.precision == 'single' and \
+            npts <= 20000:
         # the FP64 mode on the same points: one collision sweep in full
         # double precision (the parity mode), against the FP64 FMA peak
         extra['fp64'] = _fp64_line(args, stream, flush, fin)

@@ -75,15 +75,27 @@ def rel_l2(a, b):
 def run_workload(system, nsteps, sur=None, check_every=0, tol=5e-3,
                  scratch=None):
     """nsteps SSP-RK2 steps from the workload's initial state; returns the
-    final (rho, u, T), the bank index and the residual-check record."""
+    final (rho, u, T), the bank index and the record of the run: residual
+    checks, and the device time of the steps (CUDA events around every
+    stretch of steps, the residual checks between them excluded), so that
+    the step time is an average over the whole trajectory."""
     system.surrogate = sur
     _reset(system)
     st = StdTVDRK2DGFSStepper(system, system.cfg)
     fallbacks, checks, worst = [], 0, 0.0
     done = 0
+    dev = system.backend.device
+    stream = torch.cuda.current_stream(dev)
+    step_ms = 0.0
     while done < nsteps:
         n = min(check_every or nsteps, nsteps - done)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
         st.advance(n)
+        e1.record(stream)
+        e1.synchronize()
+        step_ms += e0.elapsed_time(e1)
         done += n
         if sur is not None and check_every and system.surrogate is not None \
                 and done < nsteps:
@@ -100,7 +112,8 @@ def run_workload(system, nsteps, sur=None, check_every=0, tol=5e-3,
     system.surrogate = None
     return ((m[..., 0], m[..., 1:4], m[..., 4]), st._idxcurr,
             {'checks': checks, 'worst_residual': worst,
-             'fallback_at_step': fallbacks})
+             'fallback_at_step': fallbacks,
+             'ms_per_step': step_ms/max(nsteps, 1)})
 
 
 def time_sweep(fn, reps, device):
@@ -174,10 +187,10 @@ def run_study(ini, device='cuda:0', runs=5, near_runs=10, steps=100,
     (p64, v64, S64), _, _ = run_workload(s64, nsteps)
     del s64
     torch.cuda.empty_cache()
-    (r32, u32, T32), _, _ = run_workload(s32, nsteps)
+    (r32, u32, T32), _, rec32 = run_workload(s32, nsteps)
     zero = ZeroSurrogate(s32.sm, threshold=threshold)
     (rz, uz, Tz), _, _ = run_workload(s32, nsteps, zero)
-    (rn, un, Tn), _, _ = run_workload(s32, nsteps, sur)
+    (rn, un, Tn), _, recn = run_workload(s32, nsteps, sur)
     scratch = [s32.backend.matrix(s32.bank[0].ioshape) for _ in range(2)]
     (rs, us, Ts), idx, chk = run_workload(s32, nsteps, sur, check_every,
                                           tol, scratch)
@@ -195,7 +208,7 @@ def run_study(ini, device='cuda:0', runs=5, near_runs=10, steps=100,
     for thr in (extra_thresholds or ()):
         sur.threshold = zero.threshold = thr
         (ra, ua, Ta), _, _ = run_workload(s32, nsteps, zero)
-        (rt, ut, Tt), it, _ = run_workload(s32, nsteps, sur)
+        (rt, ut, Tt), it, rect = run_workload(s32, nsteps, sur)
         ft, ot = s32.bank[it], scratch[0]
         tp = time_sweep(lambda: s32.sm.fs_all(ft, ot), reps, device)
         ts = time_sweep(lambda: sur.collide(ft, ot), reps, device)
@@ -205,6 +218,9 @@ def run_study(ini, device='cuda:0', runs=5, near_runs=10, steps=100,
                            'err_gate_without_network_vs_projected_fp64':
                            errs_proj(ra, ua, Ta),
                            'speedup': tp/ts,
+                           'step_ms': rect['ms_per_step'],
+                           'step_speedup_over_run':
+                           rec32['ms_per_step']/rect['ms_per_step'],
                            'gate_fraction':
                            float((sur._last[0] != 0).float().mean())}
     sur.threshold = zero.threshold = threshold
@@ -225,6 +241,10 @@ def run_study(ini, device='cuda:0', runs=5, near_runs=10, steps=100,
         'epochs': epochs, 'runs': runs, 'near_runs': near_runs,
         'steps_per_run': steps,
         'nsteps': nsteps, 'threshold': threshold,
+        'step_ms_plain': rec32['ms_per_step'],
+        'step_ms_surrogate': recn['ms_per_step'],
+        'step_ms_surrogate_with_checks': chk['ms_per_step'],
+        'step_speedup_over_run': rec32['ms_per_step']/recn['ms_per_step'],
         'err_surrogate': errs(rs, us, Ts),
         'err_surrogate_without_checks': errs(rn, un, Tn),
         'err_plain_fp32': errs(r32, u32, T32),

@@ -133,7 +133,13 @@ class DGFSSystem:
 
         V = vm.vsize()
         shape = (self.nupts, V, self.neles)
-        if initsoln is None:
+        ics = 'soln-ics'
+        uniform = (cfg.get(ics, 'type', None) in ('maxwellian', 'bimaxwellian',
+                                                  'bkw') and
+                   not cfg.getfloat(ics, 'noise', 0.0))
+        if initsoln is None and uniform:
+            f0 = None
+        elif initsoln is None:
             f0 = initial_distribution(cfg, vm, self.nupts, self.neles)
         elif isinstance(initsoln, dict):
             # a checkpoint (frfs's restart branch, system.py:79-112)
@@ -141,8 +147,14 @@ class DGFSSystem:
             f0 = restart_bank(initsoln, cfg, V, self.mesh)
         else:
             f0 = np.asarray(initsoln).reshape(shape)
-        mats = [backend.matrix(shape, f0 if i == 0 else None)
-                for i in range(nreg)]
+        mats = [backend.matrix(shape, f0 if i == 0 and f0 is not None
+                               else None) for i in range(nreg)]
+        if f0 is None:
+            # a state uniform in space, filled on the device from its one
+            # velocity vector (no host bank: the cylinder's full size is
+            # 42 GB per FP32 bank, 84 GB in FP64 on the host)
+            _fill_uniform(mats[0], initial_distribution(cfg, vm, 1, 1)[0, :,
+                                                                        0])
         self.bank = backend.matrix_bank(mats)
         self.eles_scal_upts_inb_full = [self.bank]
 
@@ -456,6 +468,21 @@ class DGFSSystem:
         a = buf.view(self.nfpts, ld.value)[:, :nblk*32*V].cpu().numpy()
         a = a.reshape(self.nfpts, nblk, V, 32).transpose(0, 2, 1, 3)
         return a.reshape(self.nfpts, V, nblk*32)[:, :, :E]
+
+
+def _fill_uniform(mat, f):
+    """Every solution point of an AoSoA bank (nupts, V, neles) set to the
+    velocity vector f (length V), padding lanes of the last element block
+    left zero, on the device."""
+    import torch
+    nupts, V, neles = mat.ioshape
+    nblk = (neles + 31)//32
+    view = mat.view2d()[:, :nblk*V*32].view(nupts, nblk, V, 32)
+    view.copy_(torch.as_tensor(np.asarray(f), dtype=view.dtype,
+                               device=view.device)[None, None, :, None]
+               .expand(nupts, nblk, V, 32))
+    if neles % 32:
+        view[:, nblk - 1, :, neles % 32:] = 0
 
 
 def bank_moments(bank, vm, backend):
