@@ -20,7 +20,11 @@ def fuzzysort(arr, idx, dim=0, tol=1e-6):
     coordinate agrees within ``tol`` (runs anchored at their first member,
     as in ``clean``) are ordered among themselves by the next coordinate.
     This is the face flux-point ordering frfs pairs interfaces with
-    (frfs/nputil.py:84-100)."""
+    (frfs/nputil.py:84-100).  Points that agree within ``tol`` in every
+    coordinate cannot be ordered (a degenerate face): ValueError."""
+    if dim == len(arr):
+        raise ValueError(f'flux points of a face coincide within {tol} in '
+                         'every coordinate (degenerate element)')
     key = arr[dim]
     order = sorted(idx, key=key.__getitem__)
     out = []

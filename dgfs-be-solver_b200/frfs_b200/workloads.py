@@ -211,8 +211,16 @@ uz = 0.0
     return ini
 
 
+def _ogrid_hmin(ntheta, nr, stretch, r_in=0.5, r_out=4.0):
+    """sqrt(area) of the innermost O-grid element: the first radial size
+    times the arc length at the cylinder."""
+    w = stretch**np.arange(nr)
+    dr0 = (r_out - r_in)*w[0]/np.sum(w)
+    return float(np.sqrt(dr0*r_in*2*np.pi/ntheta))
+
+
 def cylinder_n32(precision='single', ntheta=40, nr=16, order=3, Nv=32,
-                 Nrho=16, M=24, mach=2.0, dt=2e-4, tend=0.01):
+                 Nrho=16, M=24, mach=2.0, dt=None, tend=0.01):
     """Cylinder in a Mach-2 crossflow on a
     quadrilateral O-grid, p=3, N=32, Nrho=16, M=24 (M=32 has no tabulated
     symmetric design; the 48-point rule of M=24 is the nearest).  Cylinder
@@ -224,11 +232,18 @@ def cylinder_n32(precision='single', ntheta=40, nr=16, order=3, Nv=32,
 
     Full size is ntheta x nr ~ 20 000 elements (ntheta=160, nr=125: 320 000
     points, 42 GB per FP32 bank); the default, 40 x 16 = 640 elements
-    (10 240 points), has the channel's point count.  dt = 2e-4 gives
-    |c| dt / h = 0.023 on the smallest default element (h = sqrt(area) =
-    0.072) at the corner speed of the velocity box (|c| = 8.2); the p=3
-    FR-DG operator with SSP-RK2 on O-grids is stable up to 0.055
-    (eigenvalues of the operator on 12x2 and 16x3 O-grids)."""
+    (10 240 points), has the channel's point count.  The radial sizes grow
+    geometrically with a ratio of 1.15**15 (8.1) from the cylinder to the
+    far field at every nr (stretch 1.15 at nr = 16, 1.017 at nr = 125).
+    dt = 2e-4 on the default grid gives |c| dt / h = 0.023 on the smallest
+    element (h = sqrt(area) = 0.070) at the corner speed of the velocity
+    box (|c| = 8.2); the p=3 FR-DG operator with SSP-RK2 on O-grids is
+    stable up to 0.055 (eigenvalues of the operator on 12x2 and 16x3
+    O-grids).  dt = None scales 2e-4 by the smallest element's h against
+    the default grid's, which keeps |c| dt / h = 0.023 at every size."""
+    stretch = 1.15**(15.0/max(nr - 1, 1))
+    if dt is None:
+        dt = 2e-4*_ogrid_hmin(ntheta, nr, stretch)/_ogrid_hmin(40, 16, 1.15)
     u0 = _u0()
     uinf = float(mach*np.sqrt(5.0/6.0)*u0)
     ini = _BASE.format(precision=precision, Nv=Nv, NvBatchSize=Nv**3,
@@ -242,7 +257,7 @@ ntheta = {ntheta}
 nr = {nr}
 r-in = 0.5
 r-out = 4.0
-stretch = 1.15
+stretch = {stretch!r}
 
 [soln-ics]
 type = maxwellian
