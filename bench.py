@@ -49,8 +49,20 @@ METRIC = 'Q(f) evals/s'
 
 # DRAM bytes (read + write) per launch measured by ncu, keyed by (kernel,
 # workload, points, precision bits); only exact matches are reported
+# dram__bytes_read.sum + dram__bytes_write.sum per launch from ncu captures:
+# (kernel, workload, points, precision bits) -> (bytes, how it was taken)
 TRAFFIC = {
-    ('vhs_cube_kernel', 'couette-n24', 576, 32): 36.7e6,
+    ('vhs_cube_kernel', 'couette-n24', 576, 32):
+        (36.7e6, 'captured at this size'),
+    ('vhs_pair_kernel', 'channel-n32', 10368, 32):
+        (190.8e6*72, 'captured on the 4 x 4-element channel (144 points, '
+                     '190.8 MB) and scaled by the point count (x72)'),
+}
+# the same for one DG stage (interp + residual): (workload, points, bits)
+DG_TRAFFIC = {
+    ('couette-n24', 576, 32):
+        (148.9e6, 'captured at this size (interp 33.5 MB + residual '
+                  '115.4 MB, residual shape of 8 velocities per warp)'),
 }
 
 
@@ -538,7 +550,7 @@ def run_b200(args):
              'pair': 'vhs_pair_kernel',
              'pull': 'vhs_cluster_kernel'}.get(kind, kind)
     tkey = (kname, args.workload, npts, prec)
-    traffic = TRAFFIC.get(tkey)
+    traffic, tsrc = TRAFFIC.get(tkey, (None, None))
     roof = {'bound': 'fp32-simt' if prec == 32 else 'fp64-simt',
             'achieved': achieved, 'peak': tf.value, 'unit': 'TFLOP/s',
             'frac': achieved/tf.value,
@@ -547,8 +559,8 @@ def run_b200(args):
             'flops_per_point': flops_pt, 'launch_ms': vhs_ms,
             'traffic': traffic,
             'traffic_source': ('ncu dram__bytes_read.sum + '
-                               'dram__bytes_write.sum of this kernel, '
-                               'workload, size and precision') if traffic
+                               'dram__bytes_write.sum of this kernel: ' +
+                               tsrc) if traffic
             else 'not captured for this kernel/workload/size/precision',
             'kernel': kname}
     extra = {}
@@ -571,6 +583,8 @@ def run_b200(args):
         except (OSError, ValueError):
             pass
         hbm = peaks.get('hbm_gbs', 6650.0)
+        dg_traffic, dg_tsrc = DG_TRAFFIC.get((args.workload, npts, prec),
+                                             (None, None))
         extra['dg_roofline'] = {
             'bound': 'hbm', 'achieved': dg_bytes/(dg_ms*1e-3)/1e9,
             'peak': hbm, 'unit': 'GB/s',
@@ -578,6 +592,11 @@ def run_b200(args):
             'peak_source': 'MEASURED_PEAKS.json hbm_gbs' if peaks
             else 'fallback 6650 GB/s',
             'bytes_per_launch': dg_bytes, 'launch_ms': dg_ms,
+            'traffic': dg_traffic,
+            'traffic_source': ('ncu dram__bytes_read.sum + '
+                               'dram__bytes_write.sum: ' + dg_tsrc)
+            if dg_traffic else 'not captured for this workload/size/'
+                               'precision',
             'kernels': 'dg_interp_kernel + dg_residual_kernel',
             'residual_shape': system.dg_variants()[system._dg_shape],
             'ms_by_shape': dg_tune}

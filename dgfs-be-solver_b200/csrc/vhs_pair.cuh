@@ -61,8 +61,12 @@ template <int LPT> struct PairGeom {
   static constexpr int SMEM_CX = OFF_PH + 2 * PHS;
   static constexpr int SLICE = H * NN;                   // cx per spectrum in the scratch
   static constexpr int XSLAB = 16 * 16 * N;              // cx per staging buffer [k1l][j][x3]
-  // scratch per pair: F, fC, then [2 CTAs][2 alternating buffers] staging
-  static constexpr int SCRATCH = 2 * SLICE + 4 * XSLAB;
+  // F on the Nyquist planes k2 = N/2 ([k3 <= N/2][k1]) and k3 = N/2
+  // ([k2][k1]), lanes (k1) fastest: a copy per CTA
+  static constexpr int NQ2 = H * N, NQS = H * N + N * N;
+  // scratch per pair: F, fC, [2 CTAs][2 alternating buffers] staging, then
+  // [2 CTAs] Nyquist-plane copies
+  static constexpr int SCRATCH = 2 * SLICE + 4 * XSLAB + 2 * NQS;
 };
 
 // k1 ownership: K_0 = {0..7, 16, 25..31}, K_1 = {8..15, 17..24}
@@ -121,6 +125,7 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
   C* const Fg = a.fc + (size_t)cid * G::SCRATCH;
   C* const fC = Fg + G::SLICE;
   C* const Xs = fC + G::SLICE;  // staging: [rank][buffer][k1l][j][x3]
+  C* const Nq = Xs + 4 * G::XSLAB + r * G::NQS;  // this CTA's Nyquist-plane copy
   const float invV = 1.f / (float)V;
   const int npq = a.P * a.M;
   // a main thread's lines in every pass: L = tid + NM h (h < LPT), with
@@ -219,6 +224,15 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
       if (tid % N == NY) sPh[3 * N + tid / N] = cmul(mk<C>(e.x, -e.y), mk<C>(e.x, -e.y));
     }
     cl_sync();  // F complete in the scratch; the exchange buffer may be reused
+    // the planes k2 = N/2 and k3 = N/2 of F with k1 fastest, so that the
+    // Nyquist lines of those planes (one k1 per lane) read coalesced rows
+#pragma unroll 1
+    for (int t = tid; t < G::NQS; t += G::NT) {
+      const bool q2 = t < G::NQ2;
+      const int u = q2 ? t : t - G::NQ2, row = u / N, k1 = u % N;
+      Nq[t] = __ldcg(Fg + (q2 ? (row * N + k1) * N + NY : (NY * N + k1) * N + row));
+    }
+    __syncthreads();
 
     // F at (k1, k2, k3) from the half spectrum in the scratch (written by
     // both CTAs: read through L2)
@@ -286,10 +300,22 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
           const C A = mk<C>(0.5f * (B.x + B.y), 0.5f * (B.y - B.x));
           const C A3 = mk<C>(0.5f * (B3.x + B3.y), 0.5f * (B3.y - B3.x));
           const C* ev = ph + (p3 ? N : 2 * N);
+          // the line's F values, one load each: plane 1 from the half
+          // spectrum (rows k3, stride N^2), planes 2 and 3 from the copies
+          // (rows k3 or k2, stride N); k3 > N/2 from the conjugate mirror
+          const C* const qb = which == 0 ? Fg + NY * N : (which == 1 ? Nq : Nq + G::NQ2);
+          const int rs = which == 0 ? NN : N, jm = (N - j) % N;
+          const bool mir = !p3;
           C x[N];
 #pragma unroll
           for (int k = 0; k < N; ++k) {
-            const C v = which == 0 ? Fat(NY, j, k) : which == 1 ? Fat(j, NY, k) : Fat(j, k, NY);
+            C v;
+            if (k <= NY) {
+              v = __ldcg(qb + k * rs + j);
+            } else {
+              const C c = __ldcg(mir ? qb + (N - k) * rs + jm : qb + k * rs + j);
+              v = mk<C>(c.x, mir ? -c.y : c.y);
+            }
             const C& Ak = k == NY ? A3 : A;
             const C e = ev[k];
             x[k] = cscale(v, Ak.x * e.x - Ak.y * e.y);

@@ -414,24 +414,31 @@ class DGFSSystem:
     def autotune_dg(self, uin=0, out=1, reps=3):
         """Time every residual launch shape on a full Runge-Kutta stage of
         bank ``uin`` into bank ``out`` (overwritten: call before stepping)
-        and keep the fastest; returns {shape index: ms}."""
+        and keep the fastest; returns {shape index: ms}.  L2 is flushed
+        (a 256 MiB write) before every timed launch, as a step finds it."""
         import torch
         dev = self.backend.device
+        flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)
         ms = {}
+        # the flux-point values once (the same for every shape); each shape
+        # then times its residual launch alone
+        self.rk_stage(uin, out, 0.5, uin, 0.5, uin, 1e-4, uin, interp=True)
         for i in range(len(self.dg_variants())):
             self.select_dg(i)
             stage = lambda: self.rk_stage(uin, out, 0.5, uin, 0.5, uin, 1e-4,
-                                          uin, interp=(i == 0))
+                                          uin, interp=False)
             stage()
             torch.cuda.synchronize(dev)
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record()
-            for _ in range(reps):
+            ev = [(torch.cuda.Event(enable_timing=True),
+                   torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+            for e0, e1 in ev:
+                flush.zero_()
+                e0.record()
                 stage()
-            e1.record()
-            e1.synchronize()
-            ms[i] = e0.elapsed_time(e1)/reps
+                e1.record()
+            torch.cuda.synchronize(dev)
+            ms[i] = sum(e0.elapsed_time(e1) for e0, e1 in ev)/reps
+        del flush
         self.select_dg(min(ms, key=ms.get))
         return ms
 
