@@ -15,6 +15,11 @@ NA = 6.0221409e+23       # frfs/solvers/dgfs/velocitymesh.py:9
 
 
 def _workers():
+    """Threads of every FFT: DGFS_ORACLE_THREADS if set (the timed CPU
+    baseline runs one single-threaded process per core), else all cores."""
+    env = os.environ.get('DGFS_ORACLE_THREADS')
+    if env:
+        return max(1, int(env))
     try:
         return len(os.sched_getaffinity(0))
     except AttributeError:
