@@ -112,3 +112,67 @@ def test_product_mixture_mesh_matches_oracle():
     np.testing.assert_allclose(vm.qw(), mesh['qw'], rtol=1e-14)
     np.testing.assert_array_equal(vm.cv(), mesh['cv'])
     assert vm.masses() == pytest.approx(mesh['masses'], rel=1e-15)
+
+
+def test_single_species_alpha1_reduces_to_vhs():
+    """With one species, alpha = 1 and the direction integrals of the gain
+    and loss kernels taken analytically (the VHS kernels' sinc forms,
+    vhs-gll.mako:11-14 and 84-97), the VSS operator is the VHS operator of
+    the (reference-pinned) VHS oracle on the same grid: the phases
+    exp(+-i a/2), the weights over the full sphere (twice the half-sphere
+    sum at the same sw), the prefactor (sqrt(1 + mp/mq) cancels, mu = 1/2)
+    and the loss term agree.  Only the numerical direction integrals of
+    b and c (vss-gll.mako:73-91) are left out, and they are checked
+    separately against their limit."""
+    from oracle import vhs as ovhs
+    Nv, Nrho, M = 16, 8, 6
+    half = load_sphdesign(M)[:M]
+    full = np.vstack([half, -half])
+    mm, H0, T0, rho0 = 39.96e-3, 1e-3, 273.0, 1.5e-3
+    mesh = vss.mixture_mesh(Nv, Nrho, full, [mm], H0=H0, T0=T0, rho0=rho0,
+                            molarMass0=mm, cmax=0.0, Tmax=T0, dev=5.0)
+    omega, dRef = 0.81, 4.17e-10
+    params = vss.vss_parameters(mesh, alpha={'00': 1.0},
+                                omega={'00': omega}, dRef={'00': dRef},
+                                Tref={'00': T0})
+    pre = vss.vss_precompute(mesh, params, full)
+    vm = ovhs.velocity_mesh(Nv, Nrho, M, np.vstack([half, -half]), H0, T0,
+                            rho0, mm, 0.0, T0, 5.0)
+    gam, prefac = ovhs.vhs_parameters(omega, dRef, T0, H0, vm['n0'], T0)
+    assert params['00']['gamma'] == gam
+    assert params['00']['prefac'] == pytest.approx(prefac, rel=1e-14)
+    for k in ('L', 'R'):
+        assert mesh[k] == pytest.approx(vm[k], rel=1e-15)
+    vpre = ovhs.vhs_precompute(vm, gam)
+
+    # the direction integrals against their limit: the full-sphere design's
+    # sum of exp(-i k s.l) approaches 4 pi sinc(k |l|) where k |l| is small
+    # (below 0.5, the whole grid at the innermost radial node: 9e-8)
+    L, qz, qw = mesh['L'], mesh['qz'], mesh['qw']
+    lmag = np.sqrt(np.sum(vpre['l']**2, axis=0))
+    small = lmag*np.pi/L*qz[0]/2 < 0.5
+    b_exact = np.array([qz[x]**(gam + 2)*4*np.pi *
+                        ovhs._sinc(np.pi/L*qz[x]/2*lmag)
+                        for x in range(Nrho)])
+    b_num = pre['00']['b']
+    np.testing.assert_allclose(b_num[0][:, small].real,
+                               np.broadcast_to(b_exact[0][small],
+                                               b_num[0][:, small].shape),
+                               rtol=1e-6)
+    assert np.max(np.abs(b_num[0][:, small].imag)) < 1e-12*np.max(b_exact[0])
+    # analytic kernels in place of the numerical ones
+    pre['00']['b'] = np.broadcast_to(b_exact[:, None, :],
+                                     b_num.shape).astype(np.complex128)
+    pre['00']['c'] = np.sum([qw[x]*qz[x]**(gam + 2)*16*np.pi**2 *
+                             ovhs._sinc(np.pi/L*qz[x]*lmag)
+                             for x in range(Nrho)], axis=0).astype(
+                                 np.complex128)
+    np.testing.assert_allclose(b_exact, vpre['bb1'], rtol=1e-14)
+    np.testing.assert_allclose(pre['00']['c'].real, vpre['bb2'], rtol=0,
+                               atol=1e-13*np.max(np.abs(vpre['bb2'])))
+
+    f = 0.5*(ovhs.maxwellian(vm['cv'], 1.0, [0.7, -0.2, 0.1], 0.8) +
+             ovhs.maxwellian(vm['cv'], 1.0, [-0.6, 0.3, 0.0], 1.1))
+    Qv = ovhs.vhs_Q(f, vm, vpre, prefac)
+    Qs = vss.vss_Q([f], mesh, pre, params)[0]
+    assert np.max(np.abs(Qs - Qv)) < 1e-11*np.max(np.abs(Qv))
