@@ -1,5 +1,6 @@
 // Host side of the FR-DG residual: validation, device copies of geometry and
 // boundary data, the flux-point scratch and the launches behind the C ABI.
+#include <utility>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -173,6 +174,24 @@ template <typename T, int U> DgMassOps<T, U> make_mass_ops(const dgfs_dg* h) {
   return o;
 }
 
+// Launch as a programmatic dependent of the previous kernel in the stream
+// (dg_kernel.cuh: pdl_wait / pdl_trigger say what each kernel may do before
+// its predecessor has completed).
+template <typename... P, typename... A>
+cudaError_t launch_pdl(void (*kern)(P...), dim3 grid, cudaStream_t s, A&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3(256, 1, 1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...);
+}
+
 inline unsigned grid_for(const dgfs_dg* h, int nv) {
   const long long nblk = (h->E + 31) / 32;
   return (unsigned)((nblk * nv * 32 + 255) / 256);
@@ -193,13 +212,10 @@ cudaError_t run_interp(const dgfs_dg* h, const void* u, int v0, int nv, cudaStre
   // shape (small meshes: more CTAs)
   const int vs = kDgShapes[h->shape].vpt, vpt = vs <= 2 ? 2 : vs <= 4 ? 4 : kVpt;
   const dim3 grid((unsigned)((h->E + 31) / 32), (unsigned)((nv + 8 * vpt - 1) / (8 * vpt)));
-  if (vpt <= 2)
-    dg_interp_kernel<T, U, F, D, 2><<<grid, 256, 0, s>>>(a, make_ops<T, U, F, D>(h));
-  else if (vpt <= 4)
-    dg_interp_kernel<T, U, F, D, 4><<<grid, 256, 0, s>>>(a, make_ops<T, U, F, D>(h));
-  else
-    dg_interp_kernel<T, U, F, D, kVpt><<<grid, 256, 0, s>>>(a, make_ops<T, U, F, D>(h));
-  return cudaGetLastError();
+  const DgOps<T, U, F, D> ops = make_ops<T, U, F, D>(h);
+  if (vpt <= 2) return launch_pdl(dg_interp_kernel<T, U, F, D, 2>, grid, s, a, ops);
+  if (vpt <= 4) return launch_pdl(dg_interp_kernel<T, U, F, D, 4>, grid, s, a, ops);
+  return launch_pdl(dg_interp_kernel<T, U, F, D, kVpt>, grid, s, a, ops);
 }
 
 template <typename T, int U, int F, int D>
@@ -211,8 +227,7 @@ template <typename T, int U, int F, int D, int VPT, int PF, int MB>
 cudaError_t launch_rhs(const dgfs_dg* h, const DgArgs<T>& a, int nv, cudaStream_t s) {
   constexpr int mb = MB ? MB : dg_default_mb<T, U, F, D>();
   const dim3 grid((unsigned)((h->E + 31) / 32), (unsigned)((nv + 8 * VPT - 1) / (8 * VPT)));
-  dg_residual_kernel<T, U, F, D, VPT, PF, mb><<<grid, 256, 0, s>>>(a, make_ops<T, U, F, D>(h));
-  return cudaGetLastError();
+  return launch_pdl(dg_residual_kernel<T, U, F, D, VPT, PF, mb>, grid, s, a, make_ops<T, U, F, D>(h));
 }
 
 template <typename T, int U, int F, int D>
@@ -442,19 +457,23 @@ extern "C" int dgfs_dg_updatebc(dgfs_dg* h, int v0, int nv, int reset, void* str
   const int nchunks = (nv + chunk - 1) / chunk;
   const dim3 grid((unsigned)nchunks, (unsigned)((h->nb + 31) / 32));
   cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e;
   if (h->prec == 64) {
     DgArgs<double> a = make_args<double>(h);
     a.v0 = v0;
     a.nv = nv;
-    dg_bcsum_kernel<double, 2><<<grid, 256, 0, s>>>(a, h->bfpt, h->bele, h->nb, h->cw, chunk, h->bcpart);
+    e = launch_pdl(dg_bcsum_kernel<double, 2>, grid, s, a, (const int*)h->bfpt, (const int*)h->bele, h->nb, h->cw,
+                   chunk, h->bcpart);
   } else {
     DgArgs<float> a = make_args<float>(h);
     a.v0 = v0;
     a.nv = nv;
-    dg_bcsum_kernel<float, 2><<<grid, 256, 0, s>>>(a, h->bfpt, h->bele, h->nb, h->cw, chunk, h->bcpart);
+    e = launch_pdl(dg_bcsum_kernel<float, 2>, grid, s, a, (const int*)h->bfpt, (const int*)h->bele, h->nb, h->cw,
+                   chunk, h->bcpart);
   }
-  dg_bcsum_finish_kernel<<<(h->nb + 7) / 8, 256, 0, s>>>(h->bkind, h->nb, nchunks, h->bcpart, h->bcvals, reset);
-  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = launch_pdl(dg_bcsum_finish_kernel, dim3((unsigned)((h->nb + 7) / 8)), s, (const int*)h->bkind, h->nb,
+                   nchunks, (const double*)h->bcpart, h->bcvals, reset);
   if (e != cudaSuccess) return set_error(DGFS_ERR_CUDA, "DG boundary update launch: %s", cudaGetErrorString(e));
   return DGFS_OK;
 }

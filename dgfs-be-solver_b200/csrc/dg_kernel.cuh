@@ -109,8 +109,21 @@ __device__ __forceinline__ int64_t aos32(int64_t row, int64_t ldim, int64_t e, i
   return row * ldim + ((e >> 5) * V + v) * 32 + (e & 31);
 }
 
+// Programmatic dependent launch.  The interp and boundary-sum kernels wait
+// for their predecessor in the stream to complete (a no-op when they were
+// not launched as dependents), then let their own dependent start: a
+// dependent that starts early therefore finds everything before them
+// complete and may read the banks (u and the Runge-Kutta terms) before its
+// own wait; it reads their outputs (face values, boundary sums) only after
+// that wait.  The residual never triggers early: whatever follows it starts
+// after it has completed.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 template <typename T, int U, int F, int D, int VPT>
 __global__ void __launch_bounds__(256) dg_interp_kernel(const DgArgs<T> a, const DgOps<T, U, F, D> op) {
+  pdl_wait();
+  pdl_trigger();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t e = (int64_t)blockIdx.x * 32 + lane;
   if (e >= a.neles) return;
@@ -168,6 +181,8 @@ __global__ void __launch_bounds__(256) dg_bcsum_kernel(const DgArgs<T> a, const 
                                                       const int* __restrict__ bele, int nb, double cw,
                                                       int chunk, double* __restrict__ partials) {
   __shared__ double s0[8][32], s1[8][32];
+  pdl_wait();
+  pdl_trigger();
   const int bl = threadIdx.x & 31, vg = threadIdx.x >> 5;
   const int b = blockIdx.y * 32 + bl;
   const int vbeg = a.v0 + blockIdx.x * chunk;
@@ -220,6 +235,8 @@ __global__ void __launch_bounds__(256) dg_bcsum_kernel(const DgArgs<T> a, const 
 __global__ void __launch_bounds__(256) dg_bcsum_finish_kernel(const int* __restrict__ bkind, int nb, int nchunks,
                                                              const double* __restrict__ partials,
                                                              double* __restrict__ bcvals, int reset) {
+  pdl_wait();
+  pdl_trigger();
   const int b = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (b >= nb || (bkind[b] != BC_WALL_DIFFUSE && bkind[b] != BC_WALL_DIFFUSE_CYL)) return;  // uniform per warp
   double r0 = 0.0, r1 = 0.0;
@@ -350,6 +367,9 @@ __global__ void __launch_bounds__(256, MB)
         K[r] = k;
       }
     }
+    // the face values come from the interp kernel: wait for it (returns at
+    // once after the first iteration)
+    pdl_wait();
     T urv[F];
 #pragma unroll
     for (int f = 0; f < F; f += 2) {

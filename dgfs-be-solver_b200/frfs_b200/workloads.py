@@ -233,15 +233,16 @@ def cylinder_n32(precision='single', ntheta=40, nr=16, order=3, Nv=32,
     Full size is ntheta x nr ~ 20 000 elements (ntheta=160, nr=125: 320 000
     points, 42 GB per FP32 bank); the default, 40 x 16 = 640 elements
     (10 240 points), has the channel's point count.  The radial sizes grow
-    geometrically with a ratio of 1.15**15 (8.1) from the cylinder to the
-    far field at every nr (stretch 1.15 at nr = 16, 1.017 at nr = 125).
+    geometrically by 1.15 per element up to nr = 16; finer grids keep the
+    default's total growth of 1.15**15 (8.1) from the cylinder to the far
+    field (stretch 1.017 at nr = 125).
     dt = 2e-4 on the default grid gives |c| dt / h = 0.023 on the smallest
     element (h = sqrt(area) = 0.070) at the corner speed of the velocity
     box (|c| = 8.2); the p=3 FR-DG operator with SSP-RK2 on O-grids is
     stable up to 0.055 (eigenvalues of the operator on 12x2 and 16x3
     O-grids).  dt = None scales 2e-4 by the smallest element's h against
     the default grid's, which keeps |c| dt / h = 0.023 at every size."""
-    stretch = 1.15**(15.0/max(nr - 1, 1))
+    stretch = 1.15**min(1.0, 15.0/max(nr - 1, 1))
     if dt is None:
         dt = 2e-4*_ogrid_hmin(ntheta, nr, stretch)/_ogrid_hmin(40, 16, 1.15)
     u0 = _u0()

@@ -184,9 +184,10 @@ def test_cylinder_steps_run():
     """Two SSP-RK2 steps of the cylinder workload (FP32, collision and
     advection on the O-grid with its three boundary kinds): finite, and the
     density stays within a few per cent of the freestream's (the wall
-    disturbance has had four stages to spread)."""
+    disturbance has had four stages of dt = 2e-4 to spread; the workload's
+    own dt grows with the element size of this coarse 8 x 2 grid)."""
     from frfs_b200.steppers import StdTVDRK2DGFSStepper
-    cfg, m = _cylinder('single')
+    cfg, m = _cylinder('single', dt=2e-4)
     be = B200Backend(cfg, device='cuda:0')
     s = DGFSSystem(be, cfg, mesh=m)
     st = StdTVDRK2DGFSStepper(s, cfg)
