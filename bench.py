@@ -55,8 +55,9 @@ TRAFFIC = {
     ('vhs_cube_kernel', 'couette-n24', 576, 32):
         (36.7e6, 'captured at this size'),
     ('vhs_pair_kernel', 'channel-n32', 10368, 32):
-        (190.8e6*72, 'captured on the 4 x 4-element channel (144 points, '
-                     '190.8 MB) and scaled by the point count (x72)'),
+        (208.3e6*72, 'captured on the 4 x 4-element channel (144 points, '
+                     '208.3 MB, 512-thread layout) and scaled by the point '
+                     'count (x72)'),
 }
 # the same for one DG stage (interp + residual): (workload, points, bits)
 DG_TRAFFIC = {
