@@ -78,10 +78,17 @@ def run_workload(system, nsteps, sur=None, check_every=0, tol=5e-3,
     final (rho, u, T), the bank index and the record of the run: residual
     checks, and the device time of the steps (CUDA events around every
     stretch of steps, the residual checks between them excluded), so that
-    the step time is an average over the whole trajectory."""
+    the step time is an average over the whole trajectory.  One untimed
+    step from the initial state comes first and is discarded: it captures
+    the stage graphs (a one-time set-up) outside the timed steps."""
     system.surrogate = sur
     _reset(system)
     st = StdTVDRK2DGFSStepper(system, system.cfg)
+    t0 = st.tcurr
+    st.advance(1)
+    torch.cuda.synchronize(system.backend.device)
+    _reset(system)
+    st._idxcurr, st.tcurr = 0, t0
     fallbacks, checks, worst = [], 0, 0.0
     done = 0
     dev = system.backend.device
