@@ -257,9 +257,9 @@ struct dgfs_vhs {
   double* cvec;  // [3][V]
   void* fc;      // scratch: gain spectrum, one N^3 complex slice per cluster
   size_t fc_bytes;
-  void* fcp;     // single-CTA kernel: partial gain spectra of split points (4 slices per CTA)
+  void* fcp;     // single-CTA kernel: partial gain spectra of split points (kCubeSlices per CTA)
   size_t fcp_bytes;
-  int* pdone;    // ... and the chunk counters (2 per CTA, zero between launches)
+  int* pdone;    // ... and the chunk counters (kCubeSlices / 2 per CTA, zero between launches)
   int pdone_n;
   int* err;      // device flag: a bounded wait in the kernel gave up
 };
@@ -316,10 +316,11 @@ static int select_index(dgfs_vhs* h, int idx) {
     h->fc_bytes = need;
   }
   if (v->push == 2) {
-    // a launch on few points splits them into radial-node chunks: up to 4
-    // items per CTA, each with its own partial-spectrum slice, and up to 2
-    // points per CTA with a chunk counter
-    const size_t needp = (size_t)4 * ncl * (size_t)h->N * h->N * h->N * esz;
+    // a launch on few points splits them into radial-node chunks: up to
+    // kCubeSlices items per CTA, each with its own partial-spectrum slice,
+    // and (at least 2 chunks per point) up to kCubeSlices / 2 points per CTA
+    // with a chunk counter
+    const size_t needp = (size_t)kCubeSlices * ncl * (size_t)h->N * h->N * h->N * esz;
     if (needp > h->fcp_bytes) {
       cudaFree(h->fcp);
       h->fcp = nullptr;
@@ -328,15 +329,16 @@ static int select_index(dgfs_vhs* h, int idx) {
         return set_error(DGFS_ERR_NOMEM, "cudaMalloc(%zu) for the partial-spectrum scratch failed", needp);
       h->fcp_bytes = needp;
     }
-    if (2 * ncl > h->pdone_n) {
+    const int npd = kCubeSlices / 2 * ncl;
+    if (npd > h->pdone_n) {
       cudaFree(h->pdone);
       h->pdone = nullptr;
       h->pdone_n = 0;
-      if (cudaMalloc((void**)&h->pdone, (size_t)2 * ncl * sizeof(int)) != cudaSuccess)
+      if (cudaMalloc((void**)&h->pdone, (size_t)npd * sizeof(int)) != cudaSuccess)
         return set_error(DGFS_ERR_NOMEM, "cudaMalloc for the chunk counters failed");
-      if (cudaMemset(h->pdone, 0, (size_t)2 * ncl * sizeof(int)) != cudaSuccess)
+      if (cudaMemset(h->pdone, 0, (size_t)npd * sizeof(int)) != cudaSuccess)
         return set_error(DGFS_ERR_CUDA, "cudaMemset of the chunk counters failed");
-      h->pdone_n = 2 * ncl;
+      h->pdone_n = npd;
     }
   }
   h->vidx = idx;

@@ -69,10 +69,12 @@ template <int N> struct CubeGeom {
 // P chunks: with one node per chunk the final sum over the chunks' slices
 // adds the nodes in the same order as the unsplit accumulation, so a point's
 // Q does not depend on the launch it is part of (bit for bit).  Items are
-// capped at 4 per CTA of the grid (the partial-spectrum scratch).  Every CTA
+// capped at kCubeSlices per CTA of the grid (the partial-spectrum scratch:
+// with P = 12 a split covers up to two waves of whole points).  Every CTA
 // computes the same value.
+constexpr int kCubeSlices = 24;
 __device__ __forceinline__ int cube_chunks(int npts, int G, int P, int M) {
-  if (P < 2 || (long long)npts * P > 4LL * G) return 1;
+  if (P < 2 || (long long)npts * P > (long long)kCubeSlices * G) return 1;
   const double per_node = 3.0 * M + 3.0;
   const double whole = (double)((npts + G - 1) / G) * (P * per_node + 3.0);
   const double split = (double)(((long long)npts * P + G - 1) / G) * (per_node + 3.0);

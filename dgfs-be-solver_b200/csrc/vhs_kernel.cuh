@@ -59,8 +59,9 @@ template <typename T> struct VhsArgs {
   const T* b2t;         // [N][N*N]    b2 likewise (lane-contiguous for per-line access)
   cx<T>* fc;            // scratch [gridDim.x][N][NJ]: gain spectrum per CTA
   cx<T>* fcp;           // single-CTA kernel, points split over CTAs: partial gain
-                        // spectra, one [V] slice per (point, radial chunk) item (<= 4 gridDim.x)
-  int* pdone;           // ... and per point the chunks finished (<= 2 gridDim.x points;
+                        // spectra, one [V] slice per (point, radial chunk) item
+                        // (<= kCubeSlices gridDim.x)
+  int* pdone;           // ... and per point the chunks finished (<= kCubeSlices / 2 gridDim.x points;
                         // zero between launches).  NULL: never split.
   int* err;             // set to 1 when a bounded wait gives up
   const int* plist;     // optional device list of linear points (NULL: pt0 + i)
