@@ -176,9 +176,9 @@ template <typename T, int U> DgMassOps<T, U> make_mass_ops(const dgfs_dg* h) {
 
 // Launch as a programmatic dependent of the previous kernel in the stream
 // (dg_kernel.cuh: pdl_wait / pdl_trigger say what each kernel may do before
-// its predecessor has completed).
+// its predecessor has completed); pdl = false launches in plain stream order.
 template <typename... P, typename... A>
-cudaError_t launch_pdl(void (*kern)(P...), dim3 grid, cudaStream_t s, A&&... args) {
+cudaError_t launch_pdl(bool pdl, void (*kern)(P...), dim3 grid, cudaStream_t s, A&&... args) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
   cfg.blockDim = dim3(256, 1, 1);
@@ -188,7 +188,7 @@ cudaError_t launch_pdl(void (*kern)(P...), dim3 grid, cudaStream_t s, A&&... arg
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   at[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = pdl ? 1 : 0;
   return cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...);
 }
 
@@ -213,9 +213,9 @@ cudaError_t run_interp(const dgfs_dg* h, const void* u, int v0, int nv, cudaStre
   const int vs = kDgShapes[h->shape].vpt, vpt = vs <= 2 ? 2 : vs <= 4 ? 4 : kVpt;
   const dim3 grid((unsigned)((h->E + 31) / 32), (unsigned)((nv + 8 * vpt - 1) / (8 * vpt)));
   const DgOps<T, U, F, D> ops = make_ops<T, U, F, D>(h);
-  if (vpt <= 2) return launch_pdl(dg_interp_kernel<T, U, F, D, 2>, grid, s, a, ops);
-  if (vpt <= 4) return launch_pdl(dg_interp_kernel<T, U, F, D, 4>, grid, s, a, ops);
-  return launch_pdl(dg_interp_kernel<T, U, F, D, kVpt>, grid, s, a, ops);
+  if (vpt <= 2) return launch_pdl(true, dg_interp_kernel<T, U, F, D, 2>, grid, s, a, ops);
+  if (vpt <= 4) return launch_pdl(true, dg_interp_kernel<T, U, F, D, 4>, grid, s, a, ops);
+  return launch_pdl(true, dg_interp_kernel<T, U, F, D, kVpt>, grid, s, a, ops);
 }
 
 template <typename T, int U, int F, int D>
@@ -227,7 +227,11 @@ template <typename T, int U, int F, int D, int VPT, int PF, int MB>
 cudaError_t launch_rhs(const dgfs_dg* h, const DgArgs<T>& a, int nv, cudaStream_t s) {
   constexpr int mb = MB ? MB : dg_default_mb<T, U, F, D>();
   const dim3 grid((unsigned)((h->E + 31) / 32), (unsigned)((nv + 8 * VPT - 1) / (8 * VPT)));
-  return launch_pdl(dg_residual_kernel<T, U, F, D, VPT, PF, mb>, grid, s, a, make_ops<T, U, F, D>(h));
+  // with halo rows the face values of other partitions arrive by a
+  // collective on another stream: the residual then waits in plain stream
+  // order for everything before it
+  return launch_pdl(h->nhalo == 0, dg_residual_kernel<T, U, F, D, VPT, PF, mb>, grid, s, a,
+                    make_ops<T, U, F, D>(h));
 }
 
 template <typename T, int U, int F, int D>
@@ -462,17 +466,17 @@ extern "C" int dgfs_dg_updatebc(dgfs_dg* h, int v0, int nv, int reset, void* str
     DgArgs<double> a = make_args<double>(h);
     a.v0 = v0;
     a.nv = nv;
-    e = launch_pdl(dg_bcsum_kernel<double, 2>, grid, s, a, (const int*)h->bfpt, (const int*)h->bele, h->nb, h->cw,
+    e = launch_pdl(true, dg_bcsum_kernel<double, 2>, grid, s, a, (const int*)h->bfpt, (const int*)h->bele, h->nb, h->cw,
                    chunk, h->bcpart);
   } else {
     DgArgs<float> a = make_args<float>(h);
     a.v0 = v0;
     a.nv = nv;
-    e = launch_pdl(dg_bcsum_kernel<float, 2>, grid, s, a, (const int*)h->bfpt, (const int*)h->bele, h->nb, h->cw,
+    e = launch_pdl(true, dg_bcsum_kernel<float, 2>, grid, s, a, (const int*)h->bfpt, (const int*)h->bele, h->nb, h->cw,
                    chunk, h->bcpart);
   }
   if (e == cudaSuccess)
-    e = launch_pdl(dg_bcsum_finish_kernel, dim3((unsigned)((h->nb + 7) / 8)), s, (const int*)h->bkind, h->nb,
+    e = launch_pdl(true, dg_bcsum_finish_kernel, dim3((unsigned)((h->nb + 7) / 8)), s, (const int*)h->bkind, h->nb,
                    nchunks, (const double*)h->bcpart, h->bcvals, reset);
   if (e != cudaSuccess) return set_error(DGFS_ERR_CUDA, "DG boundary update launch: %s", cudaGetErrorString(e));
   return DGFS_OK;
