@@ -83,22 +83,6 @@ __device__ __forceinline__ void cl_sync() {
   cl_wait();
 }
 
-// Coefficients of a first-pass line (k1, k2): m = Re(A e3[k3]) off the
-// plane k3 = N/2 and Re(A3 e3[N/2]) on it (vhs_cube.cuh), from the axis
-// phases ph [3][N] and the Nyquist factors th1..th3 of one (p, q).
-__device__ __forceinline__ void pair_coef(const cx<float>* ph, cx<float> th1, cx<float> th2, cx<float> th3, int k1,
-                                          int k2, cx<float>& A, cx<float>& A3) {
-  constexpr int N = 32, NY = 16;
-  const cx<float> E12 = cmul(ph[k1], ph[N + k2]);
-  cx<float> t12 = mk<cx<float>>(1.f, 0.f);
-  if (k1 == NY) t12 = th1;
-  if (k2 == NY) t12 = cmul(t12, th2);
-  const cx<float> E12t = cmul(E12, t12);
-  const cx<float> s0 = cadd(E12, E12t), s3 = cadd(E12, cmul(E12t, th3));
-  A = mk<cx<float>>(0.5f * (s0.x + s0.y), 0.5f * (s0.y - s0.x));
-  A3 = mk<cx<float>>(0.5f * (s3.x + s3.y), 0.5f * (s3.y - s3.x));
-}
-
 // third-pass line (x2l = hi, x3 = lo) along k1: the k1 of this CTA from its
 // work cube (row kinv(k1) * 32 + x2, x2 = 16 r + hi), the others from the
 // peer's staging buffer ([kinv(k1)][hi][lo], written before the barrier)
@@ -267,36 +251,29 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
         const C* ph = sPh + slot * PHS;
         const C th1 = ph[3 * N], th2 = ph[3 * N + 1], th3 = ph[3 * N + 2];
         const C phn = (tid < 3 * N && pq + 1 < npq) ? a.phase[(size_t)(pq + 1) * 3 * N + tid] : mk<C>(0.f, 0.f);
-        // pass 1: lines (k1, k2) along k3 | Nyquist first axes.  LPT = 2:
-        // warp w takes the lines hi = 2 w + (lane >> 4) with k2 in the half
-        // the other CTA owns in x (h = 0; prefetched into the line's own row
-        // of W by the Nyquist threads during the previous third pass, when
-        // that pass was of the same radial node) and then in this CTA's
-        // half (h = 1).  LPT = 1: hi = warp, k2 = lane.
+        // pass 1: lines (k1, k2 = lo) along k3 | Nyquist first axes
         if (is_main) {
 #pragma unroll 1
           for (int h = 0; h < LPT; ++h) {
-            const int hi = LPT == 2 ? 2 * (tid >> 5) + ((tid >> 4) & 1) : hi0;
-            const int k2 = LPT == 2 ? 16 * (h == 0 ? 1 - r : r) + (tid & 15) : lo;
-            const int k1 = pair_kmap(r, hi);
-            C* const row = sW + (hi * N + k2) * LP;
+            const int hi = hi0 + HS * h, k1 = pair_kmap(r, hi), k2 = lo;
+            const C E12 = cmul(ph[k1], ph[N + k2]);
+            C t12 = mk<C>(1.f, 0.f);
+            if (k1 == NY) t12 = th1;
+            if (k2 == NY) t12 = cmul(t12, th2);
+            const C E12t = cmul(E12, t12);
+            const C s0 = cadd(E12, E12t), s3 = cadd(E12, cmul(E12t, th3));
+            const C A = mk<C>(0.5f * (s0.x + s0.y), 0.5f * (s0.y - s0.x));
+            const C A3 = mk<C>(0.5f * (s3.x + s3.y), 0.5f * (s3.y - s3.x));
             C x[N];
-            if (LPT == 2 && h == 0 && q > 0) {
 #pragma unroll
-              for (int k = 0; k < N; ++k) x[k] = row[k];
-            } else {
-              C A, A3;
-              pair_coef(ph, th1, th2, th3, k1, k2, A, A3);
-#pragma unroll
-              for (int k = 0; k < N; ++k) {
-                const C e3 = ph[2 * N + k];
-                const C& Ak = k == NY ? A3 : A;
-                x[k] = cscale(Fat(k1, k2, k), Ak.x * e3.x - Ak.y * e3.y);
-              }
+            for (int k = 0; k < N; ++k) {
+              const C e3 = ph[2 * N + k];
+              const C& Ak = k == NY ? A3 : A;
+              x[k] = cscale(Fat(k1, k2, k), Ak.x * e3.x - Ak.y * e3.y);
             }
             fft<float, N, +1>(x);
 #pragma unroll
-            for (int k = 0; k < N; ++k) row[k] = x[k];
+            for (int k = 0; k < N; ++k) sW[(hi * N + k2) * LP + k] = x[k];
           }
         }
         if (has_nyq) {
@@ -386,27 +363,6 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
               const float ni = s1 * t1.y + s2 * t2.y + s3 * t3.y;
               const float v = x[i].x * x[i].x - x[i].y * x[i].y + nr * nr - ni * ni;
               Sl[i * 16 * N] = q == 0 ? v : Sl[i * 16 * N] + v;
-            }
-          }
-        } else if (LPT == 2 && q + 1 < a.M) {
-          // the Nyquist threads, idle in this pass: the inputs of the next
-          // (p, q)'s first-pass lines with k2 in the other CTA's x half
-          // (F scaled by the next phases) into those lines' own rows of W,
-          // which no third-pass line reads
-          const C* phx = sPh + (slot ^ 1) * PHS;
-          const C u1 = phx[3 * N], u2 = phx[3 * N + 1], u3 = phx[3 * N + 2];
-#pragma unroll 1
-          for (int g = tq >> 5; g < 8; g += 3) {
-            const int hi = 2 * g + ((tid >> 4) & 1), k2 = 16 * (1 - r) + (tid & 15);
-            const int k1 = pair_kmap(r, hi);
-            C A, A3;
-            pair_coef(phx, u1, u2, u3, k1, k2, A, A3);
-            C* const row = sW + (hi * N + k2) * LP;
-#pragma unroll
-            for (int k = 0; k < N; ++k) {
-              const C e3 = phx[2 * N + k];
-              const C& Ak = k == NY ? A3 : A;
-              row[k] = cscale(Fat(k1, k2, k), Ak.x * e3.x - Ak.y * e3.y);
             }
           }
         }
