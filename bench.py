@@ -88,6 +88,9 @@ def _parse():
                     help='train and evaluate the learned surrogate in this run '
                          '(-1: on for couette-n24 at N=1)')
     ap.add_argument('--surrogate-steps', type=int, default=200)
+    ap.add_argument('--surrogate-harvest-steps', type=int, default=100,
+                    help='steps of every training trajectory (random '
+                         'initial states) the surrogate is harvested from')
     ap.add_argument('--initial', default='synthetic',
                     choices=['synthetic', 'workload'],
                     help='step mode: synthetic noisy Maxwellians or the '
@@ -390,6 +393,63 @@ def _timed(fn, steps, stream, flush):
     return times
 
 
+def _e2e_pipelined(step, src_bank, dst_bank, hin, hout, nsteps, stream,
+                   flush):
+    """Device time (ms) of nsteps end-to-end steps: step i's input goes
+    host -> device staging buffer on one copy stream while step i - 1
+    computes, and step i's result goes staging buffer -> host on another
+    while step i + 1 computes.  The compute stream moves the staged input
+    into the bank and the result out of it (device-to-device copies), runs
+    the step and flushes L2 before it.  Events on the compute stream bracket
+    everything from the first host-to-device copy to the last device-to-host
+    copy."""
+    import torch
+    dev = src_bank.data.device
+    h2d, d2h = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    sin = [torch.empty_like(src_bank.data) for _ in range(2)]
+    sout = [torch.empty_like(dst_bank.data) for _ in range(2)]
+    ev = lambda: torch.cuda.Event()
+    in_ready, in_free = [ev() for _ in range(2)], [ev() for _ in range(2)]
+    out_ready, out_free = [ev() for _ in range(2)], [ev() for _ in range(2)]
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    t0.record(stream)
+    h2d.wait_event(t0)
+    d2h.wait_event(t0)
+
+    def load(i):
+        b = i % 2
+        with torch.cuda.stream(h2d):
+            if i >= 2:
+                h2d.wait_event(in_free[b])
+            sin[b].copy_(hin.view_as(sin[b]), non_blocking=True)
+            in_ready[b].record(h2d)
+    load(0)
+    for i in range(nsteps):
+        b = i % 2
+        if i + 1 < nsteps:
+            load(i + 1)
+        stream.wait_event(in_ready[b])
+        flush.zero_()
+        src_bank.data.copy_(sin[b], non_blocking=True)
+        in_free[b].record(stream)
+        step()
+        if i >= 2:
+            stream.wait_event(out_free[b])
+        sout[b].copy_(dst_bank.data, non_blocking=True)
+        out_ready[b].record(stream)
+        with torch.cuda.stream(d2h):
+            d2h.wait_event(out_ready[b])
+            hout.view_as(sout[b]).copy_(sout[b], non_blocking=True)
+            out_free[b].record(d2h)
+    stream.wait_stream(d2h)
+    t1.record(stream)
+    t1.synchronize()
+    torch.cuda.synchronize(dev)
+    return t0.elapsed_time(t1)
+
+
 def _max_over_ranks(x, world, device):
     if world == 1:
         return x
@@ -548,8 +608,9 @@ def run_b200(args):
     ms_per_step = t_ms/args.steps
     value = world*evals_per_step*args.steps/(t_ms*1e-3)
 
-    # end to end through the public API: pinned host distribution ->
-    # device, the step, device -> pinned host result, all timed
+    # end to end through the public API: every step's distribution comes
+    # from pinned host memory and its result goes back to pinned host
+    # memory, all inside the timed region
     e2e = None
     if args.e2e:
         src_bank = fin
@@ -558,21 +619,23 @@ def run_b200(args):
                           pin_memory=True)
         hin.copy_(src_bank.data.cpu())
         hout = torch.empty_like(hin, pin_memory=True)
-
-        def e2e_step():
+        for _ in range(2):
             src_bank.data.copy_(hin, non_blocking=True)
             step()
             hout.copy_(dst_bank.data, non_blocking=True)
-        for _ in range(2):
-            e2e_step()
         torch.cuda.synchronize()
-        te = _max_over_ranks(float(np.sum(_timed(e2e_step, args.steps,
-                                                   stream, flush))),
+        te = _max_over_ranks(_e2e_pipelined(step, src_bank, dst_bank, hin,
+                                            hout, args.steps, stream, flush),
                              world, be.device)
         e2e = {'value': world*evals_per_step*args.steps/(te*1e-3),
                'unit': 'evals/s',
                'h2d_bytes_per_step': int(hin.numel()*hin.element_size()),
-               'd2h_bytes_per_step': int(hout.numel()*hout.element_size())}
+               'd2h_bytes_per_step': int(hout.numel()*hout.element_size()),
+               'copies': 'host to device and device to host on their own '
+                         'streams, double-buffered in device memory, '
+                         'overlapping the neighbouring steps; the first '
+                         'input and the last result are inside the timed '
+                         'region; L2 flushed before every step'}
         del hin, hout
 
     # dominant kernel: the fused VHS launch, timed alone on the same bank
@@ -668,6 +731,7 @@ def run_b200(args):
         from frfs_b200.surrogate_study import run_study
         sur = run_study(workloads.WORKLOADS[args.workload],
                         device=be.device, nsteps=args.surrogate_steps,
+                        steps=args.surrogate_harvest_steps,
                         sphdesign=SPHDESIGN, extra_thresholds=(0.1, 0.2))
 
     if rank == 0:
