@@ -476,6 +476,8 @@ def _fp64_line(args, stream, flush, fin32):
     fin = be.matrix(f.shape, f)
     fout = be.matrix(f.shape)
     npts = f.shape[0]*f.shape[2]
+    # the autotuner picks the FP64 launch shape on this bank as well
+    tune = sm.autotune(fin, fout, cache=False)
     sm.fs_all(fin, fout)
     sm.status()
     ms = float(np.mean(_timed(lambda: sm.fs_all(fin, fout), 3, stream,
@@ -493,6 +495,8 @@ def _fp64_line(args, stream, flush, fin32):
             'dtype': 'f64', 'sweep_ms': ms, 'points': npts,
             'kernel': {'push': 'vhs_push_kernel',
                        'pull': 'vhs_cluster_kernel'}.get(kind, kind),
+            'launch': sm.variants()[getattr(sm, '_variant', 0)],
+            'ms_by_variant': tune.get('all_ms', {}),
             'roofline': {'bound': 'fp64-simt', 'achieved': achieved,
                          'peak': tf.value, 'unit': 'TFLOP/s',
                          'frac': achieved/tf.value,
