@@ -682,11 +682,22 @@ def run_b200(args):
     extra = {}
     if args.mode == 'step':
         extra['dg_step_ms'] = ms_per_step
-        # DG residual + RK combination, HBM bound: time it alone
-        dg_ms = float(np.mean(_timed(
-            lambda: system.rk_stage(1, 0, 0.5, 0, 0.5, 1, 1e-3, 2,
-                                    interp=True),
-            max(2, min(args.steps, 5)), stream, flush)))
+        # DG residual + RK combination, HBM bound: time it alone, replayed
+        # from a CUDA graph as the solver's stages are (--graphs 1; the
+        # partitioned stage, with its collective, runs eagerly)
+        def dg_stage():
+            system.rk_stage(1, 0, 0.5, 0, 0.5, 1, 1e-3, 2, interp=True)
+        dg_fn = dg_stage
+        if args.graphs and system.halo is None:
+            dg_stage()
+            torch.cuda.synchronize()
+            dg_graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(dg_graph):
+                dg_stage()
+            dg_fn = dg_graph.replay
+        dg_ms = float(np.mean(_timed(dg_fn, max(2, min(args.steps, 5)),
+                                     stream, flush)))
+        dg_fn = dg_graph = None
         esz = 8 if prec == 64 else 4
         U, F, V = system.nupts, system.nfpts, vm.vsize()
         # interp: read u, write uf; residual: read u, A, B, C, uf of the
@@ -765,9 +776,121 @@ def run_b200(args):
         dist.destroy_process_group()
 
 
+def run_mixture(args):
+    """Binary-mixture VSS operator (frfs's dgfsbi 'vss-gll'): Q_p =
+    sum_q Q(f_p, f_q) for both species at every point of a 576-point bank
+    (the Couette layout, 9 x 64), one persistent launch per ordered pair.
+    One step is one sweep; evaluations count one Q_p per species and point."""
+    import torch
+    from frfs_b200 import _lib, workloads
+    from frfs_b200.backend import B200Backend
+    from frfs_b200.inifile import Inifile
+    from frfs_b200.mixture import (DGFSBiVelocityMesh,
+                                   DGFSBiVSSGLLScatteringModel)
+    cfg = Inifile(workloads.MIXTURES[args.workload](precision=args.precision))
+    cfg.set('spherical-design-rule', 'path', SPHDESIGN)
+    torch.cuda.set_device(0)
+    be = B200Backend(cfg, device='cuda:0')
+    vm = DGFSBiVelocityMesh(be, cfg)
+    sm = DGFSBiVSSGLLScatteringModel(be, cfg, vm)
+    nupts, neles = 9, 64
+    npts = nupts*neles
+    V = vm.vsize()
+    m1, m2 = vm.masses()
+    rng = np.random.default_rng(0)
+    cv = vm.cv()
+    c2 = np.sum(cv*cv, axis=0)
+    fs = []
+    for nden, m in ((0.6, m1), (0.4, m2)):
+        mx = nden*(m/np.pi)**1.5*np.exp(-m*c2)
+        fs.append(mx[None, :, None] *
+                  (1.0 + 0.01*rng.standard_normal((nupts, V, neles))))
+    f0, f1 = (be.matrix((nupts, V, neles), f) for f in fs)
+    q0, q1 = be.matrix((nupts, V, neles)), be.matrix((nupts, V, neles))
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256*1024*1024 // 4, dtype=torch.float32,
+                        device=be.device)
+
+    def step():
+        sm.fs_all(f0, f1, q0, q1)
+    for _ in range(args.warmup):
+        step()
+    sm.status()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    times = _timed(step, args.steps, stream, flush)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    sm.status()
+    t_ms = float(np.sum(times))
+    evals = 2*npts
+    value = evals*args.steps/(t_ms*1e-3)
+    # end to end: both species' banks in from pinned host memory, both
+    # results back, every step
+    hin = [torch.empty(x.data.numel(), dtype=x.data.dtype, pin_memory=True)
+           for x in (f0, f1)]
+    for h, x in zip(hin, (f0, f1)):
+        h.copy_(x.data.cpu())
+    hout = [torch.empty_like(h, pin_memory=True) for h in hin]
+
+    def e2e_step():
+        for h, x in zip(hin, (f0, f1)):
+            x.data.copy_(h.view_as(x.data), non_blocking=True)
+        step()
+        for h, x in zip(hout, (q0, q1)):
+            h.view_as(x.data).copy_(x.data, non_blocking=True)
+    e2e_step()
+    torch.cuda.synchronize()
+    te = float(np.sum(_timed(e2e_step, args.steps, stream, flush)))
+    nbytes = int(sum(h.numel()*h.element_size() for h in hin))
+    prec = 64 if args.precision == 'double' else 32
+    tf = _lib.c_double()
+    pms = _lib.ct.c_float()
+    _lib.check(_lib.load().dgfs_probe_fma_peak(
+        prec, 4096 if prec == 32 else 1024, _lib.ct.byref(tf),
+        _lib.ct.byref(pms), stream.cuda_stream), 'dgfs_probe_fma_peak')
+    achieved = sm.flops_per_point()*npts/(t_ms/args.steps*1e-3)/1e12
+    line = {
+        'metric': METRIC, 'value': value, 'unit': 'evals/s', 'n_gpus': 1,
+        'steps': args.steps, 'warmup': args.warmup,
+        'ms_per_step': t_ms/args.steps, 'higher_is_better': True,
+        'scaling': 'weak', 'vs_baseline': None,
+        'dtype': 'f32' if prec == 32 else 'f64', 'data': 'synthetic',
+        'config': {'workload': f'{args.workload}: binary-mixture VSS Q_p '
+                               f'at every point, both species',
+                   'points': npts, 'Nv': vm.Nv(), 'Nrho': vm.Nrho(),
+                   'M': vm.M(), 'species': 2, 'mode': 'collide',
+                   'l2': 'flushed between timed steps (256 MiB write)'},
+        'clocks': clk,
+        'e2e': {'value': evals*args.steps/(te*1e-3), 'unit': 'evals/s',
+                'h2d_bytes_per_step': nbytes, 'd2h_bytes_per_step': nbytes},
+        'gpu_launches': 4*args.steps,
+        'roofline': {'bound': 'fp32-simt' if prec == 32 else 'fp64-simt',
+                     'achieved': achieved, 'peak': tf.value,
+                     'unit': 'TFLOP/s', 'frac': achieved/tf.value,
+                     'peak_source': 'measured in this run: FMA loop on '
+                                    'every SM (dgfs_probe_fma_peak)',
+                     'flops_per_point': sm.flops_per_point(),
+                     'launch_ms': t_ms/args.steps, 'traffic': None,
+                     'traffic_source': 'not captured',
+                     'kernel': 'vss_push_kernel (4 launches, one per '
+                               'ordered pair)'},
+        'cpu_baseline': None,
+    }
+    print(json.dumps(line))
+
+
 def main():
     args = _parse()
-    if args.impl == 'reference':
+    from frfs_b200 import workloads
+    if args.workload in workloads.MIXTURES:
+        if args.impl == 'reference':
+            print(json.dumps({'impl': 'reference', 'unavailable':
+                              'the reference arm times the VHS workloads'}))
+            return
+        run_mixture(args)
+    elif args.impl == 'reference':
         run_reference(args)
     else:
         run_b200(args)

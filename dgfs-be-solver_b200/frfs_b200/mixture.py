@@ -206,6 +206,17 @@ class DGFSBiVSSGLLScatteringModel:
         """Q_p = sum_q Q(f_p, f_q) at every point of the banks."""
         self.fs(-1, 0, *args)
 
+    def flops_per_point(self):
+        """Algorithmic FLOPs of all ordered pairs' Q(f_p, f_q) at one
+        point: per pair 3 Nrho M + 4 complex 3D transforms (the reference's
+        count, scattering.py:227-315: F, G, two inverse and one forward
+        transform per radial node and direction, the gain and loss inverse
+        transforms) at 5 V log2 V each, plus 20 Nrho M V for the phase
+        products, g h and the weighted gain sum."""
+        V, P, M = self.vm.vsize(), self.vm.Nrho(), self.vm.M()
+        per_pair = 5.0*V*np.log2(V)*(3*P*M + 4) + 20.0*P*M*V
+        return len(self._cases)*per_pair
+
     def status(self):
         flag = c_int()
         for pq, h in self._h.items():

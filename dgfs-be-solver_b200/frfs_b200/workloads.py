@@ -295,3 +295,60 @@ WORKLOADS = {
     'channel-n32': channel_n32,
     'cylinder-n32': cylinder_n32,
 }
+
+
+def mixture_n24(precision='single', Nv=24, Nrho=12, M=32, Mpre=32):
+    """Binary argon-krypton mixture for frfs's dgfsbi VSS operator
+    (frfs/solvers/dgfsbi/velocitymesh.py:27-151, scattering.py:44-330):
+    N=24, Nrho=12, the 32-point full-sphere design for the directions and
+    for the precomputation of the direction-dependent gain kernel, and
+    Bird's VSS parameters (Ar: alpha 1.40, omega 0.81, d 4.11e-10 m; Kr:
+    alpha 1.32, omega 0.80, d 4.76e-10 m; the unlike pair takes the
+    means).  The collision operator alone: no mesh, no solver section."""
+    gas = {'0': (1.40, 0.81, 4.11e-10), '1': (1.32, 0.80, 4.76e-10)}
+    lines = []
+    for p in '01':
+        for q in '01':
+            a = 0.5*(gas[p][0] + gas[q][0])
+            w = 0.5*(gas[p][1] + gas[q][1])
+            d = 0.5*(gas[p][2] + gas[q][2])
+            lines.append(f'alpha{p}{q} = {a!r}\nomega{p}{q} = {w!r}\n'
+                         f'dRef{p}{q} = {d!r}\nTref{p}{q} = 273.0')
+    sm = '\n'.join(lines)
+    return f"""
+[backend]
+precision = {precision}
+
+[constants]
+Nv = {Nv}
+Nrho = {Nrho}
+
+[non-dim]
+T0 = 273.0
+H0 = 1e-3
+rho0 = 1.5e-3
+molarMass0 = {_MOLAR_MASS!r}
+
+[velocity-mesh]
+cmax = 0.0
+Tmax = 273.0
+dev = 5.0
+molarMass1 = {_MOLAR_MASS!r}
+molarMass2 = 83.8e-3
+
+[spherical-design-rule]
+ssrule = womersley
+M = {M}
+
+[scattering-model]
+type = vss-gll
+ssrulepre = womersley
+Mpre = {Mpre}
+{sm}
+"""
+
+
+# collision-operator-only workloads (bench.py --mode collide)
+MIXTURES = {
+    'mixture-n24': mixture_n24,
+}
