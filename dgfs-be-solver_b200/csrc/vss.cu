@@ -99,11 +99,15 @@ const VssShape* vss_shape(int prec, int N) {
 
 struct dgfs_vss {
   int N, P, M, prec, V, device;
+  int Mh;  // like pair on an antipodally symmetric design: M / 2 (one
+           // direction of each antipodal pair, tables phase_h and b_h), else 0
   double prefac;
   const VssShape* shape;
   int max_clusters;
   void* phase;  // cx<T> [P][M][2][3][N]
   void* b;      // cx<T> [P][M][V], weight w_x folded in
+  void* phase_h;  // cx<T> [P][Mh][2][3][N] (Mh > 0)
+  void* b_h;      // cx<T> [P][Mh][V]: b(y) + b(-y)
   void* c;      // cx<T> [V]
   void* fc;     // scratch [clusters * C][V / C] cx<T>
   int* err;
@@ -145,17 +149,6 @@ template <typename T> int build(dgfs_vss* h, const dgfs_vss_params* p) {
   const double kp = p->mp / (p->mp + p->mq), kq = p->mq / (p->mp + p->mq);
   std::vector<double> l0(N);
   for (int k = 0; k < N; ++k) l0[k] = k < N / 2 ? k : k - N;
-  std::vector<std::complex<double>> phase((size_t)P * M * 6 * N);
-  for (int x = 0; x < P; ++x) {
-    const double fac = pi / L * p->qz[x];
-    for (int y = 0; y < M; ++y)
-      for (int f = 0; f < 2; ++f)
-        for (int ax = 0; ax < 3; ++ax)
-          for (int k = 0; k < N; ++k) {
-            const double ang = (f == 0 ? kq : -kp) * fac * p->sz[y * 3 + ax] * l0[k];
-            phase[((((size_t)x * M + y) * 2 + f) * 3 + ax) * N + k] = std::polar(1.0, ang);
-          }
-  }
   std::vector<double> B((size_t)M * Mp);
   for (int y = 0; y < M; ++y)
     for (int y2 = 0; y2 < Mp; ++y2) {
@@ -170,7 +163,74 @@ template <typename T> int build(dgfs_vss* h, const dgfs_vss_params* p) {
     for (int v = 0; v < V; ++v)
       lpre[(size_t)y2 * V + v] = p->szpre[y2 * 3] * l0[v / (N * N)] + p->szpre[y2 * 3 + 1] * l0[(v / N) % N] +
                                  p->szpre[y2 * 3 + 2] * l0[v % N];
-  std::vector<std::complex<double>> b((size_t)P * M * V), c(V, 0.0), eb((size_t)Mp * V), ec((size_t)Mp * V);
+
+  // A like pair (equal masses, so kp = kq = 1/2) applied to one
+  // distribution twice, on a design that holds every direction's antipode:
+  // the antipode turns e^{+i a/2} F into e^{-i a/2} F and back, so its
+  // product g h and FFT(g h) are the direction's own.  A second set of
+  // tables loops over one direction of each antipodal pair with the gain
+  // kernel b(y) + b(-y): exact, with half the transforms and half the table
+  // reads; dgfs_vss_apply uses it when fp == fq.
+  std::vector<int> rep, anti(M, -1);
+  if (p->mp == p->mq) {
+    for (int y = 0; y < M; ++y) {
+      if (anti[y] >= 0) continue;
+      for (int z = y + 1; z < M; ++z) {
+        if (anti[z] >= 0) continue;
+        double d = 0.0;
+        for (int ax = 0; ax < 3; ++ax) d = std::fmax(d, std::fabs(p->sz[y * 3 + ax] + p->sz[z * 3 + ax]));
+        if (d < 1e-9) {
+          anti[y] = z;
+          anti[z] = y;
+          rep.push_back(y);
+          break;
+        }
+      }
+      if (anti[y] < 0) break;
+    }
+  }
+  const bool halve = p->mp == p->mq && 2 * (int)rep.size() == M;
+  std::vector<int> all(M);
+  for (int y = 0; y < M; ++y) all[y] = y;
+
+  // axis phases [P][K][2][3][N] and weighted gain kernels [P][K][V] of the
+  // directions `dirs` (each with its antipode's b added when `pairs`)
+  std::vector<std::complex<double>> eb((size_t)Mp * V), row(V);
+  auto tables = [&](const std::vector<int>& dirs, bool pairs, std::vector<std::complex<double>>& phase,
+                    std::vector<std::complex<double>>& b) {
+    const int K = (int)dirs.size();
+    phase.assign((size_t)P * K * 6 * N, 0.0);
+    b.assign((size_t)P * K * V, 0.0);
+    for (int x = 0; x < P; ++x) {
+      const double fac = pi / L * p->qz[x];
+      const double fac_b = swpre * std::pow(p->qz[x], gam + 2.0);
+      const double w = p->qw[x] * sw / V;
+      for (int j = 0; j < K; ++j)
+        for (int f = 0; f < 2; ++f)
+          for (int ax = 0; ax < 3; ++ax)
+            for (int k = 0; k < N; ++k) {
+              const double ang = (f == 0 ? kq : -kp) * fac * p->sz[dirs[j] * 3 + ax] * l0[k];
+              phase[((((size_t)x * K + j) * 2 + f) * 3 + ax) * N + k] = std::polar(1.0, ang);
+            }
+      for (size_t i = 0; i < eb.size(); ++i) eb[i] = std::polar(1.0, -kq * fac * lpre[i]);
+      for (int j = 0; j < K; ++j) {
+        std::complex<double>* dst = b.data() + ((size_t)x * K + j) * V;
+        for (int t = 0; t < (pairs ? 2 : 1); ++t) {
+          const int y = t == 0 ? dirs[j] : anti[dirs[j]];
+          for (int v = 0; v < V; ++v) row[v] = 0.0;
+          for (int y2 = 0; y2 < Mp; ++y2) {
+            const double bb = B[(size_t)y * Mp + y2];
+            const std::complex<double>* e = eb.data() + (size_t)y2 * V;
+            for (int v = 0; v < V; ++v) row[v] += bb * e[v];
+          }
+          for (int v = 0; v < V; ++v) dst[v] += row[v] * (w * fac_b);
+        }
+      }
+    }
+  };
+
+  // the loss kernel c (every direction of the design)
+  std::vector<std::complex<double>> c(V, 0.0), ec((size_t)Mp * V);
   std::vector<double> Bsum(Mp, 0.0);
   for (int y2 = 0; y2 < Mp; ++y2)
     for (int y = 0; y < M; ++y) Bsum[y2] += B[(size_t)y * Mp + y2];
@@ -178,30 +238,24 @@ template <typename T> int build(dgfs_vss* h, const dgfs_vss_params* p) {
     const double fac = pi / L * p->qz[x];
     const double fac_b = swpre * std::pow(p->qz[x], gam + 2.0);
     const double fac_c = p->qw[x] * sw * fac_b;
-    const double w = p->qw[x] * sw / V;
-    for (size_t i = 0; i < eb.size(); ++i) {
-      eb[i] = std::polar(1.0, -kq * fac * lpre[i]);
-      ec[i] = std::polar(1.0, -fac * lpre[i]);
-    }
-    for (int y = 0; y < M; ++y) {
-      std::complex<double>* row = b.data() + ((size_t)x * M + y) * V;
-      for (int v = 0; v < V; ++v) row[v] = 0.0;
-      for (int y2 = 0; y2 < Mp; ++y2) {
-        const double bb = B[(size_t)y * Mp + y2];
-        const std::complex<double>* e = eb.data() + (size_t)y2 * V;
-        for (int v = 0; v < V; ++v) row[v] += bb * e[v];
-      }
-      for (int v = 0; v < V; ++v) row[v] *= w * fac_b;
-    }
+    for (size_t i = 0; i < ec.size(); ++i) ec[i] = std::polar(1.0, -fac * lpre[i]);
     for (int y2 = 0; y2 < Mp; ++y2) {
       const std::complex<double>* e = ec.data() + (size_t)y2 * V;
       const double s = fac_c * Bsum[y2];
       for (int v = 0; v < V; ++v) c[v] += s * e[v];
     }
   }
+  std::vector<std::complex<double>> phase, b;
+  tables(all, false, phase, b);
   int rc;
   if ((rc = upload_cx<T>(&h->phase, phase)) || (rc = upload_cx<T>(&h->b, b)) || (rc = upload_cx<T>(&h->c, c)))
     return rc;
+  h->Mh = 0;
+  if (halve) {
+    tables(rep, true, phase, b);
+    if ((rc = upload_cx<T>(&h->phase_h, phase)) || (rc = upload_cx<T>(&h->b_h, b))) return rc;
+    h->Mh = (int)rep.size();
+  }
   return DGFS_OK;
 }
 
@@ -209,6 +263,8 @@ void free_vss(dgfs_vss* h) {
   if (!h) return;
   cudaFree(h->phase);
   cudaFree(h->b);
+  cudaFree(h->phase_h);
+  cudaFree(h->b_h);
   cudaFree(h->c);
   cudaFree(h->fc);
   cudaFree(h->err);
@@ -318,6 +374,8 @@ extern "C" int dgfs_vss_apply(dgfs_vss* h, const void* fp, const void* fq, void*
   cudaGetDevice(&dev);
   if (dev != h->device) return set_error(DGFS_ERR_INVALID, "handle built on device %d used on device %d", h->device, dev);
   const int ncl = npts < h->max_clusters ? npts : h->max_clusters;
+  // the halved tables need the same distribution on both sides
+  const bool half = h->Mh > 0 && fp == fq;
   cudaError_t e;
   if (h->prec == 64) {
     VssArgs<double> a{};
@@ -331,9 +389,9 @@ extern "C" int dgfs_vss_apply(dgfs_vss* h, const void* fp, const void* fq, void*
     a.pt0 = pt0;
     a.npts = npts;
     a.P = h->P;
-    a.M = h->M;
-    a.phase = (const double2*)h->phase;
-    a.b = (const double2*)h->b;
+    a.M = half ? h->Mh : h->M;
+    a.phase = (const double2*)(half ? h->phase_h : h->phase);
+    a.b = (const double2*)(half ? h->b_h : h->b);
     a.c = (const double2*)h->c;
     a.fc = (double2*)h->fc;
     a.err = h->err;
@@ -352,9 +410,9 @@ extern "C" int dgfs_vss_apply(dgfs_vss* h, const void* fp, const void* fq, void*
     a.pt0 = pt0;
     a.npts = npts;
     a.P = h->P;
-    a.M = h->M;
-    a.phase = (const float2*)h->phase;
-    a.b = (const float2*)h->b;
+    a.M = half ? h->Mh : h->M;
+    a.phase = (const float2*)(half ? h->phase_h : h->phase);
+    a.b = (const float2*)(half ? h->b_h : h->b);
     a.c = (const float2*)h->c;
     a.fc = (float2*)h->fc;
     a.err = h->err;
