@@ -106,8 +106,6 @@ struct dgfs_vss {
   int max_clusters;
   void* phase;  // cx<T> [P][M][2][3][N]
   void* b;      // cx<T> [P][M][V], weight w_x folded in
-  int* anti;      // [M] antipode of every direction (antipodally symmetric design), else null
-  double mp, mq;  // the pair's reduced masses
   void* phase_h;  // cx<T> [P][Mh][2][3][N] (Mh > 0)
   void* b_h;      // cx<T> [P][Mh][V]: b(y) + b(-y)
   void* c;      // cx<T> [V]
@@ -174,23 +172,24 @@ template <typename T> int build(dgfs_vss* h, const dgfs_vss_params* p) {
   // kernel b(y) + b(-y): exact, with half the transforms and half the table
   // reads; dgfs_vss_apply uses it when fp == fq.
   std::vector<int> rep, anti(M, -1);
-  for (int y = 0; y < M; ++y) {
-    if (anti[y] >= 0) continue;
-    for (int z = y + 1; z < M; ++z) {
-      if (anti[z] >= 0) continue;
-      double d = 0.0;
-      for (int ax = 0; ax < 3; ++ax) d = std::fmax(d, std::fabs(p->sz[y * 3 + ax] + p->sz[z * 3 + ax]));
-      if (d < 1e-9) {
-        anti[y] = z;
-        anti[z] = y;
-        rep.push_back(y);
-        break;
+  if (p->mp == p->mq) {
+    for (int y = 0; y < M; ++y) {
+      if (anti[y] >= 0) continue;
+      for (int z = y + 1; z < M; ++z) {
+        if (anti[z] >= 0) continue;
+        double d = 0.0;
+        for (int ax = 0; ax < 3; ++ax) d = std::fmax(d, std::fabs(p->sz[y * 3 + ax] + p->sz[z * 3 + ax]));
+        if (d < 1e-9) {
+          anti[y] = z;
+          anti[z] = y;
+          rep.push_back(y);
+          break;
+        }
       }
+      if (anti[y] < 0) break;
     }
-    if (anti[y] < 0) break;
   }
-  const bool symmetric = 2 * (int)rep.size() == M;
-  const bool halve = p->mp == p->mq && symmetric;
+  const bool halve = p->mp == p->mq && 2 * (int)rep.size() == M;
   std::vector<int> all(M);
   for (int y = 0; y < M; ++y) all[y] = y;
 
@@ -252,15 +251,6 @@ template <typename T> int build(dgfs_vss* h, const dgfs_vss_params* p) {
   if ((rc = upload_cx<T>(&h->phase, phase)) || (rc = upload_cx<T>(&h->b, b)) || (rc = upload_cx<T>(&h->c, c)))
     return rc;
   h->Mh = 0;
-  if (symmetric) {
-    // the antipode map, for launches that fuse a pair with its reverse
-    if (cudaMalloc((void**)&h->anti, (size_t)M * sizeof(int)) != cudaSuccess) {
-      h->anti = nullptr;
-      return set_error(DGFS_ERR_NOMEM, "cudaMalloc of the antipode map failed");
-    }
-    if (cudaMemcpy(h->anti, anti.data(), (size_t)M * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
-      return set_error(DGFS_ERR_CUDA, "cudaMemcpy: %s", cudaGetErrorString(cudaGetLastError()));
-  }
   if (halve) {
     tables(rep, true, phase, b);
     if ((rc = upload_cx<T>(&h->phase_h, phase)) || (rc = upload_cx<T>(&h->b_h, b))) return rc;
@@ -275,7 +265,6 @@ void free_vss(dgfs_vss* h) {
   cudaFree(h->b);
   cudaFree(h->phase_h);
   cudaFree(h->b_h);
-  cudaFree(h->anti);
   cudaFree(h->c);
   cudaFree(h->fc);
   cudaFree(h->err);
@@ -305,8 +294,6 @@ extern "C" int dgfs_vss_create(const dgfs_vss_params* p, dgfs_vss** out) {
   h->prec = p->precision;
   h->V = p->Nv * p->Nv * p->Nv;
   h->prefac = p->prefactor;
-  h->mp = p->mp;
-  h->mq = p->mq;
   h->shape = shape;
   int rc = DGFS_OK;
   if (cudaGetDevice(&h->device) != cudaSuccess) rc = set_error(DGFS_ERR_CUDA, "no CUDA device");
@@ -360,126 +347,79 @@ extern "C" int dgfs_vss_destroy(dgfs_vss* h) {
   return DGFS_OK;
 }
 
-namespace {
-
-// Bank checks shared by the entry points: sizes, the point range, no output
-// overlapping an input, the handle's device.
-int check_apply(const dgfs_vss* h, const void* fp, const void* fq, const void* const* outs, int nout, int nupts,
-                int neles, long long ldim, int soasz, int elem, int upt, int* pt0, int* npts) {
-  if (!h || !fp || !fq) return set_error(DGFS_ERR_INVALID, "null argument");
-  for (int i = 0; i < nout; ++i)
-    if (!outs[i]) return set_error(DGFS_ERR_INVALID, "null output bank");
+extern "C" int dgfs_vss_apply(dgfs_vss* h, const void* fp, const void* fq, void* Q, int nupts, int neles,
+                              long long ldim, int soasz, int elem, int upt, int accumulate, void* stream) {
+  clear_error();
+  if (!h || !fp || !fq || !Q) return set_error(DGFS_ERR_INVALID, "null argument");
   if (nupts < 1 || neles < 1 || soasz < 1)
     return set_error(DGFS_ERR_INVALID, "bad bank shape nupts=%d neles=%d soasz=%d", nupts, neles, soasz);
   const long long nblk = (neles + soasz - 1) / soasz;
   if (ldim < nblk * soasz * (long long)h->V) return set_error(DGFS_ERR_INVALID, "ldim=%lld smaller than one row", ldim);
   const size_t esz = h->prec == 64 ? 8 : 4;
   const size_t bytes = (size_t)nupts * (size_t)ldim * esz;
-  const char *pb = (const char*)fp, *fb = (const char*)fq;
-  for (int i = 0; i < nout; ++i) {
-    const char* qb = (const char*)outs[i];
-    if ((pb < qb + bytes && qb < pb + bytes) || (fb < qb + bytes && qb < fb + bytes))
-      return set_error(DGFS_ERR_INVALID, "an output bank overlaps an input bank");
-    for (int k = 0; k < i; ++k) {
-      const char* ob = (const char*)outs[k];
-      if (ob < qb + bytes && qb < ob + bytes) return set_error(DGFS_ERR_INVALID, "the output banks overlap");
-    }
-  }
+  const char *qb = (const char*)Q, *pb = (const char*)fp, *fb = (const char*)fq;
+  if ((pb < qb + bytes && qb < pb + bytes) || (fb < qb + bytes && qb < fb + bytes))
+    return set_error(DGFS_ERR_INVALID, "the output bank overlaps an input bank");
+  int pt0, npts;
   if (elem >= 0) {
     if (elem >= neles || upt < 0 || upt >= nupts)
       return set_error(DGFS_ERR_INVALID, "point (elem=%d, upt=%d) outside bank (%d, %d)", elem, upt, neles, nupts);
-    *pt0 = upt * neles + elem;
-    *npts = 1;
+    pt0 = upt * neles + elem;
+    npts = 1;
   } else {
-    *pt0 = 0;
-    *npts = nupts * neles;
+    pt0 = 0;
+    npts = nupts * neles;
   }
   int dev = -1;
   cudaGetDevice(&dev);
   if (dev != h->device) return set_error(DGFS_ERR_INVALID, "handle built on device %d used on device %d", h->device, dev);
-  return DGFS_OK;
-}
-
-// One launch of pair h (and, with h2, of the reverse pair in the same pass).
-template <typename T>
-cudaError_t run_vss(const dgfs_vss* h, const dgfs_vss* h2, const void* fp, const void* fq, void* Q, void* Q2,
-                       int nupts, int neles, long long ldim, int soasz, int pt0, int npts, int accumulate,
-                       int accumulate2, cudaStream_t stream) {
-  using CT = cx<T>;
-  // the halved tables need the same distribution on both sides
-  const bool half = !h2 && h->Mh > 0 && fp == fq;
-  VssArgs<T> a{};
-  a.fp = (const T*)fp;
-  a.fq = (const T*)fq;
-  a.Q = (T*)Q;
-  a.ldim = ldim;
-  a.nupts = nupts;
-  a.neles = neles;
-  a.soasz = soasz;
-  a.pt0 = pt0;
-  a.npts = npts;
-  a.P = h->P;
-  a.M = half ? h->Mh : h->M;
-  a.phase = (const CT*)(half ? h->phase_h : h->phase);
-  a.b = (const CT*)(half ? h->b_h : h->b);
-  a.c = (const CT*)h->c;
-  a.fc = (CT*)h->fc;
-  a.err = h->err;
-  a.prefac = (T)h->prefac;
-  a.accumulate = accumulate ? 1 : 0;
-  if (h2) {
-    a.b2 = (const CT*)h2->b;
-    a.c2 = (const CT*)h2->c;
-    a.anti = h->anti;
-    a.fc2 = (CT*)h2->fc;
-    a.Q2 = (T*)Q2;
-    a.prefac2 = (T)h2->prefac;
-    a.accumulate2 = accumulate2 ? 1 : 0;
-  }
   const int ncl = npts < h->max_clusters ? npts : h->max_clusters;
-  if constexpr (sizeof(T) == 8) return h->shape->launch64(a, ncl, stream);
-  else return h->shape->launch32(a, ncl, stream);
-}
-
-}  // namespace
-
-extern "C" int dgfs_vss_apply(dgfs_vss* h, const void* fp, const void* fq, void* Q, int nupts, int neles,
-                              long long ldim, int soasz, int elem, int upt, int accumulate, void* stream) {
-  clear_error();
-  int pt0 = 0, npts = 0;
-  const void* outs[1] = {Q};
-  int rc = check_apply(h, fp, fq, outs, 1, nupts, neles, ldim, soasz, elem, upt, &pt0, &npts);
-  if (rc) return rc;
-  const cudaError_t e =
-      h->prec == 64 ? run_vss<double>(h, nullptr, fp, fq, Q, nullptr, nupts, neles, ldim, soasz, pt0, npts,
-                                         accumulate, 0, (cudaStream_t)stream)
-                    : run_vss<float>(h, nullptr, fp, fq, Q, nullptr, nupts, neles, ldim, soasz, pt0, npts,
-                                        accumulate, 0, (cudaStream_t)stream);
-  if (e != cudaSuccess) return set_error(DGFS_ERR_CUDA, "VSS launch failed: %s", cudaGetErrorString(e));
-  return DGFS_OK;
-}
-
-extern "C" int dgfs_vss_apply_pair(dgfs_vss* hpq, dgfs_vss* hqp, const void* fp, const void* fq, void* Qp,
-                                   void* Qq, int nupts, int neles, long long ldim, int soasz, int elem, int upt,
-                                   int accumulate_p, int accumulate_q, void* stream) {
-  clear_error();
-  if (!hpq || !hqp) return set_error(DGFS_ERR_INVALID, "null handle");
-  if (hpq->prec != hqp->prec || hpq->N != hqp->N || hpq->P != hqp->P || hpq->M != hqp->M ||
-      hpq->device != hqp->device || hpq->shape != hqp->shape)
-    return set_error(DGFS_ERR_INVALID, "the two pairs differ in precision, grid, quadrature or device");
-  if (hpq->mp != hqp->mq || hpq->mq != hqp->mp)
-    return set_error(DGFS_ERR_INVALID, "the second handle is not the reverse pair (masses %g, %g against %g, %g)",
-                     hpq->mp, hpq->mq, hqp->mp, hqp->mq);
-  if (!hpq->anti) return set_error(DGFS_ERR_UNSUPPORTED, "the design is not antipodally symmetric");
-  int pt0 = 0, npts = 0;
-  const void* outs[2] = {Qp, Qq};
-  int rc = check_apply(hpq, fp, fq, outs, 2, nupts, neles, ldim, soasz, elem, upt, &pt0, &npts);
-  if (rc) return rc;
-  const cudaError_t e =
-      hpq->prec == 64 ? run_vss<double>(hpq, hqp, fp, fq, Qp, Qq, nupts, neles, ldim, soasz, pt0, npts,
-                                           accumulate_p, accumulate_q, (cudaStream_t)stream)
-                      : run_vss<float>(hpq, hqp, fp, fq, Qp, Qq, nupts, neles, ldim, soasz, pt0, npts,
-                                          accumulate_p, accumulate_q, (cudaStream_t)stream);
+  // the halved tables need the same distribution on both sides
+  const bool half = h->Mh > 0 && fp == fq;
+  cudaError_t e;
+  if (h->prec == 64) {
+    VssArgs<double> a{};
+    a.fp = (const double*)fp;
+    a.fq = (const double*)fq;
+    a.Q = (double*)Q;
+    a.ldim = ldim;
+    a.nupts = nupts;
+    a.neles = neles;
+    a.soasz = soasz;
+    a.pt0 = pt0;
+    a.npts = npts;
+    a.P = h->P;
+    a.M = half ? h->Mh : h->M;
+    a.phase = (const double2*)(half ? h->phase_h : h->phase);
+    a.b = (const double2*)(half ? h->b_h : h->b);
+    a.c = (const double2*)h->c;
+    a.fc = (double2*)h->fc;
+    a.err = h->err;
+    a.prefac = h->prefac;
+    a.accumulate = accumulate ? 1 : 0;
+    e = h->shape->launch64(a, ncl, (cudaStream_t)stream);
+  } else {
+    VssArgs<float> a{};
+    a.fp = (const float*)fp;
+    a.fq = (const float*)fq;
+    a.Q = (float*)Q;
+    a.ldim = ldim;
+    a.nupts = nupts;
+    a.neles = neles;
+    a.soasz = soasz;
+    a.pt0 = pt0;
+    a.npts = npts;
+    a.P = h->P;
+    a.M = half ? h->Mh : h->M;
+    a.phase = (const float2*)(half ? h->phase_h : h->phase);
+    a.b = (const float2*)(half ? h->b_h : h->b);
+    a.c = (const float2*)h->c;
+    a.fc = (float2*)h->fc;
+    a.err = h->err;
+    a.prefac = (float)h->prefac;
+    a.accumulate = accumulate ? 1 : 0;
+    e = h->shape->launch32(a, ncl, (cudaStream_t)stream);
+  }
   if (e != cudaSuccess) return set_error(DGFS_ERR_CUDA, "VSS launch failed: %s", cudaGetErrorString(e));
   return DGFS_OK;
 }

@@ -46,17 +46,6 @@ template <typename T> struct VssArgs {
   int* err;
   T prefac;
   int accumulate;
-  // the reverse pair (q, p) in the same launch (b2 != nullptr): its product
-  // field at direction -y is this pair's at y, so every (x, y) also adds
-  // b2[x][anti[y]] FFT(g h) to its gain spectrum fc2, and the point ends
-  // with Q2 = prefac2 (Re IFFT(fc2) - f_q Re IFFT(c2 F))
-  const cx<T>* b2;     // [P][M][V] gain kernel of (q, p)
-  const cx<T>* c2;     // [V] its loss kernel
-  const int* anti;     // [M] antipode of every direction
-  cx<T>* fc2;          // scratch like fc
-  T* Q2;               // output bank of species q
-  T prefac2;
-  int accumulate2;
 };
 
 template <int N, int C> struct VssGeom {
@@ -124,7 +113,6 @@ __global__ void __launch_bounds__(PushGeom<N, C>::NT, MINB) vss_push_kernel(cons
   const int l2g = rank * NS + jl / N, l3 = jl % N;
   const int jglob = l2g * N + l3;
   CX* fc = a.fc + (size_t)blockIdx.x * N * NJ;
-  CX* fc2 = a.b2 ? a.fc2 + (size_t)blockIdx.x * N * NJ : nullptr;
   const int npq = a.P * a.M;
   int it = 0;
 
@@ -160,10 +148,6 @@ __global__ void __launch_bounds__(PushGeom<N, C>::NT, MINB) vss_push_kernel(cons
     if (tid < NJ) {
 #pragma unroll
       for (int k = 0; k < N; ++k) fc[k * NJ + jl] = mk<CX>(T(0), T(0));
-      if (fc2) {
-#pragma unroll
-        for (int k = 0; k < N; ++k) fc2[k * NJ + jl] = mk<CX>(T(0), T(0));
-      }
     }
     load_phases(0, it & 1);
     __syncthreads();
@@ -201,32 +185,23 @@ __global__ void __launch_bounds__(PushGeom<N, C>::NT, MINB) vss_push_kernel(cons
         const CX* bb = a.b + (size_t)pq * V + jglob;
 #pragma unroll
         for (int k = 0; k < N; ++k) fc[k * NJ + jl] = cfma(bb[k * N * N], y[k], fc[k * NJ + jl]);
-        if (fc2) {
-          const int xq = pq / a.M, yq = pq % a.M;
-          const CX* b2 = a.b2 + ((size_t)xq * a.M + a.anti[yq]) * V + jglob;
-#pragma unroll
-          for (int k = 0; k < N; ++k) fc2[k * NJ + jl] = cfma(b2[k * N * N], y[k], fc2[k * NJ + jl]);
-        }
       }
       __syncthreads();
       cl_arrive();  // pending: done reading the peers' slabs
     }
 
-    // ---- QG = IFFT(QGhat) (field 0), fL = IFFT(c G) (field 1); for the
-    // reverse pair then IFFT(QGhat2) and IFFT(c2 F) ---------------------------
-    for (int rev = 0; rev < (fc2 ? 2 : 1); ++rev) {
+    // ---- QG = IFFT(QGhat) (field 0), fL = IFFT(c G) (field 1) -------------
+    {
       const int set = it & 1;
       CX x[N];
       if (active) {
         if (which) {
-          const CX* cc = (rev ? a.c2 : a.c) + jglob;
-          const CX* src = rev ? sF : sG;
+          const CX* cc = a.c + jglob;
 #pragma unroll
-          for (int k = 0; k < N; ++k) x[k] = cmul(cc[k * N * N], src[k * NJ + jl]);
+          for (int k = 0; k < N; ++k) x[k] = cmul(cc[k * N * N], sG[k * NJ + jl]);
         } else {
-          const CX* g = rev ? fc2 : fc;
 #pragma unroll
-          for (int k = 0; k < N; ++k) x[k] = g[k * NJ + jl];
+          for (int k = 0; k < N; ++k) x[k] = fc[k * NJ + jl];
         }
         fft<T, N, +1>(x);
       }
@@ -236,17 +211,13 @@ __global__ void __launch_bounds__(PushGeom<N, C>::NT, MINB) vss_push_kernel(cons
       plane_rows_cols<T, N, C>(pset, tid);
       const CX* gain = pset;
       const CX* loss = pset + BSZ;
-      const T* fo = rev ? a.fq : a.fp;
-      T* qo = rev ? a.Q2 : a.Q;
-      const T pf = rev ? a.prefac2 : a.prefac;
-      const int acc = rev ? a.accumulate2 : a.accumulate;
       for (int i = tid; i < NS * N * N; i += NT) {
         const int x1l = i / (N * N), r2 = i % (N * N);
         const int64_t v = (int64_t)(rank * NS + x1l) * (N * N) + r2;
         const int idx = (i / N) * RP + i % N;
         const int64_t ai = soa_ix(upt, a.ldim, elem, v, V, a.soasz);
-        const T qv = pf * (gain[idx].x - fo[ai] * loss[idx].x);
-        qo[ai] = acc ? qo[ai] + qv : qv;
+        const T qv = a.prefac * (gain[idx].x - a.fp[ai] * loss[idx].x);
+        a.Q[ai] = a.accumulate ? a.Q[ai] + qv : qv;
       }
       __syncthreads();
       cl_arrive();  // done reading this plane set

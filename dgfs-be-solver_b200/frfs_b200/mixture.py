@@ -51,10 +51,6 @@ _lib.declare('dgfs_vss_apply', c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                        c_int, ct.c_void_p])
 _lib.declare('dgfs_vss_status', c_int, [ct.c_void_p, ct.c_void_p,
                                         ct.POINTER(c_int)])
-_lib.declare('dgfs_vss_apply_pair', c_int,
-             [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
-              ct.c_void_p, ct.c_void_p, c_int, c_int, ct.c_longlong, c_int,
-              c_int, c_int, c_int, c_int, ct.c_void_p])
 
 
 class DGFSBiVelocityMesh:
@@ -159,11 +155,6 @@ class DGFSBiVSSGLLScatteringModel:
 
     def perform_precomputation(self):
         vm, m = self.vm, self.vm.masses()
-        # a pair and its reverse share one launch when every direction of
-        # the design has its antipode in the design
-        sz = np.asarray(vm.sz(), dtype=np.float64)
-        self._fuse = bool(np.all(np.min(np.max(
-            np.abs(sz[:, None, :] + sz[None, :, :]), axis=2), axis=1) < 1e-9))
         keep = dict(qz=np.ascontiguousarray(vm.qz(), dtype=np.float64),
                     qw=np.ascontiguousarray(vm.qw(), dtype=np.float64),
                     sz=np.ascontiguousarray(vm.sz(), dtype=np.float64),
@@ -204,36 +195,12 @@ class DGFSBiVSSGLLScatteringModel:
 
     def fs(self, elem, upt, *args):
         """Q_p(elem, upt) = sum_q Q(f_p, f_q): args = (f_0 .. f_{n-1},
-        Q_0 .. Q_{n-1}) banks (scattering.py:317-330).  On an antipodally
-        symmetric design a pair (p, q), p < q, and its reverse (q, p) run in
-        one launch (dgfs_vss_apply_pair: the reverse pair's product field at
-        direction -y is the pair's at y); the sums over q keep their order."""
+        Q_0 .. Q_{n-1}) banks (scattering.py:317-330)."""
         n = self._nspcs
         assert len(args) == 2*n, 'need n distributions and n outputs'
-        done = set()
         for p, q in self._cases:
-            if (p, q) in done:
-                continue
-            if p < q and self._fuse:
-                self._apply_pair(p, q, args, elem, upt)
-                done.add((q, p))
-            else:
-                self._apply(f'{p}{q}', args[p], args[q], args[p + n], elem,
-                            upt, 1 if q > 0 else 0)
-
-    def _apply_pair(self, p, q, args, elem, upt):
-        n = self._nspcs
-        fp, fq = args[p], args[q]
-        nupts, _, neles = fp.ioshape
-        _, ldim, _ = fp.traits
-        # Q_p gets Q(f_p, f_q) after Q(f_p, f_0..f_{q-1}); Q_q starts its sum
-        # with Q(f_q, f_p) when p = 0
-        _lib.check(self._lib.dgfs_vss_apply_pair(
-            self._h[f'{p}{q}'], self._h[f'{q}{p}'], fp._as_parameter_,
-            fq._as_parameter_, args[p + n]._as_parameter_,
-            args[q + n]._as_parameter_, nupts, neles, ldim,
-            self.backend.soasz, elem, upt, 1 if q > 0 else 0,
-            1 if p > 0 else 0, self.backend.stream), 'dgfs_vss_apply_pair')
+            self._apply(f'{p}{q}', args[p], args[q], args[p + n], elem, upt,
+                        1 if q > 0 else 0)
 
     def fs_all(self, *args):
         """Q_p = sum_q Q(f_p, f_q) at every point of the banks."""

@@ -236,19 +236,6 @@ DGFS_API int dgfs_vss_apply(dgfs_vss* h, const void* fp, const void* fq,
                             int soasz, int elem, int upt, int accumulate,
                             void* stream);
 
-/* Q(f_p, f_q) into Qp and Q(f_q, f_p) into Qq in one launch (the pairs pq
- * and qp of scattering.py:317-330's sum over q).  hqp must be the reverse
- * pair of hpq (masses swapped, same grid and quadrature), on an antipodally
- * symmetric design: the reverse pair's product field at direction -y is
- * the pair's at y, so both gain spectra come from one set of transforms.
- * accumulate_p / accumulate_q add to Qp / Qq.  DGFS_ERR_UNSUPPORTED when the
- * design holds a direction without its antipode. */
-DGFS_API int dgfs_vss_apply_pair(dgfs_vss* hpq, dgfs_vss* hqp, const void* fp,
-                                 const void* fq, void* Qp, void* Qq, int nupts,
-                                 int neles, long long ldim, int soasz, int elem,
-                                 int upt, int accumulate_p, int accumulate_q,
-                                 void* stream);
-
 /* Synchronise `stream`, then report and clear the kernel's bounded-wait
  * error flag (DGFS_ERR_CUDA when a wait gave up). */
 DGFS_API int dgfs_vss_status(dgfs_vss* h, void* stream, int* flag);

@@ -139,45 +139,3 @@ def test_vss_single_point_leaves_the_rest():
         o = outs[s].get()
         assert rel_err(o[0, :, 1], Qo[s]) < TOL['double']
         assert not np.any(o[0, :, 0]) and not np.any(o[0, :, 2])
-
-
-@pytest.mark.parametrize('precision', ['double', 'single'])
-def test_fused_reverse_pair_matches_separate_launches(precision):
-    """dgfs_vss_apply_pair (a pair and its reverse from one set of
-    transforms) against dgfs_vss_apply of each pair on its own, and its
-    argument checks: the second handle must be the reverse pair."""
-    from frfs_b200 import _lib
-    cfg = mixture_config(precision, Nv=16, Nrho=6)
-    be = B200Backend(cfg, device='cuda:0')
-    vm = DGFSBiVelocityMesh(be, cfg)
-    sm = DGFSBiVSSGLLScatteringModel(be, cfg, vm)
-    assert sm._fuse
-    mesh, _, _ = _oracle(vm, cfg)
-    nupts, neles = 2, 3
-    st = _states(mesh, nupts*neles, seed=7)
-    V = vm.vsize()
-    banks = []
-    for s in range(2):
-        a = np.array([st[i][s] for i in range(nupts*neles)])
-        banks.append(be.matrix((nupts, V, neles),
-                               a.reshape(nupts, neles, V).transpose(0, 2, 1)))
-    sep = [be.matrix((nupts, V, neles)) for _ in range(2)]
-    sm._apply('01', banks[0], banks[1], sep[0], -1, 0, 0)
-    sm._apply('10', banks[1], banks[0], sep[1], -1, 0, 0)
-    fused = [be.matrix((nupts, V, neles)) for _ in range(2)]
-    lib = _lib.load()
-    ldim = banks[0].traits[1]
-    args = (banks[0]._as_parameter_, banks[1]._as_parameter_,
-            fused[0]._as_parameter_, fused[1]._as_parameter_, nupts, neles,
-            ldim, be.soasz, -1, 0, 0, 0, be.stream)
-    _lib.check(lib.dgfs_vss_apply_pair(sm._h['01'], sm._h['10'], *args),
-               'dgfs_vss_apply_pair')
-    sm.status()
-    for s in range(2):
-        assert rel_err(fused[s].get(), sep[s].get()) < (
-            1e-12 if precision == 'double' else 1e-5)
-    # the same handle twice, or a like pair, is not the reverse pair
-    for h2 in ('01', '00'):
-        with pytest.raises(_lib.DgfsError):
-            _lib.check(lib.dgfs_vss_apply_pair(sm._h['01'], sm._h[h2], *args),
-                       'dgfs_vss_apply_pair')
