@@ -50,6 +50,7 @@ static int init_twiddles(int dev) {
 struct VhsVariant {
   int prec, N, C, db, minb, threads, push;
   size_t smem;
+  size_t scratch_cx;  // two-CTA kernel: complex scratch per cluster
   const void* fn;
   cudaError_t (*launch32)(const VhsArgs<float>&, int, cudaStream_t);
   cudaError_t (*launch64)(const VhsArgs<double>&, int, cudaStream_t);
@@ -160,11 +161,13 @@ template <int N, bool IL1> static VhsVariant make_cube() {
   return v;
 }
 
-template <int LPT> static cudaError_t launch_pair(const VhsArgs<float>& a, int nclusters, cudaStream_t s) {
+template <typename T, int N, int LPT>
+static cudaError_t launch_pair(const VhsArgs<T>& a, int nclusters, cudaStream_t s) {
+  using G = PairGeom<T, N, LPT>;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(nclusters * 2, 1, 1);
-  cfg.blockDim = dim3(PairGeom<LPT>::NT, 1, 1);
-  cfg.dynamicSmemBytes = PairGeom<LPT>::SMEM_CX * sizeof(cx<float>);
+  cfg.blockDim = dim3(G::NT, 1, 1);
+  cfg.dynamicSmemBytes = G::SMEM_CX * sizeof(cx<T>);
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -173,23 +176,26 @@ template <int LPT> static cudaError_t launch_pair(const VhsArgs<float>& a, int n
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, vhs_pair_kernel<LPT>, a);
+  return cudaLaunchKernelEx(&cfg, vhs_pair_kernel<T, N, LPT>, a);
 }
 
-// two-CTA kernel (FP32, N = 32; kind 3 in dgfs_vhs_variant_kind); LPT
-// lines per main thread and pass (db reports LPT - 1)
-template <int LPT> static VhsVariant make_pair() {
+// two-CTA kernel (FP32 N = 32, FP64 N = 24; kind 3 in dgfs_vhs_variant_kind);
+// LPT lines per main thread and pass (db reports LPT - 1)
+template <typename T, int N, int LPT> static VhsVariant make_pair() {
+  using G = PairGeom<T, N, LPT>;
   VhsVariant v{};
-  v.prec = 32;
-  v.N = 32;
+  v.prec = sizeof(T) == 8 ? 64 : 32;
+  v.N = N;
   v.C = 2;
   v.db = LPT - 1;
   v.push = 3;
   v.minb = 1;
-  v.threads = PairGeom<LPT>::NT;
-  v.smem = PairGeom<LPT>::SMEM_CX * sizeof(cx<float>);
-  v.fn = (const void*)vhs_pair_kernel<LPT>;
-  v.launch32 = launch_pair<LPT>;
+  v.threads = G::NT;
+  v.smem = G::SMEM_CX * sizeof(cx<T>);
+  v.scratch_cx = G::SCRATCH;
+  v.fn = (const void*)vhs_pair_kernel<T, N, LPT>;
+  if constexpr (sizeof(T) == 8) v.launch64 = launch_pair<T, N, LPT>;
+  else v.launch32 = launch_pair<T, N, LPT>;
   return v;
 }
 
@@ -202,12 +208,13 @@ static const std::vector<VhsVariant>& variants() {
   static const std::vector<VhsVariant> v = {
       make_push<double, 8, 1, 4>(),             make_push<double, 16, 4, 2>(),
       make_push<double, 16, 2, 1>(),            make_push<double, 24, 8, 1>(),
-      make_push<double, 24, 12, 1>(),           make_push<double, 32, 16, 1>(),
+      make_push<double, 24, 12, 1>(),           make_pair<double, 24, 2>(),
+      make_pair<double, 24, 1>(),               make_push<double, 32, 16, 1>(),
       make_push<float, 8, 1, 4>(),              make_push<float, 16, 2, 2>(),
       make_push<float, 16, 4, 4>(),             make_cube<24, false>(),
       make_push<float, 24, 8, 2>(),             make_push<float, 24, 4, 1>(),
-      make_push<float, 24, 12, 3>(),            make_pair<2>(),
-      make_pair<1>(),
+      make_push<float, 24, 12, 3>(),            make_pair<float, 32, 2>(),
+      make_pair<float, 32, 1>(),
       make_push<float, 32, 16, 2>(),
       make_push<float, 32, 8, 1>(),             make_cube<8, false>(),
       make_cube<16, false>(),                   make_cube<16, true>(),
@@ -305,7 +312,7 @@ static int select_index(dgfs_vhs* h, int idx) {
   const size_t esz = h->prec == 64 ? 16 : 8;
   // gain-spectrum scratch: one N^3 complex slice per cluster, or for the
   // two-CTA kernel the half spectra of F and fC and the staging buffers
-  const size_t need = v->push == 3 ? (size_t)ncl * PairGeom<1>::SCRATCH * esz
+  const size_t need = v->push == 3 ? (size_t)ncl * v->scratch_cx * esz
                                    : (size_t)ncl * v->C * (size_t)h->N * h->N * h->N / v->C * esz;
   if (need > h->fc_bytes) {
     cudaFree(h->fc);

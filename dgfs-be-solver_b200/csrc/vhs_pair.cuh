@@ -1,4 +1,7 @@
-// Two-CTA fast-spectral VHS kernel for FP32 and N = 32.
+// Two-CTA fast-spectral VHS kernel for grids that do not fit one SM's
+// shared memory: FP32 at N = 32 and FP64 at N = 24.  The sizes below are
+// those of N = 32 (MH = N/2 = 16); FP64 at N = 24 has MH = 12, K_0 =
+// {0..5, 12, 19..23} and 201.7 KB of shared memory.
 //
 // The same exact restatement of the reference's operator as the single-CTA
 // kernel (vhs_cube.cuh: one complex transform R = IFFT(m F) per (p, q), the
@@ -30,8 +33,8 @@
 // and the gain spectrum fC live in the pair's slice of the scratch too; S_p
 // accumulates in shared memory.
 //
-// Shared memory (complex float unless noted): W [16][32][33], S [32][16][32]
-// (float), the Nyquist planes T1..T3 [32][33], two phase slots.  352
+// Shared memory (complex unless noted): W [16][32][33], S [32][16][32]
+// (real), the Nyquist planes T1..T3 [32][33], two phase slots.  352
 // threads: 256 main threads (two of the 512 lines of every pass each, one
 // after the other: a 32-point register FFT needs ~130 registers) and 96 that
 // transform the Nyquist planes during the first two passes of every (p, q).
@@ -41,26 +44,30 @@
 
 namespace dgfs {
 
-// LPT: lines of a pass per main thread.  LPT = 2: 256 main threads (lines
-// t and t + 256, one after the other, 168 registers) and 96 threads for the
-// Nyquist planes; LPT = 1: 512 threads at 128 registers, the first 96 of
-// which also take the Nyquist lines.
-template <int LPT> struct PairGeom {
-  static constexpr int N = 32, H = 17, NY = 16, NN = 1024, V = 32768;
-  static constexpr int LP = 33;              // padded line stride
-  static constexpr int NL = 512;             // lines of a pass
+// T, N: precision and grid (FP32 N = 32, FP64 N = 24; N a multiple of 4,
+// MH = N/2 values of k1 or x2 per CTA).  LPT: lines of a pass per main
+// thread.  LPT = 2: MH N / 2 main threads (lines t and t + MH N / 2, one
+// after the other) and the Nyquist lines on threads of their own; LPT = 1:
+// MH N threads, the first 3 N of which also take the Nyquist lines.
+template <typename T, int N_, int LPT> struct PairGeom {
+  static constexpr int N = N_, H = N / 2 + 1, NY = N / 2, NN = N * N, V = N * N * N;
+  static constexpr int MH = N / 2;           // k1 (x2) values per CTA
+  static constexpr int LP = N + 1;           // padded line stride
+  static constexpr int NL = MH * N;          // lines of a pass
   static constexpr int NM = NL / LPT;        // main threads
-  static constexpr int HS = 16 / LPT;        // step of a thread's line index hi
-  static constexpr int NQ = LPT == 2 ? 96 : 0;  // threads for the Nyquist planes only
-  static constexpr int NT = NM + NQ;
+  static constexpr int NMP = (NM + 31) / 32 * 32;  // main threads padded to whole warps
+  static constexpr int HS = MH / LPT;        // step of a thread's line index hi
+  static constexpr int NQ = LPT == 2 ? (3 * N + 31) / 32 * 32 : 0;  // threads for the Nyquist planes only
+  static constexpr int NT = NMP + NQ;
   static constexpr int PHS = 3 * N + 4;
-  static constexpr int OFF_W = 0;                        // [16][32][LP] cx
-  static constexpr int OFF_S = OFF_W + 16 * N * LP;      // [32][16][32] float = 8192 cx
-  static constexpr int OFF_T = OFF_S + 8192;             // [3][32][LP] cx
+  static constexpr int OFF_W = 0;                        // [MH][N][LP] cx
+  static constexpr int OFF_S = OFF_W + MH * N * LP;      // [N][MH][N] reals
+  static constexpr int OFF_T = OFF_S + N * MH * N / 2;   // [3][N][LP] cx
   static constexpr int OFF_PH = OFF_T + 3 * N * LP;      // [2][PHS] cx
   static constexpr int SMEM_CX = OFF_PH + 2 * PHS;
   static constexpr int SLICE = H * NN;                   // cx per spectrum in the scratch
-  static constexpr int XSLAB = 16 * 16 * N;              // cx per staging buffer [k1l][j][x3]
+  static constexpr int XSLAB = MH * MH * N;              // cx per staging buffer [k1l][j][x3]
+  static_assert(N % 4 == 0 && NM % N == 0, "line mapping");
   // F on the Nyquist planes k2 = N/2 ([k3 <= N/2][k1]) and k3 = N/2
   // ([k2][k1]), lanes (k1) fastest: a copy per CTA
   static constexpr int NQ2 = H * N, NQS = H * N + N * N;
@@ -69,13 +76,20 @@ template <int LPT> struct PairGeom {
   static constexpr int SCRATCH = 2 * SLICE + 4 * XSLAB + 2 * NQS;
 };
 
-// k1 ownership: K_0 = {0..7, 16, 25..31}, K_1 = {8..15, 17..24}
-__device__ __forceinline__ int pair_owner(int k1) { return (k1 <= 7 || k1 == 16 || k1 >= 25) ? 0 : 1; }
-__device__ __forceinline__ int pair_kinv(int k1) {
-  return k1 <= 7 ? k1 : k1 == 16 ? 8 : k1 >= 25 ? k1 - 16 : k1 <= 15 ? k1 - 8 : k1 - 9;
+// k1 ownership, closed under k1 -> -k1 mod N (Q = N/4, MH = N/2):
+// K_0 = {0..Q-1, MH, N-Q+1..N-1}, K_1 = {Q..MH-1, MH+1..N-Q}; for N = 32
+// K_0 = {0..7, 16, 25..31}, K_1 = {8..15, 17..24}
+template <int N> __device__ __forceinline__ int pair_owner(int k1) {
+  constexpr int Q = N / 4, MH = N / 2;
+  return (k1 < Q || k1 == MH || k1 > N - Q) ? 0 : 1;
 }
-__device__ __forceinline__ int pair_kmap(int r, int l) {
-  return r == 0 ? (l <= 7 ? l : l == 8 ? 16 : l + 16) : (l <= 7 ? l + 8 : l + 9);
+template <int N> __device__ __forceinline__ int pair_kinv(int k1) {
+  constexpr int Q = N / 4, MH = N / 2;
+  return k1 < Q ? k1 : k1 == MH ? Q : k1 > N - Q ? k1 - N + MH : k1 < MH ? k1 - Q : k1 - Q - 1;
+}
+template <int N> __device__ __forceinline__ int pair_kmap(int r, int l) {
+  constexpr int Q = N / 4, MH = N / 2;
+  return r == 0 ? (l < Q ? l : l == Q ? MH : l + N - MH) : (l < Q ? l + Q : l + Q + 1);
 }
 
 __device__ __forceinline__ void cl_sync() {
@@ -84,27 +98,29 @@ __device__ __forceinline__ void cl_sync() {
 }
 
 // third-pass line (x2l = hi, x3 = lo) along k1: the k1 of this CTA from its
-// work cube (row kinv(k1) * 32 + x2, x2 = 16 r + hi), the others from the
+// work cube (row kinv(k1) N + x2, x2 = MH r + hi), the others from the
 // peer's staging buffer ([kinv(k1)][hi][lo], written before the barrier)
-__device__ __forceinline__ void pair_load3(float2 (&x)[32], const float2* sW, const float2* xpeer, int r, int hi,
+template <typename T, int N>
+__device__ __forceinline__ void pair_load3(cx<T> (&x)[N], const cx<T>* sW, const cx<T>* xpeer, int r, int hi,
                                            int lo) {
-  constexpr int N = 32, LP = 33;
+  constexpr int LP = N + 1, MH = N / 2;
 #pragma unroll
   for (int k1 = 0; k1 < N; ++k1)
-    x[k1] = pair_owner(k1) == r ? sW[(pair_kinv(k1) * N + 16 * r + hi) * LP + lo]
-                                : __ldcg(xpeer + (pair_kinv(k1) * 16 + hi) * N + lo);
+    x[k1] = pair_owner<N>(k1) == r ? sW[(pair_kinv<N>(k1) * N + MH * r + hi) * LP + lo]
+                                   : __ldcg(xpeer + (pair_kinv<N>(k1) * MH + hi) * N + lo);
 }
 
-template <int LPT>
-__global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const VhsArgs<float> a) {
-  using G = PairGeom<LPT>;
+template <typename T, int NV, int LPT>
+__global__ void __launch_bounds__(PairGeom<T, NV, LPT>::NT, 1) vhs_pair_kernel(const VhsArgs<T> a) {
+  using G = PairGeom<T, NV, LPT>;
   constexpr int HS = G::HS;
-  using C = cx<float>;
+  using C = cx<T>;
   constexpr int N = G::N, H = G::H, NY = G::NY, NN = G::NN, V = G::V, LP = G::LP, NM = G::NM, PHS = G::PHS;
+  constexpr int MH = G::MH;
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* const sW = reinterpret_cast<C*>(smem_raw) + G::OFF_W;
-  float* const sS = reinterpret_cast<float*>(reinterpret_cast<C*>(smem_raw) + G::OFF_S);
+  T* const sS = reinterpret_cast<T*>(reinterpret_cast<C*>(smem_raw) + G::OFF_S);
   C* const sT1 = reinterpret_cast<C*>(smem_raw) + G::OFF_T;
   C* const sT2 = sT1 + N * LP;
   C* const sT3 = sT2 + N * LP;
@@ -116,9 +132,9 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
   const int r = (int)cluster.block_rank();
   const int tid = threadIdx.x;
   const bool is_main = tid < NM;
-  // the Nyquist lines: own threads (LPT = 2) or the first 96 main threads
-  const bool has_nyq = G::NQ > 0 ? !is_main : tid < 3 * N;
-  const int tq = G::NQ > 0 ? tid - NM : tid;
+  // the Nyquist lines: own threads (LPT = 2) or the first 3 N main threads
+  const int tq = G::NQ > 0 ? tid - G::NMP : tid;
+  const bool has_nyq = tq >= 0 && tq < 3 * N;
   const int cid = blockIdx.x / 2, ncl = gridDim.x / 2;
   // the pair's scratch: F [H][N][N] then fC [H][N][N] (fC doubles as the
   // exchange buffer of the forward transform of f)
@@ -126,11 +142,11 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
   C* const fC = Fg + G::SLICE;
   C* const Xs = fC + G::SLICE;  // staging: [rank][buffer][k1l][j][x3]
   C* const Nq = Xs + 4 * G::XSLAB + r * G::NQS;  // this CTA's Nyquist-plane copy
-  const float invV = 1.f / (float)V;
+  const T invV = T(1) / T(V);
   const int npq = a.P * a.M;
   // a main thread's lines in every pass: L = tid + NM h (h < LPT), with
-  // hi = L >> 5 (k1l, or x2l in the third pass) and lo = L & 31 (k2, x3)
-  const int lo = tid & 31, hi0 = tid >> 5;  // hi of line h: hi0 + HS h
+  // hi = L / N (k1l, or x2l in the third pass) and lo = L % N (k2, x3)
+  const int lo = tid % N, hi0 = tid / N;  // hi of line h: hi0 + HS h
   const uint32_t peer = (uint32_t)(r ^ 1);
   int xb = 0;  // staging buffer of the next exchange
   auto xmine = [&](int b) { return Xs + (size_t)(r * 2 + b) * G::XSLAB; };
@@ -157,11 +173,11 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
         C x[N];
 #pragma unroll
         for (int j = 0; j < N; ++j) x[j] = sW[(hi * N + j) * LP + lo];
-        fft<float, N, +1>(x);
+        fft<T, N, +1>(x);
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          sW[(hi * N + 16 * r + j) * LP + lo] = r ? x[16 + j] : x[j];
-          __stcg(xs + (hi * 16 + j) * N + lo, r ? x[j] : x[16 + j]);
+        for (int j = 0; j < MH; ++j) {
+          sW[(hi * N + MH * r + j) * LP + lo] = r ? x[MH + j] : x[j];
+          __stcg(xs + (hi * MH + j) * N + lo, r ? x[j] : x[MH + j]);
         }
       }
     }
@@ -185,36 +201,36 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
     if (is_main) {
 #pragma unroll 1
       for (int h = 0; h < LPT; ++h) {
-        const int hi = hi0 + HS * h, x1 = 16 * r + hi;
+        const int hi = hi0 + HS * h, x1 = MH * r + hi;
         const int64_t b0 = soa_ix(upt, a.ldim, elem, (int64_t)(x1 * N + lo) * N, V, a.soasz);
         C x[N];
 #pragma unroll
-        for (int k = 0; k < N; ++k) x[k] = mk<C>(a.f[b0 + (int64_t)k * a.soasz], 0.f);
-        fft<float, N, -1>(x);
+        for (int k = 0; k < N; ++k) x[k] = mk<C>(a.f[b0 + (int64_t)k * a.soasz], T(0));
+        fft<T, N, -1>(x);
 #pragma unroll
         for (int k = 0; k <= NY; ++k) sW[(hi * N + lo) * LP + k] = x[k];
       }
     }
     __syncthreads();
 #pragma unroll 1
-    for (int t = tid; t < 16 * H; t += G::NT) {
+    for (int t = tid; t < MH * H; t += G::NT) {
       const int x1l = t / H, k3 = t % H;
       C x[N];
 #pragma unroll
       for (int j = 0; j < N; ++j) x[j] = sW[(x1l * N + j) * LP + k3];
-      fft<float, N, -1>(x);
+      fft<T, N, -1>(x);
       // exchange buffer [k3][x1][k2] (the fC slice, free until p = 0 ends)
 #pragma unroll
-      for (int j = 0; j < N; ++j) fC[(k3 * N + 16 * r + x1l) * N + j] = x[j];
+      for (int j = 0; j < N; ++j) fC[(k3 * N + MH * r + x1l) * N + j] = x[j];
     }
     cl_sync();  // the exchange buffer is complete (cluster-scope release/acquire)
 #pragma unroll 1
-    for (int t = tid; t < 16 * H; t += G::NT) {
-      const int k2 = 16 * r + t / H, k3 = t % H;
+    for (int t = tid; t < MH * H; t += G::NT) {
+      const int k2 = MH * r + t / H, k3 = t % H;
       C x[N];
 #pragma unroll
       for (int i = 0; i < N; ++i) x[i] = __ldcg(fC + (k3 * N + i) * N + k2);
-      fft<float, N, -1>(x);
+      fft<T, N, -1>(x);
 #pragma unroll
       for (int i = 0; i < N; ++i) Fg[(k3 * N + i) * N + k2] = cscale(x[i], invV);
     }
@@ -250,20 +266,20 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
         const int pq = p * a.M + q;
         const C* ph = sPh + slot * PHS;
         const C th1 = ph[3 * N], th2 = ph[3 * N + 1], th3 = ph[3 * N + 2];
-        const C phn = (tid < 3 * N && pq + 1 < npq) ? a.phase[(size_t)(pq + 1) * 3 * N + tid] : mk<C>(0.f, 0.f);
+        const C phn = (tid < 3 * N && pq + 1 < npq) ? a.phase[(size_t)(pq + 1) * 3 * N + tid] : mk<C>(T(0), T(0));
         // pass 1: lines (k1, k2 = lo) along k3 | Nyquist first axes
         if (is_main) {
 #pragma unroll 1
           for (int h = 0; h < LPT; ++h) {
-            const int hi = hi0 + HS * h, k1 = pair_kmap(r, hi), k2 = lo;
+            const int hi = hi0 + HS * h, k1 = pair_kmap<N>(r, hi), k2 = lo;
             const C E12 = cmul(ph[k1], ph[N + k2]);
-            C t12 = mk<C>(1.f, 0.f);
+            C t12 = mk<C>(T(1), T(0));
             if (k1 == NY) t12 = th1;
             if (k2 == NY) t12 = cmul(t12, th2);
             const C E12t = cmul(E12, t12);
             const C s0 = cadd(E12, E12t), s3 = cadd(E12, cmul(E12t, th3));
-            const C A = mk<C>(0.5f * (s0.x + s0.y), 0.5f * (s0.y - s0.x));
-            const C A3 = mk<C>(0.5f * (s3.x + s3.y), 0.5f * (s3.y - s3.x));
+            const C A = mk<C>(T(0.5) * (s0.x + s0.y), T(0.5) * (s0.y - s0.x));
+            const C A3 = mk<C>(T(0.5) * (s3.x + s3.y), T(0.5) * (s3.y - s3.x));
             C x[N];
 #pragma unroll
             for (int k = 0; k < N; ++k) {
@@ -271,7 +287,7 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
               const C& Ak = k == NY ? A3 : A;
               x[k] = cscale(Fat(k1, k2, k), Ak.x * e3.x - Ak.y * e3.y);
             }
-            fft<float, N, +1>(x);
+            fft<T, N, +1>(x);
 #pragma unroll
             for (int k = 0; k < N; ++k) sW[(hi * N + k2) * LP + k] = x[k];
           }
@@ -293,12 +309,12 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
             Eb = cmul(ph[j], ph[2 * N + NY]);
             tb = th3;
           }
-          C B = cmul(Eb, mk<C>(1.f - tb.x, -tb.y));
+          C B = cmul(Eb, mk<C>(T(1) - tb.x, -tb.y));
           const C tb3 = cmul(tb, th3);
-          C B3 = p3 ? mk<C>(0.f, 0.f) : cmul(Eb, mk<C>(1.f - tb3.x, -tb3.y));
-          if (which != 0 && j == NY) B = B3 = mk<C>(0.f, 0.f);
-          const C A = mk<C>(0.5f * (B.x + B.y), 0.5f * (B.y - B.x));
-          const C A3 = mk<C>(0.5f * (B3.x + B3.y), 0.5f * (B3.y - B3.x));
+          C B3 = p3 ? mk<C>(T(0), T(0)) : cmul(Eb, mk<C>(T(1) - tb3.x, -tb3.y));
+          if (which != 0 && j == NY) B = B3 = mk<C>(T(0), T(0));
+          const C A = mk<C>(T(0.5) * (B.x + B.y), T(0.5) * (B.y - B.x));
+          const C A3 = mk<C>(T(0.5) * (B3.x + B3.y), T(0.5) * (B3.y - B3.x));
           const C* ev = ph + (p3 ? N : 2 * N);
           // the line's F values, one load each: plane 1 from the half
           // spectrum (rows k3, stride N^2), planes 2 and 3 from the copies
@@ -320,10 +336,10 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
             const C e = ev[k];
             x[k] = cscale(v, Ak.x * e.x - Ak.y * e.y);
           }
-          fft<float, N, +1>(x);
-          C* T = which == 0 ? sT1 : (which == 1 ? sT2 : sT3);
+          fft<T, N, +1>(x);
+          C* Tp = which == 0 ? sT1 : (which == 1 ? sT2 : sT3);
 #pragma unroll
-          for (int k = 0; k < N; ++k) T[j * LP + k] = x[k];
+          for (int k = 0; k < N; ++k) Tp[j * LP + k] = x[k];
         }
         __syncthreads();
         if (tid < 3 * N && pq + 1 < npq) {
@@ -335,34 +351,34 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
         // every plane; the third pass reads the rows of its own x2 half)
         const int xr = pass2_exchange([&]() {
           const int which = tq / N, col = tq % N;
-          C* T = which == 0 ? sT1 : (which == 1 ? sT2 : sT3);
+          C* Tp = which == 0 ? sT1 : (which == 1 ? sT2 : sT3);
           C x[N];
 #pragma unroll
-          for (int j = 0; j < N; ++j) x[j] = T[j * LP + col];
-          fft<float, N, +1>(x);
+          for (int j = 0; j < N; ++j) x[j] = Tp[j * LP + col];
+          fft<T, N, +1>(x);
 #pragma unroll
-          for (int j = 0; j < N; ++j) T[j * LP + col] = x[j];
+          for (int j = 0; j < N; ++j) Tp[j * LP + col] = x[j];
         });
         // pass 3: lines (x2 = 16 r + hi, x3 = lo) along k1;
         // S += Re R^2 + Re Nq^2
         if (is_main) {
 #pragma unroll 1
           for (int h = 0; h < LPT; ++h) {
-            const int hi = hi0 + HS * h, x2 = 16 * r + hi, x3 = lo;
+            const int hi = hi0 + HS * h, x2 = MH * r + hi, x3 = lo;
             C x[N];
-            pair_load3(x, sW, xpeer(xr), r, hi, lo);
-            fft<float, N, +1>(x);
+            pair_load3<T, N>(x, sW, xpeer(xr), r, hi, lo);
+            fft<T, N, +1>(x);
             const C t1 = sT1[x2 * LP + x3];
-            const float s2 = (x2 & 1) ? -1.f : 1.f, s3 = (x3 & 1) ? -1.f : 1.f;
-            float* Sl = sS + hi * N + x3;
+            const T s2 = (x2 & 1) ? T(-1) : T(1), s3 = (x3 & 1) ? T(-1) : T(1);
+            T* Sl = sS + hi * N + x3;
 #pragma unroll
             for (int i = 0; i < N; ++i) {
-              const float s1 = (i & 1) ? -1.f : 1.f;
+              const T s1 = (i & 1) ? T(-1) : T(1);
               const C t2 = sT2[i * LP + x3], t3 = sT3[i * LP + x2];
-              const float nr = s1 * t1.x + s2 * t2.x + s3 * t3.x;
-              const float ni = s1 * t1.y + s2 * t2.y + s3 * t3.y;
-              const float v = x[i].x * x[i].x - x[i].y * x[i].y + nr * nr - ni * ni;
-              Sl[i * 16 * N] = q == 0 ? v : Sl[i * 16 * N] + v;
+              const T nr = s1 * t1.x + s2 * t2.x + s3 * t3.x;
+              const T ni = s1 * t1.y + s2 * t2.y + s3 * t3.y;
+              const T v = x[i].x * x[i].x - x[i].y * x[i].y + nr * nr - ni * ni;
+              Sl[i * MH * N] = q == 0 ? v : Sl[i * MH * N] + v;
             }
           }
         }
@@ -379,16 +395,16 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
         C* const xs = xmine(xb);
 #pragma unroll 1
         for (int h = 0; h < LPT; ++h) {
-          const int hi = hi0 + HS * h, x2 = 16 * r + hi;
+          const int hi = hi0 + HS * h, x2 = MH * r + hi;
           C x[N];
-          const float* Sl = sS + hi * N + lo;
+          const T* Sl = sS + hi * N + lo;
 #pragma unroll
-          for (int i = 0; i < N; ++i) x[i] = mk<C>(Sl[i * 16 * N], 0.f);
-          fft<float, N, -1>(x);
+          for (int i = 0; i < N; ++i) x[i] = mk<C>(Sl[i * MH * N], T(0));
+          fft<T, N, -1>(x);
 #pragma unroll
           for (int k1 = 0; k1 < N; ++k1) {
-            if (pair_owner(k1) == r) sW[(pair_kinv(k1) * N + x2) * LP + lo] = x[k1];
-            else __stcg(xs + (pair_kinv(k1) * 16 + hi) * N + lo, x[k1]);
+            if (pair_owner<N>(k1) == r) sW[(pair_kinv<N>(k1) * N + x2) * LP + lo] = x[k1];
+            else __stcg(xs + (pair_kinv<N>(k1) * MH + hi) * N + lo, x[k1]);
           }
         }
       }
@@ -403,22 +419,22 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
           C x[N];
 #pragma unroll
           for (int j = 0; j < N; ++j)
-            x[j] = (j >> 4) == r ? sW[(hi * N + j) * LP + lo] : __ldcg(xp + (hi * 16 + (j & 15)) * N + lo);
-          fft<float, N, -1>(x);
+            x[j] = j / MH == r ? sW[(hi * N + j) * LP + lo] : __ldcg(xp + (hi * MH + j % MH) * N + lo);
+          fft<T, N, -1>(x);
 #pragma unroll
           for (int j = 0; j < N; ++j) sW[(hi * N + j) * LP + lo] = x[j];
         }
       }
       __syncthreads();
       if (is_main) {
-        const float* w1 = a.w1t + (size_t)p * V;
+        const T* w1 = a.w1t + (size_t)p * V;
 #pragma unroll 1
         for (int h = 0; h < LPT; ++h) {
-          const int hi = hi0 + HS * h, k1 = pair_kmap(r, hi), k2 = lo, L = k1 * N + k2;
+          const int hi = hi0 + HS * h, k1 = pair_kmap<N>(r, hi), k2 = lo, L = k1 * N + k2;
           C x[N];
 #pragma unroll
           for (int k = 0; k < N; ++k) x[k] = sW[(hi * N + k2) * LP + k];
-          fft<float, N, -1>(x);
+          fft<T, N, -1>(x);
 #pragma unroll
           for (int k = 0; k <= NY; ++k) x[k] = cscale(x[k], __ldg(w1 + k * NN + L));
           if (p > 0) {
@@ -449,7 +465,7 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
       if (is_main) {
 #pragma unroll 1
         for (int h = 0; h < LPT; ++h) {
-          const int hi = hi0 + HS * h, k1 = pair_kmap(r, hi), k2 = lo, L = k1 * N + k2;
+          const int hi = hi0 + HS * h, k1 = pair_kmap<N>(r, hi), k2 = lo, L = k1 * N + k2;
           const int m1 = (N - k1) % N, m2 = (N - k2) % N;
           C x[N];
 #pragma unroll
@@ -463,7 +479,7 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
               x[k] = mk<C>(c.x, -c.y);
             }
           }
-          fft<float, N, +1>(x);
+          fft<T, N, +1>(x);
 #pragma unroll
           for (int k = 0; k < N; ++k) sW[(hi * N + k2) * LP + k] = x[k];
         }
@@ -475,24 +491,24 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
         for (int h = 0; h < LPT; ++h) {
           const int hi = hi0 + HS * h;
           C x[N];
-          pair_load3(x, sW, xpeer(xr), r, hi, lo);
-          fft<float, N, +1>(x);
-          float* Sl = sS + hi * N + lo;
+          pair_load3<T, N>(x, sW, xpeer(xr), r, hi, lo);
+          fft<T, N, +1>(x);
+          T* Sl = sS + hi * N + lo;
           if (t == 0) {
 #pragma unroll
-            for (int i = 0; i < N; ++i) Sl[i * 16 * N] = x[i].x;
+            for (int i = 0; i < N; ++i) Sl[i * MH * N] = x[i].x;
           } else {
-            // x2 = 16 r + hi, x3 = lo: bank entries v = i N^2 + x2 N + x3
-            const int64_t b0 = soa_ix(upt, a.ldim, elem, (int64_t)(16 * r + hi) * N + lo, V, a.soasz);
+            // x2 = MH r + hi, x3 = lo: bank entries v = i N^2 + x2 N + x3
+            const int64_t b0 = soa_ix(upt, a.ldim, elem, (int64_t)(MH * r + hi) * N + lo, V, a.soasz);
             const int64_t st = (int64_t)NN * a.soasz;
 #pragma unroll
             for (int i0 = 0; i0 < N; i0 += 8) {
-              float fl[8];
+              T fl[8];
 #pragma unroll
               for (int i = 0; i < 8; ++i) fl[i] = a.f[b0 + (i0 + i) * st];
 #pragma unroll
               for (int i = 0; i < 8; ++i)
-                Sl[(i0 + i) * 16 * N] = a.prefac * (x[i0 + i].x - fl[i] * Sl[(i0 + i) * 16 * N]);
+                Sl[(i0 + i) * MH * N] = a.prefac * (x[i0 + i].x - fl[i] * Sl[(i0 + i) * MH * N]);
             }
           }
         }
@@ -509,11 +525,11 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
 #pragma unroll 1
         for (int h = 0; h < LPT; ++h) {
           const int hi = hi0 + HS * h;
-          const float* Sl = sS + hi * N + lo;
+          const T* Sl = sS + hi * N + lo;
 #pragma unroll 4
           for (int i = 0; i < N; ++i) {
-            const int64_t v = (int64_t)(i * N + 16 * r + hi) * N + lo;
-            const double d = (double)Sl[i * 16 * N];
+            const int64_t v = (int64_t)(i * N + MH * r + hi) * N + lo;
+            const double d = (double)Sl[i * MH * N];
             const double c0 = a.cvec[v], c1 = a.cvec[V + v], c2 = a.cvec[2 * V + v];
             mom[0] += d;
             mom[1] += d * c0;
@@ -551,16 +567,16 @@ __global__ void __launch_bounds__(PairGeom<LPT>::NT, 1) vhs_pair_kernel(const Vh
 #pragma unroll 1
       for (int h = 0; h < LPT; ++h) {
         const int hi = hi0 + HS * h;
-        const float* Sl = sS + hi * N + lo;
-        const int64_t b0 = soa_ix(upt, a.ldim, elem, (int64_t)(16 * r + hi) * N + lo, V, a.soasz);
+        const T* Sl = sS + hi * N + lo;
+        const int64_t b0 = soa_ix(upt, a.ldim, elem, (int64_t)(MH * r + hi) * N + lo, V, a.soasz);
         const int64_t st = (int64_t)NN * a.soasz;
 #pragma unroll 4
         for (int i = 0; i < N; ++i) {
-          float qq = Sl[i * 16 * N];
+          T qq = Sl[i * MH * N];
           if (a.project) {
-            const int64_t v = (int64_t)(i * N + 16 * r + hi) * N + lo;
+            const int64_t v = (int64_t)(i * N + MH * r + hi) * N + lo;
             const double c0 = a.cvec[v], c1 = a.cvec[V + v], c2 = a.cvec[2 * V + v];
-            qq = (float)((double)qq - (lam[0] + lam[1] * c0 + lam[2] * c1 + lam[3] * c2 +
+            qq = (T)((double)qq - (lam[0] + lam[1] * c0 + lam[2] * c1 + lam[3] * c2 +
                                        lam[4] * (c0 * c0 + c1 * c1 + c2 * c2)));
           }
           a.Q[b0 + i * st] = qq;

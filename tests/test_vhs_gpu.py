@@ -257,17 +257,22 @@ def test_bounded_wait_that_runs_out_is_reported():
 
 
 @pytest.mark.parametrize('project', [0, 1])
-@pytest.mark.parametrize('variant', [0, 1])
-def test_pair_kernel_bank(project, variant):
-    """The two-CTA kernel (FP32, N = 32, the default there; both thread
-    layouts) on a bank of 10 points over two AoSoA rows, with and without
-    the FP64 projection, against the oracle point by point; a second launch
-    on the same banks gives the same values (the per-pair scratch is
-    rewritten per point)."""
-    cfg = config('channel-n32', 'single', Nrho=4, M=6)
+@pytest.mark.parametrize('layout', [0, 1])
+@pytest.mark.parametrize('name,precision', [('channel-n32', 'single'),
+                                            ('couette-n24', 'double')])
+def test_pair_kernel_bank(name, precision, project, layout):
+    """The two-CTA kernel (FP32 at N = 32, the default there, and FP64 at
+    N = 24; both thread layouts) on a bank of 10 points over two AoSoA
+    rows, with and without the FP64 projection, against the oracle point by
+    point; a second launch on the same banks gives the same values (the
+    per-pair scratch is rewritten per point)."""
+    cfg = config(name, precision, M=6,
+                 **({'Nrho': 4} if name == 'channel-n32' else {}))
     cfg.set('backend-b200', 'vhs-project', project)
     be, vm, sm = _model(cfg)
-    assert sm.variants()[variant]['exchange'] == 'pair'
+    pairs = [i for i, v in enumerate(sm.variants()) if v['exchange'] == 'pair']
+    assert len(pairs) == 2
+    variant = pairs[layout]
     sm.select(variant)
     ovm, pre, prefac = oracle_for(cfg)
     nupts, neles = 2, 5
@@ -287,4 +292,5 @@ def test_pair_kernel_bank(project, variant):
             Qo = ovhs.vhs_Q(fu[u, :, e], ovm, pre, prefac)
             if project:
                 Qo = ovhs.project_conservative(Qo, cv)
-            assert rel_err(Qg[u, :, e], Qo) < FP32_TOL, (u, e)
+            tol = FP64_TOL if precision == 'double' else FP32_TOL
+            assert rel_err(Qg[u, :, e], Qo) < tol, (u, e)
