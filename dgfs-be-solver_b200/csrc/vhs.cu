@@ -202,14 +202,15 @@ template <typename T, int N, int LPT> static VhsVariant make_pair() {
 // Compiled launch shapes: (precision, N, cluster size, double-buffered
 // exchange, minimum CTAs per SM for the register budget).  The first entry
 // of each (precision, N) family is the default (FP32 N = 24: the single-CTA
-// kernel, 14 ms against 20 ms for the best cluster shape on 576 points);
-// the autotuner times the rest.
+// kernel, 5.2 ms against 20 ms for the best cluster shape on 576 points;
+// FP64 N = 24 and FP32 N = 32: the two-CTA kernel, 15 ms against 50 ms and
+// 552 ms against 1,695 ms); the autotuner times the rest.
 static const std::vector<VhsVariant>& variants() {
   static const std::vector<VhsVariant> v = {
       make_push<double, 8, 1, 4>(),             make_push<double, 16, 4, 2>(),
-      make_push<double, 16, 2, 1>(),            make_push<double, 24, 8, 1>(),
-      make_push<double, 24, 12, 1>(),           make_pair<double, 24, 2>(),
-      make_pair<double, 24, 1>(),               make_push<double, 32, 16, 1>(),
+      make_push<double, 16, 2, 1>(),            make_pair<double, 24, 1>(),
+      make_pair<double, 24, 2>(),               make_push<double, 24, 8, 1>(),
+      make_push<double, 24, 12, 1>(),           make_push<double, 32, 16, 1>(),
       make_push<float, 8, 1, 4>(),              make_push<float, 16, 2, 2>(),
       make_push<float, 16, 4, 4>(),             make_cube<24, false>(),
       make_push<float, 24, 8, 2>(),             make_push<float, 24, 4, 1>(),
