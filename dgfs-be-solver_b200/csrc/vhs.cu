@@ -161,7 +161,7 @@ template <int N, bool IL1> static VhsVariant make_cube() {
   return v;
 }
 
-template <typename T, int N, int LPT, int MINB>
+template <typename T, int N, int LPT>
 static cudaError_t launch_pair(const VhsArgs<T>& a, int nclusters, cudaStream_t s) {
   using G = PairGeom<T, N, LPT>;
   cudaLaunchConfig_t cfg = {};
@@ -176,13 +176,12 @@ static cudaError_t launch_pair(const VhsArgs<T>& a, int nclusters, cudaStream_t 
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, vhs_pair_kernel<T, N, LPT, MINB>, a);
+  return cudaLaunchKernelEx(&cfg, vhs_pair_kernel<T, N, LPT>, a);
 }
 
-// two-CTA kernel (FP32 N = 32, FP64 N = 24, and FP32 N = 24 with two CTAs
-// per SM; kind 3 in dgfs_vhs_variant_kind); LPT lines per main thread and
-// pass (db reports LPT - 1), MINB CTAs per SM of the register budget
-template <typename T, int N, int LPT, int MINB = 1> static VhsVariant make_pair() {
+// two-CTA kernel (FP32 N = 32, FP64 N = 24; kind 3 in dgfs_vhs_variant_kind);
+// LPT lines per main thread and pass (db reports LPT - 1)
+template <typename T, int N, int LPT> static VhsVariant make_pair() {
   using G = PairGeom<T, N, LPT>;
   VhsVariant v{};
   v.prec = sizeof(T) == 8 ? 64 : 32;
@@ -190,13 +189,13 @@ template <typename T, int N, int LPT, int MINB = 1> static VhsVariant make_pair(
   v.C = 2;
   v.db = LPT - 1;
   v.push = 3;
-  v.minb = MINB;
+  v.minb = 1;
   v.threads = G::NT;
   v.smem = G::SMEM_CX * sizeof(cx<T>);
   v.scratch_cx = G::SCRATCH;
-  v.fn = (const void*)vhs_pair_kernel<T, N, LPT, MINB>;
-  if constexpr (sizeof(T) == 8) v.launch64 = launch_pair<T, N, LPT, MINB>;
-  else v.launch32 = launch_pair<T, N, LPT, MINB>;
+  v.fn = (const void*)vhs_pair_kernel<T, N, LPT>;
+  if constexpr (sizeof(T) == 8) v.launch64 = launch_pair<T, N, LPT>;
+  else v.launch32 = launch_pair<T, N, LPT>;
   return v;
 }
 
@@ -215,8 +214,7 @@ static const std::vector<VhsVariant>& variants() {
       make_push<float, 8, 1, 4>(),              make_push<float, 16, 2, 2>(),
       make_push<float, 16, 4, 4>(),             make_cube<24, false>(),
       make_push<float, 24, 8, 2>(),             make_push<float, 24, 4, 1>(),
-      make_push<float, 24, 12, 3>(),            make_pair<float, 24, 1, 2>(),
-      make_pair<float, 24, 2, 2>(),             make_pair<float, 32, 2>(),
+      make_push<float, 24, 12, 3>(),            make_pair<float, 32, 2>(),
       make_pair<float, 32, 1>(),
       make_push<float, 32, 16, 2>(),
       make_push<float, 32, 8, 1>(),             make_cube<8, false>(),

@@ -110,8 +110,8 @@ __device__ __forceinline__ void pair_load3(cx<T> (&x)[N], const cx<T>* sW, const
                                    : __ldcg(xpeer + (pair_kinv<N>(k1) * MH + hi) * N + lo);
 }
 
-template <typename T, int NV, int LPT, int MINB = 1>
-__global__ void __launch_bounds__(PairGeom<T, NV, LPT>::NT, MINB) vhs_pair_kernel(const VhsArgs<T> a) {
+template <typename T, int NV, int LPT>
+__global__ void __launch_bounds__(PairGeom<T, NV, LPT>::NT, 1) vhs_pair_kernel(const VhsArgs<T> a) {
   using G = PairGeom<T, NV, LPT>;
   constexpr int HS = G::HS;
   using C = cx<T>;
