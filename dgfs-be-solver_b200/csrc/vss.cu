@@ -11,6 +11,7 @@
 #include "../../include/dgfs_b200.h"
 #include "dgfs_internal.h"
 #include "vss_push.cuh"
+#include "vss_pair.cuh"
 
 using namespace dgfs;
 
@@ -46,7 +47,9 @@ int init_twiddles_current() {
 
 struct VssShape {
   int prec, N, C, threads;
+  int pair;           // 1: the two-CTA kernel (vss_pair.cuh)
   size_t smem;
+  size_t scratch_cx;  // complex scratch per cluster
   const void* fn;
   cudaError_t (*launch32)(const VssArgs<float>&, int, cudaStream_t);
   cudaError_t (*launch64)(const VssArgs<double>&, int, cudaStream_t);
@@ -77,21 +80,56 @@ template <typename T, int N, int C, int MINB> VssShape make_vss() {
   v.C = C;
   v.threads = PushGeom<N, C>::NT;
   v.smem = VssGeom<N, C>::SMEM_CX * sizeof(cx<T>);
+  v.scratch_cx = (size_t)N * N * N;
   v.fn = (const void*)vss_push_kernel<T, N, C, MINB>;
   if constexpr (sizeof(T) == 8) v.launch64 = launch_vss<double, N, C, MINB>;
   else v.launch32 = launch_vss<float, N, C, MINB>;
   return v;
 }
 
-// One launch shape per (precision, N); FP64 N = 32 does not fit the shared
-// memory of a 16-CTA cluster's CTA.
-const VssShape* vss_shape(int prec, int N) {
+template <int N> cudaError_t launch_vss_pair(const VssArgs<float>& a, int nclusters, cudaStream_t s) {
+  using P = VssPairGeom<N>;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nclusters * 2, 1, 1);
+  cfg.blockDim = dim3(P::NT, 1, 1);
+  cfg.dynamicSmemBytes = P::SMEM_CX * sizeof(cx<float>);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, vss_pair_kernel<N>, a);
+}
+
+template <int N> VssShape make_vss_pair() {
+  using P = VssPairGeom<N>;
+  VssShape v{};
+  v.prec = 32;
+  v.N = N;
+  v.C = 2;
+  v.pair = 1;
+  v.threads = P::NT;
+  v.smem = P::SMEM_CX * sizeof(cx<float>);
+  v.scratch_cx = P::SCRATCH;
+  v.fn = (const void*)vss_pair_kernel<N>;
+  v.launch32 = launch_vss_pair<N>;
+  return v;
+}
+
+// Launch shapes per (precision, N): the cluster push kernel everywhere
+// (FP64 N = 32 does not fit the shared memory of a 16-CTA cluster's CTA),
+// and at FP32 N = 24 the two-CTA kernel, which is the default there.
+// pair < 0: the default shape; 0 / 1: the push / two-CTA kernel.
+const VssShape* vss_shape(int prec, int N, int pair = -1) {
   static const VssShape s[] = {
-      make_vss<float, 8, 1, 2>(),   make_vss<float, 16, 4, 2>(),  make_vss<float, 24, 8, 2>(),
-      make_vss<float, 32, 16, 1>(), make_vss<double, 8, 1, 2>(), make_vss<double, 16, 4, 1>(),
-      make_vss<double, 24, 8, 1>()};
+      make_vss_pair<24>(),          make_vss<float, 8, 1, 2>(),   make_vss<float, 16, 4, 2>(),
+      make_vss<float, 24, 8, 2>(),  make_vss<float, 32, 16, 1>(), make_vss<double, 8, 1, 2>(),
+      make_vss<double, 16, 4, 1>(), make_vss<double, 24, 8, 1>()};
   for (const auto& v : s)
-    if (v.prec == prec && v.N == N) return &v;
+    if (v.prec == prec && v.N == N && (pair < 0 || v.pair == pair)) return &v;
   return nullptr;
 }
 
@@ -109,7 +147,8 @@ struct dgfs_vss {
   void* phase_h;  // cx<T> [P][Mh][2][3][N] (Mh > 0)
   void* b_h;      // cx<T> [P][Mh][V]: b(y) + b(-y)
   void* c;      // cx<T> [V]
-  void* fc;     // scratch [clusters * C][V / C] cx<T>
+  void* fc;     // scratch: [clusters * C][V / C] cx<T> (push), per pair (two-CTA)
+  size_t fc_bytes;
   int* err;
 };
 
@@ -273,6 +312,53 @@ void free_vss(dgfs_vss* h) {
 
 }  // namespace
 
+namespace {
+
+// Kernel attributes, the clusters that fit the device and the scratch of a
+// launch shape (the scratch grows, never shrinks).
+int set_shape(dgfs_vss* h, const VssShape* shape) {
+  int maxsm = 0;
+  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
+  if ((int)shape->smem > maxsm)
+    return set_error(DGFS_ERR_UNSUPPORTED, "VSS kernel Nv=%d needs %zu B shared memory", h->N, shape->smem);
+  if (cudaFuncSetAttribute(shape->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shape->smem) !=
+          cudaSuccess ||
+      (shape->C > 8 &&
+       cudaFuncSetAttribute(shape->fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess))
+    return set_error(DGFS_ERR_CUDA, "VSS kernel attributes: %s", cudaGetErrorString(cudaGetLastError()));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(shape->C, 1, 1);
+  cfg.blockDim = dim3(shape->threads, 1, 1);
+  cfg.dynamicSmemBytes = shape->smem;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = shape->C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int ncl = 0;
+  if (cudaOccupancyMaxActiveClusters(&ncl, shape->fn, &cfg) != cudaSuccess || ncl < 1) {
+    cudaGetLastError();
+    return set_error(DGFS_ERR_UNSUPPORTED, "VSS cluster of %d CTAs cannot be scheduled", shape->C);
+  }
+  const size_t esz = h->prec == 64 ? 16 : 8;
+  const size_t need = (size_t)ncl * shape->scratch_cx * esz;
+  if (need > h->fc_bytes) {
+    cudaFree(h->fc);
+    h->fc = nullptr;
+    h->fc_bytes = 0;
+    if (cudaMalloc(&h->fc, need) != cudaSuccess)
+      return set_error(DGFS_ERR_NOMEM, "VSS scratch allocation of %zu B failed", need);
+    h->fc_bytes = need;
+  }
+  h->shape = shape;
+  h->max_clusters = ncl;
+  return DGFS_OK;
+}
+
+}  // namespace
+
 extern "C" int dgfs_vss_create(const dgfs_vss_params* p, dgfs_vss** out) {
   clear_error();
   if (!p || !out) return set_error(DGFS_ERR_INVALID, "null argument");
@@ -294,41 +380,10 @@ extern "C" int dgfs_vss_create(const dgfs_vss_params* p, dgfs_vss** out) {
   h->prec = p->precision;
   h->V = p->Nv * p->Nv * p->Nv;
   h->prefac = p->prefactor;
-  h->shape = shape;
   int rc = DGFS_OK;
   if (cudaGetDevice(&h->device) != cudaSuccess) rc = set_error(DGFS_ERR_CUDA, "no CUDA device");
   if (!rc) rc = init_twiddles_current();
-  if (!rc) {
-    int maxsm = 0;
-    cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
-    if ((int)shape->smem > maxsm)
-      rc = set_error(DGFS_ERR_UNSUPPORTED, "VSS kernel Nv=%d needs %zu B shared memory", h->N, shape->smem);
-  }
-  if (!rc && (cudaFuncSetAttribute(shape->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shape->smem) !=
-                  cudaSuccess ||
-              (shape->C > 8 &&
-               cudaFuncSetAttribute(shape->fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)))
-    rc = set_error(DGFS_ERR_CUDA, "VSS kernel attributes: %s", cudaGetErrorString(cudaGetLastError()));
-  if (!rc) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(shape->C, 1, 1);
-    cfg.blockDim = dim3(shape->threads, 1, 1);
-    cfg.dynamicSmemBytes = shape->smem;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = shape->C;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    if (cudaOccupancyMaxActiveClusters(&h->max_clusters, shape->fn, &cfg) != cudaSuccess || h->max_clusters < 1) {
-      cudaGetLastError();
-      rc = set_error(DGFS_ERR_UNSUPPORTED, "VSS cluster of %d CTAs cannot be scheduled", shape->C);
-    }
-  }
-  const size_t esz = h->prec == 64 ? 16 : 8;
-  if (!rc && cudaMalloc(&h->fc, (size_t)h->max_clusters * h->V * esz) != cudaSuccess)
-    rc = set_error(DGFS_ERR_NOMEM, "VSS gain-spectrum scratch allocation failed");
+  if (!rc) rc = set_shape(h, shape);
   if (!rc && (cudaMalloc((void**)&h->err, sizeof(int)) != cudaSuccess ||
               cudaMemset(h->err, 0, sizeof(int)) != cudaSuccess))
     rc = set_error(DGFS_ERR_NOMEM, "error flag allocation failed");
@@ -422,6 +477,16 @@ extern "C" int dgfs_vss_apply(dgfs_vss* h, const void* fp, const void* fq, void*
   }
   if (e != cudaSuccess) return set_error(DGFS_ERR_CUDA, "VSS launch failed: %s", cudaGetErrorString(e));
   return DGFS_OK;
+}
+
+extern "C" int dgfs_vss_select(dgfs_vss* h, int pair) {
+  clear_error();
+  if (!h) return set_error(DGFS_ERR_INVALID, "null handle");
+  const VssShape* shape = vss_shape(h->prec, h->N, pair ? 1 : 0);
+  if (!shape)
+    return set_error(DGFS_ERR_UNSUPPORTED, "no %s VSS kernel for Nv=%d precision=%d", pair ? "two-CTA" : "cluster",
+                     h->N, h->prec);
+  return set_shape(h, shape);
 }
 
 extern "C" int dgfs_vss_status(dgfs_vss* h, void* stream, int* flag) {

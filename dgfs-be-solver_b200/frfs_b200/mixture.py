@@ -51,6 +51,7 @@ _lib.declare('dgfs_vss_apply', c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                        c_int, ct.c_void_p])
 _lib.declare('dgfs_vss_status', c_int, [ct.c_void_p, ct.c_void_p,
                                         ct.POINTER(c_int)])
+_lib.declare('dgfs_vss_select', c_int, [ct.c_void_p, c_int])
 
 
 class DGFSBiVelocityMesh:
@@ -181,6 +182,13 @@ class DGFSBiVSSGLLScatteringModel:
             if h:
                 self._lib.dgfs_vss_destroy(h)
         self._h = {}
+
+    def select(self, pair):
+        """Launch shape of every pair: 1 the two-CTA kernel (FP32, N = 24,
+        the default there), 0 the cluster exchange kernel."""
+        for pq, h in self._h.items():
+            _lib.check(self._lib.dgfs_vss_select(h, int(pair)),
+                       'dgfs_vss_select')
 
     def prefactor(self, pq):
         return self._prefactor[pq]

@@ -240,6 +240,12 @@ DGFS_API int dgfs_vss_apply(dgfs_vss* h, const void* fp, const void* fq,
  * error flag (DGFS_ERR_CUDA when a wait gave up). */
 DGFS_API int dgfs_vss_status(dgfs_vss* h, void* stream, int* flag);
 
+/* No counterpart in the reference: the launch shape of a handle.  pair = 1
+ * selects the two-CTA kernel (FP32, Nv = 24; the default there), pair = 0
+ * the cluster exchange kernel.  DGFS_ERR_UNSUPPORTED when the shape does
+ * not exist for the handle's precision and Nv. */
+DGFS_API int dgfs_vss_select(dgfs_vss* h, int pair);
+
 /* ------------------------------------------------------------------------
  * FR-DG advection residual over all velocities
  *

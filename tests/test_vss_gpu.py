@@ -86,13 +86,18 @@ def _states(mesh, npts, seed):
     return out
 
 
-@pytest.mark.parametrize('precision,Nv', [('double', 16), ('single', 16),
-                                          ('single', 24), ('double', 8)])
-def test_vss_bank_matches_oracle(precision, Nv):
+@pytest.mark.parametrize('precision,Nv,pair', [
+    ('double', 16, 0), ('single', 16, 0), ('single', 24, 1), ('single', 24, 0),
+    ('double', 8, 0)])
+def test_vss_bank_matches_oracle(precision, Nv, pair):
+    """Q_p of both species on a bank of 6 points against the oracle; at
+    FP32 N = 24 with the two-CTA kernel (the default there) and with the
+    cluster exchange kernel."""
     cfg = mixture_config(precision, Nv=Nv, Nrho=6 if Nv > 8 else 4)
     be = B200Backend(cfg, device='cuda:0')
     vm = DGFSBiVelocityMesh(be, cfg)
     sm = DGFSBiVSSGLLScatteringModel(be, cfg, vm)
+    sm.select(pair)
     mesh, params, pre = _oracle(vm, cfg)
     for pq in ('00', '01', '10', '11'):
         assert sm.prefactor(pq) == pytest.approx(params[pq]['prefac'],
