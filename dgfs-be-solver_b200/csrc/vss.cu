@@ -338,9 +338,11 @@ int set_shape(dgfs_vss* h, const VssShape* shape) {
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   int ncl = 0;
-  if (cudaOccupancyMaxActiveClusters(&ncl, shape->fn, &cfg) != cudaSuccess || ncl < 1) {
+  const cudaError_t oe = cudaOccupancyMaxActiveClusters(&ncl, shape->fn, &cfg);
+  if (oe != cudaSuccess || ncl < 1) {
     cudaGetLastError();
-    return set_error(DGFS_ERR_UNSUPPORTED, "VSS cluster of %d CTAs cannot be scheduled", shape->C);
+    return set_error(DGFS_ERR_UNSUPPORTED, "VSS cluster of %d CTAs x %d threads, %zu B shared memory cannot be "
+                     "scheduled (%s, %d clusters)", shape->C, shape->threads, shape->smem, cudaGetErrorString(oe), ncl);
   }
   const size_t esz = h->prec == 64 ? 16 : 8;
   const size_t need = (size_t)ncl * shape->scratch_cx * esz;

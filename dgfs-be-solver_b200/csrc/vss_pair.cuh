@@ -67,7 +67,7 @@ __device__ __forceinline__ void vss_pair_pass2(cx<float>* sW, cx<float>* xs, int
 }
 
 template <int N>
-__global__ void __maxnreg__(112) vss_pair_kernel(const VssArgs<float> a) {
+__global__ void __launch_bounds__(VssPairGeom<N>::NT, 1) vss_pair_kernel(const VssArgs<float> a) {
   using G = VssPairGeom<N>;
   using C = cx<float>;
   constexpr int H = G::H, NY = G::NY, NN = G::NN, V = G::V, LP = G::LP, MH = G::MH, NL = G::NL;
