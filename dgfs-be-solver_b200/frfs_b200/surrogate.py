@@ -67,6 +67,10 @@ _lib.declare('dgfs_mlp_gemm', c_int,
              [c_int, c_int, c_int, c_void_p, c_ll, c_ll, c_void_p, c_int,
               c_ll, c_ll, c_void_p, c_void_p, c_void_p, c_ll, c_int, c_int,
               c_void_p, c_void_p])
+_lib.declare('dgfs_mlp_gemm_tc', c_int,
+             [c_int, c_int, c_int, c_void_p, c_ll, c_ll, c_void_p, c_int,
+              c_ll, c_ll, c_void_p, c_void_p, c_void_p, c_ll, c_int, c_int,
+              c_void_p, c_void_p])
 _lib.declare('dgfs_mlp_tanh_bwd', c_int, [c_ll, c_void_p, c_void_p,
                                           c_void_p, c_void_p])
 _lib.declare('dgfs_mlp_colsum', c_int, [c_int, c_int, c_void_p, c_ll,

@@ -469,6 +469,17 @@ DGFS_API int dgfs_mlp_gemm(int M, int N, int K, const float* A, long long sam,
                            long long sbk, long long sbn, const float* bias,
                            float* Z, float* C, long long ldc, int act,
                            int accumulate, const int* mcount, void* stream);
+/* The same product on the tensor cores (tcgen05.mma, kind::f16): A and B
+ * are rounded to BF16 (nearest even) as they are staged, products
+ * accumulate in FP32 in tensor memory. No mcount. err (device int) is set
+ * to 1 when a bounded wait of the kernel ran out; the kernel never clears
+ * it. */
+DGFS_API int dgfs_mlp_gemm_tc(int M, int N, int K, const float* A,
+                              long long sam, long long sak, const void* B,
+                              int b_bf16, long long sbk, long long sbn,
+                              const float* bias, float* Z, float* C,
+                              long long ldc, int act, int accumulate,
+                              int* err, void* stream);
 /* dZ = dH (1 - H^2) */
 DGFS_API int dgfs_mlp_tanh_bwd(long long n, const float* H, const float* dH,
                                float* dZ, void* stream);
