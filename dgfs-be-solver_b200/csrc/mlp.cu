@@ -11,6 +11,8 @@
 //   dgfs_mlp_mse     loss = mean over rows and the first n_used columns of
 //                    w_j (Y - T)^2, and dY
 //   dgfs_mlp_adam    Adam step on FP32 weights, refreshing the BF16 copy
+//   dgfs_mlp_adam_dev  the same over a flat buffer, hyper-parameters from
+//                    device memory (dgfs_mlp_schedule writes them)
 //   dgfs_mlp_affine  y = (x - mu) * inv_sigma per column (and the inverse);
 //                    dgfs_mlp_affine_rows gathers / scatters through a row list
 #include <cuda_bf16.h>
@@ -123,14 +125,28 @@ __global__ void tanh_bwd_kernel(long long n, const float* __restrict__ H, const 
     dZ[i] = dH[i] * (1.f - H[i] * H[i]);
 }
 
-// out[n] = sum_m X[m][n] (fixed summation order: deterministic)
-__global__ void colsum_kernel(int M, int N, const float* __restrict__ X, long long ldx, float* __restrict__ out,
-                              int accumulate) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= N) return;
+// out[n] = sum_m X[m][n] in a fixed order (deterministic): a CTA of 32 x 32
+// threads takes 32 columns; thread (ty, tx) sums rows ty, ty + 32, ... of
+// column tx in FP64, then each column's 32 partial sums are added in
+// row-group order.
+__global__ void __launch_bounds__(1024) colsum_kernel(int M, int N, const float* __restrict__ X, long long ldx,
+                                                      float* __restrict__ out, int accumulate) {
+  __shared__ double part[32][33];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int n = blockIdx.x * 32 + tx;
   double s = 0.0;
-  for (int m = 0; m < M; ++m) s += X[m * ldx + n];
-  out[n] = accumulate ? out[n] + (float)s : (float)s;
+  if (n < N) {
+#pragma unroll 4
+    for (int m = ty; m < M; m += 32) s += X[m * ldx + n];
+  }
+  part[ty][tx] = s;
+  __syncthreads();
+  if (ty == 0 && n < N) {
+    double t = 0.0;
+#pragma unroll
+    for (int k = 0; k < 32; ++k) t += part[k][tx];
+    out[n] = accumulate ? out[n] + (float)t : (float)t;
+  }
 }
 
 // loss partials per row and dY = 2 w (Y - T) / (M n_used)
@@ -174,6 +190,40 @@ __global__ void adam_kernel(long long n, float* __restrict__ w, __nv_bfloat16* _
     w[i] = wi;
     if (wb) wb[i] = __float2bfloat16_rn(wi);
   }
+}
+
+// One Adam step over a flat parameter buffer: the first n_decay entries
+// take the L2 weight decay; the learning rate and the bias corrections come
+// from device memory (hyper = {lr, 1 - beta1^t, 1 - beta2^t}), so that the
+// step can be replayed from a CUDA graph.
+__global__ void adam_dev_kernel(long long n, long long n_decay, float* __restrict__ w, __nv_bfloat16* __restrict__ wb,
+                                const float* __restrict__ g, float* __restrict__ m1, float* __restrict__ m2,
+                                const float* __restrict__ hyper, float b1, float b2, float eps, float wd) {
+  const float lr = hyper[0], c1 = hyper[1], c2 = hyper[2];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float gi = g[i] + (i < n_decay ? wd * w[i] : 0.f);
+    const float a = b1 * m1[i] + (1.f - b1) * gi;
+    const float b = b2 * m2[i] + (1.f - b2) * gi * gi;
+    m1[i] = a;
+    m2[i] = b;
+    const float wi = w[i] - lr * (a / c1) / (sqrtf(b / c2) + eps);
+    w[i] = wi;
+    if (wb) wb[i] = __float2bfloat16_rn(wi);
+  }
+}
+
+// Learning-rate schedule on the device: counters = {it, step}. Writes
+// hyper = {lr (lr_min + (1 - lr_min) (1 + cos(pi it / total)) / 2),
+// 1 - beta1^(step+1), 1 - beta2^(step+1)} and advances both counters.
+__global__ void schedule_kernel(int* __restrict__ counters, float* __restrict__ hyper, float lr, float lr_min,
+                                int total, float b1, float b2) {
+  const int it = counters[0], step = counters[1] + 1;
+  counters[0] = it + 1;
+  counters[1] = step;
+  const double frac = (double)it / (double)total;
+  hyper[0] = (float)((double)lr * ((double)lr_min + (1.0 - (double)lr_min) * 0.5 * (1.0 + cospi(frac))));
+  hyper[1] = 1.f - powf(b1, (float)step);
+  hyper[2] = 1.f - powf(b2, (float)step);
 }
 
 __global__ void affine_kernel(int M, int N, const float* __restrict__ X, const float* __restrict__ mu,
@@ -261,7 +311,7 @@ extern "C" int dgfs_mlp_colsum(int M, int N, const float* X, long long ldx, floa
                                void* stream) {
   dgfs::clear_error();
   if (M < 1 || N < 1 || !X || !out) return dgfs::set_error(DGFS_ERR_INVALID, "bad arguments");
-  colsum_kernel<<<(N + 127) / 128, 128, 0, (cudaStream_t)stream>>>(M, N, X, ldx, out, accumulate);
+  colsum_kernel<<<(N + 31) / 32, 1024, 0, (cudaStream_t)stream>>>(M, N, X, ldx, out, accumulate);
   return launched("colsum");
 }
 
@@ -281,6 +331,25 @@ extern "C" int dgfs_mlp_adam(long long n, float* w, void* wbf16, const float* g,
   const float c1 = 1.f - powf(beta1, (float)step), c2 = 1.f - powf(beta2, (float)step);
   adam_kernel<<<blocks_for(n), 256, 0, (cudaStream_t)stream>>>(n, w, (__nv_bfloat16*)wbf16, g, m1, m2, lr, beta1,
                                                                beta2, eps, c1, c2, weight_decay);
+  return launched("adam");
+}
+
+extern "C" int dgfs_mlp_schedule(int* counters, float* hyper, float lr, float lr_min, int total, float beta1,
+                                 float beta2, void* stream) {
+  dgfs::clear_error();
+  if (!counters || !hyper || total < 1) return dgfs::set_error(DGFS_ERR_INVALID, "bad arguments");
+  schedule_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(counters, hyper, lr, lr_min, total, beta1, beta2);
+  return launched("schedule");
+}
+
+extern "C" int dgfs_mlp_adam_dev(long long n, long long n_decay, float* w, void* wbf16, const float* g, float* m1,
+                                 float* m2, const float* hyper, float beta1, float beta2, float eps,
+                                 float weight_decay, void* stream) {
+  dgfs::clear_error();
+  if (n < 1 || n_decay < 0 || n_decay > n || !w || !g || !m1 || !m2 || !hyper)
+    return dgfs::set_error(DGFS_ERR_INVALID, "bad arguments");
+  adam_dev_kernel<<<blocks_for(n), 256, 0, (cudaStream_t)stream>>>(n, n_decay, w, (__nv_bfloat16*)wbf16, g, m1, m2,
+                                                                   hyper, beta1, beta2, eps, weight_decay);
   return launched("adam");
 }
 

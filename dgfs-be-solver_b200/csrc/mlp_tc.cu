@@ -7,15 +7,15 @@
 //                      even) and the products accumulated in FP32 by
 //                      tcgen05.mma (kind::f16) into tensor memory.
 //
-// One CTA of 128 threads computes a 128 x BN tile of C. K advances in slices
-// of 64 (one 128-byte row of BF16): the four warps load a slice of A
-// (128 x 64) and of B (BN x 64) from global memory, round it to BF16 and
-// store it in shared memory in the K-major 128-byte-swizzled layout the
-// tensor core reads (rows of 128 B, the 16-byte chunk c of row r at chunk
-// c ^ (r & 7), 8-row groups 1024 B apart). One elected thread issues the
-// slice's four 128 x BN x 16 MMAs and commits them to the slot's mbarrier;
-// a slot is refilled only after that mbarrier reports its MMAs complete, so
-// loads of the next slices overlap the tensor core's work on this one.
+// One CTA of 256 threads computes a 128 x BN tile of C. K advances in slices
+// of 64 (one 128-byte row of BF16): the eight warps load a slice of A
+// (128 x 64) and of B (BN x 64) from global memory into registers, round it
+// to BF16 and store it in shared memory in the K-major 128-byte-swizzled
+// layout the tensor core reads (rows of 128 B, the 16-byte chunk c of row r
+// at chunk c ^ (r & 7), 8-row groups 1024 B apart), then issue the next
+// slice's loads. One thread issues the slice's four 128 x BN x 16 MMAs and
+// commits them to the slot's mbarrier; a slot is refilled only after that
+// mbarrier reports its MMAs complete.
 // The accumulator lives in BN columns of tensor memory (lane = row of the
 // tile); the epilogue reads it with tcgen05.ld, adds the bias, applies tanh
 // and writes C (and the pre-activation Z).
@@ -40,7 +40,7 @@ using dgfs::smem_u32;
 constexpr int TC_BM = 128;       // MMA M: one tensor-memory lane per row of the tile
 constexpr int TC_BK = 64;        // K slice: one 128-byte swizzle row of BF16
 constexpr int TC_UK = 16;        // K of one kind::f16 MMA
-constexpr int TC_THREADS = 128;  // four warps: warp w owns tensor-memory lanes 32w..32w+31
+constexpr int TC_THREADS = 256;  // eight warps: warp w reads tensor-memory lanes 32 (w % 4) .. + 31
 constexpr int TC_STAGES = 3;
 
 // Operand staging modes (chosen on the host from the strides).
@@ -105,85 +105,123 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// Stage rows [r0, r0 + ROWS) x K [k0, k0 + 64) of a strided matrix (element
-// (r, k) at src[r sr + k sk]) into a swizzled BF16 tile; zero outside
-// [0, nr) x [0, K). All loads of the slice are issued before its stores.
-template <int ROWS>
-__device__ __forceinline__ void stage_tile(uint8_t* tile, const float* __restrict__ src, long long sr, long long sk,
-                                           int nr, int K, int r0, int k0, int mode) {
-  const int tid = threadIdx.x;
-  if (mode == kVec) {  // sk == 1, sr % 4 == 0, K % 4 == 0, 16-byte aligned
-    constexpr int NV = ROWS * (TC_BK / 4) / TC_THREADS;
-    float4 v[NV];
-#pragma unroll
-    for (int i = 0; i < NV; ++i) {
-      const int q = tid + TC_THREADS * i, row = q >> 4, k = k0 + (q & 15) * 4, r = r0 + row;
-      v[i] = (r < nr && k < K) ? __ldg(reinterpret_cast<const float4*>(src + r * sr + k)) : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-#pragma unroll
-    for (int i = 0; i < NV; ++i) {
-      const int q = tid + TC_THREADS * i, row = q >> 4, kq = (q & 15) * 4;
-      *reinterpret_cast<uint2*>(tile + sw128(row, kq)) = make_uint2(pack_bf16(v[i].x, v[i].y), pack_bf16(v[i].z, v[i].w));
-    }
-  } else {
-    constexpr int NP = ROWS * (TC_BK / 2) / TC_THREADS;
-    float x0[NP], x1[NP];
-#pragma unroll
-    for (int i = 0; i < NP; ++i) {
-      const int q = tid + TC_THREADS * i;
-      const int row = mode == kRowFast ? q % ROWS : q >> 5, kp = mode == kRowFast ? q / ROWS : q & 31;
-      const int r = r0 + row, k = k0 + 2 * kp;
-      const float* p = src + r * sr + k * sk;
-      x0[i] = (r < nr && k < K) ? __ldg(p) : 0.f;
-      x1[i] = (r < nr && k + 1 < K) ? __ldg(p + sk) : 0.f;
-    }
-#pragma unroll
-    for (int i = 0; i < NP; ++i) {
-      const int q = tid + TC_THREADS * i;
-      const int row = mode == kRowFast ? q % ROWS : q >> 5, kp = mode == kRowFast ? q / ROWS : q & 31;
-      *reinterpret_cast<uint32_t*>(tile + sw128(row, 2 * kp)) = pack_bf16(x0[i], x1[i]);
-    }
-  }
-}
+// One K slice of an operand held in registers between its global loads and
+// its shared-memory stores: rows [r0, r0 + ROWS) x K [k0, k0 + 64) of a
+// strided matrix (element (r, k) at src[r sr + k sk]), zero outside
+// [0, nr) x [0, K), stored into a swizzled BF16 tile. Loading the next slice
+// while the tensor core works on this one hides the global-memory latency.
+template <int ROWS, typename TS>
+struct Slice;
 
 template <int ROWS>
-__device__ __forceinline__ void stage_tile(uint8_t* tile, const __nv_bfloat16* __restrict__ src, long long sr,
-                                           long long sk, int nr, int K, int r0, int k0, int mode) {
-  const int tid = threadIdx.x;
-  if (mode == kVec) {  // sk == 1, sr % 8 == 0, K % 8 == 0, 16-byte aligned: copied as is
-    constexpr int NV = ROWS * (TC_BK / 8) / TC_THREADS;
-    uint4 v[NV];
+struct Slice<ROWS, float> {
+  static constexpr int NF = ROWS * TC_BK / TC_THREADS;  // floats per thread (vectors or pairs)
+  float v[NF];
+
+  // kRowFast: lanes walk rows, two K values each; kKFast: lanes walk K pairs
+  __device__ __forceinline__ static void pair_at(int q, int mode, int& row, int& kp) {
+    row = mode == kRowFast ? q % ROWS : q >> 5;
+    kp = mode == kRowFast ? q / ROWS : q & 31;
+  }
+
+  __device__ __forceinline__ void load(const float* __restrict__ src, long long sr, long long sk, int nr, int K,
+                                       int r0, int k0, int mode) {
+    const int tid = threadIdx.x;
+    if (mode == kVec) {  // sk == 1, sr % 4 == 0, K % 4 == 0, 16-byte aligned
 #pragma unroll
-    for (int i = 0; i < NV; ++i) {
-      const int q = tid + TC_THREADS * i, row = q >> 3, k = k0 + (q & 7) * 8, r = r0 + row;
-      v[i] = (r < nr && k < K) ? __ldg(reinterpret_cast<const uint4*>(src + r * sr + k)) : make_uint4(0u, 0u, 0u, 0u);
-    }
+      for (int i = 0; i < NF / 4; ++i) {
+        const int q = tid + TC_THREADS * i, row = q >> 4, k = k0 + (q & 15) * 4, r = r0 + row;
+        const float4 x = (r < nr && k < K) ? __ldg(reinterpret_cast<const float4*>(src + r * sr + k))
+                                           : make_float4(0.f, 0.f, 0.f, 0.f);
+        v[4 * i] = x.x, v[4 * i + 1] = x.y, v[4 * i + 2] = x.z, v[4 * i + 3] = x.w;
+      }
+    } else {
 #pragma unroll
-    for (int i = 0; i < NV; ++i) {
-      const int q = tid + TC_THREADS * i, row = q >> 3, kq = (q & 7) * 8;
-      *reinterpret_cast<uint4*>(tile + sw128(row, kq)) = v[i];
-    }
-  } else {
-    constexpr int NP = ROWS * (TC_BK / 2) / TC_THREADS;
-    uint16_t x0[NP], x1[NP];
-    const uint16_t* s16 = reinterpret_cast<const uint16_t*>(src);
-#pragma unroll
-    for (int i = 0; i < NP; ++i) {
-      const int q = tid + TC_THREADS * i;
-      const int row = mode == kRowFast ? q % ROWS : q >> 5, kp = mode == kRowFast ? q / ROWS : q & 31;
-      const int r = r0 + row, k = k0 + 2 * kp;
-      const uint16_t* p = s16 + r * sr + k * sk;
-      x0[i] = (r < nr && k < K) ? __ldg(p) : (uint16_t)0;
-      x1[i] = (r < nr && k + 1 < K) ? __ldg(p + sk) : (uint16_t)0;
-    }
-#pragma unroll
-    for (int i = 0; i < NP; ++i) {
-      const int q = tid + TC_THREADS * i;
-      const int row = mode == kRowFast ? q % ROWS : q >> 5, kp = mode == kRowFast ? q / ROWS : q & 31;
-      *reinterpret_cast<uint32_t*>(tile + sw128(row, 2 * kp)) = (uint32_t)x0[i] | ((uint32_t)x1[i] << 16);
+      for (int i = 0; i < NF / 2; ++i) {
+        int row, kp;
+        pair_at(tid + TC_THREADS * i, mode, row, kp);
+        const int r = r0 + row, k = k0 + 2 * kp;
+        const float* p = src + r * sr + k * sk;
+        v[2 * i] = (r < nr && k < K) ? __ldg(p) : 0.f;
+        v[2 * i + 1] = (r < nr && k + 1 < K) ? __ldg(p + sk) : 0.f;
+      }
     }
   }
-}
+
+  __device__ __forceinline__ void store(uint8_t* tile, int mode) const {
+    const int tid = threadIdx.x;
+    if (mode == kVec) {
+#pragma unroll
+      for (int i = 0; i < NF / 4; ++i) {
+        const int q = tid + TC_THREADS * i, row = q >> 4, kq = (q & 15) * 4;
+        *reinterpret_cast<uint2*>(tile + sw128(row, kq)) =
+            make_uint2(pack_bf16(v[4 * i], v[4 * i + 1]), pack_bf16(v[4 * i + 2], v[4 * i + 3]));
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < NF / 2; ++i) {
+        int row, kp;
+        pair_at(tid + TC_THREADS * i, mode, row, kp);
+        *reinterpret_cast<uint32_t*>(tile + sw128(row, 2 * kp)) = pack_bf16(v[2 * i], v[2 * i + 1]);
+      }
+    }
+  }
+};
+
+template <int ROWS>
+struct Slice<ROWS, __nv_bfloat16> {
+  static constexpr int NU = ROWS * TC_BK / 2 / TC_THREADS;  // BF16 pairs per thread
+  uint32_t v[NU];
+
+  __device__ __forceinline__ static void pair_at(int q, int mode, int& row, int& kp) {
+    row = mode == kRowFast ? q % ROWS : q >> 5;
+    kp = mode == kRowFast ? q / ROWS : q & 31;
+  }
+
+  __device__ __forceinline__ void load(const __nv_bfloat16* __restrict__ src, long long sr, long long sk, int nr,
+                                       int K, int r0, int k0, int mode) {
+    const int tid = threadIdx.x;
+    if (mode == kVec) {  // sk == 1, sr % 8 == 0, K % 8 == 0, 16-byte aligned: copied as is
+#pragma unroll
+      for (int i = 0; i < NU / 4; ++i) {
+        const int q = tid + TC_THREADS * i, row = q >> 3, k = k0 + (q & 7) * 8, r = r0 + row;
+        const uint4 x = (r < nr && k < K) ? __ldg(reinterpret_cast<const uint4*>(src + r * sr + k))
+                                          : make_uint4(0u, 0u, 0u, 0u);
+        v[4 * i] = x.x, v[4 * i + 1] = x.y, v[4 * i + 2] = x.z, v[4 * i + 3] = x.w;
+      }
+    } else {
+      const uint16_t* s16 = reinterpret_cast<const uint16_t*>(src);
+#pragma unroll
+      for (int i = 0; i < NU; ++i) {
+        int row, kp;
+        pair_at(tid + TC_THREADS * i, mode, row, kp);
+        const int r = r0 + row, k = k0 + 2 * kp;
+        const uint16_t* p = s16 + r * sr + k * sk;
+        const uint32_t lo = (r < nr && k < K) ? __ldg(p) : 0u;
+        const uint32_t hi = (r < nr && k + 1 < K) ? __ldg(p + sk) : 0u;
+        v[i] = lo | (hi << 16);
+      }
+    }
+  }
+
+  __device__ __forceinline__ void store(uint8_t* tile, int mode) const {
+    const int tid = threadIdx.x;
+    if (mode == kVec) {
+#pragma unroll
+      for (int i = 0; i < NU / 4; ++i) {
+        const int q = tid + TC_THREADS * i, row = q >> 3, kq = (q & 7) * 8;
+        *reinterpret_cast<uint4*>(tile + sw128(row, kq)) = make_uint4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < NU; ++i) {
+        int row, kp;
+        pair_at(tid + TC_THREADS * i, mode, row, kp);
+        *reinterpret_cast<uint32_t*>(tile + sw128(row, 2 * kp)) = v[i];
+      }
+    }
+  }
+};
 
 template <int BN>
 constexpr int tc_smem_bytes() {
@@ -231,14 +269,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 
   const int nk = (K + TC_BK - 1) / TC_BK;
   int last = -1;  // last K slice whose MMAs were committed
+  Slice<TC_BM, float> sa;
+  Slice<BN, TB> sb;
+  sa.load(A, sam, sak, M, K, m0, 0, amode);
+  sb.load(B, sbn, sbk, N, K, n0, 0, bmode);
   for (int kc = 0; kc < nk; ++kc) {
     const int s = kc % TC_STAGES;
     // the slot's previous MMAs (slice kc - STAGES) must be done reading it
     if (kc >= TC_STAGES) mbar_wait_bounded(&bars[s], (uint32_t)((kc / TC_STAGES - 1) & 1), err, gave_up);
     uint8_t* ta = smem + s * STAGE_BYTES;
     uint8_t* tb = ta + A_BYTES;
-    stage_tile<TC_BM>(ta, A, sam, sak, M, K, m0, kc * TC_BK, amode);
-    stage_tile<BN>(tb, B, sbn, sbk, N, K, n0, kc * TC_BK, bmode);
+    sa.store(ta, amode);
+    sb.store(tb, bmode);
+    if (kc + 1 < nk) {  // the next slice's loads fly during the barrier and the MMAs
+      sa.load(A, sam, sak, M, K, m0, (kc + 1) * TC_BK, amode);
+      sb.load(B, sbn, sbk, N, K, n0, (kc + 1) * TC_BK, bmode);
+    }
     fence_async_smem();  // the generic-proxy stores become visible to the tensor core
     __syncthreads();
     if (*(volatile int*)gave_up) break;  // uniform: read after the barrier
@@ -260,13 +306,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   tc_fence_after();
 
   if (!*(volatile int*)gave_up && !*(volatile int*)drain_up && last == nk - 1) {
-    const int m = m0 + warp * 32 + lane;
+    // warp w: rows 32 (w % 4) + lane, the half (w / 4) of the columns
+    const int quarter = warp & 3, half = warp >> 2;
+    const int m = m0 + quarter * 32 + lane;
     const bool row_ok = m < M;
 #pragma unroll 1
-    for (int j0 = 0; j0 < BN; j0 += 16) {
+    for (int j0 = half * (BN / 2); j0 < (half + 1) * (BN / 2); j0 += 16) {
       float v[16];
       __syncwarp();  // tcgen05.ld is warp-collective
-      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)j0, v);
+      tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)j0, v);
       if (row_ok && n0 + j0 < N) {
         float* crow = C + (long long)m * ldc;
         float* zrow = Z ? Z + (long long)m * ldc : nullptr;

@@ -81,6 +81,12 @@ _lib.declare('dgfs_mlp_adam', c_int, [c_ll, c_void_p, c_void_p, c_void_p,
                                       c_void_p, c_void_p, c_float, c_float,
                                       c_float, c_float, c_int, c_float,
                                       c_void_p])
+_lib.declare('dgfs_mlp_adam_dev', c_int,
+             [c_ll, c_ll, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+              c_void_p, c_float, c_float, c_float, c_float, c_void_p])
+_lib.declare('dgfs_mlp_schedule', c_int,
+             [c_void_p, c_void_p, c_float, c_float, c_int, c_float, c_float,
+              c_void_p])
 _lib.declare('dgfs_mlp_affine', c_int, [c_int, c_int, c_void_p, c_void_p,
                                         c_void_p, c_void_p, c_int, c_void_p])
 _lib.declare('dgfs_mlp_affine_rows', c_int,
@@ -164,34 +170,65 @@ class MLP:
     """4 layers of width 512 with a linear input->output skip; FP32 master
     weights, BF16 copies for the products, Adam optimiser; every kernel is
     libdgfs_b200's.  Weights are stored W[in][out], activations row-major
-    [batch][features]."""
+    [batch][features].
+
+    The parameters live in one flat buffer (weights first, then biases) so
+    that one Adam launch updates all of them.  With ``tc`` the training
+    products (forward with ``keep``, backward) run on the tensor cores
+    (dgfs_mlp_gemm_tc: BF16 operands, FP32 accumulation); inference keeps
+    the FP32-activation SIMT product."""
 
     names = ('W1', 'b1', 'W2', 'b2', 'W3', 'b3', 'W4', 'b4', 'Ws')
+    _order = ('W1', 'W2', 'W3', 'W4', 'Ws', 'b1', 'b2', 'b3', 'b4')
 
-    def __init__(self, device, nin=NFEAT, width=WIDTH, nout=NFEAT, seed=0):
+    def __init__(self, device, nin=NFEAT, width=WIDTH, nout=NFEAT, seed=0,
+                 tc=True):
         self.device = device
         self.nin, self.width, self.nout = nin, width, nout
+        self.tc = bool(tc)
         rng = np.random.default_rng(seed)
         shapes = {'W1': (nin, width), 'b1': (width,), 'W2': (width, width),
                   'b2': (width,), 'W3': (width, width), 'b3': (width,),
                   'W4': (width, nout), 'b4': (nout,), 'Ws': (nin, nout)}
+        init = {}
+        for k, shp in shapes.items():      # same draws as per-tensor storage
+            if k in ('W1', 'W2', 'W3'):
+                init[k] = rng.standard_normal(shp)/np.sqrt(shp[0])
+            elif k == 'W4':
+                init[k] = 0.1*rng.standard_normal(shp)/np.sqrt(shp[0])
+            else:
+                init[k] = np.zeros(shp)
+        # flat layout: every slice starts on a multiple of 8 entries (16-byte
+        # aligned BF16 views for the tensor-core loads)
+        off, offs = 0, {}
+        for k in self._order:
+            offs[k] = off
+            off += -(-int(np.prod(shapes[k]))//8)*8
+        self.n = off
+        self.n_decay = offs['b1']
+        f32 = dict(dtype=torch.float32, device=device)
+        self.flat_w = torch.zeros(off, **f32)
+        self.flat_g = torch.zeros(off, **f32)
+        self.flat_m1 = torch.zeros(off, **f32)
+        self.flat_m2 = torch.zeros(off, **f32)
+        self.flat_wb = torch.zeros(off, dtype=torch.bfloat16, device=device)
         self.w, self.g, self.m1, self.m2, self.wb = {}, {}, {}, {}, {}
         for k, shp in shapes.items():
-            if k in ('W1', 'W2', 'W3'):
-                a = rng.standard_normal(shp)/np.sqrt(shp[0])
-            elif k == 'W4':
-                a = 0.1*rng.standard_normal(shp)/np.sqrt(shp[0])
-            else:
-                a = np.zeros(shp)
-            self.w[k] = torch.tensor(a, dtype=torch.float32, device=device)
-            self.g[k] = torch.zeros_like(self.w[k])
-            self.m1[k] = torch.zeros_like(self.w[k])
-            self.m2[k] = torch.zeros_like(self.w[k])
+            sl = slice(offs[k], offs[k] + int(np.prod(shp)))
+            self.w[k] = self.flat_w[sl].view(shp)
+            self.g[k] = self.flat_g[sl].view(shp)
+            self.m1[k] = self.flat_m1[sl].view(shp)
+            self.m2[k] = self.flat_m2[sl].view(shp)
             if k.startswith('W'):
-                self.wb[k] = torch.empty(self.w[k].shape, dtype=torch.bfloat16,
-                                         device=device)
+                self.wb[k] = self.flat_wb[sl].view(shp)
+            self.w[k].copy_(torch.tensor(init[k], dtype=torch.float32))
         self.step = 0
         self.ws = _Workspace(device)
+        # {it, step} of the device learning-rate schedule, and its output
+        # {lr, 1 - beta1^t, 1 - beta2^t}
+        self.counters = torch.zeros(2, dtype=torch.int32, device=device)
+        self.hyper = torch.zeros(3, **f32)
+        self.err = torch.zeros(1, dtype=torch.int32, device=device)
         self.sync_bf16()
         self._cache = None
 
@@ -202,18 +239,41 @@ class MLP:
     def nparams(self):
         return sum(t.numel() for t in self.w.values())
 
+    def train_flops_per_row(self):
+        """Multiply-add FLOPs of one training row: the forward products,
+        the weight gradients (the same sizes) and the input gradients of
+        layers 4, 3 and 2."""
+        nin, wd, nout = self.nin, self.width, self.nout
+        fwd = 2*(nin*wd + 2*wd*wd + wd*nout + nin*nout)
+        return 2*fwd + 2*(wd*nout + 2*wd*wd)
+
     def sync_bf16(self):
-        lib = _lib.load()
-        for k, t in self.wb.items():
-            _lib.check(lib.dgfs_f32_to_bf16(t.numel(), _p(self.w[k]), _p(t),
-                                            self._s), 'dgfs_f32_to_bf16')
+        _lib.check(_lib.load().dgfs_f32_to_bf16(
+            self.n, _p(self.flat_w), _p(self.flat_wb), self._s),
+            'dgfs_f32_to_bf16')
 
     def _gemm(self, A, B, C, M, N, K, sam, sak, sbk, sbn, bf16, bias=None,
-              act=0, acc=0, mcount=None):
-        _lib.check(_lib.load().dgfs_mlp_gemm(
+              act=0, acc=0, mcount=None, tc=False):
+        lib = _lib.load()
+        if tc:
+            assert mcount is None
+            _lib.check(lib.dgfs_mlp_gemm_tc(
+                M, N, K, _p(A), sam, sak, _p(B), 1 if bf16 else 0, sbk, sbn,
+                _p(bias), None, _p(C), N, act, acc, _p(self.err), self._s),
+                'dgfs_mlp_gemm_tc')
+            return
+        _lib.check(lib.dgfs_mlp_gemm(
             M, N, K, _p(A), sam, sak, _p(B), 1 if bf16 else 0, sbk, sbn,
             _p(bias), None, _p(C), N, act, acc, _p(mcount), self._s),
             'dgfs_mlp_gemm')
+
+    def check_tc(self):
+        """Raise if a bounded wait of a tensor-core product ran out (reads
+        the device flag: synchronises the stream)."""
+        if int(self.err.item()):
+            raise _lib.DgfsError(2, 'dgfs_mlp_gemm_tc',
+                                 'a bounded wait of the tensor-core GEMM '
+                                 'ran out')
 
     def forward(self, X, keep=False, mcount=None):
         """Y = W4 tanh(W3 tanh(W2 tanh(W1 X + b1) + b2) + b3) + b4 + Ws X.
@@ -221,6 +281,7 @@ class MLP:
         B = X.shape[0]
         nin, wd, nout = self.nin, self.width, self.nout
         tag = 'train' if keep else 'infer'
+        tc = keep and self.tc and mcount is None
         H1 = self.ws.get(tag + 'H1', (B, wd))
         H2 = self.ws.get(tag + 'H2', (B, wd))
         H3 = self.ws.get(tag + 'H3', (B, wd))
@@ -228,33 +289,35 @@ class MLP:
         wb, w = self.wb, self.w
         mc = mcount
         self._gemm(X, wb['W1'], H1, B, wd, nin, nin, 1, wd, 1, True,
-                   w['b1'], act=1, mcount=mc)
+                   w['b1'], act=1, mcount=mc, tc=tc)
         self._gemm(H1, wb['W2'], H2, B, wd, wd, wd, 1, wd, 1, True,
-                   w['b2'], act=1, mcount=mc)
+                   w['b2'], act=1, mcount=mc, tc=tc)
         self._gemm(H2, wb['W3'], H3, B, wd, wd, wd, 1, wd, 1, True,
-                   w['b3'], act=1, mcount=mc)
+                   w['b3'], act=1, mcount=mc, tc=tc)
         self._gemm(H3, wb['W4'], Y, B, nout, wd, wd, 1, nout, 1, True,
-                   w['b4'], mcount=mc)
+                   w['b4'], mcount=mc, tc=tc)
         self._gemm(X, wb['Ws'], Y, B, nout, nin, nin, 1, nout, 1, True,
-                   acc=1, mcount=mc)
+                   acc=1, mcount=mc, tc=tc)
         if keep:
             self._cache = (X, H1, H2, H3)
         return Y
 
     def backward(self, dY):
         """Gradients of every parameter into self.g: weight gradients from
-        the FP32 activations, input gradients through the BF16 weights that
-        the forward pass used."""
+        the activations, input gradients through the BF16 weights that the
+        forward pass used (on the tensor cores with ``tc``: activations and
+        gradients rounded to BF16 as they are staged)."""
         lib = _lib.load()
         X, H1, H2, H3 = self._cache
         B = X.shape[0]
         nin, wd, nout = self.nin, self.width, self.nout
         g, wb = self.g, self.wb
+        tc = self.tc
         dH = self.ws.get('dH', (B, wd))
         dZ = self.ws.get('dZ', (B, wd))
 
         def wgrad(A, D, name, k, n):          # g = A^T D, (k x n), K = B
-            self._gemm(A, D, g[name], k, n, B, 1, k, n, 1, False)
+            self._gemm(A, D, g[name], k, n, B, 1, k, n, 1, False, tc=tc)
 
         def bgrad(D, name, n):
             _lib.check(lib.dgfs_mlp_colsum(B, n, _p(D), n, _p(g[name]), 0,
@@ -263,7 +326,7 @@ class MLP:
         def through(D, nd, W, H):
             # dZ = (D W^T) o (1 - H^2); D may be dZ itself: the product is
             # complete (same stream) before dZ is overwritten
-            self._gemm(D, W, dH, B, wd, nd, nd, 1, 1, nd, True)
+            self._gemm(D, W, dH, B, wd, nd, nd, 1, 1, nd, True, tc=tc)
             _lib.check(lib.dgfs_mlp_tanh_bwd(dH.numel(), _p(H), _p(dH),
                                              _p(dZ), self._s),
                        'dgfs_mlp_tanh_bwd')
@@ -291,6 +354,27 @@ class MLP:
                 _p(self.g[k]), _p(self.m1[k]), _p(self.m2[k]), lr, beta1,
                 beta2, eps, self.step, wd if k.startswith('W') else 0.0,
                 self._s), 'dgfs_mlp_adam')
+
+    def start_schedule(self):
+        """Point the device schedule at iteration 0 and this MLP's Adam
+        step count."""
+        self.counters.copy_(torch.tensor([0, self.step], dtype=torch.int32))
+
+    def adam_scheduled(self, lr, lr_min, total, beta1=0.9, beta2=0.999,
+                       eps=1e-8, wd=0.0):
+        """One Adam step of every parameter (one launch) at the device
+        schedule's rate: stream-ordered, no host values that change from
+        step to step, so it can be replayed from a CUDA graph.  The caller
+        advances ``self.step`` on the host."""
+        lib = _lib.load()
+        _lib.check(lib.dgfs_mlp_schedule(
+            _p(self.counters), _p(self.hyper), lr, lr_min, total, beta1,
+            beta2, self._s), 'dgfs_mlp_schedule')
+        _lib.check(lib.dgfs_mlp_adam_dev(
+            self.n, self.n_decay, _p(self.flat_w), _p(self.flat_wb),
+            _p(self.flat_g), _p(self.flat_m1), _p(self.flat_m2),
+            _p(self.hyper), beta1, beta2, eps, wd, self._s),
+            'dgfs_mlp_adam_dev')
 
     def state(self):
         return {k: v.detach().cpu().numpy() for k, v in self.w.items()}
@@ -438,38 +522,63 @@ class VHSSurrogate:
 
     # -- training ------------------------------------------------------------
     def train(self, X, B, epochs=20, batch=1024, lr=1e-3, seed=0,
-              lr_min=0.05, weight_decay=0.0):
+              lr_min=0.05, weight_decay=0.0, graph=True):
         """Mini-batch Adam on normalised features/targets with the
         project's kernels (cosine learning-rate decay to lr*lr_min);
-        returns the per-epoch mean loss."""
+        returns the per-epoch mean loss.
+
+        A training step gathers the batch, runs the forward pass, the loss,
+        the backward pass and one Adam launch whose rate comes from the
+        device schedule.  With ``graph`` the first step runs eagerly and is
+        then captured in a CUDA graph that every later step replays; only
+        the batch's row indices are copied in between."""
         Xn = self._affine(X, self.mu_x, self.is_x)
         Bn = self._affine(B, self.mu_y, self.is_y)
         n = X.shape[0]
         batch = min(batch, n)
-        g = torch.Generator(device='cpu').manual_seed(seed)
+        gen = torch.Generator(device='cpu').manual_seed(seed)
         lib = _lib.load()
+        mlp, dev = self.mlp, self.device
         nb = n//batch
         total = max(epochs*nb, 1)
-        dY = torch.empty(batch, NFEAT, device=self.device)
-        rl = torch.empty(nb, batch, dtype=torch.float64, device=self.device)
+        idx = torch.empty(batch, dtype=torch.int64, device=dev)
+        xb = torch.empty(batch, NFEAT, device=dev)
+        yb = torch.empty(batch, NFEAT, device=dev)
+        dY = torch.empty(batch, NFEAT, device=dev)
+        rl = torch.empty(batch, dtype=torch.float64, device=dev)
+        acc = torch.zeros((), dtype=torch.float64, device=dev)
+
+        def step():
+            torch.index_select(Xn, 0, idx, out=xb)
+            torch.index_select(Bn, 0, idx, out=yb)
+            Y = mlp.forward(xb, keep=True)
+            _lib.check(lib.dgfs_mlp_mse(
+                batch, NFEAT, NMODES, _p(Y), _p(yb), None, _p(dY), _p(rl),
+                mlp._s), 'dgfs_mlp_mse')
+            acc.add_(rl.sum())
+            mlp.backward(dY)
+            mlp.adam_scheduled(lr, lr_min, total, wd=weight_decay)
+
+        mlp.start_schedule()
+        cg = None
         hist = []
-        it = 0
         for ep in range(epochs):
-            perm = torch.randperm(n, generator=g).to(self.device)
+            perm = torch.randperm(n, generator=gen).to(dev)
             for b in range(nb):
-                idx = perm[b*batch:(b + 1)*batch]
-                xb = Xn.index_select(0, idx)
-                yb = Bn.index_select(0, idx)
-                Y = self.mlp.forward(xb, keep=True)
-                _lib.check(lib.dgfs_mlp_mse(
-                    batch, NFEAT, NMODES, _p(Y), _p(yb), None, _p(dY),
-                    _p(rl[b]), self._s), 'dgfs_mlp_mse')
-                self.mlp.backward(dY)
-                frac = it/total
-                lr_t = lr*(lr_min + (1 - lr_min)*0.5*(1 + np.cos(np.pi*frac)))
-                self.mlp.adam(lr=lr_t, wd=weight_decay)
-                it += 1
-            hist.append(float(rl.sum())/(nb*batch*NMODES))
+                idx.copy_(perm[b*batch:(b + 1)*batch])
+                if cg is not None:
+                    cg.replay()
+                    continue
+                step()
+                if graph and total > 1:
+                    cg = torch.cuda.CUDAGraph()
+                    with torch.cuda.graph(cg):
+                        step()
+            hist.append(float(acc)/(nb*batch*NMODES))
+            acc.zero_()
+        del cg
+        mlp.step += total
+        mlp.check_tc()
         self.loss_history += hist
         return hist
 

@@ -179,7 +179,10 @@ def run_study(ini, device='cuda:0', runs=5, near_runs=10, steps=100,
     hist = sur.train(X, B, epochs=epochs, batch=batch, lr=lr)
     torch.cuda.synchronize(device)
     t_train = time.time() - tt
-    say(f'train: loss {hist[0]:.3e} -> {hist[-1]:.3e} in {t_train:.1f} s')
+    rows = (npairs//min(batch, npairs))*min(batch, npairs)*epochs
+    train_tflops = sur.mlp.train_flops_per_row()*rows/t_train*1e-12
+    say(f'train: loss {hist[0]:.3e} -> {hist[-1]:.3e} in {t_train:.1f} s '
+        f'({train_tflops:.1f} TFLOP/s)')
     del X, B
 
     # 3. the workload from its own initial state
@@ -245,6 +248,8 @@ def run_study(ini, device='cuda:0', runs=5, near_runs=10, steps=100,
         'points': npts, 'pairs': npairs, 'pairs_solver': npairs_solver,
         'train_loss_first': hist[0], 'train_loss_last': hist[-1],
         'harvest_s': t_harvest, 'train_s': t_train,
+        'train_tflops': train_tflops,
+        'train_products': 'tensor cores' if sur.mlp.tc else 'SIMT',
         'epochs': epochs, 'runs': runs, 'near_runs': near_runs,
         'steps_per_run': steps,
         'nsteps': nsteps, 'threshold': threshold,

@@ -497,6 +497,21 @@ DGFS_API int dgfs_mlp_adam(long long n, float* w, void* wbf16, const float* g,
                            float* m1, float* m2, float lr, float beta1,
                            float beta2, float eps, int step,
                            float weight_decay, void* stream);
+/* Adam over a flat buffer of n parameters whose first n_decay take the
+ * weight decay; hyper (device) = {lr, 1 - beta1^t, 1 - beta2^t}. */
+DGFS_API int dgfs_mlp_adam_dev(long long n, long long n_decay, float* w,
+                               void* wbf16, const float* g, float* m1,
+                               float* m2, const float* hyper, float beta1,
+                               float beta2, float eps, float weight_decay,
+                               void* stream);
+/* Cosine learning-rate schedule on the device: counters (device) =
+ * {it, step}; writes hyper = {lr (lr_min + (1 - lr_min)(1 + cos(pi it /
+ * total))/2), 1 - beta1^(step+1), 1 - beta2^(step+1)} and advances both
+ * counters by one, so a captured training step replays with the right
+ * rate. */
+DGFS_API int dgfs_mlp_schedule(int* counters, float* hyper, float lr,
+                               float lr_min, int total, float beta1,
+                               float beta2, void* stream);
 /* Y = (X - mu) inv_sigma per column, or X / inv_sigma + mu (inverse). */
 DGFS_API int dgfs_mlp_affine(int M, int N, const float* X, const float* mu,
                              const float* inv_sigma, float* Y, int inverse,

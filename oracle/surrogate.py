@@ -137,30 +137,50 @@ def reconstruct(b, mom, cv, prefac=1.0, gamma=0.0, Gw=None, f=None,
 # --------------------------------------------------------------------------
 # MLP: x -> tanh(W1) -> tanh(W2) -> tanh(W3) -> W4 (+ Ws x); W[in][out]
 # --------------------------------------------------------------------------
-def mlp_forward(params, X):
+def bf16_round(x):
+    """x rounded to FP32, then to the nearest BF16 (ties to even), as
+    float64: the rounding the tensor-core products apply to their
+    operands."""
+    u = np.ascontiguousarray(x, dtype=np.float32).view(np.uint32)
+    u = u.astype(np.uint64)
+    u = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return u.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def _same(a):
+    return a
+
+
+def mlp_forward(params, X, rnd=None):
+    """Forward pass; ``rnd`` (e.g. bf16_round) is applied to the activation
+    operand of every product, as the tensor-core training products do."""
+    r = rnd or _same
     W1, b1, W2, b2, W3, b3, W4, b4, Ws = params
-    H1 = np.tanh(X @ W1 + b1)
-    H2 = np.tanh(H1 @ W2 + b2)
-    H3 = np.tanh(H2 @ W3 + b3)
-    Y = H3 @ W4 + b4 + X @ Ws
+    H1 = np.tanh(r(X) @ W1 + b1)
+    H2 = np.tanh(r(H1) @ W2 + b2)
+    H3 = np.tanh(r(H2) @ W3 + b3)
+    Y = r(H3) @ W4 + b4 + r(X) @ Ws
     return Y, (X, H1, H2, H3)
 
 
-def mlp_backward(params, cache, dY):
+def mlp_backward(params, cache, dY, rnd=None):
+    """Backward pass; ``rnd`` is applied to both operands of every weight
+    gradient and to the gradient operand of every input gradient."""
+    r = rnd or _same
     W1, b1, W2, b2, W3, b3, W4, b4, Ws = params
     X, H1, H2, H3 = cache
     g = {}
-    g['W4'] = H3.T @ dY
+    g['W4'] = r(H3).T @ r(dY)
     g['b4'] = dY.sum(axis=0)
-    g['Ws'] = X.T @ dY
-    dZ3 = (dY @ W4.T)*(1 - H3**2)
-    g['W3'] = H2.T @ dZ3
+    g['Ws'] = r(X).T @ r(dY)
+    dZ3 = (r(dY) @ W4.T)*(1 - H3**2)
+    g['W3'] = r(H2).T @ r(dZ3)
     g['b3'] = dZ3.sum(axis=0)
-    dZ2 = (dZ3 @ W3.T)*(1 - H2**2)
-    g['W2'] = H1.T @ dZ2
+    dZ2 = (r(dZ3) @ W3.T)*(1 - H2**2)
+    g['W2'] = r(H1).T @ r(dZ2)
     g['b2'] = dZ2.sum(axis=0)
-    dZ1 = (dZ2 @ W2.T)*(1 - H1**2)
-    g['W1'] = X.T @ dZ1
+    dZ1 = (r(dZ2) @ W2.T)*(1 - H1**2)
+    g['W1'] = r(X).T @ r(dZ1)
     g['b1'] = dZ1.sum(axis=0)
     return g
 

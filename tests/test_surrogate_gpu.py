@@ -290,9 +290,16 @@ def _bf16(t):
     return t.to(torch.bfloat16).to(torch.float64).cpu().numpy()
 
 
-def test_mlp_gradients_match_oracle():
+@pytest.mark.parametrize('tc', [False, True])
+def test_mlp_gradients_match_oracle(tc):
+    """SIMT products (FP32 activations) against the FP64 oracle with the
+    same BF16 weights at 1e-4.  Tensor-core products (BF16 operands)
+    against the oracle that rounds the same operands at 4e-3: the GPU's
+    FP32 activations and the oracle's FP64 ones can round to neighbouring
+    BF16 values, one BF16 step (2^-8) in a few operands; and against the
+    unrounded oracle at 1.5e-2, the size of BF16 operand rounding."""
     dev = torch.device('cuda:0')
-    mlp = MLP(dev, seed=4)
+    mlp = MLP(dev, seed=4, tc=tc)
     rng = np.random.default_rng(6)
     for k in ('b1', 'b2', 'b3', 'b4'):
         mlp.w[k].copy_(torch.tensor(0.1*rng.standard_normal(mlp.w[k].shape)))
@@ -318,14 +325,75 @@ def test_mlp_gradients_match_oracle():
     P = [(_bf16(mlp.w[k]) if k.startswith('W') else
           mlp.w[k].double().cpu().numpy()) for k in MLP.names]
     Xn = X.double().cpu().numpy()
-    Yo, cache = osur.mlp_forward(P, Xn)
+    rnd = osur.bf16_round if tc else None
+    tol = 4e-3 if tc else 1e-4
+    Yo, cache = osur.mlp_forward(P, Xn, rnd=rnd)
     loss, dYo = osur.mse(Yo, T.double().cpu().numpy(), NMODES,
                          w.double().cpu().numpy())
-    assert rel_err(Y.cpu().numpy(), Yo) < 1e-4
-    assert abs(float(rl.sum())/(Bt*NMODES) - loss) < 1e-4*loss
-    go = osur.mlp_backward(P, cache, dYo)
+    assert rel_err(Y.cpu().numpy(), Yo) < tol
+    assert abs(float(rl.sum())/(Bt*NMODES) - loss) < tol*loss
+    go = osur.mlp_backward(P, cache, dYo, rnd=rnd)
     for k in MLP.names:
-        assert rel_err(g[k].cpu().numpy(), go[k]) < 1e-4, k
+        assert rel_err(g[k].cpu().numpy(), go[k]) < tol, k
+    if tc:
+        Yu, cu = osur.mlp_forward(P, Xn)
+        gu = osur.mlp_backward(P, cu, osur.mse(
+            Yu, T.double().cpu().numpy(), NMODES,
+            w.double().cpu().numpy())[1])
+        assert rel_err(Y.cpu().numpy(), Yu) < 1.5e-2
+        for k in MLP.names:
+            assert rel_err(g[k].cpu().numpy(), gu[k]) < 1.5e-2, k
+        mlp.check_tc()
+
+
+def test_scheduled_adam_matches_per_tensor_adam():
+    """One Adam launch over the flat buffer at the device schedule's rate
+    equals the per-tensor launches at the host-computed rate (weight decay
+    on the weights only); the schedule's counters advance."""
+    dev = torch.device('cuda:0')
+    a, b = MLP(dev, seed=2), MLP(dev, seed=2)
+    rng = np.random.default_rng(3)
+    lr, lr_min, total, wd = 2e-3, 0.1, 7, 1e-3
+    b.start_schedule()
+    for it in range(3):
+        for k in MLP.names:
+            gk = torch.tensor(rng.standard_normal(a.g[k].shape),
+                              dtype=torch.float32)
+            a.g[k].copy_(gk)
+            b.g[k].copy_(gk)
+        frac = it/total
+        a.adam(lr=lr*(lr_min + (1 - lr_min)*0.5*(1 + np.cos(np.pi*frac))),
+               wd=wd)
+        b.adam_scheduled(lr, lr_min, total, wd=wd)
+    torch.cuda.synchronize()
+    for k in MLP.names:
+        assert rel_err(b.w[k].cpu().numpy(), a.w[k].cpu().numpy()) < 1e-6, k
+        if k.startswith('W'):
+            assert torch.equal(b.wb[k], b.w[k].to(torch.bfloat16)), k
+    assert b.counters.cpu().tolist() == [3, 3]
+
+
+def test_graph_training_equals_eager_training():
+    """The CUDA-graph replay of the training step gives bit-identical
+    weights and losses to running every step eagerly."""
+    dev = torch.device('cuda:0')
+    be, vm, sm = _model('single')
+    rng = np.random.default_rng(8)
+    n = 2048
+    X = torch.tensor(rng.standard_normal((n, NFEAT)), dtype=torch.float32,
+                     device=dev)
+    Y = torch.tensor(rng.standard_normal((n, NFEAT)), dtype=torch.float32,
+                     device=dev)
+    out = []
+    for graph in (False, True):
+        sur = VHSSurrogate(sm, seed=5)
+        sur.set_normalisation(X, Y)
+        hist = sur.train(X, Y, epochs=3, batch=256, lr=1e-3, graph=graph)
+        out.append((hist, sur.mlp.state(), sur.mlp.step))
+    assert out[0][0] == out[1][0]
+    assert out[0][2] == out[1][2] == 3*(n//256)
+    for k in MLP.names:
+        assert np.array_equal(out[0][1][k], out[1][1][k]), k
 
 
 def test_adam_step_matches_formula():

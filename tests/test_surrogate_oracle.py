@@ -125,3 +125,14 @@ def test_mlp_backward_matches_finite_differences():
             fd = (lp - lm)/(2*h)
             assert abs(fd - g[name].reshape(-1)[i]) < 1e-7 + 1e-5*abs(fd), \
                 (name, i, fd, g[name].reshape(-1)[i])
+
+
+def test_bf16_round_matches_torch():
+    """The oracle's BF16 rounding (FP32 first, then nearest even) is
+    torch's float32 -> bfloat16 conversion, over 40 binades."""
+    import torch
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal(20000)*np.exp(rng.uniform(-20, 20, 20000))
+    x = np.concatenate([x, [0.0, -0.0, 1.0, 1.00390625, 1.01171875]])
+    ref = torch.tensor(x, dtype=torch.float32).to(torch.bfloat16)
+    assert np.array_equal(osur.bf16_round(x), ref.double().numpy())
