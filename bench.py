@@ -874,8 +874,9 @@ def run_mixture(args):
                      'flops_per_point': sm.flops_per_point(),
                      'launch_ms': t_ms/args.steps, 'traffic': None,
                      'traffic_source': 'not captured',
-                     'kernel': 'vss_push_kernel (4 launches, one per '
-                               'ordered pair)'},
+                     'kernel': ('vss_pair_kernel' if prec == 32 and
+                                round(V**(1/3)) == 24 else 'vss_push_kernel') +
+                               ' (4 launches, one per ordered pair)'},
         'cpu_baseline': None,
     }
     print(json.dumps(line))

@@ -7,6 +7,7 @@
 
 #include "../../include/dgfs_b200.h"
 #include "dg_kernel.cuh"
+#include "dg_tc.cuh"
 #include "dgfs_internal.h"
 
 using namespace dgfs;
@@ -26,6 +27,7 @@ struct dgfs_dg {
   int64_t* pblk;   // [nblk][32][PS] partner offsets, boundary and halo codes
   int *sfpt, *sele;  // [nsend] flux point and element of each send row
   const void* halo;  // caller's [nhalo][V] received values (dgfs_dg_set_halo)
+  int* err;          // bounded-wait flag of the tensor-core residual (dgfs_dg_status)
 };
 
 constexpr int kBcChunks = 256;  // velocity chunks of the wall-sum reduction
@@ -39,6 +41,18 @@ struct DgShape {
 };
 constexpr DgShape kDgShapes[] = {{8, 0, 0}, {8, 1, 0}, {8, 1, 2}, {16, 1, 2}, {4, 0, 0}, {4, 1, 0}, {2, 1, 0}};
 constexpr int kDgNumShapes = sizeof(kDgShapes) / sizeof(kDgShapes[0]);
+// Tensor-core residual shapes (FP32 only; dg_tc.cuh), numbered after the
+// SIMT shapes: velocities per warp of a 128-thread CTA, Runge-Kutta terms
+// always loaded ahead, CTAs per SM (0: 4 for p <= 2, 2 for p = 3, what the
+// operand tiles' shared memory allows).
+constexpr DgShape kDgTcShapes[] = {{8, 1, 0}, {16, 1, 0}, {4, 1, 0}, {32, 1, 0}};
+constexpr int kDgNumTc = sizeof(kDgTcShapes) / sizeof(kDgTcShapes[0]);
+
+inline int num_shapes(const dgfs_dg* h) { return kDgNumShapes + (h->prec == 32 ? kDgNumTc : 0); }
+inline bool tc_shape(int idx) { return idx >= kDgNumShapes; }
+inline const DgShape& shape_of(int idx) { return tc_shape(idx) ? kDgTcShapes[idx - kDgNumShapes] : kDgShapes[idx]; }
+// velocities of one CTA's chunk: 8 warps x vpt (SIMT), 4 warps x vpt (tensor cores)
+inline int chunk_of(int idx) { return (tc_shape(idx) ? 4 : 8) * shape_of(idx).vpt; }
 
 namespace {
 
@@ -134,6 +148,7 @@ template <typename T> DgArgs<T> make_args(const dgfs_dg* h) {
   a.ldim_u = h->ldim_u;
   a.ldim_f = h->ldim_f;
   a.uf = (T*)h->uf;
+  a.err = h->err;
   a.smats = (const T*)h->smats;
   a.rcpdjac = (const T*)h->rcpdjac;
   a.nrm = (const T*)h->nrm;
@@ -178,11 +193,12 @@ template <typename T, int U> DgMassOps<T, U> make_mass_ops(const dgfs_dg* h) {
 // (dg_kernel.cuh: pdl_wait / pdl_trigger say what each kernel may do before
 // its predecessor has completed); pdl = false launches in plain stream order.
 template <typename... P, typename... A>
-cudaError_t launch_pdl(bool pdl, void (*kern)(P...), dim3 grid, cudaStream_t s, A&&... args) {
+cudaError_t launch_pdl_shape(bool pdl, void (*kern)(P...), dim3 grid, int threads, int smem, cudaStream_t s,
+                             A&&... args) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
-  cfg.blockDim = dim3(256, 1, 1);
-  cfg.dynamicSmemBytes = 0;
+  cfg.blockDim = dim3((unsigned)threads, 1, 1);
+  cfg.dynamicSmemBytes = (size_t)smem;
   cfg.stream = s;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -190,6 +206,11 @@ cudaError_t launch_pdl(bool pdl, void (*kern)(P...), dim3 grid, cudaStream_t s, 
   cfg.attrs = at;
   cfg.numAttrs = pdl ? 1 : 0;
   return cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...);
+}
+
+template <typename... P, typename... A>
+cudaError_t launch_pdl(bool pdl, void (*kern)(P...), dim3 grid, cudaStream_t s, A&&... args) {
+  return launch_pdl_shape(pdl, kern, grid, 256, 0, s, std::forward<A>(args)...);
 }
 
 inline unsigned grid_for(const dgfs_dg* h, int nv) {
@@ -210,7 +231,7 @@ cudaError_t run_interp(const dgfs_dg* h, const void* u, int v0, int nv, cudaStre
   a.nv = nv;
   // the interp kernel takes the velocity chunk of the selected residual
   // shape (small meshes: more CTAs)
-  const int vs = kDgShapes[h->shape].vpt, vpt = vs <= 2 ? 2 : vs <= 4 ? 4 : kVpt;
+  const int vs = chunk_of(h->shape) / 8, vpt = vs <= 2 ? 2 : vs <= 4 ? 4 : kVpt;
   const dim3 grid((unsigned)((h->E + 31) / 32), (unsigned)((nv + 8 * vpt - 1) / (8 * vpt)));
   const DgOps<T, U, F, D> ops = make_ops<T, U, F, D>(h);
   if (vpt <= 2) return launch_pdl(true, dg_interp_kernel<T, U, F, D, 2>, grid, s, a, ops);
@@ -234,6 +255,21 @@ cudaError_t launch_rhs(const dgfs_dg* h, const DgArgs<T>& a, int nv, cudaStream_
                     make_ops<T, U, F, D>(h));
 }
 
+template <int U, int F, int D, int VPT>
+cudaError_t launch_rhs_tc(const dgfs_dg* h, const DgArgs<float>& a, int nv, cudaStream_t s) {
+  using TC = DgTc<U, F, D>;
+  constexpr int mb = U <= 9 ? 4 : 2;
+  auto kern = dg_residual_tc_kernel<U, F, D, VPT, mb>;
+  static bool configured = false;  // per instantiation
+  if (!configured) {
+    const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, TC::SMEM);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  const dim3 grid((unsigned)((h->E + 31) / 32), (unsigned)((nv + 4 * VPT - 1) / (4 * VPT)));
+  return launch_pdl_shape(h->nhalo == 0, kern, grid, 128, TC::SMEM, s, a, make_ops<float, U, F, D>(h));
+}
+
 template <typename T, int U, int F, int D>
 cudaError_t run_rhs(const dgfs_dg* h, const void* u, void* out, int v0, int nv, double alpha, const void* A,
                     double beta, const void* B, double gamma, const void* C, cudaStream_t s) {
@@ -248,6 +284,15 @@ cudaError_t run_rhs(const dgfs_dg* h, const void* u, void* out, int v0, int nv, 
   a.gamma = (T)gamma;
   a.v0 = v0;
   a.nv = nv;
+  if constexpr (sizeof(T) == 4) {
+    switch (h->shape - kDgNumShapes) {
+      case 0: return launch_rhs_tc<U, F, D, 8>(h, a, nv, s);
+      case 1: return launch_rhs_tc<U, F, D, 16>(h, a, nv, s);
+      case 2: return launch_rhs_tc<U, F, D, 4>(h, a, nv, s);
+      case 3: return launch_rhs_tc<U, F, D, 32>(h, a, nv, s);
+      default: break;
+    }
+  }
   switch (h->shape) {
     case 1: return launch_rhs<T, U, F, D, 8, 1, 0>(h, a, nv, s);
     case 2: return launch_rhs<T, U, F, D, 8, 1, 2>(h, a, nv, s);
@@ -309,7 +354,7 @@ void free_dg(dgfs_dg* h) {
   if (!h) return;
   void* ptrs[] = {h->smats, h->rcpdjac, h->nrm, h->mag, h->cvx, h->cvy, h->cvz, h->guw, h->gfw, h->bwall,
                   h->part, h->bkind, h->bgroup, h->bfpt, h->bele, h->grefl, h->bcvals, h->bcpart,
-                  h->uf, h->geoblk, h->pblk, h->sfpt, h->sele};
+                  h->uf, h->geoblk, h->pblk, h->sfpt, h->sele, h->err};
   for (void* q : ptrs) cudaFree(q);
   delete h;
 }
@@ -412,6 +457,10 @@ extern "C" int dgfs_dg_create(const dgfs_dg_params* p, dgfs_dg** out) {
         cudaMemcpy(h->bcvals, ones.data(), 2 * nb * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMalloc((void**)&h->bcpart, (size_t)kBcChunks * 2 * nb * sizeof(double)) != cudaSuccess)
       rc = set_error(DGFS_ERR_NOMEM, "boundary value allocation failed");
+  }
+  if (!rc) {
+    if (cudaMalloc((void**)&h->err, sizeof(int)) != cudaSuccess || cudaMemset(h->err, 0, sizeof(int)) != cudaSuccess)
+      rc = set_error(DGFS_ERR_NOMEM, "error flag allocation failed");
   }
   if (!rc) {
     const size_t bytes = (size_t)F * h->ldim_f * esz;
@@ -557,25 +606,53 @@ extern "C" int dgfs_dg_set_halo(dgfs_dg* h, const void* recv) {
 extern "C" int dgfs_dg_num_variants(const dgfs_dg* h, int* count) {
   clear_error();
   if (!h || !count) return set_error(DGFS_ERR_INVALID, "null argument");
-  *count = kDgNumShapes;
+  *count = num_shapes(h);
   return DGFS_OK;
 }
 
 extern "C" int dgfs_dg_variant_info(const dgfs_dg* h, int idx, int* vpt, int* prefetch, int* min_ctas_per_sm) {
   clear_error();
   if (!h || !vpt || !prefetch || !min_ctas_per_sm) return set_error(DGFS_ERR_INVALID, "null argument");
-  if (idx < 0 || idx >= kDgNumShapes) return set_error(DGFS_ERR_INVALID, "variant %d outside 0..%d", idx, kDgNumShapes - 1);
-  const DgShape& sh = kDgShapes[idx];
+  if (idx < 0 || idx >= num_shapes(h))
+    return set_error(DGFS_ERR_INVALID, "variant %d outside 0..%d", idx, num_shapes(h) - 1);
+  const DgShape& sh = shape_of(idx);
   *vpt = sh.vpt;
   *prefetch = sh.pf;
-  *min_ctas_per_sm = sh.mb ? sh.mb : (h->prec == 32 ? (h->U <= 9 ? 3 : 2) : (h->U <= 9 ? 2 : 1));
+  if (tc_shape(idx))
+    *min_ctas_per_sm = h->U <= 9 ? 4 : 2;
+  else
+    *min_ctas_per_sm = sh.mb ? sh.mb : (h->prec == 32 ? (h->U <= 9 ? 3 : 2) : (h->U <= 9 ? 2 : 1));
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_dg_variant_tc(const dgfs_dg* h, int idx, int* tensor_cores) {
+  clear_error();
+  if (!h || !tensor_cores) return set_error(DGFS_ERR_INVALID, "null argument");
+  if (idx < 0 || idx >= num_shapes(h))
+    return set_error(DGFS_ERR_INVALID, "variant %d outside 0..%d", idx, num_shapes(h) - 1);
+  *tensor_cores = tc_shape(idx) ? 1 : 0;
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_dg_status(dgfs_dg* h, void* stream, int* flag) {
+  clear_error();
+  if (!h || !flag) return set_error(DGFS_ERR_INVALID, "null argument");
+  cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+  if (e != cudaSuccess) return set_error(DGFS_ERR_CUDA, "stream: %s", cudaGetErrorString(e));
+  int v = 0;
+  if (cudaMemcpy(&v, h->err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemset(h->err, 0, sizeof(int)) != cudaSuccess)
+    return set_error(DGFS_ERR_CUDA, "error flag: %s", cudaGetErrorString(cudaGetLastError()));
+  *flag = v;
+  if (v) return set_error(DGFS_ERR_CUDA, "a tensor-core DG residual launch gave up waiting for its MMAs (flag %d)", v);
   return DGFS_OK;
 }
 
 extern "C" int dgfs_dg_select(dgfs_dg* h, int idx) {
   clear_error();
   if (!h) return set_error(DGFS_ERR_INVALID, "null handle");
-  if (idx < 0 || idx >= kDgNumShapes) return set_error(DGFS_ERR_INVALID, "variant %d outside 0..%d", idx, kDgNumShapes - 1);
+  if (idx < 0 || idx >= num_shapes(h))
+    return set_error(DGFS_ERR_INVALID, "variant %d outside 0..%d", idx, num_shapes(h) - 1);
   h->shape = idx;
   return DGFS_OK;
 }

@@ -83,6 +83,7 @@ template <typename T> struct DgArgs {
   const T* geoblk;
   const int64_t* pblk;
   const T* halo;           // [nhalo][V] partner face values from other partitions
+  int* err;                // set to 1 when a bounded wait of the tensor-core residual ran out
 };
 
 // Shared-memory row of one element (T values): metric terms S[k][i][kk]

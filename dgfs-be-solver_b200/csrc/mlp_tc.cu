@@ -30,12 +30,21 @@
 #include "../../include/dgfs_b200.h"
 #include "dgfs_internal.h"
 #include "mbarrier.cuh"
+#include "tcgen05.cuh"
 
 namespace {
 
+using dgfs::fence_async_smem;
+using dgfs::idesc_bf16;
 using dgfs::mbar_init;
 using dgfs::mbar_wait_bounded;
+using dgfs::sdesc_sw128;
 using dgfs::smem_u32;
+using dgfs::tc_fence_after;
+using dgfs::tc_fence_before;
+using dgfs::tmem_ld16;
+using dgfs::umma_commit;
+using dgfs::umma_f16;
 
 constexpr int TC_BM = 128;       // MMA M: one tensor-memory lane per row of the tile
 constexpr int TC_BK = 64;        // K slice: one 128-byte swizzle row of BF16
@@ -58,51 +67,6 @@ __device__ __forceinline__ uint32_t sw128(int row, int k) {
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
   __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
   return *reinterpret_cast<uint32_t*>(&h);
-}
-
-// Shared-memory matrix descriptor of a K-major SWIZZLE_128B tile starting at
-// shared address `saddr` (1024-byte aligned, or advanced by a multiple of 32
-// bytes inside the swizzle row for the MMA's K step): leading byte offset 16
-// (unused by swizzled K-major layouts), stride byte offset 1024 (8-row
-// groups), descriptor version 1, layout type 2 (128-byte swizzle).
-__device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr) {
-  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
-         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
-}
-
-// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both
-// K-major, M x N.
-__host__ __device__ constexpr uint32_t idesc_bf16(int m, int n) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
-}
-
-__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
-      "l"(a), "l"(b), "r"(idesc), "r"(acc)
-      : "memory");
-}
-__device__ __forceinline__ void umma_commit(uint64_t* bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-               : "memory");
-}
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-      "%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 // One K slice of an operand held in registers between its global loads and
@@ -255,12 +219,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     *drain_up = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(BN)
-                 : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-  }
+  if (warp == 0) dgfs::tmem_alloc(tmem_slot, BN);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -293,7 +252,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       const uint32_t sa = smem_u32(ta), sb = smem_u32(tb);
 #pragma unroll
       for (int j = 0; j < TC_BK / TC_UK; ++j)
-        umma_bf16(tmem, sdesc_sw128(sa + j * TC_UK * 2), sdesc_sw128(sb + j * TC_UK * 2), IDESC,
+        umma_f16(tmem, sdesc_sw128(sa + j * TC_UK * 2), sdesc_sw128(sb + j * TC_UK * 2), IDESC,
                   (kc > 0 || j > 0) ? 1u : 0u);
       umma_commit(&bars[s]);
     }
@@ -335,7 +294,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   __syncthreads();
   if (warp == 0) {
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN) : "memory");
+    dgfs::tmem_dealloc(tmem, BN);
   }
 }
 

@@ -70,6 +70,8 @@ _lib.declare('dgfs_dg_num_variants', c_int, [c_void_p, c_ip])
 _lib.declare('dgfs_dg_variant_info', c_int, [c_void_p, c_int, c_ip, c_ip,
                                              c_ip])
 _lib.declare('dgfs_dg_select', c_int, [c_void_p, c_int])
+_lib.declare('dgfs_dg_variant_tc', c_int, [c_void_p, c_int, c_ip])
+_lib.declare('dgfs_dg_status', c_int, [c_void_p, c_void_p, c_ip])
 _lib.declare('dgfs_dg_bcvals', c_int, [c_void_p, c_dp, c_int])
 _lib.declare('dgfs_dg_fpts', c_int, [c_void_p, ct.POINTER(c_void_p),
                                      ct.POINTER(c_ll)])
@@ -392,19 +394,31 @@ class DGFSSystem:
     def dg_variants(self):
         """Compiled residual launch shapes: velocities per warp, whether
         the Runge-Kutta terms are loaded ahead of the flux work, CTAs per SM
-        of the register budget."""
+        of the register budget, and whether the element-operator
+        contraction runs on the tensor cores."""
         n = c_int()
         _lib.check(self._lib.dgfs_dg_num_variants(self._dg, ct.byref(n)),
                    'dgfs_dg_num_variants')
         out = []
         for i in range(n.value):
-            v = [c_int() for _ in range(3)]
+            v = [c_int() for _ in range(4)]
             _lib.check(self._lib.dgfs_dg_variant_info(
-                self._dg, i, *[ct.byref(x) for x in v]),
+                self._dg, i, *[ct.byref(x) for x in v[:3]]),
                 'dgfs_dg_variant_info')
+            _lib.check(self._lib.dgfs_dg_variant_tc(
+                self._dg, i, ct.byref(v[3])), 'dgfs_dg_variant_tc')
             out.append(dict(vpt=v[0].value, prefetch=v[1].value,
-                            min_ctas_per_sm=v[2].value))
+                            min_ctas_per_sm=v[2].value,
+                            tensor_cores=bool(v[3].value)))
         return out
+
+    def dg_status(self):
+        """Raise if a bounded wait of the tensor-core residual ran out
+        (synchronises the stream; clears the flag)."""
+        flag = c_int()
+        _lib.check(self._lib.dgfs_dg_status(self._dg, self.backend.stream,
+                                            ct.byref(flag)),
+                   'dgfs_dg_status')
 
     def select_dg(self, idx):
         _lib.check(self._lib.dgfs_dg_select(self._dg, int(idx)),
@@ -439,6 +453,7 @@ class DGFSSystem:
             torch.cuda.synchronize(dev)
             ms[i] = sum(e0.elapsed_time(e1) for e0, e1 in ev)/reps
         del flush
+        self.dg_status()
         self.select_dg(min(ms, key=ms.get))
         return ms
 

@@ -367,6 +367,14 @@ DGFS_API int dgfs_dg_num_variants(const dgfs_dg* h, int* count);
 DGFS_API int dgfs_dg_variant_info(const dgfs_dg* h, int idx, int* vpt,
                                   int* prefetch, int* min_ctas_per_sm);
 DGFS_API int dgfs_dg_select(dgfs_dg* h, int idx);
+/* 1 when shape idx runs the element-operator contraction on the tensor
+ * cores (FP32 handles: tcgen05.mma kind::tf32 with operands split into
+ * two TF32 parts, FP32 accuracy), 0 for the SIMT shapes. */
+DGFS_API int dgfs_dg_variant_tc(const dgfs_dg* h, int idx, int* tensor_cores);
+/* Synchronise the stream and read (and clear) the bounded-wait flag of the
+ * tensor-core residual: *flag = 1 and DGFS_ERR_CUDA when a launch gave up
+ * waiting for its MMAs. */
+DGFS_API int dgfs_dg_status(dgfs_dg* h, void* stream, int* flag);
 
 /* Copy the 2*nbfpts diffuse-wall sums to host memory (synchronous). */
 DGFS_API int dgfs_dg_bcvals(const dgfs_dg* h, double* host, int n);

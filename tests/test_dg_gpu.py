@@ -253,8 +253,10 @@ def test_invmass_matches_reference_operator(precision, order):
 @pytest.mark.parametrize('order', [2, 3])
 def test_every_residual_shape_matches_oracle(precision, order):
     """Each compiled residual launch shape (velocities per warp, prefetch
-    of the Runge-Kutta terms, register budget) gives the oracle's
-    out = a A + b B + g (L(u) + C), and autotune_dg keeps one of them."""
+    of the Runge-Kutta terms, register budget; in FP32 also the shapes
+    whose element-operator contraction runs on the tensor cores) gives the
+    oracle's out = a A + b B + g (L(u) + C), and autotune_dg keeps one of
+    them."""
     cfg, m = _cfg(precision, order=order), _mesh(order)
     dg, sh, geo, vm = dg_setup(cfg, m)
     u = _states(vm, sh.nupts, geo.neles, seed=order + 20)
@@ -265,12 +267,16 @@ def test_every_residual_shape_matches_oracle(precision, order):
     R = dg.rhs(u_used, uf)
     ref = 0.3*u_used + 0.7*u_used + 2e-3*(R + u_used)
     s.updatebc(0.0, 0, 1, 0, 0)
-    for i in range(len(s.dg_variants())):
+    variants = s.dg_variants()
+    ntc = sum(v['tensor_cores'] for v in variants)
+    assert ntc == (4 if precision == 'single' else 0)
+    for i in range(len(variants)):
         s.select_dg(i)
         s.updatebc(0.0, 0, 1, 0, 0)       # the shape's interp chunk too
         s.rk_stage(0, 1, 0.3, 0, 0.7, 0, 2e-3, 0, interp=False)
         torch.cuda.synchronize()
         assert rel_err(s.bank[1].get(), ref) < TOL[precision], i
+    s.dg_status()
     ms = s.autotune_dg(0, 2)
     assert set(ms) == set(range(len(s.dg_variants())))
     assert s._dg_shape == min(ms, key=ms.get)
