@@ -6,7 +6,7 @@
 //   dgfs_mlp_gemm    C = act(op(A) op(B) + bias) [+ C], generic strides,
 //                    A FP32, B FP32 or BF16; act = identity or tanh (the
 //                    pre-activation can be kept for the backward pass)
-//   dgfs_mlp_tanh_bwd  dZ = dH (1 - H^2)
+//   dgfs_mlp_tanh_bwd  dZ = dH (1 - H^2) (and its BF16 copy: _bf16)
 //   dgfs_mlp_colsum  bias gradient (column sums, fixed order)
 //   dgfs_mlp_mse     loss = mean over rows and the first n_used columns of
 //                    w_j (Y - T)^2, and dY
@@ -120,9 +120,12 @@ __global__ void __launch_bounds__(NTH) gemm_kernel(int M, const int* __restrict_
 }
 
 __global__ void tanh_bwd_kernel(long long n, const float* __restrict__ H, const float* __restrict__ dH,
-                                float* __restrict__ dZ) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    dZ[i] = dH[i] * (1.f - H[i] * H[i]);
+                                float* __restrict__ dZ, __nv_bfloat16* __restrict__ dZb) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float z = dH[i] * (1.f - H[i] * H[i]);
+    dZ[i] = z;
+    if (dZb) dZb[i] = __float2bfloat16_rn(z);
+  }
 }
 
 // out[n] = sum_m X[m][n] in a fixed order (deterministic): a CTA of 32 x 32
@@ -303,7 +306,15 @@ extern "C" int dgfs_mlp_gemm(int M, int N, int K, const float* A, long long sam,
 extern "C" int dgfs_mlp_tanh_bwd(long long n, const float* H, const float* dH, float* dZ, void* stream) {
   dgfs::clear_error();
   if (n < 1 || !H || !dH || !dZ) return dgfs::set_error(DGFS_ERR_INVALID, "bad arguments");
-  tanh_bwd_kernel<<<blocks_for(n), 256, 0, (cudaStream_t)stream>>>(n, H, dH, dZ);
+  tanh_bwd_kernel<<<blocks_for(n), 256, 0, (cudaStream_t)stream>>>(n, H, dH, dZ, nullptr);
+  return launched("tanh_bwd");
+}
+
+extern "C" int dgfs_mlp_tanh_bwd_bf16(long long n, const float* H, const float* dH, float* dZ, void* dZb,
+                                      void* stream) {
+  dgfs::clear_error();
+  if (n < 1 || !H || !dH || !dZ || !dZb) return dgfs::set_error(DGFS_ERR_INVALID, "bad arguments");
+  tanh_bwd_kernel<<<blocks_for(n), 256, 0, (cudaStream_t)stream>>>(n, H, dH, dZ, (__nv_bfloat16*)dZb);
   return launched("tanh_bwd");
 }
 

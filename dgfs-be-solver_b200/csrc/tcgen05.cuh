@@ -54,6 +54,31 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// Shared-memory matrix descriptor of an MN-major SWIZZLE_128B tile: each
+// K row holds 64 BF16 of the M (or N) axis in 128 B, 8-row groups of K are
+// 1024 B apart (stride byte offset), and the 64-wide M groups `lbo` bytes
+// apart (leading byte offset). The MMA's K step of 16 rows advances the
+// start by 2048 bytes.
+__device__ __forceinline__ uint64_t sdesc_sw128_mn(uint32_t saddr, uint32_t lbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)(1024 >> 4) << 32) | ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+// kind::f16 with BF16 operands, FP32 accumulator, M x N; a_mn / b_mn select
+// the MN-major layout of A / B (K-major otherwise).
+__host__ __device__ constexpr uint32_t idesc_bf16_major(int m, int n, bool a_mn, bool b_mn) {
+  return idesc_bf16(m, n) | (a_mn ? (1u << 15) : 0u) | (b_mn ? (1u << 16) : 0u);
+}
+
+// 2D tiled TMA load of the box at (x = innermost element, y = row) of the
+// tensor map into shared memory, completing on `bar` (no multicast).
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const void* tmap, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
 // Instruction descriptor of kind::tf32: FP32 accumulator, TF32 A and B
 // (FP32 bit patterns whose low 13 mantissa bits the tensor core ignores),
 // both K-major, M x N.

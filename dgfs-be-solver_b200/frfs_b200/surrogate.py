@@ -71,8 +71,14 @@ _lib.declare('dgfs_mlp_gemm_tc', c_int,
              [c_int, c_int, c_int, c_void_p, c_ll, c_ll, c_void_p, c_int,
               c_ll, c_ll, c_void_p, c_void_p, c_void_p, c_ll, c_int, c_int,
               c_void_p, c_void_p])
+_lib.declare('dgfs_mlp_gemm_bf16', c_int,
+             [c_int, c_int, c_int, c_void_p, c_int, c_ll, c_void_p, c_int,
+              c_ll, c_void_p, c_void_p, c_void_p, c_void_p, c_ll, c_int,
+              c_int, c_void_p, c_void_p])
 _lib.declare('dgfs_mlp_tanh_bwd', c_int, [c_ll, c_void_p, c_void_p,
                                           c_void_p, c_void_p])
+_lib.declare('dgfs_mlp_tanh_bwd_bf16', c_int, [c_ll, c_void_p, c_void_p,
+                                               c_void_p, c_void_p, c_void_p])
 _lib.declare('dgfs_mlp_colsum', c_int, [c_int, c_int, c_void_p, c_ll,
                                         c_void_p, c_int, c_void_p])
 _lib.declare('dgfs_mlp_mse', c_int, [c_int, c_int, c_int, c_void_p, c_void_p,
@@ -173,10 +179,14 @@ class MLP:
     [batch][features].
 
     The parameters live in one flat buffer (weights first, then biases) so
-    that one Adam launch updates all of them.  With ``tc`` the training
-    products (forward with ``keep``, backward) run on the tensor cores
-    (dgfs_mlp_gemm_tc: BF16 operands, FP32 accumulation); inference keeps
-    the FP32-activation SIMT product."""
+    that one Adam launch updates all of them.  ``tc`` chooses the training
+    products (forward with ``keep``, backward): 'tma' (the default; True)
+    keeps BF16 copies of the activations and gradients, written by the
+    kernels that produce them, and multiplies them with dgfs_mlp_gemm_bf16
+    (TMA loads into the tensor cores); 'staged' rounds FP32 operands as it
+    stages them (dgfs_mlp_gemm_tc); False uses the SIMT product.  Both
+    tensor-core modes round the same operands to BF16 and accumulate in
+    FP32.  Inference keeps the FP32-activation SIMT product."""
 
     names = ('W1', 'b1', 'W2', 'b2', 'W3', 'b3', 'W4', 'b4', 'Ws')
     _order = ('W1', 'W2', 'W3', 'W4', 'Ws', 'b1', 'b2', 'b3', 'b4')
@@ -185,7 +195,8 @@ class MLP:
                  tc=True):
         self.device = device
         self.nin, self.width, self.nout = nin, width, nout
-        self.tc = bool(tc)
+        self.tc = 'tma' if tc is True else (tc or False)
+        assert self.tc in (False, 'staged', 'tma'), tc
         rng = np.random.default_rng(seed)
         shapes = {'W1': (nin, width), 'b1': (width,), 'W2': (width, width),
                   'b2': (width,), 'W3': (width, width), 'b3': (width,),
@@ -275,13 +286,97 @@ class MLP:
                                  'a bounded wait of the tensor-core GEMM '
                                  'ran out')
 
+    def _gemm_bf16(self, A, a_mn, lda, B, b_mn, ldb, C, M, N, K, bias=None,
+                   act=0, acc=0, Cb=None):
+        _lib.check(_lib.load().dgfs_mlp_gemm_bf16(
+            M, N, K, _p(A), a_mn, lda, _p(B), b_mn, ldb, _p(bias), None,
+            _p(C), _p(Cb), N, act, acc, _p(self.err), self._s),
+            'dgfs_mlp_gemm_bf16')
+
+    def _to_bf16(self, X, Xb):
+        _lib.check(_lib.load().dgfs_f32_to_bf16(X.numel(), _p(X), _p(Xb),
+                                                self._s), 'dgfs_f32_to_bf16')
+
+    def _forward_tma(self, X):
+        """Training forward pass on BF16 operands: every layer writes its
+        activations in FP32 (for the backward pass) and in BF16 (the next
+        product's operand).  Weights W[in][out] are the MN-major B operand
+        as stored."""
+        B = X.shape[0]
+        nin, wd, nout = self.nin, self.width, self.nout
+        ws, wb, w = self.ws, self.wb, self.w
+        Xb = ws.get('trainXb', (B, nin), torch.bfloat16)
+        H = [ws.get('trainH%d' % i, (B, wd)) for i in (1, 2, 3)]
+        Hb = [ws.get('trainH%db' % i, (B, wd), torch.bfloat16)
+              for i in (1, 2, 3)]
+        Y = ws.get('trainY', (B, nout))
+        self._to_bf16(X, Xb)
+        self._gemm_bf16(Xb, 0, nin, wb['W1'], 1, wd, H[0], B, wd, nin,
+                        w['b1'], act=1, Cb=Hb[0])
+        self._gemm_bf16(Hb[0], 0, wd, wb['W2'], 1, wd, H[1], B, wd, wd,
+                        w['b2'], act=1, Cb=Hb[1])
+        self._gemm_bf16(Hb[1], 0, wd, wb['W3'], 1, wd, H[2], B, wd, wd,
+                        w['b3'], act=1, Cb=Hb[2])
+        self._gemm_bf16(Hb[2], 0, wd, wb['W4'], 1, nout, Y, B, nout, wd,
+                        w['b4'])
+        self._gemm_bf16(Xb, 0, nin, wb['Ws'], 1, nout, Y, B, nout, nin,
+                        acc=1)
+        self._cache = (X, H[0], H[1], H[2])
+        self._cache_bf16 = (Xb, Hb[0], Hb[1], Hb[2])
+        return Y
+
+    def _backward_tma(self, dY):
+        """Backward pass on the BF16 copies: weight gradients g = A^T D
+        read both operands MN-major (as stored), input gradients D W^T read
+        W K-major (as stored)."""
+        lib = _lib.load()
+        X, H1, H2, H3 = self._cache
+        Xb, H1b, H2b, H3b = self._cache_bf16
+        B = X.shape[0]
+        nin, wd, nout = self.nin, self.width, self.nout
+        g, wb, ws = self.g, self.wb, self.ws
+        dYb = ws.get('dYb', (B, nout), torch.bfloat16)
+        dH = ws.get('dH', (B, wd))
+        dZ = ws.get('dZ', (B, wd))
+        dZb = ws.get('dZb', (B, wd), torch.bfloat16)
+        self._to_bf16(dY, dYb)
+
+        def wgrad(Ab, Db, name, k, n):
+            self._gemm_bf16(Ab, 1, k, Db, 1, n, g[name], k, n, B)
+
+        def bgrad(D, name, n):
+            _lib.check(lib.dgfs_mlp_colsum(B, n, _p(D), n, _p(g[name]), 0,
+                                           self._s), 'dgfs_mlp_colsum')
+
+        def through(Db, nd, W, H):
+            self._gemm_bf16(Db, 0, nd, W, 0, nd, dH, B, wd, nd)
+            _lib.check(lib.dgfs_mlp_tanh_bwd_bf16(
+                dH.numel(), _p(H), _p(dH), _p(dZ), _p(dZb), self._s),
+                'dgfs_mlp_tanh_bwd_bf16')
+
+        wgrad(H3b, dYb, 'W4', wd, nout)
+        bgrad(dY, 'b4', nout)
+        wgrad(Xb, dYb, 'Ws', nin, nout)
+        through(dYb, nout, wb['W4'], H3)
+        wgrad(H2b, dZb, 'W3', wd, wd)
+        bgrad(dZ, 'b3', wd)
+        through(dZb, wd, wb['W3'], H2)
+        wgrad(H1b, dZb, 'W2', wd, wd)
+        bgrad(dZ, 'b2', wd)
+        through(dZb, wd, wb['W2'], H1)
+        wgrad(Xb, dZb, 'W1', nin, wd)
+        bgrad(dZ, 'b1', wd)
+        return g
+
     def forward(self, X, keep=False, mcount=None):
         """Y = W4 tanh(W3 tanh(W2 tanh(W1 X + b1) + b2) + b3) + b4 + Ws X.
         With mcount (a device int), only the first *mcount rows."""
+        if keep and self.tc == 'tma' and mcount is None:
+            return self._forward_tma(X)
         B = X.shape[0]
         nin, wd, nout = self.nin, self.width, self.nout
         tag = 'train' if keep else 'infer'
-        tc = keep and self.tc and mcount is None
+        tc = keep and self.tc == 'staged' and mcount is None
         H1 = self.ws.get(tag + 'H1', (B, wd))
         H2 = self.ws.get(tag + 'H2', (B, wd))
         H3 = self.ws.get(tag + 'H3', (B, wd))
@@ -307,12 +402,14 @@ class MLP:
         the activations, input gradients through the BF16 weights that the
         forward pass used (on the tensor cores with ``tc``: activations and
         gradients rounded to BF16 as they are staged)."""
+        if self.tc == 'tma':
+            return self._backward_tma(dY)
         lib = _lib.load()
         X, H1, H2, H3 = self._cache
         B = X.shape[0]
         nin, wd, nout = self.nin, self.width, self.nout
         g, wb = self.g, self.wb
-        tc = self.tc
+        tc = self.tc == 'staged'
         dH = self.ws.get('dH', (B, wd))
         dZ = self.ws.get('dZ', (B, wd))
 

@@ -249,7 +249,10 @@ def run_study(ini, device='cuda:0', runs=5, near_runs=10, steps=100,
         'train_loss_first': hist[0], 'train_loss_last': hist[-1],
         'harvest_s': t_harvest, 'train_s': t_train,
         'train_tflops': train_tflops,
-        'train_products': 'tensor cores' if sur.mlp.tc else 'SIMT',
+        'train_products': {'tma': 'tensor cores, TMA-fed BF16 operands',
+                           'staged': 'tensor cores, operands staged by the '
+                                     'threads',
+                           False: 'SIMT'}[sur.mlp.tc],
         'epochs': epochs, 'runs': runs, 'near_runs': near_runs,
         'steps_per_run': steps,
         'nsteps': nsteps, 'threshold': threshold,

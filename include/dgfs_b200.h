@@ -488,9 +488,27 @@ DGFS_API int dgfs_mlp_gemm_tc(int M, int N, int K, const float* A,
                               const float* bias, float* Z, float* C,
                               long long ldc, int act, int accumulate,
                               int* err, void* stream);
+/* BF16 operands already in memory, loaded by TMA into the tensor cores'
+ * swizzled layout (tcgen05.mma kind::f16, FP32 accumulation): op(A) is
+ * M x K, element (m, k) at A[m lda + k] (a_mn = 0) or A[k lda + m]
+ * (a_mn = 1); op(B) is K x N, element (k, n) at B[n ldb + k] (b_mn = 0) or
+ * B[k ldb + n] (b_mn = 1). A and B 16-byte aligned, lda and ldb multiples
+ * of 8. C[m ldc + n] = act(sum + bias[n]) (+ C); Z (optional) the
+ * pre-activation; Cb (optional) C rounded to BF16, with the same ldc. err
+ * as for dgfs_mlp_gemm_tc. */
+DGFS_API int dgfs_mlp_gemm_bf16(int M, int N, int K, const void* A, int a_mn,
+                                long long lda, const void* B, int b_mn,
+                                long long ldb, const float* bias, float* Z,
+                                float* C, void* Cb, long long ldc, int act,
+                                int accumulate, int* err, void* stream);
 /* dZ = dH (1 - H^2) */
 DGFS_API int dgfs_mlp_tanh_bwd(long long n, const float* H, const float* dH,
                                float* dZ, void* stream);
+/* The same, also writing dZ rounded to BF16 into dZb (the operand of the
+ * next tensor-core product). */
+DGFS_API int dgfs_mlp_tanh_bwd_bf16(long long n, const float* H,
+                                    const float* dH, float* dZ, void* dZb,
+                                    void* stream);
 /* out[n] (+)= sum_m X[m*ldx+n], fixed order */
 DGFS_API int dgfs_mlp_colsum(int M, int N, const float* X, long long ldx,
                              float* out, int accumulate, void* stream);

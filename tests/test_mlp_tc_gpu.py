@@ -1,9 +1,11 @@
 # -*- coding: utf-8 -*-
-"""The tensor-core GEMM of the surrogate's training step (GPU):
-dgfs_mlp_gemm_tc against the FP64 product of the same operands rounded to
-BF16 (nearest even), for every operand layout the training step uses
-(activations row-major, weights as stored and transposed, both operands of
-the weight gradient transposed), ragged M, N and K, bias, tanh, the
+"""The tensor-core GEMMs of the surrogate's training step (GPU):
+dgfs_mlp_gemm_tc (FP32 operands rounded as they are staged) against the
+FP64 product of the same operands rounded to BF16 (nearest even), for every
+operand layout the training step uses (activations row-major, weights as
+stored and transposed, both operands of the weight gradient transposed);
+dgfs_mlp_gemm_bf16 (BF16 operands loaded by TMA) for every combination of
+K-major and MN-major operands. Ragged M, N and K, bias, tanh, the
 pre-activation output and accumulation into C.
 
 Tolerance: the products of BF16 operands are exact in FP32, so the only
@@ -122,3 +124,66 @@ def test_matches_simt_gemm_on_rounded_operands():
         'dgfs_mlp_gemm')
     torch.cuda.synchronize()
     _check(C, C2.double())
+
+
+def _run_bf16(M, N, K, A, a_mn, lda, B, b_mn, ldb, bias=None, act=0, acc=0,
+              C0=None, keep_z=False, want_cb=False):
+    lib = _lib.load()
+    C = (C0.clone() if C0 is not None else
+         torch.zeros(M, N, dtype=torch.float32, device=DEV))
+    Z = torch.zeros(M, N, dtype=torch.float32, device=DEV) if keep_z else None
+    Cb = torch.zeros(M, N, dtype=torch.bfloat16, device=DEV) if want_cb else None
+    err = torch.zeros(1, dtype=torch.int32, device=DEV)
+    _lib.check(lib.dgfs_mlp_gemm_bf16(
+        M, N, K, A.data_ptr(), a_mn, lda, B.data_ptr(), b_mn, ldb,
+        None if bias is None else bias.data_ptr(),
+        None if Z is None else Z.data_ptr(), C.data_ptr(),
+        None if Cb is None else Cb.data_ptr(), N, act, acc, err.data_ptr(),
+        torch.cuda.current_stream().cuda_stream), 'dgfs_mlp_gemm_bf16')
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    return C, Z, Cb
+
+
+@pytest.mark.parametrize('a_mn', [0, 1])
+@pytest.mark.parametrize('b_mn', [0, 1])
+@pytest.mark.parametrize('M,N,K', [(300, 512, 256), (70, 192, 72),
+                                   (2400, 1024, 128)])
+def test_tma_gemm_layouts(a_mn, b_mn, M, N, K):
+    """Every combination of K-major and MN-major BF16 operands, loaded by
+    TMA, against the FP64 product; ragged M, N and K (zero fill outside the
+    tensor maps); bias, tanh, the pre-activation and the BF16 copy."""
+    g = torch.Generator(device='cpu').manual_seed(M + 3*N + 7*K + a_mn + 2*b_mn)
+    Am = torch.randn(M, K, generator=g).to(torch.bfloat16)
+    Bm = torch.randn(K, N, generator=g).to(torch.bfloat16)
+    lda = -(-(M if a_mn else K)//8)*8 + 8     # padded leading dimensions
+    ldb = -(-(N if b_mn else K)//8)*8
+    As = torch.zeros((K if a_mn else M), lda, dtype=torch.bfloat16)
+    Bs = torch.zeros((K if b_mn else N), ldb, dtype=torch.bfloat16)
+    if a_mn:
+        As[:, :M] = Am.T
+    else:
+        As[:, :K] = Am
+    if b_mn:
+        Bs[:, :N] = Bm
+    else:
+        Bs[:, :K] = Bm.T
+    b = (0.1*torch.randn(N, generator=g)).to(DEV)
+    C, Z, Cb = _run_bf16(M, N, K, As.to(DEV), a_mn, lda, Bs.to(DEV), b_mn,
+                         ldb, bias=b, act=1, keep_z=True, want_cb=True)
+    z = Am.double().to(DEV) @ Bm.double().to(DEV) + b.double()
+    _check(Z, z)
+    _check(C, torch.tanh(z))
+    assert torch.equal(Cb, C.to(torch.bfloat16))
+
+
+def test_tma_gemm_accumulates():
+    """The weight-gradient shape: both operands MN-major, K = 1024 rows
+    (16 slices through the 4-slot ring), accumulated into C."""
+    M, N, K = 256, 128, 1024
+    g = torch.Generator(device='cpu').manual_seed(21)
+    X = torch.randn(K, M, generator=g).to(torch.bfloat16).to(DEV)
+    D = torch.randn(K, N, generator=g).to(torch.bfloat16).to(DEV)
+    C0 = torch.randn(M, N, generator=g).to(DEV)
+    C, _, _ = _run_bf16(M, N, K, X, 1, M, D, 1, N, acc=1, C0=C0)
+    _check(C, C0.double() + X.double().T @ D.double())

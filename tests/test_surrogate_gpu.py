@@ -290,7 +290,7 @@ def _bf16(t):
     return t.to(torch.bfloat16).to(torch.float64).cpu().numpy()
 
 
-@pytest.mark.parametrize('tc', [False, True])
+@pytest.mark.parametrize('tc', [False, 'staged', 'tma'])
 def test_mlp_gradients_match_oracle(tc):
     """SIMT products (FP32 activations) against the FP64 oracle with the
     same BF16 weights at 1e-4.  Tensor-core products (BF16 operands)
