@@ -148,7 +148,7 @@ def _run_bf16(M, N, K, A, a_mn, lda, B, b_mn, ldb, bias=None, act=0, acc=0,
 @pytest.mark.parametrize('a_mn', [0, 1])
 @pytest.mark.parametrize('b_mn', [0, 1])
 @pytest.mark.parametrize('M,N,K', [(300, 512, 256), (70, 192, 72),
-                                   (2400, 1024, 128)])
+                                   (2400, 1024, 128), (4096, 512, 512)])
 def test_tma_gemm_layouts(a_mn, b_mn, M, N, K):
     """Every combination of K-major and MN-major BF16 operands, loaded by
     TMA, against the FP64 product; ragged M, N and K (zero fill outside the
