@@ -154,8 +154,10 @@ def test_tma_gemm_layouts(a_mn, b_mn, M, N, K):
     TMA, against the FP64 product; ragged M, N and K (zero fill outside the
     tensor maps); bias, tanh, the pre-activation and the BF16 copy."""
     g = torch.Generator(device='cpu').manual_seed(M + 3*N + 7*K + a_mn + 2*b_mn)
+    # weights scaled by 1/sqrt(K) as in a layer, so that tanh is tested
+    # where it is not saturated
     Am = torch.randn(M, K, generator=g).to(torch.bfloat16)
-    Bm = torch.randn(K, N, generator=g).to(torch.bfloat16)
+    Bm = (torch.randn(K, N, generator=g)/np.sqrt(K)).to(torch.bfloat16)
     lda = -(-(M if a_mn else K)//8)*8 + 8     # padded leading dimensions
     ldb = -(-(N if b_mn else K)//8)*8
     As = torch.zeros((K if a_mn else M), lda, dtype=torch.bfloat16)
