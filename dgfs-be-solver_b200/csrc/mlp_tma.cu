@@ -15,8 +15,8 @@
 // four 128 x BN x 16 tcgen05.mma (kind::f16) and commits them to the slot's
 // `empty` mbarrier, which the producer waits on before refilling the slot.
 // The accumulator lives in BN tensor-memory columns; after the last commit
-// (`done`) the four warps read it back (warp w: rows 32w..32w+31) and write
-// the epilogue. Every wait is bounded (1 s); on expiry the kernel sets *err,
+// (`done`) the four warps read it back (warp w: rows 32w..32w+31), stage it
+// in the ring's shared memory and write the epilogue row by row. Every wait is bounded (1 s); on expiry the kernel sets *err,
 // stops issuing, drains what it issued (bounded) and frees its tensor
 // memory.
 #include <cuda.h>
@@ -48,6 +48,8 @@ struct TmaGeom {
   static constexpr int B_BYTES = BN * TB_BK * 2;
   static constexpr int STAGE = A_BYTES + B_BYTES;
   static constexpr int SMEM = 1024 + TB_STAGES * STAGE + 256;
+  // the epilogue's staging (4 warps x 32 rows x BN + 1 floats) reuses the ring
+  static_assert(4 * 32 * (BN + 1) * 4 <= TB_STAGES * STAGE, "epilogue staging fits in the ring");
 };
 
 // Issue the TMA loads of K slice kc into a slot. A K-major operand of R
@@ -152,26 +154,36 @@ __global__ void __launch_bounds__(TB_THREADS, 1)
       mbar_wait_bounded(&full[kc % TB_STAGES], (uint32_t)((kc / TB_STAGES) & 1), err, drain_up);
   }
   if (!*(volatile int*)gave_up && !*(volatile int*)drain_up) {
-    const int m = m0 + warp * 32 + lane;
-    const bool row_ok = m < M;
+    // The ring's shared memory is free now (every MMA and every load has
+    // completed): each warp stages its 32 rows x BN accumulator columns
+    // there (row stride BN + 1, so both the row-wise writes and the
+    // column-wise reads are free of bank conflicts), then writes whole rows
+    // with consecutive lanes on consecutive columns (coalesced).
+    float* stg = reinterpret_cast<float*>(smem) + warp * 32 * (BN + 1);
 #pragma unroll 1
     for (int j0 = 0; j0 < BN; j0 += 16) {
       float v[16];
       __syncwarp();  // tcgen05.ld is warp-collective
       tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)j0, v);
-      if (row_ok && n0 + j0 < N) {
-        float* crow = C + (long long)m * ldc;
 #pragma unroll
-        for (int jj = 0; jj < 16; ++jj) {
-          const int n = n0 + j0 + jj;
-          if (n < N) {
-            float z = v[jj] + (bias ? __ldg(bias + n) : 0.f);
-            if (accumulate) z += crow[n];
-            if (Z) Z[(long long)m * ldc + n] = z;
-            const float c = act == 1 ? tanhf(z) : z;
-            crow[n] = c;
-            if (Cb) Cb[(long long)m * ldc + n] = __float2bfloat16_rn(c);
-          }
+      for (int jj = 0; jj < 16; ++jj) stg[lane * (BN + 1) + j0 + jj] = v[jj];
+    }
+    __syncwarp();
+#pragma unroll 1
+    for (int r = 0; r < 32; ++r) {
+      const int m = m0 + warp * 32 + r;
+      if (m >= M) break;  // uniform over the warp
+      const long long row = (long long)m * ldc;
+#pragma unroll
+      for (int c = lane; c < BN; c += 32) {
+        const int n = n0 + c;
+        if (n < N) {
+          float z = stg[r * (BN + 1) + c] + (bias ? __ldg(bias + n) : 0.f);
+          if (accumulate) z += C[row + n];
+          if (Z) Z[row + n] = z;
+          const float cv = act == 1 ? tanhf(z) : z;
+          C[row + n] = cv;
+          if (Cb) Cb[row + n] = __float2bfloat16_rn(cv);
         }
       }
     }
