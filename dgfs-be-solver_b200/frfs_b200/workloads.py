@@ -97,7 +97,8 @@ soln-pts = gauss-legendre
 
 
 def relax0d_n16(precision='double'):
-    """Space-homogeneous relaxation; BASELINE configuration 1."""
+    """Space-homogeneous relaxation at one point: N = 16, Nrho = 8, M = 6,
+    FP64, from the bimodal state of two Maxwellians at u = +-1.5."""
     u0 = _u0()
     ini = _BASE.format(precision=precision, Nv=16, NvBatchSize=4096, Nrho=8,
                        H0=1e-3, rho0=1.5e-3, molarMass0=_MOLAR_MASS,
@@ -116,7 +117,8 @@ uz = 0.0
 
 
 def couette_n24(precision='double', M=16, nele=64, copies=1):
-    """1D/3V Couette slab as a 64x1 quad strip; BASELINE configuration 2.
+    """1D/3V Couette slab as a 64x1 quad strip (576 points at p = 2,
+    N = 24, Nrho = 12, M = 16, walls at U = +-0.5).
     ``copies`` > 1 widens the slab to that many slab widths (nele elements
     each, the same element size) for weak scaling over partitions."""
     u0 = _u0()
@@ -164,7 +166,7 @@ uz = 0.0
 
 def channel_n32(precision='double', nx=48, ny=24, Nv=32, Nrho=16, M=24,
                 copies=1):
-    """2D/3V channel on 48x24 quads; BASELINE configuration 3.  ``copies``
+    """2D/3V channel on 48x24 quads (10,368 points at p = 2, N = 32).  ``copies``
     > 1 lengthens the periodic channel to that many channel lengths (nx
     elements each) for weak scaling over partitions."""
     ini = _BASE.format(precision=precision, Nv=Nv, NvBatchSize=Nv**3,
@@ -221,7 +223,7 @@ def _ogrid_hmin(ntheta, nr, stretch, r_in=0.5, r_out=4.0):
 
 def cylinder_n32(precision='single', ntheta=40, nr=16, order=3, Nv=32,
                  Nrho=16, M=24, mach=2.0, dt=None, tend=0.01):
-    """Cylinder in a Mach-2 crossflow (BASELINE configuration 5) on a
+    """Cylinder in a Mach-2 crossflow on a
     quadrilateral O-grid, p=3, N=32, Nrho=16, M=24 (M=32 has no tabulated
     symmetric design; the 48-point rule of M=24 is the nearest).  Cylinder
     of radius 0.5 with a diffuse isothermal wall (``dgfs-wall-diffuse-cyl``,

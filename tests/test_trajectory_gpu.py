@@ -78,7 +78,8 @@ def _compare(s, bankidx, ref, vm):
 @pytest.mark.parametrize('stepper', [StdTVDRK2DGFSStepper,
                                      StdEulerDGFSStepper])
 def test_relaxation_50_steps(stepper):
-    """50 steps of dt = 0.01 in FP64."""
+    """The space-homogeneous relaxation (N = 16): 50 steps of dt = 0.01
+    in FP64."""
     cfg = config('relax0d-n16', 'double')
     m = mgen.quad_box(1, 1, 0.0, 1.0, 0.0, 1.0, periodic_x=True,
                       periodic_y=True)
@@ -106,7 +107,7 @@ def test_relaxation_50_steps(stepper):
 
 
 def test_couette_strip_two_steps():
-    """BASELINE configuration 2's discretisation on a 4x1 strip: 2 SSP-RK2
+    """The Couette workload's discretisation on a 4x1 strip: 2 SSP-RK2
     steps in FP64 with both moving diffuse walls."""
     cfg = config('couette-n24', 'double', nele=4)
     m = mgen.from_config(cfg)
