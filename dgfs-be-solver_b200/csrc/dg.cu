@@ -260,12 +260,9 @@ cudaError_t launch_rhs_tc(const dgfs_dg* h, const DgArgs<float>& a, int nv, cuda
   using TC = DgTc<U, F, D>;
   constexpr int mb = U <= 9 ? 4 : 2;
   auto kern = dg_residual_tc_kernel<U, F, D, VPT, mb>;
-  static bool configured = false;  // per instantiation
-  if (!configured) {
-    const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, TC::SMEM);
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
+  static std::atomic<unsigned long long> configured{0};  // per instantiation and device
+  const cudaError_t e = smem_limit_once(kern, TC::SMEM, configured);
+  if (e != cudaSuccess) return e;
   const dim3 grid((unsigned)((h->E + 31) / 32), (unsigned)((nv + 4 * VPT - 1) / (4 * VPT)));
   return launch_pdl_shape(h->nhalo == 0, kern, grid, 128, TC::SMEM, s, a, make_ops<float, U, F, D>(h));
 }

@@ -312,12 +312,10 @@ int gemm_tc_launch(int M, int N, int K, const float* A, long long sam, long long
                    long long sbn, const float* bias, float* Z, float* C, long long ldc, int act, int accumulate,
                    int* err, cudaStream_t s) {
   constexpr int smem = tc_smem_bytes<BN>();
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(gemm_tc_kernel<TB, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e != cudaSuccess) return dgfs::set_error(DGFS_ERR_CUDA, "tensor-core GEMM attributes: %s", cudaGetErrorString(e));
-    configured = true;
-  }
+  static std::atomic<unsigned long long> configured{0};  // per device
+  const cudaError_t e0 = dgfs::smem_limit_once(gemm_tc_kernel<TB, BN>, smem, configured);
+  if (e0 != cudaSuccess)
+    return dgfs::set_error(DGFS_ERR_CUDA, "tensor-core GEMM attributes: %s", cudaGetErrorString(e0));
   const int amode = operand_mode(A, sam, sak, K, 4);
   const int bmode = operand_mode(B, sbn, sbk, K, sizeof(TB) == 2 ? 8 : 4);
   const dim3 grid((N + BN - 1) / BN, (M + TC_BM - 1) / TC_BM);

@@ -233,11 +233,8 @@ int launch_bf16(const CUtensorMap& ta, const CUtensorMap& tb, int M, int N, int 
                 const float* bias, float* Z, float* C, void* Cb, long long ldc, int act, int accumulate, int* err,
                 cudaStream_t s) {
   constexpr int smem = TmaGeom<BN>::SMEM;
-  static std::once_flag once;
-  static cudaError_t attr = cudaSuccess;
-  std::call_once(once, [] {
-    attr = cudaFuncSetAttribute(gemm_bf16_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  });
+  static std::atomic<unsigned long long> configured{0};  // per device
+  const cudaError_t attr = smem_limit_once(gemm_bf16_kernel<BN>, smem, configured);
   if (attr != cudaSuccess) return set_error(DGFS_ERR_CUDA, "BF16 GEMM attributes: %s", cudaGetErrorString(attr));
   const dim3 grid((N + BN - 1) / BN, (M + TB_BM - 1) / TB_BM);
   gemm_bf16_kernel<BN><<<grid, TB_THREADS, smem, s>>>(ta, tb, M, N, K, a_mn, b_mn, bias, Z, C,
