@@ -17,8 +17,9 @@
 // commits them to the slot's mbarrier; a slot is refilled only after that
 // mbarrier reports its MMAs complete.
 // The accumulator lives in BN columns of tensor memory (lane = row of the
-// tile); the epilogue reads it with tcgen05.ld, adds the bias, applies tanh
-// and writes C (and the pre-activation Z).
+// tile); the epilogue reads it with tcgen05.ld, stages it in the ring's
+// shared memory, adds the bias, applies tanh and writes C (and the
+// pre-activation Z) row by row.
 //
 // Every mbarrier wait is bounded (1 s); on expiry the kernel sets *err,
 // skips the epilogue, waits (bounded) for its MMAs in flight and frees its
@@ -265,27 +266,37 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   tc_fence_after();
 
   if (!*(volatile int*)gave_up && !*(volatile int*)drain_up && last == nk - 1) {
-    // warp w: rows 32 (w % 4) + lane, the half (w / 4) of the columns
+    // warp w: rows 32 (w % 4) .. + 31, the half (w / 4) of the columns.
+    // The ring's shared memory is free now: each warp stages its 32 x BN/2
+    // block there (row stride BN/2 + 1: no bank conflicts either way) and
+    // writes whole row segments with consecutive lanes on consecutive
+    // columns (coalesced).
+    constexpr int HW = BN / 2, SP = HW + 1;
+    static_assert(8 * 32 * SP * 4 <= TC_STAGES * STAGE_BYTES, "epilogue staging fits in the ring");
     const int quarter = warp & 3, half = warp >> 2;
-    const int m = m0 + quarter * 32 + lane;
-    const bool row_ok = m < M;
+    float* stg = reinterpret_cast<float*>(smem) + warp * 32 * SP;
 #pragma unroll 1
-    for (int j0 = half * (BN / 2); j0 < (half + 1) * (BN / 2); j0 += 16) {
+    for (int j = 0; j < HW; j += 16) {
       float v[16];
       __syncwarp();  // tcgen05.ld is warp-collective
-      tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)j0, v);
-      if (row_ok && n0 + j0 < N) {
-        float* crow = C + (long long)m * ldc;
-        float* zrow = Z ? Z + (long long)m * ldc : nullptr;
+      tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(half * HW + j), v);
 #pragma unroll
-        for (int jj = 0; jj < 16; ++jj) {
-          const int n = n0 + j0 + jj;
-          if (n < N) {
-            float z = v[jj] + (bias ? __ldg(bias + n) : 0.f);
-            if (accumulate) z += crow[n];
-            if (zrow) zrow[n] = z;
-            crow[n] = act == 1 ? tanhf(z) : z;
-          }
+      for (int jj = 0; jj < 16; ++jj) stg[lane * SP + j + jj] = v[jj];
+    }
+    __syncwarp();
+#pragma unroll 1
+    for (int r = 0; r < 32; ++r) {
+      const int m = m0 + quarter * 32 + r;
+      if (m >= M) break;  // uniform over the warp
+      const long long row = (long long)m * ldc;
+#pragma unroll
+      for (int c = lane; c < HW; c += 32) {
+        const int n = n0 + half * HW + c;
+        if (n < N) {
+          float z = stg[r * SP + c] + (bias ? __ldg(bias + n) : 0.f);
+          if (accumulate) z += C[row + n];
+          if (Z) Z[row + n] = z;
+          C[row + n] = act == 1 ? tanhf(z) : z;
         }
       }
     }
