@@ -383,6 +383,29 @@ DGFS_API int dgfs_dg_bcvals(const dgfs_dg* h, double* host, int n);
 DGFS_API int dgfs_dg_fpts(const dgfs_dg* h, void** ptr, long long* ldim);
 
 /* ------------------------------------------------------------------------
+ * Stage graphs at the C ABI
+ *
+ * Replaces the per-kernel launches of a Runge-Kutta stage of
+ * StdTVDRK2DGFSStepper / StdEulerDGFSStepper
+ * (frfs/integrators/std/steppers.py:39-225) with one graph launch, for
+ * callers that reach the library through these entry points only.
+ * dgfs_graph_begin starts capturing `stream` (a created stream; capture
+ * mode thread-local); the dgfs_* calls that follow on that stream are
+ * recorded, not run; dgfs_graph_end stops the capture and instantiates the
+ * graph; dgfs_graph_launch replays it on any stream.  Every call inside a
+ * capture must have been made once before with the same handles and sizes
+ * (first calls set up kernel attributes and scratch), and the captured
+ * pointers must stay valid while the graph lives.  If a call inside the
+ * capture fails, dgfs_graph_end still ends the capture and reports it.
+ * ---------------------------------------------------------------------- */
+typedef struct dgfs_graph dgfs_graph;
+
+DGFS_API int dgfs_graph_begin(void* stream);
+DGFS_API int dgfs_graph_end(void* stream, dgfs_graph** out);
+DGFS_API int dgfs_graph_launch(dgfs_graph* g, void* stream);
+DGFS_API int dgfs_graph_destroy(dgfs_graph* g);
+
+/* ------------------------------------------------------------------------
  * Macroscopic moments
  *
  * Replaces: the 3D moment formulas of DGFSMomWriterStdPlugin
