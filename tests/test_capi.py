@@ -66,3 +66,36 @@ def test_surrogate_entry_points_validate_arguments_before_any_cuda_call():
     # scale with the log column inside the scaled range
     assert lib.dgfs_surrogate_scale(4, 256, p, 1e-3, 4, 220, 100, 0, p,
                                     None) != 0
+
+
+def test_tensor_core_and_graph_entry_points_validate_arguments():
+    """Host-side checks of the tensor-core products and the stage-graph
+    entry points (no GPU needed: each bad call is rejected before any CUDA
+    call)."""
+    import frfs_b200.surrogate  # noqa: F401  (declares the signatures)
+    lib = _lib.load()
+    p16, p8 = ct.c_void_p(16), ct.c_void_p(8)
+    # TMA-fed product: leading dimensions must be multiples of 8 ...
+    assert lib.dgfs_mlp_gemm_bf16(64, 64, 64, p16, 0, 12, p16, 0, 64, None,
+                                  None, p16, None, 64, 0, 0, p16, None) == 1
+    assert b'multiples of 8' in lib.dgfs_last_error()
+    # ... operands 16-byte aligned for the tensor maps ...
+    assert lib.dgfs_mlp_gemm_bf16(64, 64, 64, p8, 0, 64, p16, 0, 64, None,
+                                  None, p16, None, 64, 0, 0, p16, None) == 1
+    assert b'aligned' in lib.dgfs_last_error()
+    # ... and an error flag is required
+    assert lib.dgfs_mlp_gemm_bf16(64, 64, 64, p16, 0, 64, p16, 0, 64, None,
+                                  None, p16, None, 64, 0, 0, None, None) == 1
+    # staged product: unknown activation
+    assert lib.dgfs_mlp_gemm_tc(4, 4, 4, p16, 4, 1, p16, 0, 4, 1, None, None,
+                                p16, 4, 2, 0, p16, None) == 1
+    # stage graphs: the legacy default stream cannot be captured
+    lib.dgfs_graph_begin.argtypes = [ct.c_void_p]
+    lib.dgfs_graph_end.argtypes = [ct.c_void_p, ct.c_void_p]
+    lib.dgfs_graph_launch.argtypes = [ct.c_void_p, ct.c_void_p]
+    lib.dgfs_graph_destroy.argtypes = [ct.c_void_p]
+    assert lib.dgfs_graph_begin(None) == 1
+    assert b'legacy default stream' in lib.dgfs_last_error()
+    assert lib.dgfs_graph_end(None, None) == 1
+    assert lib.dgfs_graph_launch(None, None) == 1
+    assert lib.dgfs_graph_destroy(None) == 0
